@@ -1,0 +1,281 @@
+/*
+ * Test infrastructure (oracle build only).  Replacement object for the
+ * reference's src/wrapper/eigs.cpp of mcbapo/mpsdyn.
+ *
+ * The reference calls PRIMME (wrapper::eigs_primme, eigs.cpp:325-369 and
+ * call_eigs_primme, eigs.cpp:371-422) for every local eigenproblem with
+ * dimension >= 801 (Contractor.cpp:3126-3136), and ARPACK through
+ * wrapper::eigs (eigs.cpp:71-244).  The shipped binary archives of both do
+ * not run in this image, and the PRIMME source (version unpinned; the build
+ * files expect v3) is not part of the reference tree.  This file provides the
+ * same entry points, answered by a restarted Lanczos iteration with full
+ * reorthogonalisation (Lanczos 1950; Paige 1972; restart from the current
+ * Ritz vector, as in explicitly restarted Lanczos) that calls the reference's
+ * own Multiplier::product for every matrix-vector product.
+ *
+ * Contract kept from eigs_primme: one eigenpair (nev == 1), target "smallest
+ * algebraic" (the "SR" used by findGroundState, Contractor.cpp:1408-1410 and
+ * findGroundStateWithProjectorPenalty, :2833-2836), initial guess = first
+ * column of U when U is not empty (eigs.cpp:383-393), eigenvalue returned in
+ * Dval[0] as a complex number with zero imaginary part and eigenvector in
+ * U(:,0) (eigs.cpp:405-414).
+ *
+ * Convergence: ||H x - theta x|| <= tol * max(|theta_min|, |theta_max|) over
+ * the Ritz values of the current Krylov space (the PRIMME convention
+ * ||r|| <= eps*||A|| with ||A|| estimated from the Ritz values).  tol is the
+ * caller's eigtol, or 1e-12 when that is 0.
+ */
+#include "wrapper.h"
+#include "mwArray.h"
+#include "Multiplier.h"
+#include "BasicMultiplier.h"
+#include "Indices.h"
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <vector>
+
+using namespace std;
+using namespace shrt;
+
+namespace {
+
+typedef std::complex<double> cd;
+
+const int kMaxKrylov = 64;     // Krylov vectors kept per restart
+const int kMaxRestarts = 60;   // restarts before giving up
+const double kDefaultTol = 1e-12;
+
+// Number of eigenvalues of the symmetric tridiagonal (a, b) below x
+// (Sturm sequence count, LDL^T pivots).
+int sturm_count(const double* a, const double* b, int k, double x) {
+  int count = 0;
+  double q = a[0] - x;
+  if (q < 0) count++;
+  for (int i = 1; i < k; i++) {
+    double den = (q == 0.0) ? 1e-300 : q;
+    q = a[i] - x - b[i - 1] * b[i - 1] / den;
+    if (q < 0) count++;
+  }
+  return count;
+}
+
+// Lowest eigenvalue by bisection on the Gershgorin interval, eigenvector by
+// inverse iteration with a pivoted tridiagonal solve.  Returns theta and the
+// normalised eigenvector s (length k), and the largest |eigenvalue| bound.
+void tridiag_lowest(const vector<double>& a, const vector<double>& b, int k,
+                    double& theta, vector<double>& s, double& normT) {
+  double lo = a[0], hi = a[0];
+  for (int i = 0; i < k; i++) {
+    double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i < k - 1 ? fabs(b[i]) : 0.0);
+    lo = min(lo, a[i] - r);
+    hi = max(hi, a[i] + r);
+  }
+  normT = max(fabs(lo), fabs(hi));
+  double l = lo, h = hi;
+  for (int it = 0; it < 200 && (h - l) > 4e-16 * max(fabs(l), fabs(h)) + 1e-300; it++) {
+    double mid = 0.5 * (l + h);
+    if (mid == l || mid == h) break;
+    if (sturm_count(a.data(), b.data(), k, mid) >= 1) h = mid; else l = mid;
+  }
+  theta = 0.5 * (l + h);
+  s.assign(k, 1.0);
+  if (k == 1) { s[0] = 1.0; return; }
+  // Inverse iteration: solve (T - theta I) y = s with partial pivoting.
+  double shift = theta - 1e-14 * max(normT, 1e-300);
+  for (int rep = 0; rep < 3; rep++) {
+    // Gaussian elimination with row interchanges on a tridiagonal matrix:
+    // rows carry (d, u, u2) = diagonal, first and second super-diagonal.
+    vector<double> d(k), u(k, 0.0), u2(k, 0.0), y(s);
+    vector<double> sub(k, 0.0);
+    const double tiny = 1e-15 * max(normT, 1e-300);
+    for (int i = 0; i < k; i++) { d[i] = a[i] - shift; if (i < k - 1) { u[i] = b[i]; sub[i] = b[i]; } }
+    for (int i = 0; i < k - 1; i++) {
+      if (fabs(sub[i]) > fabs(d[i])) {
+        // swap rows i and i+1
+        double nd = sub[i], nu = d[i + 1], nu2 = (i + 1 < k - 1) ? u[i + 1] : 0.0;
+        double od = d[i], ou = u[i], ou2 = u2[i];
+        d[i] = nd; u[i] = nu; u2[i] = nu2;
+        double yi = y[i]; y[i] = y[i + 1]; y[i + 1] = yi;
+        // old row i becomes row i+1 (to be eliminated)
+        double m = od / nd;
+        d[i + 1] = ou - m * nu;
+        u[i + 1] = ou2 - m * nu2;
+        y[i + 1] -= m * y[i];
+      } else {
+        double den = (fabs(d[i]) < tiny) ? tiny : d[i];
+        double m = sub[i] / den;
+        d[i + 1] -= m * u[i];
+        // u[i+1] unchanged (row i has no entry at column i+2 unless swapped earlier)
+        if (i + 1 < k - 1) u[i + 1] -= m * u2[i];
+        y[i + 1] -= m * y[i];
+      }
+    }
+    // back substitution
+    for (int i = k - 1; i >= 0; i--) {
+      double acc = y[i];
+      if (i + 1 < k) acc -= u[i] * y[i + 1];
+      if (i + 2 < k) acc -= u2[i] * y[i + 2];
+      double den = (fabs(d[i]) < tiny) ? tiny : d[i];
+      y[i] = acc / den;
+    }
+    double nrm = 0;
+    for (int i = 0; i < k; i++) nrm += y[i] * y[i];
+    nrm = sqrt(nrm);
+    for (int i = 0; i < k; i++) s[i] = y[i] / nrm;
+  }
+}
+
+void apply(Multiplier& multi, const vector<cd>& x, vector<cd>& y, int N) {
+  mwArray in(Indices(N, 1), (const complex_t*)x.data());
+  mwArray out;
+  multi.product(in, out);
+  y.resize(N);
+  for (int i = 0; i < N; i++) {
+    complex_t c = out.getElement(i);
+    y[i] = cd(c.re, c.im);
+  }
+}
+
+double nrm2(const vector<cd>& x) {
+  double s = 0;
+  for (size_t i = 0; i < x.size(); i++) s += norm(x[i]);
+  return sqrt(s);
+}
+
+// Restarted Lanczos for the lowest eigenpair of the Hermitian operator.
+int lanczos_lowest(Multiplier& multi, const mwArray& U0, double tol,
+                   double& lambda, vector<cd>& x) {
+  const int N = multi.getSize();
+  if (tol <= 0) tol = kDefaultTol;
+  x.assign(N, cd(0, 0));
+  bool have = false;
+  if (!U0.isEmpty() && U0.getNrComponents() >= N) {
+    for (int i = 0; i < N; i++) {
+      complex_t c = U0.getElement(i);
+      x[i] = cd(c.re, c.im);
+    }
+    have = nrm2(x) > 0;
+  }
+  if (!have)
+    for (int i = 0; i < N; i++) x[i] = cd(1.0 / sqrt((double)N), 0);
+  double nx = nrm2(x);
+  for (int i = 0; i < N; i++) x[i] /= nx;
+
+  const int m = min(N, kMaxKrylov);
+  vector<vector<cd> > V;
+  vector<double> a, b, s;
+  vector<cd> w;
+  double theta = 0, normT = 0;
+  for (int restart = 0; restart < kMaxRestarts; restart++) {
+    V.assign(1, x);
+    a.clear(); b.clear();
+    bool conv = false;
+    int j = 0;
+    for (j = 0; j < m; j++) {
+      apply(multi, V[j], w, N);
+      cd dot(0, 0);
+      for (int i = 0; i < N; i++) dot += conj(V[j][i]) * w[i];
+      a.push_back(dot.real());
+      for (int i = 0; i < N; i++) w[i] -= a[j] * V[j][i];
+      if (j > 0)
+        for (int i = 0; i < N; i++) w[i] -= b[j - 1] * V[j - 1][i];
+      for (int pass = 0; pass < 2; pass++)
+        for (int l = 0; l <= j; l++) {
+          cd c(0, 0);
+          for (int i = 0; i < N; i++) c += conj(V[l][i]) * w[i];
+          for (int i = 0; i < N; i++) w[i] -= c * V[l][i];
+        }
+      double beta = nrm2(w);
+      b.push_back(beta);
+      tridiag_lowest(a, b, j + 1, theta, s, normT);
+      double res = beta * fabs(s[j]);
+      double scale = max(normT, fabs(theta));
+      if (res <= tol * scale || beta <= 1e-14 * scale || j + 1 == N) {
+        conv = true;
+        j++;
+        break;
+      }
+      if (j + 1 < m) {
+        vector<cd> nv(N);
+        for (int i = 0; i < N; i++) nv[i] = w[i] / beta;
+        V.push_back(nv);
+      }
+    }
+    int k = (int)a.size();
+    vector<cd> y(N, cd(0, 0));
+    for (int l = 0; l < k; l++)
+      for (int i = 0; i < N; i++) y[i] += s[l] * V[l][i];
+    double ny = nrm2(y);
+    for (int i = 0; i < N; i++) x[i] = y[i] / ny;
+    if (conv) {
+      lambda = theta;
+      return 0;
+    }
+  }
+  lambda = theta;
+  cout << "eigs_shim: Lanczos did not reach tolerance " << tol << endl;
+  return 1;
+}
+
+int solve_into(Multiplier& multi, int nev, bool smallest,
+               std::vector<complex_t>& Dval, mwArray& U, double tol) {
+  if (nev != 1 || !smallest) {
+    cout << "eigs_shim: only the lowest eigenpair (nev=1, target smallest) "
+         << "is provided by this replacement solver" << endl;
+    exit(1);
+  }
+  double lambda;
+  vector<cd> x;
+  int ret = lanczos_lowest(multi, U, tol, lambda, x);
+  int N = multi.getSize();
+  Dval.clear();
+  Dval.push_back((complex_t){lambda, 0.});
+  U = mwArray(Indices(N, 1), (const complex_t*)x.data());
+  return ret;
+}
+
+}  // namespace
+
+int wrapper::eigs(const mwArray& A, const int k, const char* which,
+                  std::vector<complex_t>& D, mwArray& U, bool eigv, double tol) {
+  BasicMultiplier aux(A);
+  return wrapper::eigs(aux, k, which, D, U, eigv, tol);
+}
+
+int wrapper::eigs(Multiplier& multi, const int k, const char* which,
+                  std::vector<complex_t>& D, mwArray& U, bool eigv, double tol) {
+  bool smallest = !strcmp(which, "SR") || !strcmp(which, "SA");
+  return solve_into(multi, k, smallest, D, U, tol);
+}
+
+int wrapper::eigs_primme(const mwArray& A, const int k, primme_target which,
+                         std::vector<complex_t>& D, mwArray& U, double tol,
+                         primme_preset_method method) {
+  BasicMultiplier aux(A);
+  return wrapper::eigs_primme(aux, k, which, D, U, tol, method);
+}
+
+int wrapper::eigs_primme(Multiplier& multi, const int nev, primme_target which,
+                         std::vector<complex_t>& Dval, mwArray& U, double tol,
+                         primme_preset_method method, int numShifts,
+                         double* targetShifts) {
+  return solve_into(multi, nev, which == primme_smallest, Dval, U, tol);
+}
+
+int wrapper::eigsgen_primme(Multiplier& multiA, Multiplier& multiB,
+                            const int nev, primme_target which,
+                            std::vector<complex_t>& Dval, mwArray& U,
+                            double tol, primme_preset_method method,
+                            int numShifts, double* targetShifts) {
+  cout << "eigs_shim: generalized eigenproblems are not provided" << endl;
+  exit(1);
+}
+
+int wrapper::call_eigs_primme(primme_params* primme,
+                              std::vector<complex_t>& Dval, mwArray& U) {
+  cout << "eigs_shim: call_eigs_primme is not provided" << endl;
+  exit(1);
+}
