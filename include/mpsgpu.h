@@ -1,0 +1,189 @@
+/*
+ * mpsgpu -- C ABI of the B200 DMRG sweep library (sm_100a, complex FP64).
+ *
+ * This is the drop-in boundary for the single-site DMRG hot path of
+ * mcbapo/mpsdyn.  Every entry point takes plain pointers and sizes; tensors
+ * cross the boundary in the reference's own layout:
+ *
+ *   complex128 = two doubles (re, im), interleaved (src/wrapper/complex.h)
+ *   all tensors column-major ("Fortran order", src/wrapper/mwArray.cpp:452-470)
+ *   site tensor     A(d, Dl, Dr)              (src/core/cpp/Site.cpp:16-21)
+ *   MPO tensor      W(du, Dl, dd, Dr)         (src/core/cpp/Operator.cpp:17-24)
+ *   environments    L(Dbra, w, Dket), R(Dbra, w, Dket)
+ *                                             (src/core/cpp/Operator.cpp:273-387)
+ *   local vector    vec(A(d, Dl, Dr))         (src/wrapper/multipliers/TensorMultiplier.h:28)
+ *
+ * Inside the library the state lives in HBM in its own layout (see the design
+ * notes); uploads and downloads convert.  Every function returns an
+ * mpsgpu_status; the reference's convention of printing and calling exit()
+ * (e.g. exit(212) on an energy increase, Contractor.cpp:1418-1427) becomes a
+ * status code, and the C++ facade restores the reference behaviour.
+ *
+ * Threading: calls on one context are serialised on that context's CUDA
+ * stream; different contexts may be used from different host threads.
+ */
+#ifndef MPSGPU_H
+#define MPSGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MPSGPU_OK = 0,
+  MPSGPU_BAD_SHAPE = 1,       /* inconsistent or unsupported dimensions */
+  MPSGPU_NOT_CONVERGED = 2,   /* eigensolver or sweep limit reached */
+  MPSGPU_ENERGY_INCREASE = 3, /* Contractor.cpp:1418-1427 (reference: exit 212) */
+  MPSGPU_NAN = 4,             /* non-finite value (Contractor.cpp:954-960: exit 1) */
+  MPSGPU_OOM = 5,             /* device allocation failed */
+  MPSGPU_CANCELLED = 6,       /* cancel flag raised by the caller */
+  MPSGPU_TIMEOUT = 7,         /* bounded device wait gave up */
+  MPSGPU_CUDA_ERROR = 8,      /* CUDA runtime error (see mpsgpu_last_error) */
+  MPSGPU_INVALID = 9          /* null handle or bad argument */
+} mpsgpu_status;
+
+typedef struct mpsgpu_context mpsgpu_context;
+typedef struct mpsgpu_mpo mpsgpu_mpo;
+typedef struct mpsgpu_mps mpsgpu_mps;
+
+/* Solver options.  Defaults (mpsgpu_default_options) are the reference
+ * Contractor's: convtol 1e-5, eigtol 0 (Contractor.cpp:39-42). */
+typedef struct {
+  double convtol;      /* setConvTol (Contractor.h:213) */
+  double eigtol;       /* setEigTol; 0 = 1e-12 relative Lanczos residual */
+  double excorthtol;   /* setExcOrthTol (Contractor.h:229); 0 = no check */
+  int max_rounds;      /* half-sweep cap; 0 = 1000 (MAX_ROUND_EXCTD, Contractor.cpp:26) */
+  int max_krylov;      /* Lanczos vectors per restart; 0 = 64 */
+  int precision;       /* 0 = complex FP64 throughout */
+  int verbose;         /* 1 = one line per half-sweep on stdout */
+} mpsgpu_options;
+
+/* Counters of one solve (host-side; the flop count is algorithmic). */
+typedef struct {
+  int rounds;                /* half-sweeps */
+  long long site_solves;     /* local eigenproblems */
+  long long matvecs;         /* effective-Hamiltonian products */
+  long long env_updates;     /* environment contractions */
+  long long qr_calls;        /* gauge moves */
+  double flops;              /* algorithmic flops, all kernels */
+  double seconds;            /* wall time of the call */
+  double matvec_seconds;     /* device time spent in matvec kernels (events) */
+} mpsgpu_stats;
+
+/* ---- context ------------------------------------------------------------ */
+void mpsgpu_default_options(mpsgpu_options* opt);
+mpsgpu_status mpsgpu_create(int device, mpsgpu_context** ctx);
+mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx);
+const char* mpsgpu_status_string(mpsgpu_status s);
+const char* mpsgpu_last_error(mpsgpu_context* ctx);
+/* Counts this library's kernel launches on the context (for reporting). */
+long long mpsgpu_launch_count(mpsgpu_context* ctx);
+mpsgpu_status mpsgpu_synchronize(mpsgpu_context* ctx);
+
+/* ---- MPO (replaces MPO / Operator storage, src/core/headers/MPO.h:33-176) --
+ * dims[4k..4k+3] = (du, Dl, dd, Dr) of operator k; data[k] its column-major
+ * complex128 tensor (host memory). */
+mpsgpu_status mpsgpu_mpo_upload(mpsgpu_context* ctx, int L, const int* dims,
+                                const double* const* data, mpsgpu_mpo** out);
+mpsgpu_status mpsgpu_mpo_free(mpsgpu_context* ctx, mpsgpu_mpo* mpo);
+
+/* ---- MPS (replaces MPS / Site storage, src/core/headers/MPS.h) ------------
+ * dims[3k..3k+2] = (d, Dl, Dr) of site k; data[k] column-major complex128. */
+mpsgpu_status mpsgpu_mps_upload(mpsgpu_context* ctx, int L, const int* dims,
+                                const double* const* data, double normfact,
+                                mpsgpu_mps** out);
+/* Seeded i.i.d. complex Gaussian MPS on the bond schedule
+ * D_k = min(d^k, d^(L-k), D), generated on the device from the SplitMix64
+ * counter stream (entry i of the chain uses draws 2i, 2i+1, Box-Muller). */
+mpsgpu_status mpsgpu_mps_random(mpsgpu_context* ctx, int L, int d, int D,
+                                uint64_t seed, mpsgpu_mps** out);
+/* MPS(L,D,d) of the reference (src/core/cpp/MPS.cpp:15-35): element (0,0,0)
+ * of every site is 1, bonds D (D=1: the product state |0...0>). */
+mpsgpu_status mpsgpu_mps_product(mpsgpu_context* ctx, int L, int d, int D,
+                                 mpsgpu_mps** out);
+mpsgpu_status mpsgpu_mps_copy(mpsgpu_context* ctx, const mpsgpu_mps* src,
+                              mpsgpu_mps** out);
+mpsgpu_status mpsgpu_mps_info(mpsgpu_context* ctx, const mpsgpu_mps* mps,
+                              int* L, int* dims, double* normfact);
+mpsgpu_status mpsgpu_mps_download(mpsgpu_context* ctx, const mpsgpu_mps* mps,
+                                  double* const* data);
+mpsgpu_status mpsgpu_mps_free(mpsgpu_context* ctx, mpsgpu_mps* mps);
+/* MPS::gaugeCond(dir, normal=true) (src/core/cpp/MPS.cpp:306-364). */
+mpsgpu_status mpsgpu_mps_gauge(mpsgpu_context* ctx, mpsgpu_mps* mps, char dir);
+
+/* ---- Contractor (src/core/headers/Contractor.h:46-604) ------------------- */
+/* findGroundState(ops, D, &lambda, init, offset) (Contractor.cpp:1352-1533). */
+mpsgpu_status mpsgpu_find_ground_state(mpsgpu_context* ctx, const mpsgpu_mpo* ops,
+                                       int D, double offset,
+                                       const mpsgpu_options* opt, mpsgpu_mps* init,
+                                       double* lambda, mpsgpu_stats* stats);
+/* findNextExcitedState(ops, D, levels, &lambda, init, offset)
+ * (Contractor.cpp:2676-2727 -> findGroundStateWithProjectorPenalty :2739-2956). */
+mpsgpu_status mpsgpu_find_next_excited_state(mpsgpu_context* ctx,
+                                             const mpsgpu_mpo* ops, int D,
+                                             const mpsgpu_mps* const* levels,
+                                             int nlevels, double offset,
+                                             const mpsgpu_options* opt,
+                                             mpsgpu_mps* init, double* lambda,
+                                             mpsgpu_stats* stats);
+/* optimize(ops, orig, init, D, errN, errT) (Contractor.cpp:77-278): the
+ * variational MPO.MPS product used for time evolution.  errN may be null. */
+mpsgpu_status mpsgpu_optimize(mpsgpu_context* ctx, const mpsgpu_mpo* ops,
+                              const mpsgpu_mps* orig, mpsgpu_mps* init, int D,
+                              const mpsgpu_options* opt, double* errN,
+                              double* errT, mpsgpu_stats* stats);
+/* contract(ket, ops, bra) = <bra|ops|ket> (Contractor.cpp:528-556); ops may be
+ * null for contract(ket, bra) (Contractor.cpp:467-499). */
+mpsgpu_status mpsgpu_contract(mpsgpu_context* ctx, const mpsgpu_mps* ket,
+                              const mpsgpu_mpo* ops, const mpsgpu_mps* bra,
+                              double* re, double* im);
+/* <op_k> / <psi|psi> for every site k, op a d x d column-major matrix
+ * (programs/banulsm/curved/flatIsing.cpp:258-282). out has L entries. */
+mpsgpu_status mpsgpu_expectation_local(mpsgpu_context* ctx, const mpsgpu_mps* mps,
+                                       const double* op, double* out);
+/* getEntropy(state, pos) (Contractor.cpp:2045-2076). */
+mpsgpu_status mpsgpu_entropy(mpsgpu_context* ctx, const mpsgpu_mps* mps, int pos,
+                             double* entropy);
+/* getSchmidtValues(state, lambdas, pos) (Contractor.cpp:2243-2270); writes at
+ * most cap values (ascending), the count into *n. */
+mpsgpu_status mpsgpu_schmidt_values(mpsgpu_context* ctx, const mpsgpu_mps* mps,
+                                    int pos, double* values, int cap, int* n);
+
+/* ---- kernel-level entry points (host buffers, reference layouts) ---------
+ * TensorMultiplier(Offset)::product (TensorMultiplier.cpp:61-93,
+ * TensorMultiplierOffset.cpp:14-17); hermitian!=0 gives
+ * TensorMultiplierHermitian(Offset)::product (TensorMultiplierHermitian.cpp:37-70).
+ * ldims = (Dlb, wl, Dlk), wdims = (du, wl, dd, wr), rdims = (Drb, wr, Drk);
+ * x has dd*Dlk*Drk entries, y gets du*Dlb*Drb. */
+mpsgpu_status mpsgpu_heff_matvec(mpsgpu_context* ctx, const int* ldims,
+                                 const double* L, const int* wdims,
+                                 const double* W, const int* rdims,
+                                 const double* R, const double* x, double* y,
+                                 double offset, int hermitian);
+/* Operator::contractL / contractR (Operator.cpp:273-398): out gets
+ * (Dr_bra, wr, Dr_ket) resp. (Dl_bra, wl, Dl_ket). */
+mpsgpu_status mpsgpu_env_left(mpsgpu_context* ctx, const int* tdims,
+                              const double* T, const int* kdims,
+                              const double* ket, const int* wdims,
+                              const double* W, const int* bdims,
+                              const double* bra, double* out);
+mpsgpu_status mpsgpu_env_right(mpsgpu_context* ctx, const int* tdims,
+                               const double* T, const int* kdims,
+                               const double* ket, const int* wdims,
+                               const double* W, const int* bdims,
+                               const double* bra, double* out);
+/* wrapper::qr / wrapper::lq (src/wrapper/qr.cpp:33-188): Householder with
+ * the LAPACK zgeqrf/zungqr conventions; K = min(m, n); Q is m x K and R is
+ * K x n (qr), L is m x K and Q is K x n (lq). */
+mpsgpu_status mpsgpu_qr(mpsgpu_context* ctx, int m, int n, const double* A,
+                        double* Q, double* R);
+mpsgpu_status mpsgpu_lq(mpsgpu_context* ctx, int m, int n, const double* A,
+                        double* Lf, double* Q);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPSGPU_H */

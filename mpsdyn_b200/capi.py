@@ -1,0 +1,305 @@
+"""ctypes binding of libmpsgpu (include/mpsgpu.h) for tests, benchmarks and
+Python callers.  Arrays cross the boundary in the reference layout
+(column-major complex128).  There is no CPU fallback: if the library or a
+GPU is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpsgpu.so")
+
+STATUS = {
+    0: "ok", 1: "bad shape", 2: "not converged", 3: "energy increase", 4: "non-finite value",
+    5: "out of memory", 6: "cancelled", 7: "timeout", 8: "CUDA error", 9: "invalid argument",
+}
+
+EXPORTS = [
+    "mpsgpu_default_options", "mpsgpu_create", "mpsgpu_destroy", "mpsgpu_status_string",
+    "mpsgpu_last_error", "mpsgpu_launch_count", "mpsgpu_synchronize", "mpsgpu_mpo_upload",
+    "mpsgpu_mpo_free", "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_product",
+    "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
+    "mpsgpu_mps_gauge", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
+    "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_expectation_local", "mpsgpu_entropy",
+    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_env_left", "mpsgpu_env_right",
+    "mpsgpu_qr", "mpsgpu_lq",
+]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("convtol", C.c_double), ("eigtol", C.c_double), ("excorthtol", C.c_double),
+        ("max_rounds", C.c_int), ("max_krylov", C.c_int), ("precision", C.c_int),
+        ("verbose", C.c_int),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("rounds", C.c_int), ("site_solves", C.c_longlong), ("matvecs", C.c_longlong),
+        ("env_updates", C.c_longlong), ("qr_calls", C.c_longlong), ("flops", C.c_double),
+        ("seconds", C.c_double), ("matvec_seconds", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class MpsgpuError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"mpsgpu: {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load libmpsgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (run mpsdyn_b200/build.py)")
+        lib = C.CDLL(path)
+        P = C.c_void_p
+        lib.mpsgpu_status_string.restype = C.c_char_p
+        lib.mpsgpu_last_error.restype = C.c_char_p
+        lib.mpsgpu_last_error.argtypes = [P]
+        lib.mpsgpu_launch_count.restype = C.c_longlong
+        lib.mpsgpu_launch_count.argtypes = [P]
+        lib.mpsgpu_default_options.argtypes = [C.POINTER(Options)]
+        lib.mpsgpu_mps_random.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]
+        lib.mpsgpu_find_ground_state.argtypes = [P, P, C.c_int, C.c_double, C.POINTER(Options), P,
+                                                 C.POINTER(C.c_double), C.POINTER(Stats)]
+        lib.mpsgpu_find_next_excited_state.argtypes = [P, P, C.c_int, C.POINTER(P), C.c_int, C.c_double,
+                                                       C.POINTER(Options), P, C.POINTER(C.c_double),
+                                                       C.POINTER(Stats)]
+        lib.mpsgpu_optimize.argtypes = [P, P, P, P, C.c_int, C.POINTER(Options), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double), C.POINTER(Stats)]
+        lib.mpsgpu_mps_upload.argtypes = [P, C.c_int, P, P, C.c_double, C.POINTER(P)]
+        lib.mpsgpu_heff_matvec.argtypes = [P, P, P, P, P, P, P, P, P, C.c_double, C.c_int]
+        lib.mpsgpu_entropy.argtypes = [P, P, C.c_int, C.POINTER(C.c_double)]
+        lib.mpsgpu_mps_gauge.argtypes = [P, P, C.c_char]
+        _lib = lib
+    return _lib
+
+
+def _fortran(a) -> np.ndarray:
+    return np.asfortranarray(np.asarray(a, dtype=np.complex128))
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def _ints(v) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(v, dtype=np.int32))
+
+
+class Context:
+    """One CUDA stream on one device, and the objects created on it."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        self._check(self.lib.mpsgpu_create(device, C.byref(h)), ctx=False)
+        self.h = h
+
+    def _check(self, st: int, ctx: bool = True) -> None:
+        if st != 0:
+            msg = self.lib.mpsgpu_last_error(self.h).decode() if ctx else ""
+            raise MpsgpuError(st, msg)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mpsgpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.mpsgpu_launch_count(self.h))
+
+    def synchronize(self) -> None:
+        self._check(self.lib.mpsgpu_synchronize(self.h))
+
+    # ---- objects ----
+    def mpo(self, ops: list) -> "DeviceMPO":
+        arrs = [_fortran(w) for w in ops]
+        dims = _ints([s for w in arrs for s in w.shape])
+        ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        h = C.c_void_p()
+        self._check(self.lib.mpsgpu_mpo_upload(self.h, len(arrs), _ptr(dims), ptrs, C.byref(h)))
+        return DeviceMPO(self, h, len(arrs))
+
+    def mps(self, sites: list, normfact: float = 1.0) -> "DeviceMPS":
+        arrs = [_fortran(a) for a in sites]
+        dims = _ints([s for a in arrs for s in a.shape])
+        ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        h = C.c_void_p()
+        self._check(self.lib.mpsgpu_mps_upload(self.h, len(arrs), _ptr(dims), ptrs, float(normfact), C.byref(h)))
+        return DeviceMPS(self, h)
+
+    def mps_random(self, L: int, d: int, D: int, seed: int) -> "DeviceMPS":
+        h = C.c_void_p()
+        self._check(self.lib.mpsgpu_mps_random(self.h, L, d, D, C.c_uint64(seed), C.byref(h)))
+        return DeviceMPS(self, h)
+
+    def mps_product(self, L: int, d: int, D: int) -> "DeviceMPS":
+        h = C.c_void_p()
+        self._check(self.lib.mpsgpu_mps_product(self.h, L, d, D, C.byref(h)))
+        return DeviceMPS(self, h)
+
+    @staticmethod
+    def options(convtol=1e-5, eigtol=0.0, excorthtol=0.0, max_rounds=1000, max_krylov=64,
+                precision=0, verbose=0) -> Options:
+        return Options(convtol, eigtol, excorthtol, max_rounds, max_krylov, precision, verbose)
+
+    # ---- Contractor ----
+    def find_ground_state(self, ops: "DeviceMPO", D: int, init: "DeviceMPS", offset: float = 0.0,
+                          opts: Options = None):
+        e = C.c_double()
+        st = Stats()
+        o = opts or self.options()
+        self._check(self.lib.mpsgpu_find_ground_state(self.h, ops.h, D, offset, C.byref(o), init.h,
+                                                      C.byref(e), C.byref(st)))
+        return e.value, st.as_dict()
+
+    def find_next_excited_state(self, ops, D, levels, init, offset=0.0, opts=None):
+        e = C.c_double()
+        st = Stats()
+        o = opts or self.options()
+        arr = (C.c_void_p * len(levels))(*[lv.h.value for lv in levels])
+        self._check(self.lib.mpsgpu_find_next_excited_state(self.h, ops.h, D, arr, len(levels), offset,
+                                                            C.byref(o), init.h, C.byref(e), C.byref(st)))
+        return e.value, st.as_dict()
+
+    def optimize(self, ops, orig, init, D=0, opts=None, want_err=False):
+        st = Stats()
+        o = opts or self.options()
+        en, et = C.c_double(), C.c_double()
+        self._check(self.lib.mpsgpu_optimize(self.h, ops.h, orig.h, init.h, D, C.byref(o),
+                                             C.byref(en) if want_err else None,
+                                             C.byref(et) if want_err else None, C.byref(st)))
+        return (en.value, et.value, st.as_dict()) if want_err else st.as_dict()
+
+    def contract(self, ket, ops, bra) -> complex:
+        re, im = C.c_double(), C.c_double()
+        self._check(self.lib.mpsgpu_contract(self.h, ket.h, ops.h if ops is not None else None, bra.h,
+                                             C.byref(re), C.byref(im)))
+        return complex(re.value, im.value)
+
+    def expectation_local(self, mps, op2) -> np.ndarray:
+        op = _fortran(op2)
+        L = mps.info()[0]
+        out = np.zeros(L)
+        self._check(self.lib.mpsgpu_expectation_local(self.h, mps.h, _ptr(op), _ptr(out)))
+        return out
+
+    def entropy(self, mps, pos: int) -> float:
+        s = C.c_double()
+        self._check(self.lib.mpsgpu_entropy(self.h, mps.h, pos, C.byref(s)))
+        return s.value
+
+    def schmidt_values(self, mps, pos: int) -> np.ndarray:
+        cap = 4096
+        out = np.zeros(cap)
+        n = C.c_int()
+        self._check(self.lib.mpsgpu_schmidt_values(self.h, mps.h, pos, _ptr(out), cap, C.byref(n)))
+        return out[: n.value].copy()
+
+    # ---- kernel-level ----
+    def heff_matvec(self, L, W, R, x, offset=0.0, hermitian=False) -> np.ndarray:
+        L, W, R, x = _fortran(L), _fortran(W), _fortran(R), _fortran(x)
+        y = np.zeros(W.shape[0] * L.shape[0] * R.shape[0], dtype=np.complex128)
+        ld, wd, rd = _ints(L.shape), _ints(W.shape), _ints(R.shape)  # kept alive across the call
+        self._check(self.lib.mpsgpu_heff_matvec(
+            self.h, _ptr(ld), _ptr(L), _ptr(wd), _ptr(W), _ptr(rd),
+            _ptr(R), _ptr(x), _ptr(y), float(offset), int(hermitian)))
+        return y
+
+    def env_left(self, T, ket, W, bra) -> np.ndarray:
+        T, ket, W, bra = _fortran(T), _fortran(ket), _fortran(W), _fortran(bra)
+        out = np.zeros((bra.shape[2], W.shape[3], ket.shape[2]), dtype=np.complex128, order="F")
+        td, kd, wd, bd = _ints(T.shape), _ints(ket.shape), _ints(W.shape), _ints(bra.shape)
+        self._check(self.lib.mpsgpu_env_left(self.h, _ptr(td), _ptr(T), _ptr(kd), _ptr(ket), _ptr(wd),
+                                             _ptr(W), _ptr(bd), _ptr(bra), _ptr(out)))
+        return out
+
+    def env_right(self, T, ket, W, bra) -> np.ndarray:
+        T, ket, W, bra = _fortran(T), _fortran(ket), _fortran(W), _fortran(bra)
+        out = np.zeros((bra.shape[1], W.shape[1], ket.shape[1]), dtype=np.complex128, order="F")
+        td, kd, wd, bd = _ints(T.shape), _ints(ket.shape), _ints(W.shape), _ints(bra.shape)
+        self._check(self.lib.mpsgpu_env_right(self.h, _ptr(td), _ptr(T), _ptr(kd), _ptr(ket), _ptr(wd),
+                                              _ptr(W), _ptr(bd), _ptr(bra), _ptr(out)))
+        return out
+
+    def qr(self, A):
+        A = _fortran(A)
+        m, n = A.shape
+        K = min(m, n)
+        Q = np.zeros((m, K), dtype=np.complex128, order="F")
+        R = np.zeros((K, n), dtype=np.complex128, order="F")
+        self._check(self.lib.mpsgpu_qr(self.h, m, n, _ptr(A), _ptr(Q), _ptr(R)))
+        return Q, R
+
+    def lq(self, A):
+        A = _fortran(A)
+        m, n = A.shape
+        K = min(m, n)
+        Lm = np.zeros((m, K), dtype=np.complex128, order="F")
+        Q = np.zeros((K, n), dtype=np.complex128, order="F")
+        self._check(self.lib.mpsgpu_lq(self.h, m, n, _ptr(A), _ptr(Lm), _ptr(Q)))
+        return Lm, Q
+
+
+class DeviceMPO:
+    def __init__(self, ctx: Context, h, L: int):
+        self.ctx, self.h, self.L = ctx, h, L
+
+    def free(self) -> None:
+        if self.h:
+            self.ctx.lib.mpsgpu_mpo_free(self.ctx.h, self.h)
+            self.h = None
+
+
+class DeviceMPS:
+    def __init__(self, ctx: Context, h):
+        self.ctx, self.h = ctx, h
+
+    def info(self):
+        L = C.c_int()
+        self.ctx._check(self.ctx.lib.mpsgpu_mps_info(self.ctx.h, self.h, C.byref(L), None, None))
+        dims = np.zeros(3 * L.value, dtype=np.int32)
+        nf = C.c_double()
+        self.ctx._check(self.ctx.lib.mpsgpu_mps_info(self.ctx.h, self.h, C.byref(L), _ptr(dims), C.byref(nf)))
+        return L.value, dims.reshape(L.value, 3), nf.value
+
+    def download(self):
+        L, dims, nf = self.info()
+        sites = [np.zeros(tuple(d), dtype=np.complex128, order="F") for d in dims]
+        ptrs = (C.c_void_p * L)(*[a.ctypes.data for a in sites])
+        self.ctx._check(self.ctx.lib.mpsgpu_mps_download(self.ctx.h, self.h, ptrs))
+        return sites, nf
+
+    def copy(self) -> "DeviceMPS":
+        h = C.c_void_p()
+        self.ctx._check(self.ctx.lib.mpsgpu_mps_copy(self.ctx.h, self.h, C.byref(h)))
+        return DeviceMPS(self.ctx, h)
+
+    def gauge(self, direction: str) -> None:
+        self.ctx._check(self.ctx.lib.mpsgpu_mps_gauge(self.ctx.h, self.h, direction.encode()))
+
+    def free(self) -> None:
+        if self.h:
+            self.ctx.lib.mpsgpu_mps_free(self.ctx.h, self.h)
+            self.h = None

@@ -1,0 +1,72 @@
+// Shared device/host helpers of the mpsgpu library: complex FP64 arithmetic on
+// double2 (re, im interleaved, the reference's complex_t layout), error
+// plumbing and the per-context state every kernel launcher receives.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <stdexcept>
+
+#include "mpsgpu.h"
+
+namespace mpsgpu {
+
+typedef double2 cplx;
+
+__host__ __device__ inline cplx cmake(double re, double im) { return make_double2(re, im); }
+__host__ __device__ inline cplx cadd(cplx a, cplx b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ inline cplx csub(cplx a, cplx b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ inline cplx cmul(cplx a, cplx b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ inline cplx cconj(cplx a) { return make_double2(a.x, -a.y); }
+__host__ __device__ inline cplx cscale(cplx a, double s) { return make_double2(a.x * s, a.y * s); }
+// a * conj(b)
+__host__ __device__ inline cplx cmulc(cplx a, cplx b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+// conj(a) * b
+__host__ __device__ inline cplx ccmul(cplx a, cplx b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ inline double cabs2(cplx a) { return a.x * a.x + a.y * a.y; }
+
+// Error carrying a status code; every C-ABI function catches it.
+struct Error : public std::runtime_error {
+  mpsgpu_status status;
+  Error(mpsgpu_status s, const std::string& msg) : std::runtime_error(msg), status(s) {}
+};
+
+#define MPSGPU_CUDA(call)                                                        \
+  do {                                                                           \
+    cudaError_t _e = (call);                                                     \
+    if (_e != cudaSuccess) {                                                     \
+      throw ::mpsgpu::Error(_e == cudaErrorMemoryAllocation ? MPSGPU_OOM         \
+                                                            : MPSGPU_CUDA_ERROR, \
+                            std::string(#call) + ": " + cudaGetErrorString(_e)); \
+    }                                                                            \
+  } while (0)
+
+#define MPSGPU_CHECK(cond, status, msg)                    \
+  do {                                                     \
+    if (!(cond)) throw ::mpsgpu::Error((status), (msg));   \
+  } while (0)
+
+// Launch bookkeeping: every kernel launcher calls after_launch().
+struct Stream {
+  cudaStream_t s = nullptr;
+  long long* launches = nullptr;
+};
+
+inline void after_launch(const Stream& st) {
+  if (st.launches) ++(*st.launches);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw Error(MPSGPU_CUDA_ERROR, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace mpsgpu

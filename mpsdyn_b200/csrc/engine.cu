@@ -1,0 +1,842 @@
+// Sweep engine: the reference Contractor's single-site algorithms
+// (src/core/cpp/Contractor.cpp) on device-resident tensors.
+//
+// Device layout of a site tensor: X(a, s, r) with the left bond fastest, so
+// that the first GEMM of every contraction reads it as a plain (Dl x d*Dr)
+// matrix.  Left environments are stored as the reference stores them,
+// L(bra, w, ket); right environments transposed, Rt(ket, w, bra), so that the
+// last GEMM of the matvec reads them as a plain ((Dr*w) x Dr) matrix.  With
+// these layouts every step of
+//   y[s',a',r'] = sum L[a',b,a] W[s',b,s,c] R[r',c,r] x[s,a,r]
+// is one GEMM or one MPO-leg contraction; none of the explicit permutes of
+// TensorMultiplier::product (TensorMultiplier.cpp:61-93) remain.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+#include "tridiag.h"
+
+namespace mpsgpu {
+
+// ---------------------------------------------------------------------------
+// buffers
+// ---------------------------------------------------------------------------
+
+void dbuf_reserve(Context& c, DBuf& b, long long n) {
+  if (n <= b.cap) return;
+  if (b.p) MPSGPU_CUDA(cudaFreeAsync(b.p, c.stream));
+  b.p = nullptr;
+  b.cap = 0;
+  long long nn = std::max<long long>(n, 1);
+  MPSGPU_CUDA(cudaMallocAsync((void**)&b.p, nn * sizeof(cplx), c.stream));
+  b.cap = nn;
+}
+
+void dbuf_free(Context& c, DBuf& b) {
+  if (b.p) cudaFreeAsync(b.p, c.stream);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+int MpsDev::max_bond() const {
+  int m = 1;
+  for (auto& d : dims) m = std::max(m, std::max(d[1], d[2]));
+  return m;
+}
+
+static inline long long nel(const std::array<int, 3>& d) { return (long long)d[0] * d[1] * d[2]; }
+
+// ---------------------------------------------------------------------------
+// MPO upload: reference tensors plus the small leg matrices of each operator
+// ---------------------------------------------------------------------------
+
+void mpo_upload(Context& c, MpoDev& m, int L, const int* dims, const double* const* data,
+                bool check_edges) {
+  MPSGPU_CHECK(L >= 1, MPSGPU_BAD_SHAPE, "mpo: L < 1");
+  m.L = L;
+  m.dims.resize(L);
+  m.W.assign(L, DBuf());
+  m.Wlr.assign(L, DBuf());
+  m.Wrl.assign(L, DBuf());
+  m.Wlr_h.assign(L, DBuf());
+  m.Wrl_h.assign(L, DBuf());
+  for (int k = 0; k < L; k++) {
+    const int du = dims[4 * k], wl = dims[4 * k + 1], dd = dims[4 * k + 2], wr = dims[4 * k + 3];
+    MPSGPU_CHECK(du > 0 && wl > 0 && dd > 0 && wr > 0, MPSGPU_BAD_SHAPE, "mpo: non-positive dimension");
+    MPSGPU_CHECK(du * wr <= 32 && wl * dd <= 32 && wl * du <= 32 && dd * wr <= 32, MPSGPU_BAD_SHAPE,
+                 "mpo: d*w must not exceed 32");
+    if (k > 0) MPSGPU_CHECK(m.dims[k - 1][3] == wl, MPSGPU_BAD_SHAPE, "mpo: bond mismatch");
+    m.dims[k] = {du, wl, dd, wr};
+    const long long n = (long long)du * wl * dd * wr;
+    const cplx* W = reinterpret_cast<const cplx*>(data[k]);
+    auto at = [&](int sp, int b, int s, int cc) { return W[sp + du * (b + wl * (s + dd * cc))]; };
+    std::vector<cplx> lr(n), rl(n), lrh(n), rlh(n);
+    const int nout_lr = du * wr, nout_rl = wl * du;
+    for (int sp = 0; sp < du; sp++)
+      for (int b = 0; b < wl; b++)
+        for (int s = 0; s < dd; s++)
+          for (int cc = 0; cc < wr; cc++) {
+            cplx w = at(sp, b, s, cc);
+            lr[(sp + du * cc) + (long long)nout_lr * (b + wl * s)] = w;
+            rl[(b + wl * sp) + (long long)nout_rl * (s + dd * cc)] = w;
+            if (du == dd) {
+              // adjoint operator W^dag[s', b, s, c] = conj(W[s, b, s', c])
+              cplx wa = at(s, b, sp, cc);
+              wa.y = -wa.y;
+              lrh[(sp + du * cc) + (long long)nout_lr * (b + wl * s)] = wa;
+              rlh[(b + wl * sp) + (long long)nout_rl * (s + dd * cc)] = wa;
+            }
+          }
+    dbuf_reserve(c, m.W[k], n);
+    dbuf_reserve(c, m.Wlr[k], n);
+    dbuf_reserve(c, m.Wrl[k], n);
+    MPSGPU_CUDA(cudaMemcpyAsync(m.W[k].p, W, n * sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+    MPSGPU_CUDA(cudaMemcpyAsync(m.Wlr[k].p, lr.data(), n * sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+    MPSGPU_CUDA(cudaMemcpyAsync(m.Wrl[k].p, rl.data(), n * sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+    if (du == dd) {
+      dbuf_reserve(c, m.Wlr_h[k], n);
+      dbuf_reserve(c, m.Wrl_h[k], n);
+      MPSGPU_CUDA(cudaMemcpyAsync(m.Wlr_h[k].p, lrh.data(), n * sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+      MPSGPU_CUDA(cudaMemcpyAsync(m.Wrl_h[k].p, rlh.data(), n * sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+    }
+    // host vectors must outlive the async copies
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  if (check_edges)
+    MPSGPU_CHECK(m.dims[0][1] == 1 && m.dims[L - 1][3] == 1, MPSGPU_BAD_SHAPE,
+                 "mpo: edge bonds must be 1");
+}
+
+void mpo_free(Context& c, MpoDev& m) {
+  for (auto* v : {&m.W, &m.Wlr, &m.Wrl, &m.Wlr_h, &m.Wrl_h})
+    for (auto& b : *v) dbuf_free(c, b);
+  m.L = 0;
+}
+
+// ---------------------------------------------------------------------------
+// MPS storage
+// ---------------------------------------------------------------------------
+
+void mps_upload(Context& c, MpsDev& s, int L, const int* dims, const double* const* data, double nf) {
+  MPSGPU_CHECK(L >= 1, MPSGPU_BAD_SHAPE, "mps: L < 1");
+  s.L = L;
+  s.dims.resize(L);
+  s.A.resize(L);
+  long long maxn = 0;
+  for (int k = 0; k < L; k++) {
+    s.dims[k] = {dims[3 * k], dims[3 * k + 1], dims[3 * k + 2]};
+    MPSGPU_CHECK(s.dims[k][0] > 0 && s.dims[k][1] > 0 && s.dims[k][2] > 0, MPSGPU_BAD_SHAPE,
+                 "mps: non-positive dimension");
+    if (k > 0) MPSGPU_CHECK(s.dims[k - 1][2] == s.dims[k][1], MPSGPU_BAD_SHAPE, "mps: bond mismatch");
+    maxn = std::max(maxn, nel(s.dims[k]));
+  }
+  MPSGPU_CHECK(s.dims[0][1] == 1 && s.dims[L - 1][2] == 1, MPSGPU_BAD_SHAPE, "mps: edge bonds must be 1");
+  dbuf_reserve(c, c.t1, maxn);
+  for (int k = 0; k < L; k++) {
+    long long n = nel(s.dims[k]);
+    dbuf_reserve(c, s.A[k], n);
+    MPSGPU_CUDA(cudaMemcpyAsync(c.t1.p, data[k], n * sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+    site_ref_to_dev(c.st(), s.dims[k][0], s.dims[k][1], s.dims[k][2], c.t1.p, s.A[k].p);
+  }
+  s.normfact = nf;
+  s.gauge = 0;
+  s.bond = s.max_bond();
+}
+
+void mps_random(Context& c, MpsDev& s, int L, int d, int D, uint64_t seed) {
+  MPSGPU_CHECK(L >= 2 && d >= 1 && D >= 1, MPSGPU_BAD_SHAPE, "mps_random: bad sizes");
+  s.L = L;
+  s.dims.resize(L);
+  s.A.resize(L);
+  std::vector<int> bonds(L + 1);
+  for (int k = 0; k <= L; k++) {
+    double lk = std::min(k, L - k) * std::log((double)d);
+    bonds[k] = lk > std::log((double)D) ? D : std::min<long long>(D, (long long)std::llround(std::pow((double)d, std::min(k, L - k))));
+  }
+  long long off = 0;
+  for (int k = 0; k < L; k++) {
+    s.dims[k] = {d, bonds[k], bonds[k + 1]};
+    dbuf_reserve(c, s.A[k], nel(s.dims[k]));
+    gaussian_site(c.st(), seed, off, d, bonds[k], bonds[k + 1], s.A[k].p);
+    off += nel(s.dims[k]);
+  }
+  s.normfact = 1.0;
+  s.gauge = 0;
+  s.bond = s.max_bond();
+}
+
+void mps_product(Context& c, MpsDev& s, int L, int d, int D) {
+  s.L = L;
+  s.dims.resize(L);
+  s.A.resize(L);
+  for (int k = 0; k < L; k++) {
+    int dl = k == 0 ? 1 : D, dr = k == L - 1 ? 1 : D;
+    s.dims[k] = {d, dl, dr};
+    dbuf_reserve(c, s.A[k], nel(s.dims[k]));
+    zfill(c.st(), nel(s.dims[k]), make_double2(0.0, 0.0), s.A[k].p);
+    cplx one = make_double2(1.0, 0.0);
+    MPSGPU_CUDA(cudaMemcpyAsync(s.A[k].p, &one, sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+  }
+  MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  s.normfact = 1.0;
+  s.gauge = 0;
+  s.bond = D;
+}
+
+void mps_copy(Context& c, const MpsDev& src, MpsDev& dst) {
+  if (&src == &dst) return;
+  dst.L = src.L;
+  dst.dims = src.dims;
+  dst.A.resize(src.L);
+  for (int k = 0; k < src.L; k++) {
+    dbuf_reserve(c, dst.A[k], nel(src.dims[k]));
+    zcopy(c.st(), (int)nel(src.dims[k]), src.A[k].p, dst.A[k].p);
+  }
+  dst.normfact = src.normfact;
+  dst.gauge = src.gauge;
+  dst.bond = src.bond;
+}
+
+void mps_download(Context& c, const MpsDev& s, double* const* data) {
+  long long maxn = 0;
+  for (int k = 0; k < s.L; k++) maxn = std::max(maxn, nel(s.dims[k]));
+  dbuf_reserve(c, c.t1, maxn);
+  for (int k = 0; k < s.L; k++) {
+    long long n = nel(s.dims[k]);
+    site_dev_to_ref(c.st(), s.dims[k][0], s.dims[k][1], s.dims[k][2], s.A[k].p, c.t1.p);
+    MPSGPU_CUDA(cudaMemcpyAsync(data[k], c.t1.p, n * sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  }
+}
+
+void mps_free(Context& c, MpsDev& s) {
+  for (auto& b : s.A) dbuf_free(c, b);
+  s.A.clear();
+  s.dims.clear();
+  s.L = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Gauge moves (Site::gaugeR / gaugeL, src/core/cpp/Site.cpp:179-283;
+// MPS::gaugeCond, src/core/cpp/MPS.cpp:306-419)
+// ---------------------------------------------------------------------------
+
+// Move the norm of site pos into a factor: dir 'R' -> site = Q (left
+// isometry), factor R (K x Dr) left in c.matR (ld K); dir 'L' -> site = Q^H
+// rows (right isometry), factor R' (K x Dl) with L = R'^H.  Returns K.
+static int site_factor(Context& c, MpsDev& s, int pos, char dir, cplx* r00) {
+  const int d = s.dims[pos][0], Dl = s.dims[pos][1], Dr = s.dims[pos][2];
+  int m, n;
+  View2 v;
+  if (dir == 'R') {
+    m = d * Dl; n = Dr;
+    // row i = s + d a  (reference order), column r
+    v.rd = d; v.r0 = Dl; v.r1 = 1; v.cd = 1; v.c0 = 0; v.c1 = (long long)Dl * d;
+  } else {
+    // QR of M^H, M = X viewed as (Dl x d*Dr): B(i, j) = conj(X[j + Dl i])
+    m = d * Dr; n = Dl;
+    v.rd = 1; v.r0 = 0; v.r1 = Dl; v.cd = 1; v.c0 = 0; v.c1 = 1; v.conj = true;
+  }
+  const int K = std::min(m, n);
+  dbuf_reserve(c, c.matA, (long long)m * n);
+  dbuf_reserve(c, c.matQ, (long long)m * K);
+  dbuf_reserve(c, c.matR, (long long)K * n);
+  gather2(c.st(), m, n, s.A[pos].p, v, c.matA.p);
+  householder_qr_inplace(c.st(), m, n, c.matA.p, c.matQ.p, m, c.matR.p, K, c.qrws);
+  // write the isometry back into the site
+  View2 w;
+  if (dir == 'R') {
+    s.dims[pos] = {d, Dl, K};
+    w.rd = d; w.r0 = Dl; w.r1 = 1; w.cd = 1; w.c0 = 0; w.c1 = (long long)Dl * d;
+  } else {
+    s.dims[pos] = {d, K, Dr};
+    // site X'(k, s, r) at k + K (s + d r) = conj(Q'(c = s + d r, k))
+    w.rd = 1; w.r0 = 0; w.r1 = K; w.cd = 1; w.c0 = 0; w.c1 = 1; w.conj = true;
+  }
+  scatter2(c.st(), m, K, c.matQ.p, s.A[pos].p, w);
+  if (r00 && K == 1 && n == 1) {
+    MPSGPU_CUDA(cudaMemcpyAsync(r00, c.matR.p, sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  return K;
+}
+
+// Single-element phase handling of Site::gaugeR/gaugeL on the last/first site.
+static double edge_phase(Context& c, MpsDev& s, int pos, char dir, cplx aux) {
+  double a = std::sqrt(cabs2(aux));
+  if (dir == 'L') aux.y = -aux.y;  // L = R'^H
+  cplx phase = a > 0 ? make_double2(aux.x / a, aux.y / a) : make_double2(1.0, 0.0);
+  zaxpby(c.st(), (int)nel(s.dims[pos]), phase, s.A[pos].p, make_double2(0.0, 0.0), s.A[pos].p);
+  return a;
+}
+
+// A_next <- R * A_next on its left bond (Site::reduceDimR); A_prev <- A_prev * L
+// on its right bond (Site::reduceDimL) with L = R'^H.
+static void absorb(Context& c, MpsDev& s, int target, char dir, int K, int n) {
+  const int d = s.dims[target][0], Dl = s.dims[target][1], Dr = s.dims[target][2];
+  GemmArgs g;
+  if (dir == 'R') {
+    MPSGPU_CHECK(Dl == n, MPSGPU_BAD_SHAPE, "absorb R: bond mismatch");
+    dbuf_reserve(c, c.t3, (long long)K * d * Dr);
+    g.M = K; g.N = d * Dr; g.K = Dl;
+    g.A = c.matR.p; g.lda = K; g.opA = OP_N;
+    g.B = s.A[target].p; g.ldb = Dl; g.opB = OP_N;
+    g.C = c.t3.p; g.ldc = K;
+    zgemm(c.st(), g, c.scratch);
+    s.dims[target] = {d, K, Dr};
+  } else {
+    MPSGPU_CHECK(Dr == n, MPSGPU_BAD_SHAPE, "absorb L: bond mismatch");
+    dbuf_reserve(c, c.t3, (long long)Dl * d * K);
+    g.M = Dl * d; g.N = K; g.K = Dr;
+    g.A = s.A[target].p; g.lda = (long long)Dl * d; g.opA = OP_N;
+    g.B = c.matR.p; g.ldb = K; g.opB = OP_C;  // (R')^H : Dr x K
+    g.C = c.t3.p; g.ldc = (long long)Dl * d;
+    zgemm(c.st(), g, c.scratch);
+    s.dims[target] = {d, Dl, K};
+  }
+  dbuf_reserve(c, s.A[target], nel(s.dims[target]));
+  zcopy(c.st(), (int)nel(s.dims[target]), c.t3.p, s.A[target].p);
+}
+
+// QR/LQ of site pos; when the factor is the 1x1 of a bond of dimension 1
+// the phase goes into the site and |factor| is returned (else -1, factor
+// left in c.matR).  Site::gaugeR / gaugeL, Site.cpp:199-207 and :229-237.
+static int gauge_factor(Context& c, MpsDev& s, int pos, char dir, double* scalar, Counters* cnt) {
+  const auto old = s.dims[pos];
+  const int n = dir == 'R' ? old[2] : old[1];
+  cplx r00 = make_double2(0.0, 0.0);
+  const int K = site_factor(c, s, pos, dir, &r00);
+  *scalar = -1.0;
+  if (K == 1 && n == 1) *scalar = edge_phase(c, s, pos, dir, r00);
+  if (cnt) {
+    cnt->qr_calls++;
+    const double m = dir == 'R' ? (double)old[0] * old[1] : (double)old[0] * old[2];
+    const double kk = K;
+    cnt->flops += 8.0 * 2.0 * (2.0 * m * n * kk - (m + n) * kk * kk + 2.0 * kk * kk * kk / 3.0);
+  }
+  return K;
+}
+
+// Site::reduceDimR / reduceDimL with the factor of gauge_factor.
+static void pass_factor(Context& c, MpsDev& s, int target, char dir, int K, int n, double scalar) {
+  if (scalar >= 0.0) {
+    zaxpby(c.st(), (int)nel(s.dims[target]), make_double2(scalar, 0.0), s.A[target].p,
+           make_double2(0.0, 0.0), s.A[target].p);
+  } else {
+    absorb(c, s, target, dir, K, n);
+  }
+}
+
+// MPS::gaugeCond(pos, dir, next) (MPS.cpp:366-419).
+void mps_gauge_site(Context& c, MpsDev& s, int pos, char dir, bool next, Counters* cnt) {
+  const auto old = s.dims[pos];
+  const int n = dir == 'R' ? old[2] : old[1];
+  double scalar = -1.0;
+  const int K = gauge_factor(c, s, pos, dir, &scalar, cnt);
+  if (dir == 'L') {
+    if ((s.dims[pos][1] != old[1] || next) && pos > 0) pass_factor(c, s, pos - 1, 'L', K, n, scalar);
+    if (pos == 0 && next) {
+      MPSGPU_CHECK(scalar >= 0.0, MPSGPU_BAD_SHAPE, "gaugeL on site 0: factor is not a scalar");
+      s.normfact *= scalar;
+    }
+  } else {
+    if (pos < s.L - 1 && (s.dims[pos][2] != old[2] || next)) pass_factor(c, s, pos + 1, 'R', K, n, scalar);
+    if (next && pos == s.L - 1) {
+      MPSGPU_CHECK(scalar >= 0.0, MPSGPU_BAD_SHAPE, "gaugeR on the last site: factor is not a scalar");
+      s.normfact *= scalar;
+    }
+  }
+  s.gauge = 0;
+}
+
+// MPS::gaugeCond(dir, normal) (MPS.cpp:306-364): a full QR (or LQ) sweep
+// carrying the factor along; the final scalar becomes the norm factor.
+void mps_gauge_all(Context& c, MpsDev& s, char dir, bool normal) {
+  double last = 1.0;
+  if (dir == 'R') {
+    for (int pos = 0; pos < s.L; pos++) {
+      const int n = s.dims[pos][2];
+      double scalar = -1.0;
+      const int K = gauge_factor(c, s, pos, 'R', &scalar, nullptr);
+      if (pos < s.L - 1) pass_factor(c, s, pos + 1, 'R', K, n, scalar);
+      else last = scalar;
+    }
+    s.gauge = 2;
+  } else {
+    for (int pos = s.L - 1; pos >= 0; pos--) {
+      const int n = s.dims[pos][1];
+      double scalar = -1.0;
+      const int K = gauge_factor(c, s, pos, 'L', &scalar, nullptr);
+      if (pos > 0) pass_factor(c, s, pos - 1, 'L', K, n, scalar);
+      else last = scalar;
+    }
+    s.gauge = 1;
+  }
+  s.bond = std::min(s.bond > 0 ? s.bond : 1 << 30, s.max_bond());
+  if (normal) s.normfact = 1.0;
+  else s.normfact *= last;
+}
+
+// MPS::increaseBondDimensionWithNoise(D, 0) (MPS.cpp:654-719): integer bond
+// schedule, zero padding of every site.
+void mps_increase_bond(Context& c, MpsDev& s, int D) {
+  if (D <= s.bond) return;
+  const int L = s.L;
+  long long cumd = 1, cumdr_last = 1;
+  int boundR = L - 1;
+  bool done = false;
+  while (!done && boundR > 0) {
+    int dim = s.dims[boundR][0];
+    if (cumdr_last * dim < D) { boundR--; cumdr_last *= dim; }
+    else done = true;
+  }
+  long long cumdr = boundR > 0 ? D : cumdr_last * s.dims[0][0];
+  int maxbond = 1;
+  for (int k = 0; k < L; k++) {
+    auto old = s.dims[k];
+    long long newDl, newDr;
+    if (k == 0) newDl = old[1];
+    else newDl = (cumd < D || cumdr < D) ? std::min(cumd, cumdr) : D;
+    int posd = s.dims[k][0];
+    if (cumd < D) cumd *= posd;
+    if (k == boundR) cumdr = cumdr_last;
+    else if (k > boundR) cumdr = cumdr / posd;
+    if (k == L - 1) newDr = old[2];
+    else newDr = (cumd < D || cumdr < D) ? std::min(cumd, cumdr) : D;
+    std::array<int, 3> nd = {old[0], (int)newDl, (int)newDr};
+    // zero-padded copy: X'(a, s, r) = X(a, s, r) inside the old box
+    DBuf nb;
+    dbuf_reserve(c, nb, nel(nd));
+    zfill(c.st(), nel(nd), make_double2(0.0, 0.0), nb.p);
+    const int m1 = std::min(old[1], nd[1]), m2 = std::min(old[2], nd[2]);
+    // rows = (a, s) with a < m1, columns r < m2
+    const int rows = m1 * old[0];
+    View2 vi; vi.rd = m1; vi.r0 = 1; vi.r1 = old[1]; vi.cd = 1; vi.c0 = 0; vi.c1 = (long long)old[1] * old[0];
+    View2 vo; vo.rd = m1; vo.r0 = 1; vo.r1 = nd[1]; vo.cd = 1; vo.c0 = 0; vo.c1 = (long long)nd[1] * nd[0];
+    dbuf_reserve(c, c.t3, (long long)rows * m2);
+    gather2(c.st(), rows, m2, s.A[k].p, vi, c.t3.p);
+    scatter2(c.st(), rows, m2, c.t3.p, nb.p, vo);
+    dbuf_free(c, s.A[k]);
+    s.A[k] = nb;
+    s.dims[k] = nd;
+    maxbond = std::max(maxbond, (int)std::max(newDl, newDr));
+  }
+  s.bond = maxbond;
+  s.gauge = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Contractions
+// ---------------------------------------------------------------------------
+
+static double mv_flops(int d, int w1, int w2, int dl, int dr) {
+  // complex MACs of the three steps, 8 real flops each
+  double a = (double)dl * w1 * dl * d * dr;       // L . X
+  double b = (double)dl * d * d * w1 * w2 * dr;   // W
+  double cc = (double)dl * d * dr * w2 * dr;      // . R
+  return 8.0 * (a + b + cc);
+}
+
+void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpoDev& m, int k,
+                bool adjoint, const cplx* Rt, const std::array<int, 3>& rd, const cplx* x, cplx* y,
+                cplx offset, Counters* cnt) {
+  const auto& wd = m.dims[k];
+  const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
+  const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
+  MPSGPU_CHECK(ld[1] == wl && rd[1] == wr, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
+  // step 1: T1[(a',b),(s,r)] = L((Dlb*wl) x Dlk) . X(Dlk x dd*Drk)
+  const long long n1 = (long long)Dlb * wl * dd * Drk;
+  dbuf_reserve(c, c.t1, n1);
+  GemmArgs g;
+  g.M = Dlb * wl; g.N = dd * Drk; g.K = Dlk;
+  g.A = Le; g.lda = (long long)Dlb * wl;
+  g.B = x; g.ldb = Dlk;
+  g.C = c.t1.p; g.ldc = (long long)Dlb * wl;
+  zgemm(c.st(), g, c.scratch);
+  // step 2: T2[a', s', r, c] = sum_{b,s} W[s',b,s,c] T1[a',b,s,r]
+  const long long n2 = (long long)Dlb * du * Drk * wr;
+  dbuf_reserve(c, c.t2, n2);
+  WContractArgs wa;
+  wa.nx = Dlb; wa.ny = Drk;
+  wa.in = c.t1.p; wa.ix = 1; wa.iy = (long long)Dlb * wl * dd; wa.si0 = Dlb; wa.si1 = (long long)Dlb * wl;
+  wa.n_i0 = wl; wa.n_i1 = dd;
+  wa.out = c.t2.p; wa.ox = 1; wa.oy = (long long)Dlb * du; wa.so0 = Dlb; wa.so1 = (long long)Dlb * du * Drk;
+  wa.n_o0 = du; wa.n_o1 = wr;
+  wa.Wm = adjoint ? m.Wlr_h[k].p : m.Wlr[k].p;
+  MPSGPU_CHECK(wa.Wm != nullptr, MPSGPU_BAD_SHAPE, "heff: adjoint needs du == dd");
+  wcontract(c.st(), wa);
+  // step 3: Y[(a',s'), r'] = T2((Dlb*du) x (Drk*wr)) . Rt((Drk*wr) x Drb) + offset X
+  GemmArgs h;
+  h.M = Dlb * du; h.N = Drb; h.K = Drk * wr;
+  h.A = c.t2.p; h.lda = (long long)Dlb * du;
+  h.B = Rt; h.ldb = (long long)Drk * wr;
+  h.C = y; h.ldc = (long long)Dlb * du;
+  if (offset.x != 0.0 || offset.y != 0.0) {
+    h.Cin = x; h.ldcin = (long long)Dlb * du; h.beta = offset;
+  }
+  zgemm(c.st(), h, c.scratch);
+  if (cnt) {
+    cnt->matvecs++;
+    cnt->flops += mv_flops(dd, wl, wr, Dlb, Drb);
+  }
+}
+
+void env_left_update(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpsDev& ket,
+                     const MpoDev* m, int k, const MpsDev& bra, DBuf& out, std::array<int, 3>& od,
+                     Counters* cnt) {
+  const auto& kd = ket.dims[k];
+  const auto& bd = bra.dims[k];
+  const int dd = kd[0], Dlk = kd[1], Drk = kd[2];
+  const int du = bd[0], Dlb = bd[1], Drb = bd[2];
+  const int wl = m ? m->dims[k][1] : 1, wr = m ? m->dims[k][3] : 1;
+  MPSGPU_CHECK(ld[0] == Dlb && ld[2] == Dlk && ld[1] == wl, MPSGPU_BAD_SHAPE, "envL: dims");
+  // T1 = L . X_ket  -> [a', b, s, r']
+  dbuf_reserve(c, c.t1, (long long)Dlb * wl * dd * Drk);
+  GemmArgs g;
+  g.M = Dlb * wl; g.N = dd * Drk; g.K = Dlk;
+  g.A = Le; g.lda = (long long)Dlb * wl;
+  g.B = ket.A[k].p; g.ldb = Dlk;
+  g.C = c.t1.p; g.ldc = (long long)Dlb * wl;
+  zgemm(c.st(), g, c.scratch);
+  const cplx* T2 = c.t1.p;
+  if (m) {
+    // T2[a', t, c, r'] = sum W[t,b,s,c] T1[a',b,s,r']
+    dbuf_reserve(c, c.t2, (long long)Dlb * du * wr * Drk);
+    WContractArgs wa;
+    wa.nx = Dlb; wa.ny = Drk;
+    wa.in = c.t1.p; wa.ix = 1; wa.iy = (long long)Dlb * wl * dd; wa.si0 = Dlb; wa.si1 = (long long)Dlb * wl;
+    wa.n_i0 = wl; wa.n_i1 = dd;
+    wa.out = c.t2.p; wa.ox = 1; wa.oy = (long long)Dlb * du * wr; wa.so0 = Dlb; wa.so1 = (long long)Dlb * du;
+    wa.n_o0 = du; wa.n_o1 = wr;
+    wa.Wm = m->Wlr[k].p;
+    wcontract(c.st(), wa);
+    T2 = c.t2.p;
+  }
+  // Lnew[r, (c, r')] = X_bra^H . T2
+  od = {Drb, wr, Drk};
+  dbuf_reserve(c, out, (long long)Drb * wr * Drk);
+  GemmArgs h;
+  h.M = Drb; h.N = wr * Drk; h.K = Dlb * du;
+  h.A = bra.A[k].p; h.lda = (long long)Dlb * du; h.opA = OP_C;
+  h.B = T2; h.ldb = (long long)Dlb * du;
+  h.C = out.p; h.ldc = Drb;
+  zgemm(c.st(), h, c.scratch);
+  if (cnt) {
+    cnt->env_updates++;
+    cnt->flops += mv_flops(dd, wl, wr, Dlb, Drb);
+  }
+}
+
+void env_right_update(Context& c, const cplx* Rt, const std::array<int, 3>& rd, const MpsDev& ket,
+                      const MpoDev* m, int k, const MpsDev& bra, DBuf& out, std::array<int, 3>& od,
+                      Counters* cnt) {
+  const auto& kd = ket.dims[k];
+  const auto& bd = bra.dims[k];
+  const int dd = kd[0], Dlk = kd[1], Drk = kd[2];
+  const int du = bd[0], Dlb = bd[1], Drb = bd[2];
+  const int wl = m ? m->dims[k][1] : 1, wr = m ? m->dims[k][3] : 1;
+  MPSGPU_CHECK(rd[0] == Drk && rd[2] == Drb && rd[1] == wr, MPSGPU_BAD_SHAPE, "envR: dims");
+  // T1[(l', s), (c, r)] = X_ket((Dlk*dd) x Drk) . Rt(Drk x (wr*Drb))
+  dbuf_reserve(c, c.t1, (long long)Dlk * dd * wr * Drb);
+  GemmArgs g;
+  g.M = Dlk * dd; g.N = wr * Drb; g.K = Drk;
+  g.A = ket.A[k].p; g.lda = (long long)Dlk * dd;
+  g.B = Rt; g.ldb = Drk;
+  g.C = c.t1.p; g.ldc = (long long)Dlk * dd;
+  zgemm(c.st(), g, c.scratch);
+  const cplx* T2 = c.t1.p;
+  if (m) {
+    // T2[l', b, t, r] = sum_{s,c} W[t,b,s,c] T1[l', s, c, r]
+    dbuf_reserve(c, c.t2, (long long)Dlk * wl * du * Drb);
+    WContractArgs wa;
+    wa.nx = Dlk; wa.ny = Drb;
+    wa.in = c.t1.p; wa.ix = 1; wa.iy = (long long)Dlk * dd * wr; wa.si0 = Dlk; wa.si1 = (long long)Dlk * dd;
+    wa.n_i0 = dd; wa.n_i1 = wr;
+    wa.out = c.t2.p; wa.ox = 1; wa.oy = (long long)Dlk * wl * du; wa.so0 = Dlk; wa.so1 = (long long)Dlk * wl;
+    wa.n_o0 = wl; wa.n_o1 = du;
+    wa.Wm = m->Wrl[k].p;
+    wcontract(c.st(), wa);
+    T2 = c.t2.p;
+  }
+  // Rt_new[(l', b), l] = T2((Dlk*wl) x (du*Drb)) . X_bra^H  (X_bra as Dlb x (du*Drb))
+  od = {Dlk, wl, Dlb};
+  dbuf_reserve(c, out, (long long)Dlk * wl * Dlb);
+  GemmArgs h;
+  h.M = Dlk * wl; h.N = Dlb; h.K = du * Drb;
+  h.A = T2; h.lda = (long long)Dlk * wl;
+  h.B = bra.A[k].p; h.ldb = Dlb; h.opB = OP_C;
+  h.C = out.p; h.ldc = (long long)Dlk * wl;
+  zgemm(c.st(), h, c.scratch);
+  if (cnt) {
+    cnt->env_updates++;
+    cnt->flops += mv_flops(dd, wl, wr, Dlb, Drb);
+  }
+}
+
+void EnvCache::init(Context& c, int L_) {
+  L = L_;
+  Le.assign(L, DBuf());
+  Re.assign(L, DBuf());
+  ldims.assign(L, {1, 1, 1});
+  rdims.assign(L, {1, 1, 1});
+  okL.assign(L, 0);
+  okR.assign(L, 0);
+  cplx one = make_double2(1.0, 0.0);
+  dbuf_reserve(c, Le[0], 1);
+  dbuf_reserve(c, Re[L - 1], 1);
+  MPSGPU_CUDA(cudaMemcpyAsync(Le[0].p, &one, sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+  MPSGPU_CUDA(cudaMemcpyAsync(Re[L - 1].p, &one, sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+  MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  okL[0] = 1;
+  okR[L - 1] = 1;
+}
+
+void EnvCache::release(Context& c) {
+  for (auto& b : Le) dbuf_free(c, b);
+  for (auto& b : Re) dbuf_free(c, b);
+}
+
+// Contractor::calculateL / calculateR (Contractor.cpp:723-764)
+static void calc_left(Context& c, EnvCache& E, int pos, const MpoDev* ops, const MpsDev& ket,
+                      const MpsDev& bra, Counters* cnt) {
+  if (E.okL[pos]) return;
+  calc_left(c, E, pos - 1, ops, ket, bra, cnt);
+  env_left_update(c, E.Le[pos - 1].p, E.ldims[pos - 1], ket, ops, pos - 1, bra, E.Le[pos], E.ldims[pos], cnt);
+  E.okL[pos] = 1;
+}
+
+static void calc_right(Context& c, EnvCache& E, int pos, const MpoDev* ops, const MpsDev& ket,
+                       const MpsDev& bra, Counters* cnt) {
+  if (E.okR[pos]) return;
+  calc_right(c, E, pos + 1, ops, ket, bra, cnt);
+  env_right_update(c, E.Re[pos + 1].p, E.rdims[pos + 1], ket, ops, pos + 1, bra, E.Re[pos], E.rdims[pos], cnt);
+  E.okR[pos] = 1;
+}
+
+// Contractor::contract(ket, ops, bra) (Contractor.cpp:467-556)
+cplx contract(Context& c, const MpsDev& ket, const MpoDev* ops, const MpsDev& bra) {
+  MPSGPU_CHECK(ket.L == bra.L && (!ops || ops->L == ket.L), MPSGPU_BAD_SHAPE, "contract: lengths");
+  DBuf a, b;
+  std::array<int, 3> ad = {1, 1, 1}, bd;
+  dbuf_reserve(c, a, 1);
+  cplx one = make_double2(1.0, 0.0);
+  MPSGPU_CUDA(cudaMemcpyAsync(a.p, &one, sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+  for (int k = 0; k < ket.L; k++) {
+    env_left_update(c, a.p, ad, ket, ops, k, bra, b, bd, nullptr);
+    std::swap(a, b);
+    ad = bd;
+  }
+  cplx r;
+  MPSGPU_CUDA(cudaMemcpyAsync(&r, a.p, sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+  MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  dbuf_free(c, a);
+  dbuf_free(c, b);
+  return cscale(r, ket.normfact * bra.normfact);
+}
+
+// ---------------------------------------------------------------------------
+// Lanczos for the lowest eigenpair (replaces the PRIMME call of
+// Contractor::solveEigs, Contractor.cpp:3067-3138; and its dense branch).
+// Restarted Lanczos with full (twice classical Gram-Schmidt)
+// reorthogonalisation, FP64; convergence ||r|| <= tol * max|Ritz|.
+// ---------------------------------------------------------------------------
+
+template <class Op>
+static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, int max_krylov,
+                             int* iters) {
+  const int m = std::min(N, std::max(2, max_krylov));
+  dbuf_reserve(c, c.lanV, (long long)N * (m + 1));
+  dbuf_reserve(c, c.lanW, N);
+  cplx* V = c.lanV.p;
+  cplx* w = c.lanW.p;
+  const Stream st = c.st();
+  double* d_beta = c.dscal;          // [0..m)
+  double* d_tmp = c.dscal + 512;
+  cplx* h1 = c.dcplx;
+  cplx* h2 = c.dcplx + 256;
+  // v0 = x / ||x||
+  dznrm2(st, N, x, d_tmp, c.scratch);
+  MPSGPU_CUDA(cudaMemcpyAsync(c.hscal, d_tmp, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  if (!(c.hscal[0] > 0.0) || !std::isfinite(c.hscal[0])) {
+    zfill(st, N, make_double2(1.0 / std::sqrt((double)N), 0.0), x);
+    dznrm2(st, N, x, d_tmp, c.scratch);
+  }
+  zscal_inv(st, N, x, d_tmp, V);
+  std::vector<double> a, b, s;
+  double theta = 0.0;
+  int total = 0;
+  const int max_restarts = 60;
+  TridiagLowest tri;
+  for (int restart = 0; restart < max_restarts; restart++) {
+    a.clear();
+    b.clear();
+    bool conv = false;
+    int j = 0;
+    for (j = 0; j < m; j++) {
+      cplx* vj = V + (long long)j * N;
+      apply(vj, w);
+      total++;
+      cgemv_c(st, N, j + 1, V, N, w, h1, c.scratch);
+      cgemv_n_sub(st, N, j + 1, V, N, h1, w);
+      cgemv_c(st, N, j + 1, V, N, w, h2, c.scratch);
+      cgemv_n_sub(st, N, j + 1, V, N, h2, w);
+      dznrm2(st, N, w, d_beta + j, c.scratch);
+      // fetch alpha_j = Re(h1[j] + h2[j]) and beta_j
+      MPSGPU_CUDA(cudaMemcpyAsync(c.hcplx, h1 + j, sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+      MPSGPU_CUDA(cudaMemcpyAsync(c.hcplx + 1, h2 + j, sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+      MPSGPU_CUDA(cudaMemcpyAsync(c.hscal, d_beta + j, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+      if (j + 1 < m) zscal_inv(st, N, w, d_beta + j, V + (long long)(j + 1) * N);
+      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+      const double alpha = c.hcplx[0].x + c.hcplx[1].x;
+      const double beta = c.hscal[0];
+      MPSGPU_CHECK(std::isfinite(alpha) && std::isfinite(beta), MPSGPU_NAN, "lanczos: non-finite value");
+      a.push_back(alpha);
+      b.push_back(beta);
+      double normT = 0.0;
+      tri.solve(a, b, (int)a.size(), theta, s, normT);
+      const double res = beta * std::fabs(s[j]);
+      const double scale = std::max(normT, std::fabs(theta));
+      if (res <= tol * scale || beta <= 1e-14 * scale || j + 1 == N) {
+        conv = true;
+        j++;
+        break;
+      }
+    }
+    const int k = (int)a.size();
+    MPSGPU_CUDA(cudaMemcpyAsync(c.dS, s.data(), k * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    combine_real(st, N, k, V, N, c.dS, x);
+    dznrm2(st, N, x, d_tmp, c.scratch);
+    zscal_inv(st, N, x, d_tmp, V);  // V[:,0] = normalised Ritz vector (restart vector)
+    zcopy(st, N, V, x);
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    if (conv) {
+      if (iters) *iters = total;
+      return theta;
+    }
+  }
+  if (iters) *iters = total;
+  throw Error(MPSGPU_NOT_CONVERGED, "lanczos: no convergence");
+}
+
+// ---------------------------------------------------------------------------
+// findGroundState (Contractor.cpp:1352-1533)
+// ---------------------------------------------------------------------------
+
+static void prepare_init(Context& c, MpsDev& init, int D) {
+  if (D > 0) {
+    if (D > init.bond) mps_increase_bond(c, init, D);
+    else MPSGPU_CHECK(D >= init.bond, MPSGPU_BAD_SHAPE,
+                      "D smaller than the initial bond (truncation of the initial state is not supported)");
+  }
+  mps_gauge_all(c, init, 'R', true);
+  mps_gauge_all(c, init, 'L', true);
+}
+
+double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
+                         const SolveOptions& opt, Counters& cnt) {
+  const int L = ops.L;
+  MPSGPU_CHECK(init.L == L, MPSGPU_BAD_SHAPE, "findGroundState: lengths differ");
+  for (int k = 0; k < L; k++)
+    MPSGPU_CHECK(init.dims[k][0] == ops.dims[k][2] && ops.dims[k][0] == ops.dims[k][2],
+                 MPSGPU_BAD_SHAPE, "findGroundState: physical dimensions differ");
+  prepare_init(c, init, D);
+  EnvCache E;
+  E.init(c, L);
+  double energy = contract(c, init, &ops, init).x;
+  double val = energy;
+  bool right = true, done = false;
+  int pos = 0, round = 0;
+  const double tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
+  const cplx off = make_double2(offset, 0.0);
+  try {
+    while (!done) {
+      calc_left(c, E, pos, &ops, init, init, &cnt);
+      calc_right(c, E, pos, &ops, init, init, &cnt);
+      const auto dims = init.dims[pos];
+      const int N = (int)nel(dims);
+      const cplx* Le = E.Le[pos].p;
+      const cplx* Rt = E.Re[pos].p;
+      auto ld = E.ldims[pos];
+      auto rd = E.rdims[pos];
+      auto apply = [&](const cplx* xin, cplx* yout) {
+        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, off, &cnt);
+      };
+      int its = 0;
+      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, tol, opt.max_krylov, &its);
+      cnt.site_solves++;
+      val = theta - offset;
+      if ((val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
+        if (val - energy > std::fabs(energy + offset) * opt.convtol)
+          throw Error(MPSGPU_ENERGY_INCREASE, "findGroundState: energy increasing");
+      }
+      mps_gauge_site(c, init, pos, right ? 'R' : 'L', true, &cnt);
+      for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
+      for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
+      if (right) {
+        if (pos == L - 1) {
+          right = false;
+          done = std::fabs(energy - val) < opt.convtol * std::fabs(energy + offset);
+          if (!done && std::fabs(val) < 1e-13) done = true;
+          energy = val;
+          if (opt.verbose) printf("mpsgpu: round %d energy %.15g\n", round, val);
+          if (!done) {
+            mps_gauge_site(c, init, pos, 'L', true, &cnt);
+            pos--;
+          }
+          round++;
+        } else {
+          pos++;
+        }
+      } else {
+        if (pos == 0) {
+          right = true;
+          done = std::fabs(energy - val) < opt.convtol * std::fabs(energy + offset);
+          if (!done && std::fabs(val) < 1e-13) done = true;
+          energy = val;
+          if (opt.verbose) printf("mpsgpu: round %d energy %.15g\n", round, val);
+          if (!done) {
+            mps_gauge_site(c, init, pos, 'R', true, &cnt);
+            pos++;
+          }
+          round++;
+        } else {
+          pos--;
+        }
+      }
+      if (!done && round >= opt.max_rounds)
+        throw Error(MPSGPU_NOT_CONVERGED, "findGroundState: round limit reached");
+    }
+  } catch (...) {
+    E.release(c);
+    throw;
+  }
+  E.release(c);
+  cnt.rounds += round;
+  return energy;
+}
+
+}  // namespace mpsgpu
+
+namespace mpsgpu {
+
+double find_next_excited_state(Context&, const MpoDev&, int, const std::vector<const MpsDev*>&, MpsDev&, double,
+                               const SolveOptions&, Counters&) {
+  throw Error(MPSGPU_INVALID, "findNextExcitedState: not built yet");
+}
+void optimize(Context&, const MpoDev&, const MpsDev&, MpsDev&, int, const SolveOptions&, double*, double*,
+              Counters&) {
+  throw Error(MPSGPU_INVALID, "optimize: not built yet");
+}
+void expectation_local(Context&, const MpsDev&, const double*, double*) {
+  throw Error(MPSGPU_INVALID, "expectation_local: not built yet");
+}
+void schmidt_values(Context&, const MpsDev&, int, std::vector<double>&) {
+  throw Error(MPSGPU_INVALID, "schmidt_values: not built yet");
+}
+double entropy(Context&, const MpsDev&, int) { throw Error(MPSGPU_INVALID, "entropy: not built yet"); }
+
+}  // namespace mpsgpu

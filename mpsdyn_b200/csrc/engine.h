@@ -1,0 +1,142 @@
+// Host-side engine of the mpsgpu library: device-resident MPO/MPS/environment
+// storage and the sweep algorithms of the reference's Contractor, driving the
+// CUDA kernels of kernels.h on one stream per context.
+#pragma once
+
+#include <array>
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mpsgpu {
+
+// Device buffer owned by the engine (stream-ordered allocation).
+struct DBuf {
+  cplx* p = nullptr;
+  long long cap = 0;  // complex elements
+};
+
+struct Context;
+
+void dbuf_reserve(Context& c, DBuf& b, long long n);
+void dbuf_free(Context& c, DBuf& b);
+
+struct MpoDev {
+  int L = 0;
+  std::vector<std::array<int, 4>> dims;  // (du, wl, dd, wr)
+  std::vector<DBuf> W;      // reference layout (du, wl, dd, wr)
+  std::vector<DBuf> Wlr;    // (du*wr) x (wl*dd): out (s', c), in (b, s)   [matvec, left env]
+  std::vector<DBuf> Wrl;    // (wl*du) x (dd*wr): out (b, t), in (s, c)   [right env]
+  std::vector<DBuf> Wlr_h;  // same as Wlr for the adjoint operator (du == dd only)
+  std::vector<DBuf> Wrl_h;
+};
+
+struct MpsDev {
+  int L = 0;
+  std::vector<std::array<int, 3>> dims;  // (d, Dl, Dr)
+  std::vector<DBuf> A;                   // device layout X(a, s, r): a fastest
+  double normfact = 1.0;
+  int gauge = 0;  // enum Gauge of the reference: gNone=0, gLeft=1, gRight=2, gBoth=3
+  int bond = 0;
+  int max_bond() const;
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  long long launches = 0;
+  Scratch scratch;   // short-lived (GEMM split-K partials, reductions)
+  Scratch qrws;      // QR T factors
+  std::string last_error;
+  // reusable workspaces (complex elements)
+  DBuf t1, t2, t3, t4, matA, matQ, matR;
+  DBuf lanV, lanW;     // Lanczos basis and work vector
+  double* dscal = nullptr;     // device scalars (alpha, beta, norms)
+  cplx* dcplx = nullptr;       // device complex scalars (dots)
+  double* hscal = nullptr;     // pinned host mirror
+  cplx* hcplx = nullptr;
+  double* dS = nullptr;        // Ritz coefficients on device
+  cudaEvent_t ev = nullptr;
+  cudaEvent_t mv0 = nullptr, mv1 = nullptr;
+  Stream st() { return Stream{stream, &launches}; }
+};
+
+// Environment cache (TmpManager, src/core/cpp/TmpManager.cpp:22-160):
+// L[pos] (Dbra, w, Dket) and Rt[pos] (Dket, w, Dbra) (R transposed), with
+// validity flags; L[0] = Rt[L-1] = 1.
+struct EnvCache {
+  int L = 0;
+  std::vector<DBuf> Le, Re;
+  std::vector<std::array<int, 3>> ldims, rdims;  // ldims (Db, w, Dk); rdims (Dk, w, Db)
+  std::vector<char> okL, okR;
+  void init(Context& c, int L);
+  void release(Context& c);
+  void outofdate_l(int l) { if (l > 0) okL[l] = 0; }
+  void outofdate_r(int l) { if (l < L - 1) okR[l] = 0; }
+};
+
+// Norm caches between the state and one projected level (TmpManagerExc,
+// src/core/headers/TmpManagerExc.h:29-45): nL[pos] (Dlevel, Dket), nRt[pos]
+// (Dket, Dlevel).
+struct NormCache {
+  std::vector<DBuf> nL, nR;
+  std::vector<std::array<int, 2>> ldims, rdims;
+  void init(Context& c, int L);
+  void release(Context& c);
+};
+
+struct Counters {
+  long long site_solves = 0, matvecs = 0, env_updates = 0, qr_calls = 0;
+  double flops = 0.0;
+  double mv_ms = 0.0;
+  int rounds = 0;
+};
+
+struct SolveOptions {
+  double convtol = 1e-5, eigtol = 0.0, excorthtol = 0.0;
+  int max_rounds = 1000, max_krylov = 64, verbose = 0;
+};
+
+// ---- building blocks (device layout) ----
+void mpo_upload(Context& c, MpoDev& m, int L, const int* dims, const double* const* data,
+                bool check_edges = true);
+void mpo_free(Context& c, MpoDev& m);
+void mps_upload(Context& c, MpsDev& s, int L, const int* dims, const double* const* data, double nf);
+void mps_random(Context& c, MpsDev& s, int L, int d, int D, uint64_t seed);
+void mps_product(Context& c, MpsDev& s, int L, int d, int D);
+void mps_copy(Context& c, const MpsDev& src, MpsDev& dst);
+void mps_download(Context& c, const MpsDev& s, double* const* data);
+void mps_free(Context& c, MpsDev& s);
+void mps_gauge_all(Context& c, MpsDev& s, char dir, bool normal);
+void mps_gauge_site(Context& c, MpsDev& s, int pos, char dir, bool next, Counters* cnt);
+void mps_increase_bond(Context& c, MpsDev& s, int D);
+
+// y = Heff x (+ offset x); environments in device layout.
+void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpoDev& m, int k,
+                bool adjoint, const cplx* Rt, const std::array<int, 3>& rd, const cplx* x,
+                cplx* y, cplx offset, Counters* cnt);
+// Left/right environment update (Operator::contractleftop / contractrightop).
+void env_left_update(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpsDev& ket,
+                     const MpoDev* m, int k, const MpsDev& bra, DBuf& out,
+                     std::array<int, 3>& od, Counters* cnt);
+void env_right_update(Context& c, const cplx* Rt, const std::array<int, 3>& rd, const MpsDev& ket,
+                      const MpoDev* m, int k, const MpsDev& bra, DBuf& out,
+                      std::array<int, 3>& od, Counters* cnt);
+
+// ---- algorithms (Contractor) ----
+double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
+                         const SolveOptions& opt, Counters& cnt);
+double find_next_excited_state(Context& c, const MpoDev& ops, int D,
+                               const std::vector<const MpsDev*>& levels, MpsDev& init,
+                               double offset, const SolveOptions& opt, Counters& cnt);
+void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, int D,
+              const SolveOptions& opt, double* errN, double* errT, Counters& cnt);
+cplx contract(Context& c, const MpsDev& ket, const MpoDev* ops, const MpsDev& bra);
+void expectation_local(Context& c, const MpsDev& s, const double* op, double* out);
+void schmidt_values(Context& c, const MpsDev& s, int pos, std::vector<double>& vals);
+double entropy(Context& c, const MpsDev& s, int pos);
+
+}  // namespace mpsgpu

@@ -1,0 +1,112 @@
+// Launchers of the mpsgpu CUDA kernels (host-callable, stream-ordered).
+#pragma once
+
+#include "common.cuh"
+
+namespace mpsgpu {
+
+enum { OP_N = 0, OP_C = 1, OP_T = 2 };
+
+// Stream-ordered device buffer that grows on demand (cudaMallocAsync pool).
+struct Scratch {
+  cudaStream_t stream = nullptr;
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void* get(size_t need) {
+    if (need > bytes) {
+      if (ptr) cudaFreeAsync(ptr, stream);
+      size_t nb = need + need / 4 + 4096;
+      cudaError_t e = cudaMallocAsync(&ptr, nb, stream);
+      if (e != cudaSuccess) {
+        ptr = nullptr;
+        bytes = 0;
+        throw Error(MPSGPU_OOM, "scratch allocation failed");
+      }
+      bytes = nb;
+    }
+    return ptr;
+  }
+  void release() {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = nullptr;
+    bytes = 0;
+  }
+};
+
+struct GemmArgs {
+  int M = 0, N = 0, K = 0, batch = 1;
+  const cplx* A = nullptr; long long lda = 0, strideA = 0; int opA = OP_N;
+  const cplx* B = nullptr; long long ldb = 0, strideB = 0; int opB = OP_N;
+  cplx* C = nullptr; long long ldc = 0, strideC = 0;
+  cplx alpha = {1.0, 0.0};
+  const cplx* Cin = nullptr; long long ldcin = 0, strideCin = 0;
+  cplx beta = {0.0, 0.0};
+};
+
+// C = alpha op(A) op(B) + beta Cin  (complex FP64, DMMA tensor pipe)
+void zgemm(const Stream& st, const GemmArgs& g, Scratch& scratch);
+
+// MPO-leg contraction: for every pixel (x, y) in [0,nx) x [0,ny)
+//   out[x*ox + y*oy + o0*so0 + o1*so1] =
+//       sum_{i0,i1} Wm[(o0 + n_o0*o1) + nout*(i0 + n_i0*i1)] in[x*ix + y*iy + i0*si0 + i1*si1]
+// with Wm an (n_o0*n_o1) x (n_i0*n_i1) column-major complex matrix in device memory.
+struct WContractArgs {
+  int nx = 0, ny = 0;
+  const cplx* in = nullptr; long long ix = 0, iy = 0, si0 = 0, si1 = 0; int n_i0 = 0, n_i1 = 0;
+  cplx* out = nullptr; long long ox = 0, oy = 0, so0 = 0, so1 = 0; int n_o0 = 0, n_o1 = 0;
+  const cplx* Wm = nullptr;
+};
+void wcontract(const Stream& st, const WContractArgs& a);
+
+// ---- vector kernels (Lanczos, norms) ----
+// dots[j] = sum_i conj(V[i + j*ldv]) w[i], j < k   (two-stage, deterministic)
+void cgemv_c(const Stream& st, int n, int k, const cplx* V, long long ldv, const cplx* w,
+             cplx* dots, Scratch& scratch);
+// w -= V h  (h on device, length k)
+void cgemv_n_sub(const Stream& st, int n, int k, const cplx* V, long long ldv, const cplx* h,
+                 cplx* w);
+// out[0] = ||x||_2 (deterministic two-stage reduction)
+void dznrm2(const Stream& st, int n, const cplx* x, double* out, Scratch& scratch);
+// y = x / (*nrm)   (device scalar)
+void zscal_inv(const Stream& st, int n, const cplx* x, const double* nrm, cplx* y);
+// y = a x + b y (host scalars)
+void zaxpby(const Stream& st, int n, cplx a, const cplx* x, cplx b, cplx* y);
+// y = sum_j s[j] V[:, j]  (s real, device)
+void combine_real(const Stream& st, int n, int k, const cplx* V, long long ldv, const double* s,
+                  cplx* y);
+// dst = src (n complex)
+void zcopy(const Stream& st, int n, const cplx* src, cplx* dst);
+void zfill(const Stream& st, long long n, cplx v, cplx* dst);
+
+// ---- layout conversions between the reference and the device layout ----
+// site: ref A(s, a, r) -> dev X(a, s, r) and back
+void site_ref_to_dev(const Stream& st, int d, int Dl, int Dr, const cplx* ref, cplx* dev);
+void site_dev_to_ref(const Stream& st, int d, int Dl, int Dr, const cplx* dev, cplx* ref);
+// 3-index transpose T(p, q, r) -> U(r, q, p) (used for R environments)
+void transpose_pqr_to_rqp(const Stream& st, int p, int q, int r, const cplx* in, cplx* out);
+
+// Seeded complex Gaussian fill (SplitMix64 counter stream + Box-Muller),
+// entry i uses draws 2(offset+i), 2(offset+i)+1; written in the reference
+// site order (s fastest) into the device layout (a fastest).
+void gaussian_site(const Stream& st, uint64_t seed, long long offset, int d, int Dl, int Dr,
+                   cplx* dev);
+
+// ---- Householder QR (LAPACK zgeqrf/zungqr conventions) ----
+// Factor the m x n column-major matrix A (ld = m; overwritten by R above and
+// the reflectors below the diagonal).  Q (m x K, ld = ldq) and R (K x n,
+// ld = ldr, zero below the diagonal) are written when non-null; K = min(m, n).
+void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, long long ldq,
+                            cplx* R, long long ldr, Scratch& scratch);
+
+// Two-level strided view: element (i, j) lives at
+//   (i % rd)*r0 + (i / rd)*r1 + (j % cd)*c0 + (j / cd)*c1, optionally conjugated.
+struct View2 {
+  long long rd = 1, r0 = 1, r1 = 0, cd = 1, c0 = 0, c1 = 0;
+  bool conj = false;
+};
+// dst (m x n, col-major, ld m) = view(src)
+void gather2(const Stream& st, int m, int n, const cplx* src, const View2& v, cplx* dst);
+// view(dst) = src (m x n, col-major, ld m)
+void scatter2(const Stream& st, int m, int n, const cplx* src, cplx* dst, const View2& v);
+
+}  // namespace mpsgpu

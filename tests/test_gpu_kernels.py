@@ -1,0 +1,93 @@
+"""GPU parity of the CUDA kernels against the oracle, through the C ABI.
+
+Tolerances: complex FP64 throughout, so products agree with the oracle to a
+few ulps of the largest term (relative error <= 1e-13 of max |y|).
+"""
+import numpy as np
+import pytest
+
+from oracle import mps_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+
+def rand_c(rng, shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_matvec_and_env_vs_reference_fixture(ctx, kernels_npz, tag):
+    g = lambda n: kernels_npz[f"{tag}_{n}"]
+    L, W, R, x = g("L"), g("W"), g("R"), g("x")
+    assert rel(ctx.heff_matvec(L, W, R, x, 0.75), g("y_off075")) < 1e-13
+    assert rel(ctx.heff_matvec(L, W, R, x, hermitian=True), g("yherm")) < 1e-13
+    assert rel(ctx.env_left(g("TL"), g("ket"), W, g("bra")), g("envL")) < 1e-13
+    assert rel(ctx.env_right(g("TR"), g("ket"), W, g("bra")), g("envR")) < 1e-13
+
+
+@pytest.mark.parametrize("D,w,d", [(8, 3, 2), (20, 3, 2), (64, 5, 2), (128, 5, 2), (33, 4, 3)])
+def test_matvec_random_shapes(ctx, D, w, d):
+    rng = np.random.default_rng(D * 10 + w)
+    Dl, Dr = D, D + 3
+    L = rand_c(rng, (Dl, w, Dl))
+    W = rand_c(rng, (d, w, d, w))
+    R = rand_c(rng, (Dr, w, Dr))
+    x = rand_c(rng, (d * Dl * Dr,))
+    y = ctx.heff_matvec(L, W, R, x, 0.3)
+    assert rel(y, mo.heff_matvec(L, W, R, x, 0.3)) < 1e-13
+    T = rand_c(rng, (Dl, w, Dl))
+    ket = rand_c(rng, (d, Dl, Dr))
+    bra = rand_c(rng, (d, Dl, Dr))
+    assert rel(ctx.env_left(T, ket, W, bra), mo.env_left(T, ket, W, bra)) < 1e-13
+    T2 = rand_c(rng, (Dr, w, Dr))
+    assert rel(ctx.env_right(T2, ket, W, bra), mo.env_right(T2, ket, W, bra)) < 1e-13
+
+
+def test_matvec_rectangular_environments(ctx):
+    rng = np.random.default_rng(5)
+    L = rand_c(rng, (7, 3, 5))
+    W = rand_c(rng, (2, 3, 2, 3))
+    R = rand_c(rng, (6, 3, 9))
+    x = rand_c(rng, (2 * 5 * 9,))
+    assert rel(ctx.heff_matvec(L, W, R, x), mo.heff_matvec(L, W, R, x)) < 1e-13
+
+
+@pytest.mark.parametrize("m,n", [(2, 1), (4, 2), (40, 20), (256, 128), (200, 256), (512, 256), (17, 17), (3, 9)])
+def test_qr_matches_lapack(ctx, m, n):
+    rng = np.random.default_rng(m + 7 * n)
+    A = rand_c(rng, (m, n))
+    Q, R = ctx.qr(A)
+    Qn, Rn = np.linalg.qr(A, mode="reduced")  # LAPACK zgeqrf/zungqr
+    K = min(m, n)
+    assert Q.shape == (m, K) and R.shape == (K, n)
+    scale = np.abs(A).max()
+    assert np.abs(Q @ R - A).max() < 1e-13 * scale * max(m, n) ** 0.5
+    assert np.abs(Q.conj().T @ Q - np.eye(K)).max() < 1e-13 * max(m, n) ** 0.5
+    assert np.abs(np.tril(R, -1)).max() == 0
+    # same Householder conventions as LAPACK: same factors, not only the same product
+    assert rel(R, Rn) < 1e-11
+    assert rel(Q, Qn) < 1e-11
+
+
+def test_qr_zero_padded_matches_lapack(ctx):
+    # rank-deficient, zero-padded site as MPS(L, D, d) produces them
+    A = np.zeros((8, 6), dtype=complex)
+    A[0, 0] = 1.0
+    A[3, 1] = 0.5 - 0.25j
+    Q, R = ctx.qr(A)
+    Qn, Rn = np.linalg.qr(A, mode="reduced")
+    assert rel(Q, Qn) < 1e-14 and rel(R, Rn) < 1e-14
+
+
+@pytest.mark.parametrize("m,n", [(6, 20), (20, 6), (128, 256)])
+def test_lq_matches_lapack(ctx, m, n):
+    rng = np.random.default_rng(m * n)
+    A = rand_c(rng, (m, n))
+    Lm, Q = ctx.lq(A)
+    Lr, Qr = mo.lq_reduced(A)
+    assert np.abs(Lm @ Q - A).max() < 1e-13 * np.abs(A).max() * max(m, n) ** 0.5
+    assert rel(Lm, Lr) < 1e-11 and rel(Q, Qr) < 1e-11
