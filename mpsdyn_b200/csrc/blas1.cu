@@ -99,7 +99,7 @@ __global__ void reduce_partials(int k, int nblk, const cplx* __restrict__ partia
 }
 
 __global__ void cgemv_n_sub_kernel(int n, int k, const cplx* __restrict__ V, long long ldv,
-                                   const cplx* __restrict__ h, cplx* __restrict__ w) {
+                                   const cplx* __restrict__ h, cplx* __restrict__ w, double sign) {
   __shared__ cplx hs[256];
   for (int t = threadIdx.x; t < k; t += blockDim.x) hs[t] = h[t];
   __syncthreads();
@@ -107,7 +107,7 @@ __global__ void cgemv_n_sub_kernel(int n, int k, const cplx* __restrict__ V, lon
        i += (long long)gridDim.x * blockDim.x) {
     cplx s = make_double2(0.0, 0.0);
     for (int j = 0; j < k; j++) s = cadd(s, cmul(V[i + j * ldv], hs[j]));
-    w[i] = csub(w[i], s);
+    w[i] = cadd(w[i], cscale(s, sign));
   }
 }
 
@@ -203,7 +203,7 @@ __global__ void site_dev_to_ref_kernel(int d, int Dl, int Dr, const cplx* __rest
 }
 
 __global__ void transpose_pqr_kernel(int P, int Q, int R, const cplx* __restrict__ in,
-                                     cplx* __restrict__ out) {
+                                     cplx* __restrict__ out, bool conj) {
   const long long n = (long long)P * Q * R;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
@@ -212,7 +212,9 @@ __global__ void transpose_pqr_kernel(int P, int Q, int R, const cplx* __restrict
     long long rest = t / R;
     int q = (int)(rest % Q);
     long long p = rest / Q;
-    out[t] = in[p + (long long)P * q + (long long)P * Q * r];
+    cplx v = in[p + (long long)P * q + (long long)P * Q * r];
+    if (conj) v.y = -v.y;
+    out[t] = v;
   }
 }
 
@@ -301,10 +303,11 @@ void cgemv_c(const Stream& st, int n, int k, const cplx* V, long long ldv, const
   after_launch(st);
 }
 
-void cgemv_n_sub(const Stream& st, int n, int k, const cplx* V, long long ldv, const cplx* h, cplx* w) {
+void cgemv_n_sub(const Stream& st, int n, int k, const cplx* V, long long ldv, const cplx* h, cplx* w,
+                 double sign) {
   MPSGPU_CHECK(k <= 256, MPSGPU_BAD_SHAPE, "cgemv_n_sub: k > 256");
   if (k <= 0) return;
-  cgemv_n_sub_kernel<<<grid_for(n), TPB, 0, st.s>>>(n, k, V, ldv, h, w);
+  cgemv_n_sub_kernel<<<grid_for(n), TPB, 0, st.s>>>(n, k, V, ldv, h, w, sign);
   after_launch(st);
 }
 
@@ -355,8 +358,8 @@ void site_dev_to_ref(const Stream& st, int d, int Dl, int Dr, const cplx* dev, c
   after_launch(st);
 }
 
-void transpose_pqr_to_rqp(const Stream& st, int p, int q, int r, const cplx* in, cplx* out) {
-  transpose_pqr_kernel<<<grid_for((long long)p * q * r), TPB, 0, st.s>>>(p, q, r, in, out);
+void transpose_pqr_to_rqp(const Stream& st, int p, int q, int r, const cplx* in, cplx* out, bool conj) {
+  transpose_pqr_kernel<<<grid_for((long long)p * q * r), TPB, 0, st.s>>>(p, q, r, in, out, conj);
   after_launch(st);
 }
 

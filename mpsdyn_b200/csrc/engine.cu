@@ -823,17 +823,364 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
 
 namespace mpsgpu {
 
-double find_next_excited_state(Context&, const MpoDev&, int, const std::vector<const MpsDev*>&, MpsDev&, double,
-                               const SolveOptions&, Counters&) {
-  throw Error(MPSGPU_INVALID, "findNextExcitedState: not built yet");
+// ---------------------------------------------------------------------------
+// Excited states: findNextExcitedState (Contractor.cpp:2676-2727) and
+// findGroundStateWithProjectorPenalty (:2739-2956) with the Hermitian,
+// projected multiplier TensorMultiplierProjMulti(hermitian=true)
+// (TensorMultiplierProjMulti.cpp:81-90):
+//   y = 1/2 (H x + H^dag x) + sum_k pen_k u_k (u_k^H x) + offset x,
+// u_k = the level-k state contracted with the norm environments
+// (Contractor::contractMbraId, Contractor.cpp:880-903).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int MAX_ROUND_EXCTD = 1000;  // Contractor.cpp:26
+
+struct LevelCache {
+  EnvCache n;  // w = 1 environments between init (ket) and the level (bra)
+};
+
+}  // namespace
+
+static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, const std::vector<double>& pens,
+                                        const std::vector<const MpsDev*>& levels, MpsDev& init, double offset,
+                                        const SolveOptions& opt, Counters& cnt) {
+  const int L = ops.L;
+  const int nk = (int)levels.size();
+  prepare_init(c, init, D);
+  double energy = contract(c, init, &ops, init).x + offset;
+  for (int k = 0; k < nk; k++) {
+    cplx ov = contract(c, init, nullptr, *levels[k]);
+    energy += pens[k] * cabs2(ov);
+  }
+  energy -= offset;
+  EnvCache E;
+  E.init(c, L);
+  std::vector<EnvCache> NC(nk);
+  for (auto& n : NC) n.init(c, L);
+  DBuf Lh, Rth, U, y2, sq;
+  double val = energy;
+  bool right = true, done = false;
+  int pos = 0, round = 0;
+  const double tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
+  auto cleanup = [&]() {
+    E.release(c);
+    for (auto& n : NC) n.release(c);
+    for (DBuf* b : {&Lh, &Rth, &U, &y2, &sq}) dbuf_free(c, *b);
+  };
+  try {
+    while (!done) {
+      // calculateLexck / calculateRexck (Contractor.cpp:2958-2988): one set of flags
+      {
+        std::vector<int> needL, needR;
+        int p = pos;
+        while (!E.okL[p]) needL.push_back(p--);
+        for (int q = (int)needL.size() - 1; q >= 0; q--) {
+          const int pp = needL[q];
+          env_left_update(c, E.Le[pp - 1].p, E.ldims[pp - 1], init, &ops, pp - 1, init, E.Le[pp], E.ldims[pp], &cnt);
+          for (int k = 0; k < nk; k++)
+            env_left_update(c, NC[k].Le[pp - 1].p, NC[k].ldims[pp - 1], init, nullptr, pp - 1, *levels[k],
+                            NC[k].Le[pp], NC[k].ldims[pp], &cnt);
+          E.okL[pp] = 1;
+        }
+        p = pos;
+        while (!E.okR[p]) needR.push_back(p++);
+        for (int q = (int)needR.size() - 1; q >= 0; q--) {
+          const int pp = needR[q];
+          env_right_update(c, E.Re[pp + 1].p, E.rdims[pp + 1], init, &ops, pp + 1, init, E.Re[pp], E.rdims[pp], &cnt);
+          for (int k = 0; k < nk; k++)
+            env_right_update(c, NC[k].Re[pp + 1].p, NC[k].rdims[pp + 1], init, nullptr, pp + 1, *levels[k],
+                             NC[k].Re[pp], NC[k].rdims[pp], &cnt);
+          E.okR[pp] = 1;
+        }
+      }
+      const auto dims = init.dims[pos];
+      const int N = (int)nel(dims);
+      const int Dlk = dims[1], d = dims[0], Drk = dims[2];
+      const auto ld = E.ldims[pos];
+      const auto rd = E.rdims[pos];
+      // adjoint environments: L^dag(bra,w,ket) = conj(L(ket,w,bra)), Rt^dag likewise
+      dbuf_reserve(c, Lh, nel(ld));
+      dbuf_reserve(c, Rth, nel(rd));
+      transpose_pqr_to_rqp(c.st(), ld[0], ld[1], ld[2], E.Le[pos].p, Lh.p, true);
+      transpose_pqr_to_rqp(c.st(), rd[0], rd[1], rd[2], E.Re[pos].p, Rth.p, true);
+      // projector vectors u_k (sqrt(pen_k) folded in), columns of U (N x nk)
+      dbuf_reserve(c, U, (long long)N * nk);
+      for (int k = 0; k < nk; k++) {
+        const MpsDev& lv = *levels[k];
+        const auto bd = lv.dims[pos];
+        const auto nl = NC[k].ldims[pos];  // (Dlb, 1, Dlk)
+        const auto nr = NC[k].rdims[pos];  // (Drk, 1, Drb)
+        dbuf_reserve(c, c.t3, (long long)Dlk * d * bd[2]);
+        GemmArgs g1;
+        g1.M = Dlk; g1.N = d * bd[2]; g1.K = nl[0];
+        g1.A = NC[k].Le[pos].p; g1.lda = nl[0]; g1.opA = OP_C;
+        g1.B = lv.A[pos].p; g1.ldb = bd[1];
+        g1.C = c.t3.p; g1.ldc = Dlk;
+        zgemm(c.st(), g1, c.scratch);
+        GemmArgs g2;
+        g2.M = Dlk * d; g2.N = Drk; g2.K = bd[2];
+        g2.A = c.t3.p; g2.lda = (long long)Dlk * d;
+        g2.B = NC[k].Re[pos].p; g2.ldb = nr[0]; g2.opB = OP_C;
+        g2.C = U.p + (long long)k * N; g2.ldc = (long long)Dlk * d;
+        g2.alpha = make_double2(std::sqrt(pens[k]), 0.0);
+        zgemm(c.st(), g2, c.scratch);
+      }
+      dbuf_reserve(c, y2, N);
+      cplx* dots = c.dcplx + 512;
+      const cplx* Le = E.Le[pos].p;
+      const cplx* Rt = E.Re[pos].p;
+      auto apply = [&](const cplx* xin, cplx* yout) {
+        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(0.0, 0.0), &cnt);
+        heff_apply(c, Lh.p, ld, ops, pos, true, Rth.p, rd, xin, y2.p, make_double2(0.0, 0.0), &cnt);
+        cnt.matvecs--;  // the pair counts as one product of the Hermitian multiplier
+        zaxpby(c.st(), N, make_double2(0.5, 0.0), y2.p, make_double2(0.5, 0.0), yout);
+        if (offset != 0.0) zaxpby(c.st(), N, make_double2(offset, 0.0), xin, make_double2(1.0, 0.0), yout);
+        cgemv_c(c.st(), N, nk, U.p, N, xin, dots, c.scratch);
+        cgemv_n_sub(c.st(), N, nk, U.p, N, dots, yout, 1.0);
+      };
+      int its = 0;
+      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, tol, opt.max_krylov, &its);
+      cnt.site_solves++;
+      val = theta - offset;
+      if ((val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
+        if (val - energy > std::fabs(energy + offset) * 1e-6)
+          throw Error(MPSGPU_ENERGY_INCREASE, "findNextExcitedState: energy increasing");
+      }
+      mps_gauge_site(c, init, pos, right ? 'R' : 'L', true, &cnt);
+      for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
+      for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
+      const bool at_end = (right && pos == L - 1) || (!right && pos == 0);
+      if (at_end) {
+        done = std::fabs(energy - val) < opt.convtol * std::fabs(energy + offset);
+        if (!done && (std::fabs(energy - val) < 1e-12 || round > MAX_ROUND_EXCTD)) done = true;
+        energy = val;
+        if (opt.verbose) printf("mpsgpu: excited round %d energy %.15g\n", round, val);
+        if (!done) {
+          if (right) { mps_gauge_site(c, init, pos, 'L', true, &cnt); pos--; }
+          else { mps_gauge_site(c, init, pos, 'R', true, &cnt); pos++; }
+        }
+        right = !right;
+        round++;
+        if (!done && round >= opt.max_rounds)
+          throw Error(MPSGPU_NOT_CONVERGED, "findNextExcitedState: round limit reached");
+      } else {
+        pos += right ? 1 : -1;
+      }
+    }
+  } catch (...) {
+    cleanup();
+    throw;
+  }
+  cleanup();
+  cnt.rounds += round;
+  return energy;
 }
-void optimize(Context&, const MpoDev&, const MpsDev&, MpsDev&, int, const SolveOptions&, double*, double*,
-              Counters&) {
-  throw Error(MPSGPU_INVALID, "optimize: not built yet");
+
+double find_next_excited_state(Context& c, const MpoDev& ops, int D, const std::vector<const MpsDev*>& levels,
+                               MpsDev& init, double offset, const SolveOptions& opt, Counters& cnt) {
+  const int nk = (int)levels.size();
+  MPSGPU_CHECK(nk >= 1, MPSGPU_INVALID, "findNextExcitedState: no levels");
+  for (auto* lv : levels) MPSGPU_CHECK(lv->L == ops.L, MPSGPU_BAD_SHAPE, "findNextExcitedState: level length");
+  MPSGPU_CHECK(init.L == ops.L, MPSGPU_BAD_SHAPE, "findNextExcitedState: init length");
+  double minE = 0, maxE = 0;
+  for (int k = 0; k < nk; k++) {
+    double e = contract(c, *levels[k], &ops, *levels[k]).x + offset;
+    if (k == 0 || e < minE) minE = e;
+    if (k == 0 || e > maxE) maxE = e;
+  }
+  double newOffset = std::max(20 * (maxE - minE), std::fabs(offset));
+  if (nk == 1 || newOffset < 1e-6) newOffset = levels[0]->L * 0.5;
+  std::vector<double> pens(nk, newOffset);
+  for (;;) {
+    double e = gs_with_projector_penalty(c, ops, D, pens, levels, init, offset, opt, cnt);
+    if (opt.excorthtol <= 0) return e;
+    bool again = false;
+    for (int k = 0; k < nk; k++) {
+      cplx ov = contract(c, init, nullptr, *levels[k]);
+      if (std::sqrt(cabs2(ov)) > opt.excorthtol) {
+        pens[k] *= 2;
+        again = true;
+      }
+    }
+    if (!again) return e;
+  }
 }
-void expectation_local(Context&, const MpsDev&, const double*, double*) {
-  throw Error(MPSGPU_INVALID, "expectation_local: not built yet");
+
+// ---------------------------------------------------------------------------
+// optimize (Contractor.cpp:77-278): variational |init> ~ ops |orig> at fixed
+// bond dimension, the time-evolution step of the reference.
+// ---------------------------------------------------------------------------
+
+// Contractor::checkDistanceConvergence (Contractor.cpp:940-999)
+static bool check_distance(double& distance, cplx c1, cplx c2, double normA, double normB, double convtol) {
+  const double newd = normA * (normA * c1.x - 2 * c2.x) + normB * normB;
+  MPSGPU_CHECK(std::isfinite(newd), MPSGPU_NAN, "optimize: NaN distance");
+  bool done = false;
+  if ((newd - distance) > convtol * std::fabs(distance)) {
+    if (std::fabs(newd) > convtol && std::fabs(newd - distance) > 1e-12)
+      throw Error(MPSGPU_ENERGY_INCREASE, "optimize: distance increasing");
+    done = true;
+  }
+  if (std::fabs((distance - newd) / distance) < convtol) done = true;
+  else done = false;
+  if ((std::fabs(distance) + std::fabs(newd)) * convtol < 1e-14)
+    if (std::fabs(distance - newd) < convtol) done = true;
+  distance = newd;
+  return done;
 }
+
+void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, int D, const SolveOptions& opt,
+              double* errN, double* errT, Counters& cnt) {
+  const int L = orig.L;
+  MPSGPU_CHECK(ops.L == L && init.L == L, MPSGPU_BAD_SHAPE, "optimize: lengths");
+  // errN = <orig|ops^dag ops|orig> + <init|init> - 2 Re <init|ops|orig>
+  // (Contractor.cpp:263-276) needs the doubled operator of
+  // Contractor::contract2, which this library does not provide yet.
+  MPSGPU_CHECK(errN == nullptr, MPSGPU_INVALID, "optimize: errN is not provided (pass null)");
+  prepare_init(c, init, D);
+  EnvCache E;
+  E.init(c, L);
+  double distance = std::sqrt(cabs2(contract(c, orig, nullptr, orig))) + std::sqrt(cabs2(contract(c, init, nullptr, init)));
+  bool right = true, done = false;
+  int pos = 0, round = 1;
+  cplx c1 = make_double2(0, 0), c2 = make_double2(0, 0);
+  DBuf M;
+  double* dn = c.dscal + 600;
+  try {
+    while (!done) {
+      calc_left(c, E, pos, &ops, orig, init, &cnt);
+      calc_right(c, E, pos, &ops, orig, init, &cnt);
+      // M = L W R applied to the orig site (Operator::contractMket, Operator.cpp:427-478)
+      const auto od = orig.dims[pos];
+      const auto ld = E.ldims[pos];
+      const auto rd = E.rdims[pos];
+      const int du = ops.dims[pos][0];
+      const long long nM = (long long)ld[0] * du * rd[2];
+      dbuf_reserve(c, M, nM);
+      MPSGPU_CHECK(ld[2] == od[1] && rd[0] == od[2], MPSGPU_BAD_SHAPE, "optimize: dims");
+      heff_apply(c, E.Le[pos].p, ld, ops, pos, false, E.Re[pos].p, rd, orig.A[pos].p, M.p, make_double2(0, 0), &cnt);
+      // solveSiteGauge (Contractor.cpp:921-936): newA = M / |M|
+      dznrm2(c.st(), (int)nM, M.p, dn, c.scratch);
+      init.dims[pos] = {du, ld[0], rd[2]};
+      dbuf_reserve(c, init.A[pos], nM);
+      zscal_inv(c.st(), (int)nM, M.p, dn, init.A[pos].p);
+      mps_gauge_site(c, init, pos, right ? 'R' : 'L', false, &cnt);
+      // contr1 = <A|A>, contr2 = <A|M> with the gauged tensor (Contractor.cpp:183-186)
+      const auto nd = init.dims[pos];
+      const long long nA = nel(nd);
+      if (nA == nM) {
+        cgemv_c(c.st(), (int)nA, 1, init.A[pos].p, nA, init.A[pos].p, c.dcplx + 700, c.scratch);
+        cgemv_c(c.st(), (int)nA, 1, init.A[pos].p, nA, M.p, c.dcplx + 701, c.scratch);
+      } else {
+        // the gauge move changed the shape (bond clipped to min(m, n)): only the
+        // chain ends enter the convergence check, where shapes never change
+        zfill(c.st(), 2, make_double2(0, 0), c.dcplx + 700);
+      }
+      for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
+      for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
+      const bool at_end = (right && pos == L - 1) || (!right && pos == 0);
+      if (at_end) {
+        MPSGPU_CUDA(cudaMemcpyAsync(c.hcplx, c.dcplx + 700, 2 * sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+        MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+        c1 = c.hcplx[0];
+        c2 = c.hcplx[1];
+        done = check_distance(distance, c1, c2, init.normfact, orig.normfact, opt.convtol);
+        if (!done) {
+          if (right) { mps_gauge_site(c, init, pos, 'L', false, &cnt); if (pos > 0) pos--; }
+          else { mps_gauge_site(c, init, pos, 'R', false, &cnt); if (pos < L - 1) pos++; }
+        }
+        right = !right;
+        round++;
+        if (!done && round >= opt.max_rounds) throw Error(MPSGPU_NOT_CONVERGED, "optimize: round limit reached");
+      } else {
+        pos += right ? 1 : -1;
+      }
+    }
+  } catch (...) {
+    E.release(c);
+    dbuf_free(c, M);
+    throw;
+  }
+  E.release(c);
+  dbuf_free(c, M);
+  init.normfact = c2.x / c1.x;
+  init.normfact *= orig.normfact;
+  cnt.rounds += round;
+  (void)errT;
+}
+
+// ---------------------------------------------------------------------------
+// Local observables: <op_k> / <psi|psi> for every site (flatIsing.cpp:258-282)
+// with one left and one right pass of w=1 environments.
+// ---------------------------------------------------------------------------
+
+void expectation_local(Context& c, const MpsDev& s, const double* op, double* out) {
+  const int L = s.L;
+  const int d = s.dims[0][0];
+  for (int k = 0; k < L; k++) MPSGPU_CHECK(s.dims[k][0] == d, MPSGPU_BAD_SHAPE, "expectation: mixed d");
+  MpoDev one;
+  int dims4[4] = {d, 1, d, 1};
+  const double* wp[1] = {op};
+  mpo_upload(c, one, 1, dims4, wp, false);
+  EnvCache E;
+  E.init(c, L);
+  std::vector<cplx> vals(L);
+  DBuf T;
+  try {
+    for (int p = 1; p < L; p++) {
+      env_left_update(c, E.Le[p - 1].p, E.ldims[p - 1], s, nullptr, p - 1, s, E.Le[p], E.ldims[p], nullptr);
+      E.okL[p] = 1;
+    }
+    for (int p = L - 2; p >= 0; p--) {
+      env_right_update(c, E.Re[p + 1].p, E.rdims[p + 1], s, nullptr, p + 1, s, E.Re[p], E.rdims[p], nullptr);
+      E.okR[p] = 1;
+    }
+    // norm = L[L-1] contracted with the last site
+    std::array<int, 3> td;
+    MpsDev view;  // site views sharing the buffers of s
+    view.L = L;
+    view.dims = s.dims;
+    view.A = s.A;
+    for (int k = 0; k < L; k++) {
+      // operator on site k: MPO index k of a one-site MPO -> use a temporary MpoDev view
+      MpoDev opk;
+      opk.L = L;
+      opk.dims.assign(L, {d, 1, d, 1});
+      opk.W.assign(L, one.W[0]);
+      opk.Wlr.assign(L, one.Wlr[0]);
+      opk.Wrl.assign(L, one.Wrl[0]);
+      env_left_update(c, E.Le[k].p, E.ldims[k], view, &opk, k, view, T, td, nullptr);
+      // <op_k> = sum T[rb, 0, rk] Rt[rk, 0, rb]
+      const int Db = td[0], Dk = td[2];
+      dbuf_reserve(c, c.t4, (long long)Db * Dk);
+      transpose_pqr_to_rqp(c.st(), E.rdims[k][0], 1, E.rdims[k][2], E.Re[k].p, c.t4.p, true);
+      // sum_i T_i * R^T_i = conj( sum conj(T_i) ... ) : use cgemv_c with conj(Rt^T) as the "V" column
+      cgemv_c(c.st(), Db * Dk, 1, c.t4.p, (long long)Db * Dk, T.p, c.dcplx + 800 + k % 100, c.scratch);
+      MPSGPU_CUDA(cudaMemcpyAsync(&vals[k], c.dcplx + 800 + k % 100, sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    // norm: contract the last left environment with the last site
+    DBuf nb;
+    std::array<int, 3> nd;
+    env_left_update(c, E.Le[L - 1].p, E.ldims[L - 1], s, nullptr, L - 1, s, nb, nd, nullptr);
+    cplx nrm;
+    MPSGPU_CUDA(cudaMemcpyAsync(&nrm, nb.p, sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    dbuf_free(c, nb);
+    for (int k = 0; k < L; k++) out[k] = vals[k].x / nrm.x;
+  } catch (...) {
+    E.release(c);
+    dbuf_free(c, T);
+    mpo_free(c, one);
+    throw;
+  }
+  E.release(c);
+  dbuf_free(c, T);
+  mpo_free(c, one);
+}
+
 void schmidt_values(Context&, const MpsDev&, int, std::vector<double>&) {
   throw Error(MPSGPU_INVALID, "schmidt_values: not built yet");
 }

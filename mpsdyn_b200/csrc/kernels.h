@@ -62,9 +62,9 @@ void wcontract(const Stream& st, const WContractArgs& a);
 // dots[j] = sum_i conj(V[i + j*ldv]) w[i], j < k   (two-stage, deterministic)
 void cgemv_c(const Stream& st, int n, int k, const cplx* V, long long ldv, const cplx* w,
              cplx* dots, Scratch& scratch);
-// w -= V h  (h on device, length k)
+// w += sign * V h  (h on device, length k; sign = -1 subtracts)
 void cgemv_n_sub(const Stream& st, int n, int k, const cplx* V, long long ldv, const cplx* h,
-                 cplx* w);
+                 cplx* w, double sign = -1.0);
 // out[0] = ||x||_2 (deterministic two-stage reduction)
 void dznrm2(const Stream& st, int n, const cplx* x, double* out, Scratch& scratch);
 // y = x / (*nrm)   (device scalar)
@@ -83,7 +83,8 @@ void zfill(const Stream& st, long long n, cplx v, cplx* dst);
 void site_ref_to_dev(const Stream& st, int d, int Dl, int Dr, const cplx* ref, cplx* dev);
 void site_dev_to_ref(const Stream& st, int d, int Dl, int Dr, const cplx* dev, cplx* ref);
 // 3-index transpose T(p, q, r) -> U(r, q, p) (used for R environments)
-void transpose_pqr_to_rqp(const Stream& st, int p, int q, int r, const cplx* in, cplx* out);
+void transpose_pqr_to_rqp(const Stream& st, int p, int q, int r, const cplx* in, cplx* out,
+                          bool conj = false);
 
 // Seeded complex Gaussian fill (SplitMix64 counter stream + Box-Muller),
 // entry i uses draws 2(offset+i), 2(offset+i)+1; written in the reference

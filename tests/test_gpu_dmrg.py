@@ -89,3 +89,58 @@ def test_errors_are_status_codes(ctx):
     with pytest.raises(capi.MpsgpuError) as ei:
         ctx.find_ground_state(ops, 4, s)
     assert ei.value.status == 1
+
+
+def test_excited_state_matches_reference(ctx, golden):
+    ops = ctx.mpo(mo.ising_hmpo(10, 1, 1, 0))
+    g = ctx.mps(mo.random_mps(10, 2, 16, 1).sites)
+    x = ctx.mps(mo.random_mps(10, 2, 16, 11).sites)
+    o = ctx.options(convtol=1e-10)
+    e0, _ = ctx.find_ground_state(ops, 16, g, 0.0, o)
+    e1, st = ctx.find_next_excited_state(ops, 16, [g], x, 0.0, o)
+    r0, r1 = golden["ising_L10_D16_exc_E0"], golden["ising_L10_D16_exc_E1"]
+    assert abs(e0 - r0) <= 1e-10 * abs(r0)
+    assert abs(e1 - r1) <= 1e-10 * abs(r1), (e1, r1)
+    # orthogonal to the ground state
+    assert abs(ctx.contract(x, None, g)) < 1e-6
+
+
+def test_imaginary_time_matches_reference(ctx, golden):
+    L, D = 10, 6
+    H = ctx.mpo(mo.ising_hmpo(L, 1, 1, 0))
+    U = ctx.mpo(mo.ising_umpo(L, 1, 1, 0, 0.05, True))
+    st = ctx.mps_product(L, 2, D)
+    o = ctx.options(convtol=1e-10)
+    es = []
+    for _ in range(20):
+        aux = st.copy()
+        ctx.optimize(U, aux, st, D, o)
+        aux.free()
+        st.gauge("R")
+        es.append(ctx.contract(st, H, st).real)
+    np.testing.assert_allclose(es, golden["ising_L10_D6_imag_dt005_energies"], rtol=1e-10, atol=0)
+
+
+def test_real_time_quench_observables(ctx, golden):
+    L, D = 8, 8
+    H = ctx.mpo(mo.ising_hmpo(L, 1, 1.2, 0.1))
+    U = ctx.mpo(mo.ising_umpo(L, 1, 1.2, 0.1, 0.05, False))
+    st = ctx.mps(mo.product_mps(L, 2, 1).sites)
+    o = ctx.options(convtol=1e-10)
+    sx, en = [], []
+    for _ in range(10):
+        aux = st.copy()
+        ctx.optimize(U, aux, st, D, o)
+        aux.free()
+        sx.append(ctx.expectation_local(st, mo.SIGX)[L // 2])
+        st.gauge("L")
+        en.append(ctx.contract(st, H, st).real)
+    np.testing.assert_allclose(sx, golden["ising_L8_D8_quench_sx_center"], rtol=0, atol=1e-8)
+    np.testing.assert_allclose(en, golden["ising_L8_D8_quench_energies"], rtol=1e-10, atol=0)
+
+
+def test_expectation_values_vs_oracle(ctx):
+    m = mo.random_mps(9, 2, 6, 21)
+    s = ctx.mps(m.sites)
+    for op in (mo.SIGX, mo.SIGZ, mo.SIGY):
+        np.testing.assert_allclose(ctx.expectation_local(s, op), mo.expectation_values(m, op), rtol=0, atol=1e-12)
