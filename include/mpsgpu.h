@@ -81,6 +81,15 @@ const char* mpsgpu_last_error(mpsgpu_context* ctx);
 /* Counts this library's kernel launches on the context (for reporting). */
 long long mpsgpu_launch_count(mpsgpu_context* ctx);
 mpsgpu_status mpsgpu_synchronize(mpsgpu_context* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time the
+ * library's work with their own events on that stream. */
+mpsgpu_status mpsgpu_get_stream(mpsgpu_context* ctx, void** stream);
+/* Device-time accounting of the tensor-pipe GEMMs: between begin and end,
+ * CUDA events bracket every GEMM launch on the context's stream; end
+ * returns their summed device time (ms), algorithmic flops and count. */
+mpsgpu_status mpsgpu_profile_begin(mpsgpu_context* ctx);
+mpsgpu_status mpsgpu_profile_end(mpsgpu_context* ctx, double* gemm_ms, double* gemm_flops,
+                                 long long* gemm_calls);
 
 /* ---- MPO (replaces MPO / Operator storage, src/core/headers/MPO.h:33-176) --
  * dims[4k..4k+3] = (du, Dl, dd, Dr) of operator k; data[k] its column-major
@@ -88,6 +97,17 @@ mpsgpu_status mpsgpu_synchronize(mpsgpu_context* ctx);
 mpsgpu_status mpsgpu_mpo_upload(mpsgpu_context* ctx, int L, const int* dims,
                                 const double* const* data, mpsgpu_mpo** out);
 mpsgpu_status mpsgpu_mpo_free(mpsgpu_context* ctx, mpsgpu_mpo* mpo);
+/* Model MPOs built by the library (host tensors as the reference builds
+ * them, then uploaded):
+ *   IsingHamiltonian(L, 2, J, g, h).getHMPO() (models/cpp/IsingHamiltonian.cpp:70-121)
+ *   IsingHamiltonian::getUMPO(mpo, delta, 0, imag, 2)     (IsingHamiltonian.cpp:131-148)
+ *   SchwingerHamiltonian(N, mu, x, l0, alpha).getHMPO()    (models/cpp/SchwingerHamiltonian.cpp:13-121) */
+mpsgpu_status mpsgpu_mpo_ising(mpsgpu_context* ctx, int L, double J, double g, double h,
+                               mpsgpu_mpo** out);
+mpsgpu_status mpsgpu_mpo_ising_evolution(mpsgpu_context* ctx, int L, double J, double g,
+                                         double h, double delta, int imag, mpsgpu_mpo** out);
+mpsgpu_status mpsgpu_mpo_schwinger(mpsgpu_context* ctx, int N, double mu, double x, double l0,
+                                   double alpha, mpsgpu_mpo** out);
 
 /* ---- MPS (replaces MPS / Site storage, src/core/headers/MPS.h) ------------
  * dims[3k..3k+2] = (d, Dl, Dr) of site k; data[k] column-major complex128. */

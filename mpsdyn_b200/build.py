@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmpsgpu.so")
 
-SOURCES = ["zgemm.cu", "blas1.cu", "qr.cu", "engine.cu", "capi.cu"]
+SOURCES = ["zgemm.cu", "blas1.cu", "qr.cu", "engine.cu", "capi.cu", "models.cpp"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [
     "-std=c++17", "-O3",
@@ -31,7 +31,7 @@ FLAGS = [
 
 
 def _compile(src: str) -> str:
-    obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+    obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
     srcp = os.path.join(CSRC, src)
     deps = [srcp] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     deps.append(os.path.join(ROOT, "include", "mpsgpu.h"))

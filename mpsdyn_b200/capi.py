@@ -20,8 +20,10 @@ STATUS = {
 
 EXPORTS = [
     "mpsgpu_default_options", "mpsgpu_create", "mpsgpu_destroy", "mpsgpu_status_string",
-    "mpsgpu_last_error", "mpsgpu_launch_count", "mpsgpu_synchronize", "mpsgpu_mpo_upload",
-    "mpsgpu_mpo_free", "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_product",
+    "mpsgpu_last_error", "mpsgpu_launch_count", "mpsgpu_synchronize", "mpsgpu_get_stream",
+    "mpsgpu_profile_begin", "mpsgpu_profile_end", "mpsgpu_mpo_upload",
+    "mpsgpu_mpo_free", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger",
+    "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_product",
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
     "mpsgpu_mps_gauge", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_expectation_local", "mpsgpu_entropy",
@@ -84,6 +86,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         lib.mpsgpu_heff_matvec.argtypes = [P, P, P, P, P, P, P, P, P, C.c_double, C.c_int]
         lib.mpsgpu_entropy.argtypes = [P, P, C.c_int, C.POINTER(C.c_double)]
         lib.mpsgpu_mps_gauge.argtypes = [P, P, C.c_char]
+        D_ = C.c_double
+        lib.mpsgpu_mpo_ising.argtypes = [P, C.c_int, D_, D_, D_, C.POINTER(P)]
+        lib.mpsgpu_mpo_ising_evolution.argtypes = [P, C.c_int, D_, D_, D_, D_, C.c_int, C.POINTER(P)]
+        lib.mpsgpu_mpo_schwinger.argtypes = [P, C.c_int, D_, D_, D_, D_, C.POINTER(P)]
         _lib = lib
     return _lib
 
@@ -132,6 +138,21 @@ class Context:
     def synchronize(self) -> None:
         self._check(self.lib.mpsgpu_synchronize(self.h))
 
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer handle."""
+        s = C.c_void_p()
+        self._check(self.lib.mpsgpu_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def profile_begin(self) -> None:
+        self._check(self.lib.mpsgpu_profile_begin(self.h))
+
+    def profile_end(self) -> dict:
+        ms, fl, n = C.c_double(), C.c_double(), C.c_longlong()
+        self._check(self.lib.mpsgpu_profile_end(self.h, C.byref(ms), C.byref(fl), C.byref(n)))
+        return {"gemm_ms": ms.value, "gemm_flops": fl.value, "gemm_calls": n.value}
+
     # ---- objects ----
     def mpo(self, ops: list) -> "DeviceMPO":
         arrs = [_fortran(w) for w in ops]
@@ -140,6 +161,21 @@ class Context:
         h = C.c_void_p()
         self._check(self.lib.mpsgpu_mpo_upload(self.h, len(arrs), _ptr(dims), ptrs, C.byref(h)))
         return DeviceMPO(self, h, len(arrs))
+
+    def mpo_ising(self, L: int, J: float, g: float, h: float) -> "DeviceMPO":
+        h_ = C.c_void_p()
+        self._check(self.lib.mpsgpu_mpo_ising(self.h, L, J, g, h, C.byref(h_)))
+        return DeviceMPO(self, h_, L)
+
+    def mpo_ising_evolution(self, L: int, J: float, g: float, h: float, delta: float, imag: bool) -> "DeviceMPO":
+        h_ = C.c_void_p()
+        self._check(self.lib.mpsgpu_mpo_ising_evolution(self.h, L, J, g, h, delta, int(imag), C.byref(h_)))
+        return DeviceMPO(self, h_, L)
+
+    def mpo_schwinger(self, N: int, mu: float, x: float, l0: float = 0.0, alpha: float = 0.0) -> "DeviceMPO":
+        h_ = C.c_void_p()
+        self._check(self.lib.mpsgpu_mpo_schwinger(self.h, N, mu, x, l0, alpha, C.byref(h_)))
+        return DeviceMPO(self, h_, N)
 
     def mps(self, sites: list, normfact: float = 1.0) -> "DeviceMPS":
         arrs = [_fortran(a) for a in sites]

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "models.h"
 #include "mpsgpu.h"
 
 struct mpsgpu_context {
@@ -192,6 +193,31 @@ mpsgpu_status mpsgpu_synchronize(mpsgpu_context* ctx) {
   return guarded(ctx, [&] { MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
 }
 
+mpsgpu_status mpsgpu_get_stream(mpsgpu_context* ctx, void** stream) {
+  if (!ctx || !stream) return MPSGPU_INVALID;
+  *stream = (void*)ctx->c.stream;
+  return MPSGPU_OK;
+}
+
+mpsgpu_status mpsgpu_profile_begin(mpsgpu_context* ctx) {
+  if (!ctx) return MPSGPU_INVALID;
+  ctx->c.prof.reset();
+  ctx->c.prof.on = true;
+  return MPSGPU_OK;
+}
+
+mpsgpu_status mpsgpu_profile_end(mpsgpu_context* ctx, double* gemm_ms, double* gemm_flops, long long* gemm_calls) {
+  if (!ctx) return MPSGPU_INVALID;
+  return guarded(ctx, [&] {
+    ctx->c.prof.on = false;
+    const double ms = ctx->c.prof.resolve_ms();
+    if (gemm_ms) *gemm_ms = ms;
+    if (gemm_flops) *gemm_flops = ctx->c.prof.flops;
+    if (gemm_calls) *gemm_calls = ctx->c.prof.calls;
+    ctx->c.prof.reset();
+  });
+}
+
 mpsgpu_status mpsgpu_mpo_upload(mpsgpu_context* ctx, int L, const int* dims, const double* const* data,
                                 mpsgpu_mpo** out) {
   if (!ctx || !dims || !data || !out) return MPSGPU_INVALID;
@@ -206,6 +232,49 @@ mpsgpu_status mpsgpu_mpo_upload(mpsgpu_context* ctx, int L, const int* dims, con
   }
   *out = h;
   return MPSGPU_OK;
+}
+
+static mpsgpu_status upload_host_mpo(mpsgpu_context* ctx, const std::function<HostMPO()>& make, mpsgpu_mpo** out) {
+  if (!ctx || !out) return MPSGPU_INVALID;
+  *out = nullptr;
+  auto* h = new (std::nothrow) mpsgpu_mpo();
+  if (!h) return MPSGPU_OOM;
+  mpsgpu_status st = guarded(ctx, [&] {
+    HostMPO m;
+    try {
+      m = make();
+    } catch (const std::invalid_argument& e) {
+      throw Error(MPSGPU_BAD_SHAPE, e.what());
+    }
+    std::vector<int> dims;
+    std::vector<const double*> ptrs;
+    for (size_t k = 0; k < m.W.size(); k++) {
+      for (int j = 0; j < 4; j++) dims.push_back(m.dims[k][j]);
+      ptrs.push_back(reinterpret_cast<const double*>(m.W[k].data()));
+    }
+    mpo_upload(ctx->c, h->m, (int)m.W.size(), dims.data(), ptrs.data());
+  });
+  if (st != MPSGPU_OK) {
+    mpo_free(ctx->c, h->m);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return MPSGPU_OK;
+}
+
+mpsgpu_status mpsgpu_mpo_ising(mpsgpu_context* ctx, int L, double J, double g, double h, mpsgpu_mpo** out) {
+  return upload_host_mpo(ctx, [&] { return ising_hmpo(L, J, g, h); }, out);
+}
+
+mpsgpu_status mpsgpu_mpo_ising_evolution(mpsgpu_context* ctx, int L, double J, double g, double h, double delta,
+                                         int imag, mpsgpu_mpo** out) {
+  return upload_host_mpo(ctx, [&] { return ising_umpo(L, J, g, h, delta, imag != 0); }, out);
+}
+
+mpsgpu_status mpsgpu_mpo_schwinger(mpsgpu_context* ctx, int N, double mu, double x, double l0, double alpha,
+                                   mpsgpu_mpo** out) {
+  return upload_host_mpo(ctx, [&] { return schwinger_hmpo(N, mu, x, l0, alpha); }, out);
 }
 
 mpsgpu_status mpsgpu_mpo_free(mpsgpu_context* ctx, mpsgpu_mpo* mpo) {

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <string>
 #include <stdexcept>
+#include <vector>
 
 #include "mpsgpu.h"
 
@@ -54,10 +55,44 @@ struct Error : public std::runtime_error {
     if (!(cond)) throw ::mpsgpu::Error((status), (msg));   \
   } while (0)
 
+// Device-time accounting of the tensor-pipe GEMM launches: CUDA events are
+// recorded on the launching stream around every GEMM while active and
+// resolved once at the end (no synchronisation inside the sweep).
+struct GemmProfiler {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  double flops = 0.0;
+  long long calls = 0;
+  cudaEvent_t next() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void reset() { used = 0; flops = 0.0; calls = 0; }
+  // Sum of (end - start) over the recorded pairs; synchronises on the last event.
+  double resolve_ms() {
+    double ms = 0.0;
+    if (used >= 2) cudaEventSynchronize(pool[used - 1]);
+    for (size_t i = 0; i + 1 < used; i += 2) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, pool[i], pool[i + 1]) == cudaSuccess) ms += t;
+    }
+    return ms;
+  }
+  ~GemmProfiler() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+
 // Launch bookkeeping: every kernel launcher calls after_launch().
 struct Stream {
   cudaStream_t s = nullptr;
   long long* launches = nullptr;
+  GemmProfiler* prof = nullptr;
 };
 
 inline void after_launch(const Stream& st) {

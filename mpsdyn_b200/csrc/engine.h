@@ -61,7 +61,8 @@ struct Context {
   double* dS = nullptr;        // Ritz coefficients on device
   cudaEvent_t ev = nullptr;
   cudaEvent_t mv0 = nullptr, mv1 = nullptr;
-  Stream st() { return Stream{stream, &launches}; }
+  GemmProfiler prof;
+  Stream st() { return Stream{stream, &launches, &prof}; }
 };
 
 // Environment cache (TmpManager, src/core/cpp/TmpManager.cpp:22-160):

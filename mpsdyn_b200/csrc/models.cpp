@@ -1,0 +1,201 @@
+// MPO builders (host side).  Each operator is assembled exactly as the
+// reference assembles it: a coefficient tensor C(Dl, Dr, nops) contracted
+// with the stack of single-site operators Z(nops, d, d), then reordered to
+// W(du, Dl, dd, Dr) (IsingHamiltonian.cpp:111-116, SchwingerHamiltonian.cpp:114-118).
+// Identical operators of the reference's shared middle sites are built once
+// and copied.
+#include "models.h"
+
+#include <cmath>
+#include <stdexcept>
+
+namespace mpsgpu {
+
+namespace {
+
+typedef std::complex<double> cd;
+
+// W[s', l, s, r] = sum_op C[l, r, op] Z[op][s', s]
+std::vector<cd> contract_coeffs(const std::vector<cd>& C, int Dl, int Dr, int nops,
+                                const std::vector<std::array<cd, 4>>& Z) {
+  const int d = 2;
+  std::vector<cd> W((size_t)d * Dl * d * Dr, cd(0, 0));
+  for (int l = 0; l < Dl; l++)
+    for (int r = 0; r < Dr; r++)
+      for (int op = 0; op < nops; op++) {
+        const cd c = C[l + Dl * (r + Dr * op)];
+        if (c == cd(0, 0)) continue;
+        for (int sp = 0; sp < d; sp++)
+          for (int s = 0; s < d; s++)
+            W[sp + d * (l + Dl * (s + d * r))] += c * Z[op][sp + d * s];
+      }
+  return W;
+}
+
+// column-major 2x2 matrices
+const std::array<cd, 4> SIG0 = {cd(1, 0), cd(0, 0), cd(0, 0), cd(1, 0)};
+const std::array<cd, 4> SIGX = {cd(0, 0), cd(1, 0), cd(1, 0), cd(0, 0)};
+const std::array<cd, 4> SIGZ = {cd(1, 0), cd(0, 0), cd(0, 0), cd(-1, 0)};
+// The Schwinger builder fills its sigma_y column-major from {0, -i, i, 0}
+// (SchwingerHamiltonian.cpp:30-31), i.e. [[0, i], [-i, 0]].
+const std::array<cd, 4> SIGY_SCHW = {cd(0, 0), cd(0, -1), cd(0, 1), cd(0, 0)};
+
+}  // namespace
+
+HostMPO ising_hmpo(int L, double J, double g, double h, double K) {
+  if (L < 2) throw std::invalid_argument("ising_hmpo: L < 2");
+  const std::vector<std::array<cd, 4>> Z = {SIG0, SIGZ, SIGX};
+  const int D = 3;
+  HostMPO m;
+  for (int k = 0; k < L; k++) {
+    if (k > 1 && k < L - 1) {
+      m.dims.push_back(m.dims[k - 1]);
+      m.W.push_back(m.W[k - 1]);
+      continue;
+    }
+    const int Dl = k == 0 ? 1 : D, Dr = k == L - 1 ? 1 : D;
+    std::vector<cd> C((size_t)Dl * Dr * 3, cd(0, 0));
+    auto at = [&](int l, int r, int op) -> cd& { return C[l + Dl * (r + Dr * op)]; };
+    const cd effJ = J < 0 ? cd(0, std::sqrt(std::fabs(J))) : cd(std::sqrt(J), 0);
+    if (k != L - 1) at(0, 0, 0) = 1.0;
+    if (k != 0) at(Dl - 1, Dr - 1, 0) = 1.0;
+    at(0, Dr - 1, 2) = g;
+    at(0, Dr - 1, 1) = h;
+    at(0, Dr - 1, 0) = K / L;
+    if (k != L - 1) at(0, 1, 1) = effJ;
+    if (k != 0) at(1, Dr - 1, 1) = effJ;
+    m.dims.push_back({2, Dl, 2, Dr});
+    m.W.push_back(contract_coeffs(C, Dl, Dr, 3, Z));
+  }
+  return m;
+}
+
+namespace {
+
+// isingU1MPO (IsingHamiltonian.cpp:203-218): exp(eps (g sx + h sz)) as a 2x2
+std::array<cd, 4> ising_u1(cd eps, double g, double h) {
+  const double nrm = std::sqrt(g * g + h * h);
+  std::array<cd, 4> r;
+  for (int i = 0; i < 4; i++) r[i] = std::cosh(nrm * eps) * SIG0[i];
+  if (nrm != 0)
+    for (int i = 0; i < 4; i++)
+      r[i] += (h / nrm) * std::sinh(nrm * eps) * SIGZ[i] + (g / nrm) * std::sinh(nrm * eps) * SIGX[i];
+  return r;
+}
+
+// isingU2MPO (IsingHamiltonian.cpp:169-201): exp(eps sz sz) split over bond 2
+std::vector<cd> ising_u2(cd eps, int pos, int L, int& Dl, int& Dr) {
+  const std::vector<std::array<cd, 4>> Z = {SIG0, SIGZ, SIGX};
+  if (eps == cd(0, 0)) {
+    Dl = Dr = 1;
+    return std::vector<cd>(SIG0.begin(), SIG0.end());
+  }
+  const int D = 2;
+  if (pos != 0 && pos != L - 1) {
+    Dl = Dr = D;
+    std::vector<cd> C((size_t)D * D * 3, cd(0, 0));
+    auto at = [&](int l, int r, int op) -> cd& { return C[l + D * (r + D * op)]; };
+    at(0, 0, 0) = std::cosh(eps);
+    at(1, 1, 0) = std::sinh(eps);
+    at(0, 1, 1) = std::sqrt(std::cosh(eps) * std::sinh(eps));
+    at(1, 0, 1) = std::sqrt(std::cosh(eps) * std::sinh(eps));
+    return contract_coeffs(C, Dl, Dr, 3, Z);
+  }
+  // edge: C(1, D, 3) reinterpreted as (Dl, Dr) = (1, D) or (D, 1)
+  std::vector<cd> C((size_t)D * 3, cd(0, 0));
+  C[0 + D * 0] = std::sqrt(std::cosh(eps));
+  C[1 + D * 1] = std::sqrt(std::sinh(eps));
+  if (pos == 0) { Dl = 1; Dr = D; }
+  else { Dl = D; Dr = 1; }
+  return contract_coeffs(C, Dl, Dr, 3, Z);
+}
+
+}  // namespace
+
+HostMPO ising_umpo(int L, double J, double g, double h, double delta, bool imag) {
+  if (L < 2) throw std::invalid_argument("ising_umpo: L < 2");
+  const cd eps = imag ? cd(-delta, 0) : cd(0, -delta);
+  HostMPO m;
+  for (int k = 0; k < L; k++) {
+    if (k > 1 && k < L - 1) {
+      m.dims.push_back(m.dims[k - 1]);
+      m.W.push_back(m.W[k - 1]);
+      continue;
+    }
+    // constructU2T (IsingHamiltonian.cpp:220-244): U1(eps/2) . U2(J eps) . U1(eps/2)
+    const std::array<cd, 4> U1 = ising_u1(0.5 * eps, g, h);
+    int Dl, Dr;
+    const std::vector<cd> U2 = ising_u2(J * eps, k, L, Dl, Dr);
+    const int d = 2;
+    std::vector<cd> W((size_t)d * Dl * d * Dr, cd(0, 0));
+    for (int sp = 0; sp < d; sp++)
+      for (int l = 0; l < Dl; l++)
+        for (int s = 0; s < d; s++)
+          for (int r = 0; r < Dr; r++) {
+            cd acc(0, 0);
+            for (int a = 0; a < d; a++)
+              for (int b = 0; b < d; b++)
+                acc += U1[sp + d * a] * U2[a + d * (l + Dl * (b + d * r))] * U1[b + d * s];
+            W[sp + d * (l + Dl * (s + d * r))] = acc;
+          }
+    m.dims.push_back({d, Dl, d, Dr});
+    m.W.push_back(W);
+  }
+  return m;
+}
+
+HostMPO schwinger_hmpo(int N, double mu, double x, double l0, double alpha, double offset, double nu,
+                       double y) {
+  if (N < 3) throw std::invalid_argument("schwinger_hmpo: N < 3");
+  const std::vector<std::array<cd, 4>> Z = {SIG0, SIGX, SIGY_SCHW, SIGZ};
+  const int D = 5;
+  const double alpha_ = alpha + l0;
+  std::vector<double> alphas(N), sumA(N, 0.0);
+  for (int k = 0; k < N; k++) {
+    const double signo = (k + 1) % 2 == 0 ? 1.0 : -1.0;
+    alphas[k] = alpha_ - 0.25 * (1.0 - signo);
+  }
+  double tot = 0.0;
+  for (int k = N - 2; k >= 0; k--) {
+    tot += alphas[k];
+    sumA[k] = tot;
+  }
+  const double gw = y;
+  const double sx = std::sqrt(x / 2);
+  HostMPO m;
+  for (int k = 0; k < N; k++) {
+    const int Dl = k == 0 ? 1 : D, Dr = k == N - 1 ? 1 : D;
+    std::vector<cd> C((size_t)Dl * Dr * 4, cd(0, 0));
+    auto at = [&](int l, int r, int op) -> cd& { return C[l + Dl * (r + Dr * op)]; };
+    if (k != N - 1) at(0, 0, 0) = 1.0;
+    if (k != 0) at(D - 1, Dr - 1, 0) = 1.0;
+    if (k > 0 && k < N - 2) at(3, 3, 0) = 1.0;
+    const double ak = alphas[k];
+    const double signok = (k + 1) % 2 == 0 ? 1.0 : -1.0;
+    if (k != N - 1) {
+      at(0, Dr - 1, 0) = gw * ak * ak + (gw * (k + 1) / 4.0 + mu / 2.0 + nu / 2.0 + offset / N);
+      at(0, Dr - 1, 3) = (signok * mu / 2.0 + nu / 2.0) + gw * sumA[k];
+    } else {
+      at(0, Dr - 1, 0) = mu / 2.0 + nu / 2.0 + offset / N;
+      at(0, Dr - 1, 3) = signok * mu / 2.0 + nu / 2.0;
+    }
+    if (k != N - 1) {
+      at(0, 1, 1) = sx;
+      at(0, 2, 2) = sx;
+      if (k < N - 2) at(0, 3, 3) = gw;
+      if (k != 0) {
+        at(1, 4, 1) = sx;
+        at(2, 4, 2) = sx;
+        at(3, 4, 3) = (N - k - 1) / 2.0;
+      }
+    } else {
+      at(1, 0, 1) = sx;
+      at(2, 0, 2) = sx;
+    }
+    m.dims.push_back({2, Dl, 2, Dr});
+    m.W.push_back(contract_coeffs(C, Dl, Dr, 4, Z));
+  }
+  return m;
+}
+
+}  // namespace mpsgpu

@@ -258,12 +258,23 @@ void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
   cplx* partial = nullptr;
   if (splits > 1)
     partial = (cplx*)scratch.get((size_t)splits * g.batch * (size_t)g.M * g.N * sizeof(cplx));
+  const bool prof = st.prof && st.prof->on;
+  if (prof) {
+    cudaEvent_t e0 = st.prof->next();
+    if (e0) cudaEventRecord(e0, st.s);
+  }
   if (big) launch_tiles<64, 64>(st, g, splits, kchunk, partial);
   else launch_tiles<32, 32>(st, g, splits, kchunk, partial);
   if (splits > 1) {
     long long total = (long long)g.M * g.N * g.batch;
     splitk_reduce_kernel<<<std::min<long long>(ceil_div(total, 256), 4096), 256, 0, st.s>>>(g, splits, partial);
     after_launch(st);
+  }
+  if (prof) {
+    cudaEvent_t e1 = st.prof->next();
+    if (e1) cudaEventRecord(e1, st.s);
+    st.prof->flops += 8.0 * (double)g.M * g.N * g.K * g.batch;
+    st.prof->calls++;
   }
 }
 

