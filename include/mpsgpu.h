@@ -202,6 +202,26 @@ mpsgpu_status mpsgpu_qr(mpsgpu_context* ctx, int m, int n, const double* A,
 mpsgpu_status mpsgpu_lq(mpsgpu_context* ctx, int m, int n, const double* A,
                         double* Lf, double* Q);
 
+/* QR of a device-resident m x n matrix that allocates nothing.  No
+ * counterpart in the reference: it is a variant of mpsgpu_qr for callers that
+ * cannot allocate device memory when they need a gauge move (a serving
+ * process whose allocator owns the whole HBM, a caller recording a CUDA
+ * graph, a loop that must not fail on allocation mid-sweep).
+ *   A: m x n column-major complex128 on the device (read only);
+ *   Q: m x K (ld m), R: K x n (ld K), K = min(m, n), on the device; either may
+ *      be null.  Same results as mpsgpu_qr (LAPACK zgeqrf/zungqr conventions).
+ *   stream: the cudaStream_t to run on (null = default stream); the call is
+ *      asynchronous on it and returns after enqueueing.
+ * Limit: m, n <= 640 and m*n <= 131072; larger sizes return MPSGPU_BAD_SHAPE.
+ * Working memory is one fixed 2.1 MiB device array inside the library,
+ * reserved on every GPU that loads it until the process exits.  The first
+ * call on a device looks up that array's address (cudaGetSymbolAddress):
+ * make that first call before any stream capture.  All calls share the
+ * array, so calls that overlap on the GPU (different streams, or concurrent
+ * host threads) race; serialise them on one stream. */
+mpsgpu_status mpsgpu_qr_device_noalloc(int m, int n, const double* A, double* Q,
+                                       double* R, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

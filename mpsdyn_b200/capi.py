@@ -28,7 +28,7 @@ EXPORTS = [
     "mpsgpu_mps_gauge", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_expectation_local", "mpsgpu_entropy",
     "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_env_left", "mpsgpu_env_right",
-    "mpsgpu_qr", "mpsgpu_lq",
+    "mpsgpu_qr", "mpsgpu_lq", "mpsgpu_qr_device_noalloc",
 ]
 
 
@@ -339,3 +339,15 @@ class DeviceMPS:
         if self.h:
             self.ctx.lib.mpsgpu_mps_free(self.ctx.h, self.h)
             self.h = None
+
+
+def qr_device_noalloc(m: int, n: int, a_ptr: int, q_ptr: int, r_ptr: int, stream: int = 0) -> None:
+    """mpsgpu_qr_device_noalloc on device pointers (integers): QR of the m x n
+    column-major complex128 matrix at a_ptr into Q (m x K) and R (K x n)
+    without any allocation; asynchronous on `stream`."""
+    lib = load()
+    P = C.c_void_p
+    lib.mpsgpu_qr_device_noalloc.argtypes = [C.c_int, C.c_int, P, P, P, P]
+    st = lib.mpsgpu_qr_device_noalloc(m, n, P(a_ptr), P(q_ptr or None), P(r_ptr or None), P(stream or None))
+    if st != 0:
+        raise MpsgpuError(st, "mpsgpu_qr_device_noalloc")

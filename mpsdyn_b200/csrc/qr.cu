@@ -19,6 +19,8 @@
 // column slice (independent, no barrier) and extracts R.
 #include <cooperative_groups.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -319,3 +321,109 @@ void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, lo
 }
 
 }  // namespace mpsgpu
+
+// ---------------------------------------------------------------------------
+// QR without allocation (mpsgpu_qr_device_noalloc, include/mpsgpu.h).
+//
+// Some callers cannot allocate device memory at the moment they need a gauge
+// move: a serving process whose memory manager has reserved the whole HBM
+// for its request slots, a caller recording work into a CUDA graph (no
+// allocation may happen while a stream is being captured), or a real-time
+// loop that must not meet an allocation failure half way through a sweep.
+// For them this variant keeps every byte of its working memory in one
+// file-scope device array: the working copy of A (factored in place), the
+// block-reflector factors T and the scalars tau.  The array is reserved when
+// the library is loaded, on every GPU that loads it, and held until exit.
+// ---------------------------------------------------------------------------
+
+namespace mpsgpu {
+namespace {
+
+// Capacity: m*n <= 131072 complex (for example 512 x 256), m, n <= 640
+// (nb = 16), i.e. at most 40 panels of 16 x 16 T factors and 640 tau values.
+constexpr long long NOALLOC_MAX_ELEMS = 131072;
+constexpr int NOALLOC_MAX_DIM = 640;
+constexpr int NOALLOC_NB = 16;
+constexpr long long NOALLOC_T_ELEMS = (long long)(NOALLOC_MAX_DIM / NOALLOC_NB) * NOALLOC_NB * NOALLOC_NB;
+constexpr long long NOALLOC_TOTAL = NOALLOC_MAX_ELEMS + NOALLOC_T_ELEMS + NOALLOC_MAX_DIM;
+
+// 2.1 MiB.  Host code must not use this name as an address: it is a host-side
+// stand-in for the device symbol; the device address comes from
+// cudaGetSymbolAddress, once per device (noalloc_scratch_on below).
+static __device__ __align__(256) double2 g_qr_noalloc_scratch[NOALLOC_TOTAL];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double2* g_noalloc_ptr[MAX_DEVICES] = {nullptr};
+bool g_noalloc_attr[MAX_DEVICES] = {false};
+
+// Device address of the scratch array on the current device (set-up on the
+// first call per device; later calls only read the cached pointer).
+mpsgpu_status noalloc_scratch_on(int dev, double2** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_qr_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) return MPSGPU_CUDA_ERROR;
+    g_noalloc_ptr[dev] = static_cast<double2*>(p);
+  }
+  if (!g_noalloc_attr[dev]) {
+    if (cudaFuncSetAttribute(qr_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(qr_form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+            cudaSuccess)
+      return MPSGPU_CUDA_ERROR;
+    g_noalloc_attr[dev] = true;
+  }
+  *out = g_noalloc_ptr[dev];
+  return MPSGPU_OK;
+}
+
+}  // namespace
+}  // namespace mpsgpu
+
+extern "C" mpsgpu_status mpsgpu_qr_device_noalloc(int m, int n, const double* A, double* Q, double* R,
+                                                  void* stream) {
+  using namespace mpsgpu;
+  if (m <= 0 || n <= 0 || !A || (!Q && !R)) return MPSGPU_INVALID;
+  if (m > NOALLOC_MAX_DIM || n > NOALLOC_MAX_DIM || (long long)m * n > NOALLOC_MAX_ELEMS) {
+    fprintf(stderr,
+            "mpsgpu_qr_device_noalloc: %d x %d exceeds the fixed scratch (m, n <= %d and m*n <= %lld)\n", m,
+            n, NOALLOC_MAX_DIM, NOALLOC_MAX_ELEMS);
+    return MPSGPU_BAD_SHAPE;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return MPSGPU_CUDA_ERROR;
+  double2* scratch = nullptr;
+  mpsgpu_status st = noalloc_scratch_on(dev, &scratch);
+  if (st != MPSGPU_OK) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int K = std::min(m, n);
+  QrParams p;
+  p.m = m; p.n = n; p.K = K; p.nb = NOALLOC_NB; p.npanel = (K + NOALLOC_NB - 1) / NOALLOC_NB;
+  // Layout of the shared array: [A copy | T factors | tau].  Every element
+  // the kernels read is written first in the same call (the copy of A, then
+  // T and tau by the factorisation), so nothing needs clearing.
+  p.A = scratch;
+  p.T = scratch + NOALLOC_MAX_ELEMS;
+  p.tau = p.T + NOALLOC_T_ELEMS;
+  if (cudaMemcpyAsync(p.A, A, (size_t)m * n * sizeof(double2), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return MPSGPU_CUDA_ERROR;
+  const size_t smem = (size_t)m * NOALLOC_NB * sizeof(double2);
+  int nsm = 148, per_sm = 1;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qr_factor_kernel, QR_THREADS, smem) != cudaSuccess ||
+      per_sm < 1)
+    return MPSGPU_CUDA_ERROR;
+  const int grid = std::min(std::max(1, (n + NOALLOC_NB - 1) / NOALLOC_NB), nsm * per_sm);
+  void* args[] = {&p};
+  if (cudaLaunchCooperativeKernel((void*)qr_factor_kernel, dim3(grid), dim3(QR_THREADS), args, smem, s) !=
+      cudaSuccess)
+    return MPSGPU_CUDA_ERROR;
+  int qgrid = std::max(1, std::min((K + NOALLOC_NB - 1) / NOALLOC_NB, nsm));
+  if (R && !Q) qgrid = std::max(qgrid, 8);
+  qr_form_q_kernel<<<qgrid, QR_THREADS, smem, s>>>(p, reinterpret_cast<double2*>(Q), m,
+                                                   reinterpret_cast<double2*>(R), K);
+  if (cudaGetLastError() != cudaSuccess) return MPSGPU_CUDA_ERROR;
+  return MPSGPU_OK;
+}
