@@ -6,9 +6,13 @@ penalty (seed-11 initial MPS), convergence 1e-10, complex FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpsgpu|reference]
 
+One step is a batch of B (default 8) independent solves with different seeds,
+run concurrently, one library context (CUDA stream) and host thread each.
 One process per GPU; the path does not shard (independent solves), so N GPUs
 run N replicas of the workload ("replicas only", weak scaling) and `value`
 is the total solves of all ranks divided by the max-over-ranks device time.
+The line also carries the plain form (one solve alone) and the p50/p99
+latency of the solves inside the batches.
 
 Prints one JSON line (rank 0).  `value` is timed with CUDA events on the
 library's stream with the initial states already in HBM; `e2e` is the same
@@ -40,7 +44,7 @@ UNIT = "solves/s"
 # Algorithmic flops of one solve of this workload as counted by the library
 # (GS + excited state); used by the reference arm to turn its measured flop
 # rate into solves/s when no GPU run is available in the same process.
-FLOPS_PER_SOLVE_DEFAULT = 2.4e13
+FLOPS_PER_SOLVE_DEFAULT = 2.47e13
 
 
 def parse():
@@ -51,6 +55,8 @@ def parse():
     p.add_argument("--impl", default="mpsgpu", choices=["mpsgpu", "reference"])
     p.add_argument("--cpu-sample-sites", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--batch", type=int, default=8, help="concurrent solves per step")
+    p.add_argument("--plain", type=int, default=1, help="also time one solve alone (the plain form)")
     return p.parse_args()
 
 
@@ -192,117 +198,146 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         if dist is not None:
             dist.barrier()
 
-    def allmax(x: float) -> float:
+    def allreduce(x: float, op) -> float:
         if dist is None:
             return x
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def allsum(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        dist.all_reduce(t, op=op)
         return float(t.item())
 
     W = WORKLOAD
-    ctx = capi.Context(local_rank)
-    ext = torch.cuda.ExternalStream(ctx.stream)
+    B = args.batch
+    # one library context (own CUDA stream) and one host thread per concurrent solve
+    ctxs = [capi.Context(local_rank) for _ in range(B)]
+    exts = [torch.cuda.ExternalStream(c.stream) for c in ctxs]
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    opts = ctxs[0].options(convtol=W["convtol"])
+    mpos = [c.mpo_schwinger(W["N"], MU, W["x"]) for c in ctxs]
+    seeds = [(W["seed_gs"] + 1000 * (rank * B + i), W["seed_exc"] + 1000 * (rank * B + i)) for i in range(B)]
+    inits = [(c.mps_random(W["N"], 2, W["D"], sg), c.mps_random(W["N"], 2, W["D"], se))
+             for c, (sg, se) in zip(ctxs, seeds)]
+    hosts = [(g.download()[0], x.download()[0]) for g, x in inits]
+    h2d_mps = sum(a.nbytes for a in hosts[0][0]) + sum(a.nbytes for a in hosts[0][1])
+    mpo_bytes = 16 * (2 * 1 * 2 * 5 + 2 * 5 * 2 * 1 + (W["N"] - 2) * 2 * 5 * 2 * 5)
+    results = [None] * B
 
-    def flush_l2():
-        with torch.cuda.stream(ext):
-            flush_buf.zero_()
-
-    opts = ctx.options(convtol=W["convtol"])
-    mpo = ctx.mpo_schwinger(W["N"], MU, W["x"])
-    init_gs = ctx.mps_random(W["N"], 2, W["D"], W["seed_gs"] + 1000 * rank)
-    init_ex = ctx.mps_random(W["N"], 2, W["D"], W["seed_exc"] + 1000 * rank)
-
-    stats = {}
-
-    def solve_resident():
-        g = init_gs.copy()
-        x = init_ex.copy()
-        e0, s0 = ctx.find_ground_state(mpo, W["D"], g, 0.0, opts)
-        e1, s1 = ctx.find_next_excited_state(mpo, W["D"], [g], x, 0.0, opts)
-        stats.update(gs=s0, exc=s1, E0=e0, E1=e1)
+    def solve_resident(i):
+        c = ctxs[i]
+        g, x = inits[i][0].copy(), inits[i][1].copy()
+        e0, s0 = c.find_ground_state(mpos[i], W["D"], g, 0.0, opts)
+        e1, s1 = c.find_next_excited_state(mpos[i], W["D"], [g], x, 0.0, opts)
         g.free()
         x.free()
-        return e0, e1
+        results[i] = {"E0": e0, "E1": e1, "gs": s0, "exc": s1}
 
-    # host copies of the inputs for the end-to-end arm
-    host_gs, _ = init_gs.download()
-    host_ex, _ = init_ex.download()
-    h2d_mps = sum(a.nbytes for a in host_gs) + sum(a.nbytes for a in host_ex)
-    mpo_bytes = 16 * (2 * 1 * 2 * 5 + 2 * 5 * 2 * 1 + (W["N"] - 2) * 2 * 5 * 2 * 5)
-
-    def solve_e2e():
-        m = ctx.mpo_schwinger(W["N"], MU, W["x"])           # host build + upload
-        g = ctx.mps(host_gs)                                  # H2D
-        x = ctx.mps(host_ex)
-        e0, _ = ctx.find_ground_state(m, W["D"], g, 0.0, opts)
-        e1, _ = ctx.find_next_excited_state(m, W["D"], [g], x, 0.0, opts)
-        out_g, _ = g.download()                               # D2H
-        out_x, _ = x.download()
-        d2h = sum(a.nbytes for a in out_g) + sum(a.nbytes for a in out_x) + 16
+    def solve_e2e(i):
+        c = ctxs[i]
+        m = c.mpo_schwinger(W["N"], MU, W["x"])           # host build + upload
+        g, x = c.mps(hosts[i][0]), c.mps(hosts[i][1])      # host -> device
+        e0, _ = c.find_ground_state(m, W["D"], g, 0.0, opts)
+        e1, _ = c.find_next_excited_state(m, W["D"], [g], x, 0.0, opts)
+        og, _ = g.download()                               # device -> host
+        ox, _ = x.download()
+        results[i] = {"E0": e0, "E1": e1, "d2h": sum(a.nbytes for a in og) + sum(a.nbytes for a in ox) + 16}
         g.free()
         x.free()
         m.free()
-        return e0, e1, d2h
+
+    def run_batch(fn, timed_events=True):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(B)]
+        go = threading.Barrier(B)
+
+        def body(i):
+            go.wait()
+            if timed_events:
+                evs[i][0].record(exts[i])
+            fn(i)
+            if timed_events:
+                evs[i][1].record(exts[i])
+
+        ths = [threading.Thread(target=body, args=(i,)) for i in range(B)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        torch.cuda.synchronize()
+        if not timed_events:
+            return None, None
+        # batch time on the device: earliest start to latest end (events of
+        # different streams on one device are comparable)
+        t0 = min(range(B), key=lambda i: 0.0 if i == 0 else evs[0][0].elapsed_time(evs[i][0]))
+        span = max(evs[t0][0].elapsed_time(evs[i][1]) for i in range(B))
+        per = [evs[i][0].elapsed_time(evs[i][1]) for i in range(B)]
+        return span, per
+
+    def flush_l2():
+        with torch.cuda.stream(exts[0]):
+            flush_buf.zero_()
+        torch.cuda.synchronize()
 
     # ---- warm-up ----
     for _ in range(args.warmup):
-        solve_resident()
-    ctx.synchronize()
+        run_batch(solve_resident, timed_events=False)
 
     # ---- timed: inputs resident in HBM ----
     clocks = ClockSampler(local_rank)
     clocks.start()
-    launches0 = ctx.launches
-    step_ms = []
-    energies = []
-    ctx.profile_begin()
+    launches0 = sum(c.launches for c in ctxs)
+    for c in ctxs:
+        c.profile_begin()
     barrier()
+    spans, lat = [], []
+    energies = []
     for _ in range(args.steps):
         flush_l2()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(ext)
-        energies.append(solve_resident())
-        ev1.record(ext)
-        ev1.synchronize()
-        step_ms.append(ev0.elapsed_time(ev1))
-    prof = ctx.profile_end()
-    launches = ctx.launches - launches0
+        span, per = run_batch(solve_resident)
+        spans.append(span)
+        lat.extend(per)
+        energies.append([(r["E0"], r["E1"]) for r in results])
+    profs = [c.profile_end() for c in ctxs]
+    launches = sum(c.launches for c in ctxs) - launches0
     barrier()
     clk = clocks.stop()
-    total_ms = allmax(float(sum(step_ms)))
-    solves = allsum(float(args.steps))
+    stats = results[0]
+    total_ms = allreduce(float(sum(spans)), torch.distributed.ReduceOp.MAX if dist else None)
+    solves = allreduce(float(args.steps * B), torch.distributed.ReduceOp.SUM if dist else None)
     value = solves / (total_ms * 1e-3)
 
     # ---- timed: end to end through the C ABI with host buffers ----
     barrier()
     e2e_ms = []
-    d2h = 0
     for _ in range(args.steps):
         flush_l2()
-        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        e0, e1, d2h = solve_e2e()
+        run_batch(solve_e2e, timed_events=False)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_total = allmax(float(sum(e2e_ms)))
+    d2h = sum(r["d2h"] for r in results)
+    e2e_total = allreduce(float(sum(e2e_ms)), torch.distributed.ReduceOp.MAX if dist else None)
     e2e_value = solves / (e2e_total * 1e-3)
 
+    # ---- the plain form: one solve alone on the GPU ----
+    plain_ms = None
+    if args.plain:
+        flush_l2()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(exts[0])
+        solve_resident(0)
+        ev1.record(exts[0])
+        ev1.synchronize()
+        plain_ms = ev0.elapsed_time(ev1)
+
     if rank != 0:
-        ctx.close()
+        for c in ctxs:
+            c.close()
         if dist is not None:
             dist.destroy_process_group()
         return
 
     # ---- roofline of the dominant kernel (the DMMA complex GEMM) ----
     peak = fp64_gemm_peak(torch)
-    gemm_tflops = prof["gemm_flops"] / (prof["gemm_ms"] * 1e-3) / 1e12 if prof["gemm_ms"] > 0 else 0.0
+    gemm_ms = sum(p["gemm_ms"] for p in profs)
+    gemm_flops = sum(p["gemm_flops"] for p in profs)
+    gemm_tflops = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else 0.0
     s_gs, s_ex = stats["gs"], stats["exc"]
     flops_per_solve = s_gs["flops"] + s_ex["flops"]
     roofline = {"bound": "tensor", "achieved": gemm_tflops, "peak": peak, "unit": "TFLOP/s",
@@ -313,8 +348,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                 "traffic": 1.85e6, "traffic_unit": "bytes per launch",
                 "kernel": "zgemm_dmma_kernel (complex FP64, mma.sync m8n8k4 f64)",
                 "peak_source": "cuBLAS complex128 GEMM 4096^3 measured in this run (FP64 tensor pipe)",
-                "gemm_share_of_step": prof["gemm_ms"] / sum(step_ms),
-                "all_kernels_tflops": flops_per_solve * args.steps / (sum(step_ms) * 1e-3) / 1e12}
+                "note": "achieved = GEMM flops / summed per-launch event time over all streams",
+                "gemm_aggregate_tflops": gemm_flops / (sum(spans) * 1e-3) / 1e12,
+                "all_kernels_tflops": flops_per_solve * args.steps * B / (sum(spans) * 1e-3) / 1e12}
 
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -330,26 +366,31 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
-    e0, e1 = energies[-1]
+    lat_s = np.array(lat) * 1e-3
+    e0s = [e for step in energies for e in step]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (seeded complex Gaussian initial MPS, model MPO built in-library)",
         "config": {**WORKLOAD, "mu": MU, "parallelism": f"replicas{world}", "precision": "fp64",
+                   "batch": B, "batch_form": "concurrent independent solves, one stream each",
                    "l2": "flushed between steps (256 MB write)"},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_mps + mpo_bytes,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B * (h2d_mps + mpo_bytes),
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.steps},
+        "latency_s": {"p50": float(np.percentile(lat_s, 50)), "p99": float(np.percentile(lat_s, 99))},
+        "plain_single_solve_ms": plain_ms,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
-        "results": {"E0": e0, "E1": e1, "gap": e1 - e0,
+        "results": {"E0": e0s[0][0], "E1": e0s[0][1], "gap": e0s[0][1] - e0s[0][0],
                     "gs": {k: s_gs[k] for k in ("rounds", "site_solves", "matvecs", "flops")},
                     "exc": {k: s_ex[k] for k in ("rounds", "site_solves", "matvecs", "flops")}},
     }
     print(json.dumps(line), flush=True)
-    ctx.close()
+    for c in ctxs:
+        c.close()
     if dist is not None:
         dist.destroy_process_group()
 

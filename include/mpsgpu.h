@@ -85,8 +85,9 @@ mpsgpu_status mpsgpu_synchronize(mpsgpu_context* ctx);
  * library's work with their own events on that stream. */
 mpsgpu_status mpsgpu_get_stream(mpsgpu_context* ctx, void** stream);
 /* Device-time accounting of the tensor-pipe GEMMs: between begin and end,
- * CUDA events bracket every GEMM launch on the context's stream; end
- * returns their summed device time (ms), algorithmic flops and count. */
+ * CUDA events bracket one GEMM launch in 32 on the context's stream; end
+ * returns the summed device time (ms), algorithmic flops and count of the
+ * sampled launches (their ratio is the average per-launch throughput). */
 mpsgpu_status mpsgpu_profile_begin(mpsgpu_context* ctx);
 mpsgpu_status mpsgpu_profile_end(mpsgpu_context* ctx, double* gemm_ms, double* gemm_flops,
                                  long long* gemm_calls);

@@ -154,6 +154,12 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
     MPSGPU_CUDA(cudaEventCreate(&c.ev));
     MPSGPU_CUDA(cudaEventCreate(&c.mv0));
     MPSGPU_CUDA(cudaEventCreate(&c.mv1));
+    MPSGPU_CUDA(cudaMalloc((void**)&c.dsc, sizeof(LanczosScalars)));
+    MPSGPU_CUDA(cudaMallocHost((void**)&c.hsc, sizeof(LanczosScalars)));
+    MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 64 * sizeof(unsigned)));
+    MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 64 * sizeof(unsigned)));
+    c.iter_ev.resize(257);
+    for (auto& e : c.iter_ev) MPSGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   });
   if (st != MPSGPU_OK) {
     delete ctx;
@@ -179,6 +185,11 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   if (c.ev) cudaEventDestroy(c.ev);
   if (c.mv0) cudaEventDestroy(c.mv0);
   if (c.mv1) cudaEventDestroy(c.mv1);
+  for (auto e : c.iter_ev)
+    if (e) cudaEventDestroy(e);
+  cudaFree(c.dsc);
+  cudaFreeHost(c.hsc);
+  cudaFree(c.dcounter);
   if (c.stream) cudaStreamDestroy(c.stream);
   delete ctx;
   return MPSGPU_OK;

@@ -60,10 +60,13 @@ struct Error : public std::runtime_error {
 // resolved once at the end (no synchronisation inside the sweep).
 struct GemmProfiler {
   bool on = false;
+  int every = 32;       // sample one GEMM launch in `every` (keeps event traffic low)
+  long long seen = 0;   // GEMM launches since begin
   std::vector<cudaEvent_t> pool;
   size_t used = 0;
-  double flops = 0.0;
-  long long calls = 0;
+  double flops = 0.0;   // algorithmic flops of the sampled launches
+  long long calls = 0;  // sampled launches
+  bool sample() { return on && (seen++ % every) == 0; }
   cudaEvent_t next() {
     if (used == pool.size()) {
       cudaEvent_t e;
@@ -72,7 +75,7 @@ struct GemmProfiler {
     }
     return pool[used++];
   }
-  void reset() { used = 0; flops = 0.0; calls = 0; }
+  void reset() { used = 0; flops = 0.0; calls = 0; seen = 0; }
   // Sum of (end - start) over the recorded pairs; synchronises on the last event.
   double resolve_ms() {
     double ms = 0.0;

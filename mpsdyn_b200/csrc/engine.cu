@@ -647,13 +647,12 @@ cplx contract(Context& c, const MpsDev& ket, const MpoDev* ops, const MpsDev& br
 template <class Op>
 static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, int max_krylov,
                              int* iters) {
-  const int m = std::min(N, std::max(2, max_krylov));
+  const int m = std::min(N, std::max(2, std::min(max_krylov, 200)));
   dbuf_reserve(c, c.lanV, (long long)N * (m + 1));
   dbuf_reserve(c, c.lanW, N);
   cplx* V = c.lanV.p;
   cplx* w = c.lanW.p;
   const Stream st = c.st();
-  double* d_beta = c.dscal;          // [0..m)
   double* d_tmp = c.dscal + 512;
   cplx* h1 = c.dcplx;
   cplx* h2 = c.dcplx + 256;
@@ -671,28 +670,31 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
   int total = 0;
   const int max_restarts = 60;
   TridiagLowest tri;
+  // Iteration j: matvec, fused reorthogonalisation, async copy of
+  // (alpha_j, beta_j) to pinned memory, event.  The host enqueues iteration
+  // j+1 before it waits for j, so the convergence test (tridiagonal
+  // eigenpair on the host) overlaps the device work; a speculative iteration
+  // after convergence is discarded (it only writes V[:, j+2] and w).
+  auto enqueue = [&](int j) {
+    apply(V + (long long)j * N, w);
+    lanczos_orthonormalize(st, N, j, V, N, w, j + 1 < m, c.dsc, h1, h2, c.dcounter, c.scratch);
+    MPSGPU_CUDA(cudaMemcpyAsync(&c.hsc->alpha[j], &c.dsc->alpha[j], sizeof(double), cudaMemcpyDeviceToHost,
+                                c.stream));
+    MPSGPU_CUDA(cudaMemcpyAsync(&c.hsc->beta[j], &c.dsc->beta[j], sizeof(double), cudaMemcpyDeviceToHost,
+                                c.stream));
+    MPSGPU_CUDA(cudaEventRecord(c.iter_ev[j], c.stream));
+    total++;
+  };
   for (int restart = 0; restart < max_restarts; restart++) {
     a.clear();
     b.clear();
     bool conv = false;
-    int j = 0;
-    for (j = 0; j < m; j++) {
-      cplx* vj = V + (long long)j * N;
-      apply(vj, w);
-      total++;
-      cgemv_c(st, N, j + 1, V, N, w, h1, c.scratch);
-      cgemv_n_sub(st, N, j + 1, V, N, h1, w);
-      cgemv_c(st, N, j + 1, V, N, w, h2, c.scratch);
-      cgemv_n_sub(st, N, j + 1, V, N, h2, w);
-      dznrm2(st, N, w, d_beta + j, c.scratch);
-      // fetch alpha_j = Re(h1[j] + h2[j]) and beta_j
-      MPSGPU_CUDA(cudaMemcpyAsync(c.hcplx, h1 + j, sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
-      MPSGPU_CUDA(cudaMemcpyAsync(c.hcplx + 1, h2 + j, sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
-      MPSGPU_CUDA(cudaMemcpyAsync(c.hscal, d_beta + j, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-      if (j + 1 < m) zscal_inv(st, N, w, d_beta + j, V + (long long)(j + 1) * N);
-      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
-      const double alpha = c.hcplx[0].x + c.hcplx[1].x;
-      const double beta = c.hscal[0];
+    enqueue(0);
+    for (int j = 0; j < m; j++) {
+      if (j + 1 < m) enqueue(j + 1);
+      MPSGPU_CUDA(cudaEventSynchronize(c.iter_ev[j]));
+      const double alpha = c.hsc->alpha[j];
+      const double beta = c.hsc->beta[j];
       MPSGPU_CHECK(std::isfinite(alpha) && std::isfinite(beta), MPSGPU_NAN, "lanczos: non-finite value");
       a.push_back(alpha);
       b.push_back(beta);
@@ -702,7 +704,6 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
       const double scale = std::max(normT, std::fabs(theta));
       if (res <= tol * scale || beta <= 1e-14 * scale || j + 1 == N) {
         conv = true;
-        j++;
         break;
       }
     }

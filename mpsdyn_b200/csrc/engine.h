@@ -59,6 +59,10 @@ struct Context {
   double* hscal = nullptr;     // pinned host mirror
   cplx* hcplx = nullptr;
   double* dS = nullptr;        // Ritz coefficients on device
+  LanczosScalars* dsc = nullptr;  // alpha/beta written by the fused kernels
+  LanczosScalars* hsc = nullptr;  // pinned host mirror
+  unsigned* dcounter = nullptr;   // last-block ticket of the fused reductions
+  std::vector<cudaEvent_t> iter_ev;  // one per Lanczos iteration in flight
   cudaEvent_t ev = nullptr;
   cudaEvent_t mv0 = nullptr, mv1 = nullptr;
   GemmProfiler prof;

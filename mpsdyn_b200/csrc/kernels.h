@@ -65,6 +65,20 @@ void cgemv_c(const Stream& st, int n, int k, const cplx* V, long long ldv, const
 // w += sign * V h  (h on device, length k; sign = -1 subtracts)
 void cgemv_n_sub(const Stream& st, int n, int k, const cplx* V, long long ldv, const cplx* h,
                  cplx* w, double sign = -1.0);
+// Lanczos coefficients written by the fused orthogonalisation kernels.
+struct LanczosScalars {
+  double alpha[256];
+  double beta[256];
+};
+// One reorthogonalised Lanczos step after the matvec (lanczos.cu): with
+// k = j+1 basis vectors V[:, 0..j] and w = H v_j,
+//   w <- w - V (V^H w) twice (classical Gram-Schmidt, two passes),
+//   sc->alpha[j] = Re(v_j^H H v_j), sc->beta[j] = ||w||,
+//   V[:, j+1] = w / beta_j when write_next.
+// counter: one device unsigned, zero on entry, left zero.
+void lanczos_orthonormalize(const Stream& st, int n, int j, cplx* V, long long ldv, cplx* w,
+                            bool write_next, LanczosScalars* sc, cplx* h1, cplx* h2,
+                            unsigned* counter, Scratch& scratch);
 // out[0] = ||x||_2 (deterministic two-stage reduction)
 void dznrm2(const Stream& st, int n, const cplx* x, double* out, Scratch& scratch);
 // y = x / (*nrm)   (device scalar)

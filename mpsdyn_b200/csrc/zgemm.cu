@@ -258,7 +258,7 @@ void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
   cplx* partial = nullptr;
   if (splits > 1)
     partial = (cplx*)scratch.get((size_t)splits * g.batch * (size_t)g.M * g.N * sizeof(cplx));
-  const bool prof = st.prof && st.prof->on;
+  const bool prof = st.prof && st.prof->sample();
   if (prof) {
     cudaEvent_t e0 = st.prof->next();
     if (e0) cudaEventRecord(e0, st.s);
