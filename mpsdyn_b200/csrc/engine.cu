@@ -1182,9 +1182,48 @@ void expectation_local(Context& c, const MpsDev& s, const double* op, double* ou
   mpo_free(c, one);
 }
 
-void schmidt_values(Context&, const MpsDev&, int, std::vector<double>&) {
-  throw Error(MPSGPU_INVALID, "schmidt_values: not built yet");
+// Contractor::getSchmidtValues (Contractor.cpp:2243-2270): eigenvalues of the
+// reduced density matrix of sites pos..L-1 (pos = 0 means L/2), ascending.
+// Here: left-canonical copy (gaugeCond R), right-canonicalise sites L-1..pos+1
+// with LQ moves, then the bond matrix L of the LQ of site pos carries the
+// Schmidt coefficients of bond (pos-1, pos); lambda = sigma^2.
+void schmidt_values(Context& c, const MpsDev& s, int pos, std::vector<double>& vals) {
+  const int L = s.L;
+  MPSGPU_CHECK(pos >= 0 && pos <= L, MPSGPU_BAD_SHAPE, "schmidt values: position out of range");
+  if (pos == L) {
+    vals.assign(1, 1.0);
+    return;
+  }
+  if (pos == 0) pos = L / 2;
+  MpsDev aux;
+  try {
+    mps_copy(c, s, aux);
+    mps_gauge_all(c, aux, 'R', true);
+    for (int p = L - 1; p > pos; p--) mps_gauge_site(c, aux, p, 'L', true, nullptr);
+    const int Dl = aux.dims[pos][1];
+    cplx r00;
+    const int K = site_factor(c, aux, pos, 'L', &r00);
+    // c.matR holds R' (K x Dl) with L = R'^H: same singular values
+    std::vector<double> sv = singular_values(c.st(), K, Dl, c.matR.p, K, c.scratch);
+    vals.resize(sv.size());
+    for (size_t i = 0; i < sv.size(); i++) vals[i] = sv[sv.size() - 1 - i] * sv[sv.size() - 1 - i];
+  } catch (...) {
+    mps_free(c, aux);
+    throw;
+  }
+  mps_free(c, aux);
 }
-double entropy(Context&, const MpsDev&, int) { throw Error(MPSGPU_INVALID, "entropy: not built yet"); }
+
+// Contractor::getEntropy (Contractor.cpp:2045-2076): -sum lambda log2 lambda
+// over |lambda| > 1e-12.
+double entropy(Context& c, const MpsDev& s, int pos) {
+  if (pos == s.L) return 0.0;
+  std::vector<double> lam;
+  schmidt_values(c, s, pos, lam);
+  double S = 0.0;
+  for (double t : lam)
+    if (std::fabs(t) > 1e-12) S += -t * std::log2(t);
+  return S;
+}
 
 }  // namespace mpsgpu

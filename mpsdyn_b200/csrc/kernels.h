@@ -106,6 +106,11 @@ void transpose_pqr_to_rqp(const Stream& st, int p, int q, int r, const cplx* in,
 void gaussian_site(const Stream& st, uint64_t seed, long long offset, int d, int Dl, int Dr,
                    cplx* dev);
 
+// Singular values (descending) of the m x n matrix A (device, ld lda) by
+// one-sided Jacobi (svd.cu); host-synchronous, A untouched.
+std::vector<double> singular_values(const Stream& st, int m, int n, const cplx* A, long long lda,
+                                    Scratch& scratch);
+
 // ---- Householder QR (LAPACK zgeqrf/zungqr conventions) ----
 // Factor the m x n column-major matrix A (ld = m; overwritten by R above and
 // the reflectors below the diagonal).  Q (m x K, ld = ldq) and R (K x n,

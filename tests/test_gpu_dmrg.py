@@ -139,6 +139,32 @@ def test_real_time_quench_observables(ctx, golden):
     np.testing.assert_allclose(en, golden["ising_L8_D8_quench_energies"], rtol=1e-10, atol=0)
 
 
+@pytest.mark.parametrize("pos", [0, 3, 5, 9])
+def test_schmidt_values_and_entropy_vs_oracle(ctx, pos):
+    m = mo.random_mps(9, 2, 6, 33)
+    s = ctx.mps(m.sites)
+    lam = ctx.schmidt_values(s, pos)
+    ref = mo.schmidt_values(m, pos)
+    assert lam.shape == ref.shape
+    np.testing.assert_allclose(lam, ref, rtol=0, atol=1e-12)
+    assert abs(ctx.entropy(s, pos) - mo.entropy(m, pos)) < 1e-10
+
+
+def test_quench_entropy_matches_reference(ctx, golden):
+    L, D = 8, 8
+    U = ctx.mpo(mo.ising_umpo(L, 1, 1.2, 0.1, 0.05, False))
+    st = ctx.mps(mo.product_mps(L, 2, 1).sites)
+    o = ctx.options(convtol=1e-10)
+    ent = []
+    for _ in range(10):
+        aux = st.copy()
+        ctx.optimize(U, aux, st, D, o)
+        aux.free()
+        st.gauge("L")
+        ent.append(ctx.entropy(st, L // 2))
+    np.testing.assert_allclose(ent, golden["ising_L8_D8_quench_entropy"], rtol=0, atol=1e-8)
+
+
 def test_expectation_values_vs_oracle(ctx):
     m = mo.random_mps(9, 2, 6, 21)
     s = ctx.mps(m.sites)
