@@ -58,6 +58,9 @@ typedef struct {
   int max_krylov;      /* Lanczos vectors per restart; 0 = 64 */
   int precision;       /* 0 = complex FP64 throughout */
   int verbose;         /* 1 = one line per half-sweep on stdout */
+  /* Optional: when *cancel_flag becomes non-zero (set by another host
+   * thread), the sweep stops between two site steps with MPSGPU_CANCELLED. */
+  const volatile int* cancel_flag;
 } mpsgpu_options;
 
 /* Counters of one solve (host-side; the flop count is algorithmic). */
@@ -171,6 +174,51 @@ mpsgpu_status mpsgpu_entropy(mpsgpu_context* ctx, const mpsgpu_mps* mps, int pos
  * most cap values (ascending), the count into *n. */
 mpsgpu_status mpsgpu_schmidt_values(mpsgpu_context* ctx, const mpsgpu_mps* mps,
                                     int pos, double* values, int cap, int* n);
+
+/* ---- solve server (continuous batching of independent requests) ---------
+ * Requests are ground-state solves of model chains.  The server owns
+ * `slots` worker threads, each with its own context (CUDA stream); a request
+ * starts when a slot is free and its HBM footprint fits in what the running
+ * requests leave of `hbm_budget_bytes` (admission in arrival order), so
+ * requests that arrive while others run are admitted as slots and memory
+ * free up and their device work overlaps.  State (MPO, MPS, environments,
+ * Lanczos basis) stays on the device for the whole solve. */
+typedef struct mpsgpu_server mpsgpu_server;
+
+typedef enum { MPSGPU_MODEL_ISING = 0, MPSGPU_MODEL_SCHWINGER = 1 } mpsgpu_model;
+
+typedef struct {
+  int model;         /* mpsgpu_model */
+  int L;             /* sites */
+  int D;             /* bond dimension */
+  double p0, p1, p2; /* Ising: J, g, h.  Schwinger: mu, x, alpha (l0 = 0) */
+  uint64_t seed;     /* initial MPS: mpsgpu_mps_random(L, 2, D, seed) */
+  double convtol;    /* 0 = 1e-10 */
+} mpsgpu_request;
+
+typedef struct {
+  uint64_t id;
+  int status;                /* mpsgpu_status */
+  double energy;
+  int rounds;
+  long long matvecs;
+  double flops;
+  double t_submit, t_start, t_end;  /* seconds since the server was created */
+  long long footprint_bytes;
+} mpsgpu_result;
+
+mpsgpu_status mpsgpu_server_create(int device, int slots, long long hbm_budget_bytes,
+                                   mpsgpu_server** out);
+mpsgpu_status mpsgpu_server_submit(mpsgpu_server* srv, const mpsgpu_request* req, uint64_t* id);
+/* Moves up to cap finished results into out (in completion order). */
+mpsgpu_status mpsgpu_server_poll(mpsgpu_server* srv, mpsgpu_result* out, int cap, int* n);
+/* Cancels a queued request, or stops a running one between two site steps. */
+mpsgpu_status mpsgpu_server_cancel(mpsgpu_server* srv, uint64_t id);
+/* Waits until no request is queued or running (timeout_s <= 0: no limit). */
+mpsgpu_status mpsgpu_server_drain(mpsgpu_server* srv, double timeout_s);
+/* Estimated device footprint of a request (the admission criterion). */
+long long mpsgpu_request_footprint(const mpsgpu_request* req);
+mpsgpu_status mpsgpu_server_destroy(mpsgpu_server* srv);
 
 /* ---- kernel-level entry points (host buffers, reference layouts) ---------
  * TensorMultiplier(Offset)::product (TensorMultiplier.cpp:61-93,

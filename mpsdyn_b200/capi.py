@@ -29,6 +29,8 @@ EXPORTS = [
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_expectation_local", "mpsgpu_entropy",
     "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_env_left", "mpsgpu_env_right",
     "mpsgpu_qr", "mpsgpu_lq", "mpsgpu_qr_device_noalloc",
+    "mpsgpu_server_create", "mpsgpu_server_submit", "mpsgpu_server_poll", "mpsgpu_server_cancel",
+    "mpsgpu_server_drain", "mpsgpu_request_footprint", "mpsgpu_server_destroy",
 ]
 
 
@@ -36,7 +38,7 @@ class Options(C.Structure):
     _fields_ = [
         ("convtol", C.c_double), ("eigtol", C.c_double), ("excorthtol", C.c_double),
         ("max_rounds", C.c_int), ("max_krylov", C.c_int), ("precision", C.c_int),
-        ("verbose", C.c_int),
+        ("verbose", C.c_int), ("cancel_flag", C.c_void_p),
     ]
 
 
@@ -351,3 +353,85 @@ def qr_device_noalloc(m: int, n: int, a_ptr: int, q_ptr: int, r_ptr: int, stream
     st = lib.mpsgpu_qr_device_noalloc(m, n, P(a_ptr), P(q_ptr or None), P(r_ptr or None), P(stream or None))
     if st != 0:
         raise MpsgpuError(st, "mpsgpu_qr_device_noalloc")
+
+
+class Request(C.Structure):
+    _fields_ = [("model", C.c_int), ("L", C.c_int), ("D", C.c_int), ("p0", C.c_double), ("p1", C.c_double),
+                ("p2", C.c_double), ("seed", C.c_uint64), ("convtol", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int), ("energy", C.c_double), ("rounds", C.c_int),
+                ("matvecs", C.c_longlong), ("flops", C.c_double), ("t_submit", C.c_double),
+                ("t_start", C.c_double), ("t_end", C.c_double), ("footprint_bytes", C.c_longlong)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+MODEL_ISING, MODEL_SCHWINGER = 0, 1
+
+
+class Server:
+    """mpsgpu_server: continuous batching of ground-state requests on one GPU."""
+
+    def __init__(self, device: int = 0, slots: int = 8, hbm_budget_bytes: int = 64 << 30):
+        self.lib = load()
+        P = C.c_void_p
+        self.lib.mpsgpu_server_create.argtypes = [C.c_int, C.c_int, C.c_longlong, C.POINTER(P)]
+        self.lib.mpsgpu_server_submit.argtypes = [P, C.POINTER(Request), C.POINTER(C.c_uint64)]
+        self.lib.mpsgpu_server_poll.argtypes = [P, C.POINTER(Result), C.c_int, C.POINTER(C.c_int)]
+        self.lib.mpsgpu_server_cancel.argtypes = [P, C.c_uint64]
+        self.lib.mpsgpu_server_drain.argtypes = [P, C.c_double]
+        self.lib.mpsgpu_server_destroy.argtypes = [P]
+        self.lib.mpsgpu_request_footprint.argtypes = [C.POINTER(Request)]
+        self.lib.mpsgpu_request_footprint.restype = C.c_longlong
+        h = P()
+        st = self.lib.mpsgpu_server_create(device, slots, hbm_budget_bytes, C.byref(h))
+        if st != 0:
+            raise MpsgpuError(st, "mpsgpu_server_create")
+        self.h = h
+
+    def submit(self, model: int, L: int, D: int, p0: float, p1: float, p2: float, seed: int,
+               convtol: float = 1e-10) -> int:
+        r = Request(model, L, D, p0, p1, p2, seed, convtol)
+        rid = C.c_uint64()
+        st = self.lib.mpsgpu_server_submit(self.h, C.byref(r), C.byref(rid))
+        if st != 0:
+            raise MpsgpuError(st, "mpsgpu_server_submit")
+        return rid.value
+
+    def footprint(self, model: int, L: int, D: int) -> int:
+        r = Request(model, L, D, 0, 0, 0, 0, 0)
+        return int(self.lib.mpsgpu_request_footprint(C.byref(r)))
+
+    def poll(self) -> list:
+        buf = (Result * 256)()
+        n = C.c_int()
+        out = []
+        while True:
+            st = self.lib.mpsgpu_server_poll(self.h, buf, 256, C.byref(n))
+            if st != 0:
+                raise MpsgpuError(st, "mpsgpu_server_poll")
+            out.extend(buf[i].as_dict() for i in range(n.value))
+            if n.value < 256:
+                return out
+
+    def cancel(self, rid: int) -> None:
+        st = self.lib.mpsgpu_server_cancel(self.h, rid)
+        if st != 0:
+            raise MpsgpuError(st, "mpsgpu_server_cancel")
+
+    def drain(self, timeout_s: float = 0.0) -> bool:
+        return self.lib.mpsgpu_server_drain(self.h, timeout_s) == 0
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mpsgpu_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

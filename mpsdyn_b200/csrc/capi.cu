@@ -53,6 +53,7 @@ SolveOptions to_opts(const mpsgpu_options* o) {
     s.max_rounds = o->max_rounds > 0 ? o->max_rounds : 1000;
     s.max_krylov = o->max_krylov > 0 ? o->max_krylov : 64;
     s.verbose = o->verbose;
+    s.cancel = o->cancel_flag;
   }
   return s;
 }

@@ -755,6 +755,7 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
   const cplx off = make_double2(offset, 0.0);
   try {
     while (!done) {
+      opt.check_cancel();
       calc_left(c, E, pos, &ops, init, init, &cnt);
       calc_right(c, E, pos, &ops, init, init, &cnt);
       const auto dims = init.dims[pos];

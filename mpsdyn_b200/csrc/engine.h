@@ -103,6 +103,12 @@ struct Counters {
 struct SolveOptions {
   double convtol = 1e-5, eigtol = 0.0, excorthtol = 0.0;
   int max_rounds = 1000, max_krylov = 64, verbose = 0;
+  // Raised by another host thread to stop a sweep between two site steps
+  // (MPSGPU_CANCELLED); nothing is in flight on the device when it returns.
+  const volatile int* cancel = nullptr;
+  void check_cancel() const {
+    if (cancel && *cancel) throw Error(MPSGPU_CANCELLED, "solve cancelled");
+  }
 };
 
 // ---- building blocks (device layout) ----
