@@ -231,6 +231,28 @@ mpsgpu_status mpsgpu_heff_matvec(mpsgpu_context* ctx, const int* ldims,
                                  const double* W, const int* rdims,
                                  const double* R, const double* x, double* y,
                                  double offset, int hermitian);
+/* Grouped matvec over many independent instances (the batched form of
+ * TensorMultiplier::product), all operands already on the device in the
+ * library's layouts:
+ *   L  (Dl, wl, Dl)  left environment (bra, w, ket), as the reference stores it
+ *   W  (d, wl, d, wr) MPO tensor, as the reference stores it
+ *   Rt (Dr, wr, Dr)  right environment in (ket, w, bra) order
+ *   x, y (Dl, d, Dr) site vector with the left bond fastest
+ * The three grouped launches (GEMM, MPO-leg contraction, GEMM) run once; with
+ * repeats > 0 they are captured in a CUDA graph and replayed `repeats` times,
+ * and *ms_per_run gets the device time per product (CUDA events).  *flops
+ * gets the algorithmic flops of one grouped product. */
+typedef struct {
+  int d, wl, wr, Dl, Dr;
+  const double* L;
+  const double* W;
+  const double* Rt;
+  const double* x;
+  double* y;
+} mpsgpu_heff_instance;
+mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgpu_heff_instance* inst,
+                                         int repeats, double* ms_per_run, double* flops);
+
 /* Operator::contractL / contractR (Operator.cpp:273-398): out gets
  * (Dr_bra, wr, Dr_ket) resp. (Dl_bra, wl, Dl_ket). */
 mpsgpu_status mpsgpu_env_left(mpsgpu_context* ctx, const int* tdims,

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmpsgpu.so")
 
-SOURCES = ["zgemm.cu", "blas1.cu", "lanczos.cu", "qr.cu", "svd.cu", "engine.cu", "capi.cu", "models.cpp", "server.cpp"]
+SOURCES = ["zgemm.cu", "blas1.cu", "lanczos.cu", "qr.cu", "svd.cu", "grouped.cu", "engine.cu", "capi.cu", "models.cpp", "server.cpp"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [
     "-std=c++17", "-O3",

@@ -27,7 +27,8 @@ EXPORTS = [
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
     "mpsgpu_mps_gauge", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_expectation_local", "mpsgpu_entropy",
-    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_env_left", "mpsgpu_env_right",
+    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped",
+    "mpsgpu_env_left", "mpsgpu_env_right",
     "mpsgpu_qr", "mpsgpu_lq", "mpsgpu_qr_device_noalloc",
     "mpsgpu_server_create", "mpsgpu_server_submit", "mpsgpu_server_poll", "mpsgpu_server_cancel",
     "mpsgpu_server_drain", "mpsgpu_request_footprint", "mpsgpu_server_destroy",
@@ -353,6 +354,27 @@ def qr_device_noalloc(m: int, n: int, a_ptr: int, q_ptr: int, r_ptr: int, stream
     st = lib.mpsgpu_qr_device_noalloc(m, n, P(a_ptr), P(q_ptr or None), P(r_ptr or None), P(stream or None))
     if st != 0:
         raise MpsgpuError(st, "mpsgpu_qr_device_noalloc")
+
+
+class HeffInstance(C.Structure):
+    _fields_ = [("d", C.c_int), ("wl", C.c_int), ("wr", C.c_int), ("Dl", C.c_int), ("Dr", C.c_int),
+                ("L", C.c_void_p), ("W", C.c_void_p), ("Rt", C.c_void_p), ("x", C.c_void_p), ("y", C.c_void_p)]
+
+
+def heff_matvec_grouped(ctx: "Context", instances: list, repeats: int = 0):
+    """mpsgpu_heff_matvec_grouped.  `instances`: dicts with d, wl, wr, Dl, Dr and
+    device pointers (integers) L, W, Rt, x, y in the library's layouts.
+    Returns (ms_per_run or None, flops per grouped product)."""
+    lib = ctx.lib
+    P = C.c_void_p
+    lib.mpsgpu_heff_matvec_grouped.argtypes = [P, C.c_int, C.POINTER(HeffInstance), C.c_int,
+                                               C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    arr = (HeffInstance * len(instances))()
+    for i, s in enumerate(instances):
+        arr[i] = HeffInstance(s["d"], s["wl"], s["wr"], s["Dl"], s["Dr"], s["L"], s["W"], s["Rt"], s["x"], s["y"])
+    ms, fl = C.c_double(), C.c_double()
+    ctx._check(lib.mpsgpu_heff_matvec_grouped(ctx.h, len(instances), arr, repeats, C.byref(ms), C.byref(fl)))
+    return (ms.value if repeats > 0 else None), fl.value
 
 
 class Request(C.Structure):

@@ -510,6 +510,58 @@ mpsgpu_status mpsgpu_heff_matvec(mpsgpu_context* ctx, const int* ldims, const do
   });
 }
 
+mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgpu_heff_instance* inst, int repeats,
+                                         double* ms_per_run, double* flops) {
+  if (!ctx || n <= 0 || !inst || repeats < 0) return MPSGPU_INVALID;
+  return guarded(ctx, [&] {
+    Context& c = ctx->c;
+    std::vector<HeffInstance> v(n);
+    for (int i = 0; i < n; i++) {
+      const auto& s = inst[i];
+      MPSGPU_CHECK(s.L && s.W && s.Rt && s.x && s.y, MPSGPU_INVALID, "grouped matvec: null pointer");
+      v[i].d = s.d; v[i].wl = s.wl; v[i].wr = s.wr; v[i].Dl = s.Dl; v[i].Dr = s.Dr;
+      v[i].L = (const cplx*)s.L; v[i].W = (const cplx*)s.W; v[i].Rt = (const cplx*)s.Rt;
+      v[i].x = (const cplx*)s.x; v[i].y = (cplx*)s.y;
+    }
+    int nsm = 148;
+    MPSGPU_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
+    GroupedMatvecPlan plan;
+    const Stream st = c.st();
+    grouped_matvec_plan(st, v, plan, nsm);
+    try {
+      grouped_matvec_run(st, plan);
+      if (flops) *flops = plan.flops;
+      if (repeats > 0) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        Stream cap = st;
+        cap.launches = nullptr;  // the captured launches are counted per replay below
+        MPSGPU_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        grouped_matvec_run(cap, plan);
+        MPSGPU_CUDA(cudaStreamEndCapture(c.stream, &graph));
+        MPSGPU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        MPSGPU_CUDA(cudaGraphLaunch(exec, c.stream));  // warm replay
+        MPSGPU_CUDA(cudaEventRecord(c.mv0, c.stream));
+        for (int r = 0; r < repeats; r++) MPSGPU_CUDA(cudaGraphLaunch(exec, c.stream));
+        MPSGPU_CUDA(cudaEventRecord(c.mv1, c.stream));
+        MPSGPU_CUDA(cudaEventSynchronize(c.mv1));
+        float ms = 0.f;
+        MPSGPU_CUDA(cudaEventElapsedTime(&ms, c.mv0, c.mv1));
+        if (ms_per_run) *ms_per_run = ms / repeats;
+        c.launches += 4LL * (repeats + 1);
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+      }
+      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    } catch (...) {
+      grouped_matvec_free(st, plan);
+      throw;
+    }
+    grouped_matvec_free(st, plan);
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
 static mpsgpu_status env_common(mpsgpu_context* ctx, bool left, const int* tdims, const double* T,
                                 const int* kdims, const double* ket, const int* wdims, const double* W,
                                 const int* bdims, const double* bra, double* out) {

@@ -1,0 +1,192 @@
+// Grouped effective-Hamiltonian matvec: y_i = L_i . W_i . R_i . x_i for many
+// independent instances of different shapes (bond dimensions, MPO bonds) in
+// three launches -- grouped GEMM (L.x), grouped MPO-leg contraction, grouped
+// GEMM (.R) -- each a persistent grid over the flattened tiles or pixels of
+// all instances.  The three launches can be captured once in a CUDA graph and
+// replayed.  Instances are scheduled largest first so that the tail of each
+// launch is filled by small tiles.
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mpsgpu {
+
+namespace {
+
+struct WGroup {
+  WContractArgs a;
+  long long pix_begin;
+};
+
+// Wm[(s' + du*c) + (du*wr)*(b + wl*s)] = W[s' + du*(b + wl*(s + dd*c))] for every instance
+struct WPerm {
+  const cplx* W;
+  cplx* Wm;
+  int du, wl, dd, wr;
+  long long begin;
+};
+
+__global__ void wperm_kernel(const WPerm* __restrict__ d, int n, long long total) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (d[mid].begin <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const WPerm& p = d[lo];
+    long long e = t - p.begin;
+    const int sp = (int)(e % p.du); e /= p.du;
+    const int b = (int)(e % p.wl); e /= p.wl;
+    const int s = (int)(e % p.dd); e /= p.dd;
+    const int c = (int)e;
+    p.Wm[(sp + p.du * c) + (long long)(p.du * p.wr) * (b + p.wl * s)] = p.W[t - p.begin];
+  }
+}
+
+template <int NIN>
+__global__ void wcontract_grouped_kernel(const WGroup* __restrict__ g, int n, long long total) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (g[mid].pix_begin <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const WContractArgs& a = g[lo].a;
+    const long long p = t - g[lo].pix_begin;
+    const int x = (int)(p % a.nx), y = (int)(p / a.nx);
+    const int nin = a.n_i0 * a.n_i1, nout = a.n_o0 * a.n_o1;
+    cplx in[NIN];
+    const cplx* ib = a.in + x * a.ix + y * a.iy;
+#pragma unroll
+    for (int i = 0; i < NIN; i++) {
+      if (i < nin) in[i] = ib[(i % a.n_i0) * a.si0 + (i / a.n_i0) * a.si1];
+      else in[i] = make_double2(0.0, 0.0);
+    }
+    cplx* ob = a.out + x * a.ox + y * a.oy;
+    for (int o = 0; o < nout; o++) {
+      cplx s = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int i = 0; i < NIN; i++)
+        if (i < nin) s = cadd(s, cmul(a.Wm[o + nout * i], in[i]));
+      ob[(o % a.n_o0) * a.so0 + (o / a.n_o0) * a.so1] = s;
+    }
+  }
+}
+
+}  // namespace
+
+GroupedMatvecPlan::~GroupedMatvecPlan() {}
+
+void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst, GroupedMatvecPlan& plan,
+                         int nsm) {
+  const int n = (int)inst.size();
+  MPSGPU_CHECK(n > 0, MPSGPU_INVALID, "grouped matvec: no instances");
+  // largest first
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  auto work = [&](int i) { return (double)inst[i].Dl * inst[i].Dr * (inst[i].Dl + inst[i].Dr) * inst[i].wl; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+  long long t1_total = 0, wm_total = 0, pix_total = 0, wel_total = 0;
+  for (const auto& h : inst) {
+    MPSGPU_CHECK(h.d > 0 && h.wl > 0 && h.wr > 0 && h.Dl > 0 && h.Dr > 0 && h.d * h.wl <= 32 && h.d * h.wr <= 32,
+                 MPSGPU_BAD_SHAPE, "grouped matvec: bad instance shape");
+    t1_total += (long long)h.Dl * h.wl * h.d * h.Dr;
+    wm_total += (long long)h.d * h.wl * h.d * h.wr;
+    pix_total += (long long)h.Dl * h.Dr;
+  }
+  wel_total = wm_total;
+  plan.n = n;
+  dbuf_alloc(st, plan.t1, t1_total);
+  dbuf_alloc(st, plan.t2, t1_total);
+  dbuf_alloc(st, plan.wm, wm_total);
+  std::vector<GroupedGemm> g1(n), g3(n);
+  std::vector<WGroup> wg(n);
+  std::vector<WPerm> wp(n);
+  long long o1 = 0, ow = 0, pix = 0;
+  int maxnin = 1;
+  for (int q = 0; q < n; q++) {
+    const int i = order[q];
+    const HeffInstance& h = inst[i];
+    const int d = h.d, wl = h.wl, wr = h.wr, Dl = h.Dl, Dr = h.Dr;
+    cplx* T1 = plan.t1.p + o1;
+    cplx* T2 = plan.t2.p + o1;
+    cplx* Wm = plan.wm.p + ow;
+    wp[q] = WPerm{h.W, Wm, d, wl, d, wr, ow};
+    GroupedGemm& a = g1[q];
+    a.M = Dl * wl; a.N = d * Dr; a.K = Dl;
+    a.A = h.L; a.lda = (long long)Dl * wl;
+    a.B = h.x; a.ldb = Dl;
+    a.C = T1; a.ldc = (long long)Dl * wl;
+    WContractArgs& w = wg[q].a;
+    w.nx = Dl; w.ny = Dr;
+    w.in = T1; w.ix = 1; w.iy = (long long)Dl * wl * d; w.si0 = Dl; w.si1 = (long long)Dl * wl;
+    w.n_i0 = wl; w.n_i1 = d;
+    w.out = T2; w.ox = 1; w.oy = (long long)Dl * d; w.so0 = Dl; w.so1 = (long long)Dl * d * Dr;
+    w.n_o0 = d; w.n_o1 = wr;
+    w.Wm = Wm;
+    wg[q].pix_begin = pix;
+    GroupedGemm& b = g3[q];
+    b.M = Dl * d; b.N = Dr; b.K = Dr * wr;
+    b.A = T2; b.lda = (long long)Dl * d;
+    b.B = h.Rt; b.ldb = (long long)Dr * wr;
+    b.C = h.y; b.ldc = (long long)Dl * d;
+    o1 += (long long)Dl * wl * d * Dr;
+    ow += (long long)d * wl * d * wr;
+    pix += (long long)Dl * Dr;
+    maxnin = std::max(maxnin, wl * d);
+    plan.flops += 8.0 * ((double)Dl * wl * Dl * d * Dr + (double)Dl * d * d * wl * wr * Dr +
+                         (double)Dl * d * Dr * wr * Dr);
+  }
+  plan.tiles1 = grouped_tiles(g1.data(), n);
+  plan.tiles3 = grouped_tiles(g3.data(), n);
+  plan.pixels = pix;
+  plan.wel = wel_total;
+  plan.maxnin = maxnin;
+  // descriptor tables in device memory
+  const size_t bytes = n * (2 * sizeof(GroupedGemm) + sizeof(WGroup) + sizeof(WPerm));
+  MPSGPU_CUDA(cudaMallocAsync(&plan.desc, bytes, st.s));
+  char* p = (char*)plan.desc;
+  plan.d_g1 = (GroupedGemm*)p; p += n * sizeof(GroupedGemm);
+  plan.d_g3 = (GroupedGemm*)p; p += n * sizeof(GroupedGemm);
+  plan.d_wg = p; p += n * sizeof(WGroup);
+  plan.d_wp = p;
+  MPSGPU_CUDA(cudaMemcpyAsync(plan.d_g1, g1.data(), n * sizeof(GroupedGemm), cudaMemcpyHostToDevice, st.s));
+  MPSGPU_CUDA(cudaMemcpyAsync(plan.d_g3, g3.data(), n * sizeof(GroupedGemm), cudaMemcpyHostToDevice, st.s));
+  MPSGPU_CUDA(cudaMemcpyAsync(plan.d_wg, wg.data(), n * sizeof(WGroup), cudaMemcpyHostToDevice, st.s));
+  MPSGPU_CUDA(cudaMemcpyAsync(plan.d_wp, wp.data(), n * sizeof(WPerm), cudaMemcpyHostToDevice, st.s));
+  MPSGPU_CUDA(cudaStreamSynchronize(st.s));
+  plan.ctas = nsm;
+}
+
+void grouped_matvec_run(const Stream& st, GroupedMatvecPlan& plan) {
+  // W leg matrices (cheap; part of every product so inputs stay the raw W)
+  wperm_kernel<<<std::min<long long>(ceil_div(plan.wel, 256), 4096), 256, 0, st.s>>>(
+      (const WPerm*)plan.d_wp, plan.n, plan.wel);
+  after_launch(st);
+  zgemm_grouped(st, plan.d_g1, plan.n, plan.tiles1, plan.ctas);
+  const int g = (int)std::min<long long>(ceil_div(plan.pixels, 128), 148LL * 16);
+  if (plan.maxnin <= 8) wcontract_grouped_kernel<8><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
+  else if (plan.maxnin <= 16) wcontract_grouped_kernel<16><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
+  else wcontract_grouped_kernel<32><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
+  after_launch(st);
+  zgemm_grouped(st, plan.d_g3, plan.n, plan.tiles3, plan.ctas);
+}
+
+void grouped_matvec_free(const Stream& st, GroupedMatvecPlan& plan) {
+  if (plan.desc) cudaFreeAsync(plan.desc, st.s);
+  plan.desc = nullptr;
+  for (DevMem* b : {&plan.t1, &plan.t2, &plan.wm})
+    if (b->p) {
+      cudaFreeAsync(b->p, st.s);
+      b->p = nullptr;
+    }
+}
+
+}  // namespace mpsgpu

@@ -46,6 +46,59 @@ struct GemmArgs {
 // C = alpha op(A) op(B) + beta Cin  (complex FP64, DMMA tensor pipe)
 void zgemm(const Stream& st, const GemmArgs& g, Scratch& scratch);
 
+// One GEMM C = A B (op N, N) of a grouped launch; tile_begin / tiles_m are
+// filled by grouped_tiles (64 x 64 tiles).
+struct GroupedGemm {
+  int M = 0, N = 0, K = 0;
+  const cplx* A = nullptr; long long lda = 0;
+  const cplx* B = nullptr; long long ldb = 0;
+  cplx* C = nullptr; long long ldc = 0;
+  long long tile_begin = 0;
+  int tiles_m = 0;
+};
+// Host: assigns tile ranges in order; returns the total number of tiles.
+long long grouped_tiles(GroupedGemm* descs, int n);
+// All tiles of n GEMMs (descriptors in device memory) in one persistent launch of `ctas` CTAs.
+void zgemm_grouped(const Stream& st, const GroupedGemm* d_descs, int n, long long total_tiles, int ctas);
+
+// ---- grouped effective-Hamiltonian matvec (grouped.cu) ----
+// One instance in device layouts: L (Dl, wl, Dl) = (bra, w, ket); W
+// (d, wl, d, wr) as the reference stores it; Rt (Dr, wr, Dr) = (ket, w, bra);
+// x, y (Dl, d, Dr) with the left bond fastest.
+struct HeffInstance {
+  int d = 0, wl = 0, wr = 0, Dl = 0, Dr = 0;
+  const cplx* L = nullptr;
+  const cplx* W = nullptr;
+  const cplx* Rt = nullptr;
+  const cplx* x = nullptr;
+  cplx* y = nullptr;
+};
+struct DevMem {
+  cplx* p = nullptr;
+  long long n = 0;
+};
+inline void dbuf_alloc(const Stream& st, DevMem& m, long long n) {
+  MPSGPU_CUDA(cudaMallocAsync((void**)&m.p, std::max<long long>(n, 1) * sizeof(cplx), st.s));
+  m.n = n;
+}
+struct GroupedMatvecPlan {
+  int n = 0;
+  DevMem t1, t2, wm;
+  void* desc = nullptr;
+  GroupedGemm* d_g1 = nullptr;
+  GroupedGemm* d_g3 = nullptr;
+  void* d_wg = nullptr;
+  void* d_wp = nullptr;
+  long long tiles1 = 0, tiles3 = 0, pixels = 0, wel = 0;
+  int maxnin = 1, ctas = 148;
+  double flops = 0.0;  // algorithmic flops of one grouped product
+  ~GroupedMatvecPlan();
+};
+void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst, GroupedMatvecPlan& plan,
+                         int nsm);
+void grouped_matvec_run(const Stream& st, GroupedMatvecPlan& plan);
+void grouped_matvec_free(const Stream& st, GroupedMatvecPlan& plan);
+
 // MPO-leg contraction: for every pixel (x, y) in [0,nx) x [0,ny)
 //   out[x*ox + y*oy + o0*so0 + o1*so1] =
 //       sum_{i0,i1} Wm[(o0 + n_o0*o1) + nout*(i0 + n_i0*i1)] in[x*ix + y*iy + i0*si0 + i1*si1]

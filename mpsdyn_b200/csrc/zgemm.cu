@@ -9,14 +9,18 @@
 // (src/core/cpp/Operator.cpp:273-387), the block-reflector updates of the
 // Householder QR and the absorption of R/L factors into neighbouring sites.
 //
-// Tiles: BM x BN complex per CTA, BK = 16 complex per stage, 4 warps in a
-// 2x2 grid, each warp a (BM/2)x(BN/2) tile of 8x8 DMMA fragments.  Complex
-// products are four real MMAs (re*re - im*im, re*im + im*re) accumulated in
-// FP64 registers.  Operands are staged through shared memory as separate
-// real/imaginary planes (padded rows: conflict-free fragment loads); the next
-// K-slab is prefetched into registers while the current one is consumed.
-// Large-K, small-MN problems are split over K into a workspace and reduced by
-// a second kernel that also applies the epilogue (deterministic order).
+// Tiles: BM x BN complex per CTA, BK = 16 complex per stage, a WMW x WNW grid
+// of warps, each warp a (BM/WMW) x (BN/WNW) tile of 8x8 DMMA fragments.
+// Complex products are four real MMAs accumulated in four independent FP64
+// register sets (re*re, -im*im, re*im, im*re), summed in the epilogue, so that
+// consecutive MMAs of a warp do not wait on each other's accumulators.
+// Operands are staged through shared memory as separate real/imaginary planes
+// (padded rows: conflict-free fragment loads); the next K-slab is prefetched
+// into registers while the current one is consumed.  Large-K, small-MN
+// problems are split over K into a workspace and reduced by a second kernel
+// that also applies the epilogue (deterministic order).  A grouped variant
+// runs the tiles of many independent GEMMs (different shapes) in one
+// persistent launch.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -40,62 +44,61 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <int BM, int BN, int OPA, int OPB>
-__global__ void __launch_bounds__(128)
-zgemm_dmma_kernel(GemmArgs g, int splits, int kchunk, cplx* __restrict__ partial) {
-  constexpr int WM = BM / 2, WN = BN / 2;
-  constexpr int MT = WM / 8, NT = WN / 8;
-  constexpr int AE = BM * BK / 128;  // complex elements per thread per slab
-  constexpr int BE = BN * BK / 128;
-  __shared__ double As_re[BK][BM + PAD], As_im[BK][BM + PAD];
-  __shared__ double Bs_re[BK][BN + PAD], Bs_im[BK][BN + PAD];
+template <int BM, int BN>
+struct TileSmem {
+  double A_re[BK][BM + PAD], A_im[BK][BM + PAD];
+  double B_re[BK][BN + PAD], B_im[BK][BN + PAD];
+};
 
+// One BM x BN output tile of op(A) op(B) over k in [kbeg, kend); result in
+// the caller's accumulators acc[i][j][set][h] (set: 0 re*re, 1 -im*im,
+// 2 re*im, 3 im*re).
+template <int BM, int BN, int WMW, int WNW, int OPA, int OPB>
+__device__ __forceinline__ void gemm_tile(const cplx* __restrict__ A, long long lda, const cplx* __restrict__ B,
+                                          long long ldb, int M, int N, int m0, int n0, int kbeg, int kend,
+                                          TileSmem<BM, BN>& sm,
+                                          double (&acc)[BM / WMW / 8][BN / WNW / 8][4][2]) {
+  constexpr int NT_ = WMW * WNW * 32;
+  constexpr int WM = BM / WMW, WN = BN / WNW;
+  constexpr int MT = WM / 8, NT = WN / 8;
+  constexpr int AE = BM * BK / NT_;
+  constexpr int BE = BN * BK / NT_;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  const int wm0 = (warp & 1) * WM, wn0 = (warp >> 1) * WN;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int zb = blockIdx.z / splits, zs = blockIdx.z % splits;
-  const int kbeg = zs * kchunk;
-  const int kend = min(g.K, kbeg + kchunk);
-
-  const cplx* A = g.A + (long long)zb * g.strideA;
-  const cplx* B = g.B + (long long)zb * g.strideB;
-
-  double acc_re[MT][NT][2], acc_im[MT][NT][2];
+  const int wm0 = (warp % WMW) * WM, wn0 = (warp / WMW) * WN;
 #pragma unroll
   for (int i = 0; i < MT; i++)
 #pragma unroll
-    for (int j = 0; j < NT; j++) {
-      acc_re[i][j][0] = acc_re[i][j][1] = 0.0;
-      acc_im[i][j][0] = acc_im[i][j][1] = 0.0;
-    }
+    for (int j = 0; j < NT; j++)
+#pragma unroll
+      for (int s = 0; s < 4; s++) acc[i][j][s][0] = acc[i][j][s][1] = 0.0;
 
   cplx ra[AE], rb[BE];
   auto load_slab = [&](int k0) {
 #pragma unroll
     for (int e = 0; e < AE; e++) {
-      int idx = tid + e * 128;
+      const int idx = tid + e * NT_;
       int m, k;
       if (OPA == OP_N) { m = idx % BM; k = idx / BM; }
       else { k = idx % BK; m = idx / BK; }
-      int gm = m0 + m, gk = k0 + k;
+      const int gm = m0 + m, gk = k0 + k;
       cplx v = make_double2(0.0, 0.0);
-      if (gm < g.M && gk < kend) {
-        long long off = (OPA == OP_N) ? (gm + (long long)gk * g.lda) : (gk + (long long)gm * g.lda);
+      if (gm < M && gk < kend) {
+        const long long off = (OPA == OP_N) ? (gm + (long long)gk * lda) : (gk + (long long)gm * lda);
         v = load_op<OPA>(A, off);
       }
       ra[e] = v;
     }
 #pragma unroll
     for (int e = 0; e < BE; e++) {
-      int idx = tid + e * 128;
+      const int idx = tid + e * NT_;
       int n, k;
       if (OPB == OP_N) { k = idx % BK; n = idx / BK; }
       else { n = idx % BN; k = idx / BN; }
-      int gn = n0 + n, gk = k0 + k;
+      const int gn = n0 + n, gk = k0 + k;
       cplx v = make_double2(0.0, 0.0);
-      if (gn < g.N && gk < kend) {
-        long long off = (OPB == OP_N) ? (gk + (long long)gn * g.ldb) : (gn + (long long)gk * g.ldb);
+      if (gn < N && gk < kend) {
+        const long long off = (OPB == OP_N) ? (gk + (long long)gn * ldb) : (gn + (long long)gk * ldb);
         v = load_op<OPB>(B, off);
       }
       rb[e] = v;
@@ -104,21 +107,21 @@ zgemm_dmma_kernel(GemmArgs g, int splits, int kchunk, cplx* __restrict__ partial
   auto store_slab = [&]() {
 #pragma unroll
     for (int e = 0; e < AE; e++) {
-      int idx = tid + e * 128;
+      const int idx = tid + e * NT_;
       int m, k;
       if (OPA == OP_N) { m = idx % BM; k = idx / BM; }
       else { k = idx % BK; m = idx / BK; }
-      As_re[k][m] = ra[e].x;
-      As_im[k][m] = ra[e].y;
+      sm.A_re[k][m] = ra[e].x;
+      sm.A_im[k][m] = ra[e].y;
     }
 #pragma unroll
     for (int e = 0; e < BE; e++) {
-      int idx = tid + e * 128;
+      const int idx = tid + e * NT_;
       int n, k;
       if (OPB == OP_N) { k = idx % BK; n = idx / BK; }
       else { n = idx % BN; k = idx / BN; }
-      Bs_re[k][n] = rb[e].x;
-      Bs_im[k][n] = rb[e].y;
+      sm.B_re[k][n] = rb[e].x;
+      sm.B_im[k][n] = rb[e].y;
     }
   };
 
@@ -134,60 +137,103 @@ zgemm_dmma_kernel(GemmArgs g, int splits, int kchunk, cplx* __restrict__ partial
       double are[MT], aim[MT], naim[MT], bre[NT], bim[NT];
 #pragma unroll
       for (int i = 0; i < MT; i++) {
-        are[i] = As_re[kk + fc][wm0 + i * 8 + fr];
-        aim[i] = As_im[kk + fc][wm0 + i * 8 + fr];
+        are[i] = sm.A_re[kk + fc][wm0 + i * 8 + fr];
+        aim[i] = sm.A_im[kk + fc][wm0 + i * 8 + fr];
         naim[i] = -aim[i];
       }
 #pragma unroll
       for (int j = 0; j < NT; j++) {
-        bre[j] = Bs_re[kk + fc][wn0 + j * 8 + fr];
-        bim[j] = Bs_im[kk + fc][wn0 + j * 8 + fr];
+        bre[j] = sm.B_re[kk + fc][wn0 + j * 8 + fr];
+        bim[j] = sm.B_im[kk + fc][wn0 + j * 8 + fr];
       }
 #pragma unroll
       for (int i = 0; i < MT; i++)
 #pragma unroll
         for (int j = 0; j < NT; j++) {
-          dmma(acc_re[i][j][0], acc_re[i][j][1], are[i], bre[j]);
-          dmma(acc_re[i][j][0], acc_re[i][j][1], naim[i], bim[j]);
-          dmma(acc_im[i][j][0], acc_im[i][j][1], are[i], bim[j]);
-          dmma(acc_im[i][j][0], acc_im[i][j][1], aim[i], bre[j]);
+          dmma(acc[i][j][0][0], acc[i][j][0][1], are[i], bre[j]);
+          dmma(acc[i][j][1][0], acc[i][j][1][1], naim[i], bim[j]);
+          dmma(acc[i][j][2][0], acc[i][j][2][1], are[i], bim[j]);
+          dmma(acc[i][j][3][0], acc[i][j][3][1], aim[i], bre[j]);
         }
     }
   }
+}
 
-  // Epilogue: accumulator element (r, c) of fragment (i, j):
-  // r = i*8 + lane/4, c = j*8 + 2*(lane%4) + h.
-  if (splits == 1) {
-    cplx* C = g.C + (long long)zb * g.strideC;
-    const cplx* Cin = g.Cin ? g.Cin + (long long)zb * g.strideCin : nullptr;
+// Epilogue for accumulator element (r, c) of fragment (i, j):
+// r = i*8 + lane/4, c = j*8 + 2*(lane%4) + h.
+template <int BM, int BN, int WMW, int WNW>
+__device__ __forceinline__ void tile_store(const double (&acc)[BM / WMW / 8][BN / WNW / 8][4][2], int M, int N,
+                                           int m0, int n0, cplx alpha, const cplx* Cin, long long ldcin,
+                                           cplx beta, cplx* C, long long ldc, bool raw) {
+  constexpr int WM = BM / WMW, WN = BN / WNW;
+  constexpr int MT = WM / 8, NT = WN / 8;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm0 = (warp % WMW) * WM, wn0 = (warp / WMW) * WN;
+  const int fr = lane >> 2, fc = lane & 3;
 #pragma unroll
-    for (int i = 0; i < MT; i++)
+  for (int i = 0; i < MT; i++)
 #pragma unroll
-      for (int j = 0; j < NT; j++)
+    for (int j = 0; j < NT; j++)
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-          int gm = m0 + wm0 + i * 8 + fr;
-          int gn = n0 + wn0 + j * 8 + 2 * fc + h;
-          if (gm < g.M && gn < g.N) {
-            cplx v = make_double2(acc_re[i][j][h], acc_im[i][j][h]);
-            cplx out = cmul(g.alpha, v);
-            if (Cin) out = cadd(out, cmul(g.beta, Cin[gm + (long long)gn * g.ldcin]));
-            C[gm + (long long)gn * g.ldc] = out;
+      for (int h = 0; h < 2; h++) {
+        const int gm = m0 + wm0 + i * 8 + fr;
+        const int gn = n0 + wn0 + j * 8 + 2 * fc + h;
+        if (gm < M && gn < N) {
+          const cplx v = make_double2(acc[i][j][0][h] + acc[i][j][1][h], acc[i][j][2][h] + acc[i][j][3][h]);
+          if (raw) {
+            C[gm + (long long)gn * ldc] = v;
+          } else {
+            cplx out = cmul(alpha, v);
+            if (Cin) out = cadd(out, cmul(beta, Cin[gm + (long long)gn * ldcin]));
+            C[gm + (long long)gn * ldc] = out;
           }
         }
+      }
+}
+
+template <int BM, int BN, int WMW, int WNW, int OPA, int OPB>
+__global__ void __launch_bounds__(WMW* WNW * 32)
+zgemm_dmma_kernel(GemmArgs g, int splits, int kchunk, cplx* __restrict__ partial) {
+  __shared__ TileSmem<BM, BN> sm;
+  double acc[BM / WMW / 8][BN / WNW / 8][4][2];
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int zb = blockIdx.z / splits, zs = blockIdx.z % splits;
+  const int kbeg = zs * kchunk;
+  const int kend = min(g.K, kbeg + kchunk);
+  gemm_tile<BM, BN, WMW, WNW, OPA, OPB>(g.A + (long long)zb * g.strideA, g.lda, g.B + (long long)zb * g.strideB,
+                                        g.ldb, g.M, g.N, m0, n0, kbeg, kend, sm, acc);
+  if (splits == 1) {
+    tile_store<BM, BN, WMW, WNW>(acc, g.M, g.N, m0, n0, g.alpha,
+                                 g.Cin ? g.Cin + (long long)zb * g.strideCin : nullptr, g.ldcin, g.beta,
+                                 g.C + (long long)zb * g.strideC, g.ldc, false);
   } else {
     cplx* P = partial + ((long long)zs * g.batch + zb) * (long long)g.M * g.N;
-#pragma unroll
-    for (int i = 0; i < MT; i++)
-#pragma unroll
-      for (int j = 0; j < NT; j++)
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          int gm = m0 + wm0 + i * 8 + fr;
-          int gn = n0 + wn0 + j * 8 + 2 * fc + h;
-          if (gm < g.M && gn < g.N)
-            P[gm + (long long)gn * g.M] = make_double2(acc_re[i][j][h], acc_im[i][j][h]);
-        }
+    tile_store<BM, BN, WMW, WNW>(acc, g.M, g.N, m0, n0, g.alpha, nullptr, 0, g.beta, P, g.M, true);
+  }
+}
+
+// Grouped GEMMs (op N, N): descriptor d covers tiles [tile_begin(d), tile_begin(d+1)).
+template <int BM, int BN, int WMW, int WNW>
+__global__ void __launch_bounds__(WMW* WNW * 32)
+zgemm_grouped_kernel(const GroupedGemm* __restrict__ descs, int ndesc, long long total_tiles) {
+  __shared__ TileSmem<BM, BN> sm;
+  double acc[BM / WMW / 8][BN / WNW / 8][4][2];
+  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    // binary search for the descriptor owning tile t
+    int lo = 0, hi = ndesc - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (descs[mid].tile_begin <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const GroupedGemm& d = descs[lo];
+    const long long local = t - d.tile_begin;
+    const int tm = (int)(local % d.tiles_m), tn = (int)(local / d.tiles_m);
+    const int m0 = tm * BM, n0 = tn * BN;
+    gemm_tile<BM, BN, WMW, WNW, OP_N, OP_N>(d.A, d.lda, d.B, d.ldb, d.M, d.N, m0, n0, 0, d.K, sm, acc);
+    tile_store<BM, BN, WMW, WNW>(acc, d.M, d.N, m0, n0, make_double2(1.0, 0.0), nullptr, 0,
+                                 make_double2(0.0, 0.0), d.C, d.ldc, false);
+    __syncthreads();
   }
 }
 
@@ -207,14 +253,15 @@ __global__ void splitk_reduce_kernel(GemmArgs g, int splits, const cplx* __restr
   }
 }
 
-template <int BM, int BN>
+template <int BM, int BN, int WMW, int WNW>
 void launch_tiles(const Stream& st, const GemmArgs& g, int splits, int kchunk, cplx* partial) {
   dim3 grid(ceil_div(g.M, BM), ceil_div(g.N, BN), g.batch * splits);
-#define MPSGPU_GEMM_CASE(oa, ob)                                                        \
-  if (g.opA == oa && g.opB == ob) {                                                     \
-    zgemm_dmma_kernel<BM, BN, oa, ob><<<grid, 128, 0, st.s>>>(g, splits, kchunk, partial); \
-    after_launch(st);                                                                   \
-    return;                                                                             \
+  const int threads = WMW * WNW * 32;
+#define MPSGPU_GEMM_CASE(oa, ob)                                                                    \
+  if (g.opA == oa && g.opB == ob) {                                                                 \
+    zgemm_dmma_kernel<BM, BN, WMW, WNW, oa, ob><<<grid, threads, 0, st.s>>>(g, splits, kchunk, partial); \
+    after_launch(st);                                                                               \
+    return;                                                                                         \
   }
   MPSGPU_GEMM_CASE(OP_N, OP_N)
   MPSGPU_GEMM_CASE(OP_N, OP_T)
@@ -228,11 +275,6 @@ void launch_tiles(const Stream& st, const GemmArgs& g, int splits, int kchunk, c
 
 }  // namespace
 
-size_t zgemm_workspace_bytes(const GemmArgs& g) {
-  // Upper bound used by the split-K path (splits <= 8).
-  return (size_t)8 * g.batch * (size_t)g.M * g.N * sizeof(cplx);
-}
-
 void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
   GemmArgs g = g0;
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
@@ -245,7 +287,8 @@ void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
     after_launch(st);
     return;
   }
-  // Tile choice: large tiles when they already fill the GPU, otherwise 32x32.
+  // Tile choice: 64x64 (8 warps) when that already fills the GPU, otherwise
+  // 32x32 (4 warps) plus a split over K.
   const long long target = 2 * 148;
   long long ctas64 = (long long)ceil_div(g.M, 64) * ceil_div(g.N, 64) * g.batch;
   bool big = ctas64 >= target;
@@ -263,8 +306,8 @@ void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
     cudaEvent_t e0 = st.prof->next();
     if (e0) cudaEventRecord(e0, st.s);
   }
-  if (big) launch_tiles<64, 64>(st, g, splits, kchunk, partial);
-  else launch_tiles<32, 32>(st, g, splits, kchunk, partial);
+  if (big) launch_tiles<64, 64, 2, 4>(st, g, splits, kchunk, partial);
+  else launch_tiles<32, 32, 2, 2>(st, g, splits, kchunk, partial);
   if (splits > 1) {
     long long total = (long long)g.M * g.N * g.batch;
     splitk_reduce_kernel<<<std::min<long long>(ceil_div(total, 256), 4096), 256, 0, st.s>>>(g, splits, partial);
@@ -276,6 +319,23 @@ void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
     st.prof->flops += 8.0 * (double)g.M * g.N * g.K * g.batch;
     st.prof->calls++;
   }
+}
+
+long long grouped_tiles(GroupedGemm* descs, int n) {
+  long long t = 0;
+  for (int i = 0; i < n; i++) {
+    descs[i].tiles_m = ceil_div(descs[i].M, 64);
+    const int tiles_n = ceil_div(descs[i].N, 64);
+    descs[i].tile_begin = t;
+    t += (long long)descs[i].tiles_m * tiles_n;
+  }
+  return t;
+}
+
+void zgemm_grouped(const Stream& st, const GroupedGemm* d_descs, int n, long long total_tiles, int ctas) {
+  if (n <= 0 || total_tiles <= 0) return;
+  zgemm_grouped_kernel<64, 64, 2, 4><<<ctas, 256, 0, st.s>>>(d_descs, n, total_tiles);
+  after_launch(st);
 }
 
 }  // namespace mpsgpu
