@@ -1065,6 +1065,12 @@ void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, i
       heff_apply(c, E.Le[pos].p, ld, ops, pos, false, E.Re[pos].p, rd, orig.A[pos].p, M.p, make_double2(0, 0), &cnt);
       // solveSiteGauge (Contractor.cpp:921-936): newA = M / |M|
       dznrm2(c.st(), (int)nM, M.p, dn, c.scratch);
+      if (opt.verbose > 1) {
+        double h = 0;
+        MPSGPU_CUDA(cudaMemcpyAsync(&h, dn, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+        printf("mpsgpu: optimize round %d pos %d M (%d,%d,%d) |M| %.17g\n", round, pos, du, ld[0], rd[2], h);
+      }
       init.dims[pos] = {du, ld[0], rd[2]};
       dbuf_reserve(c, init.A[pos], nM);
       zscal_inv(c.st(), (int)nM, M.p, dn, init.A[pos].p);
@@ -1088,6 +1094,7 @@ void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, i
         MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
         c1 = c.hcplx[0];
         c2 = c.hcplx[1];
+        if (opt.verbose) printf("mpsgpu: optimize round %d pos %d c1 %.17g c2 %.17g%+.17gi\n", round, pos, c1.x, c2.x, c2.y);
         done = check_distance(distance, c1, c2, init.normfact, orig.normfact, opt.convtol);
         if (!done) {
           if (right) { mps_gauge_site(c, init, pos, 'L', false, &cnt); if (pos > 0) pos--; }

@@ -44,6 +44,61 @@ __device__ double block_sum(double v, double* red) {
   return s;
 }
 
+__device__ double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int w = 0; w < nw; w++) s = fmax(s, red[w]);
+  return s;
+}
+
+// 2-norm of x[0..n) without underflow or overflow of the squares: the
+// entries are divided by the largest component magnitude before squaring
+// (the scaled sum of LAPACK's dznrm2).  Rank-deficient sites produce
+// trailing columns with entries far below 1e-154, whose plain squares
+// underflow to zero.  Every thread of the block gets the result.
+__device__ double block_scaled_norm(int n, const cplx* x, double* red) {
+  double mx = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) mx = fmax(mx, fmax(fabs(x[r].x), fabs(x[r].y)));
+  mx = block_max(mx, red);
+  if (mx == 0.0) return 0.0;
+  const double inv = 1.0 / mx;
+  double part = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const double a = x[r].x * inv, b = x[r].y * inv;
+    part += a * a + b * b;
+  }
+  return mx * sqrt(block_sum(part, red));
+}
+
+// sqrt(a^2 + b^2 + c^2) with the largest magnitude factored out (dlapy3).
+__device__ __forceinline__ double hypot3(double a, double b, double c) {
+  a = fabs(a); b = fabs(b); c = fabs(c);
+  const double w = fmax(a, fmax(b, c));
+  if (w == 0.0) return 0.0;
+  a /= w; b /= w; c /= w;
+  return w * sqrt(a * a + b * b + c * c);
+}
+
+// 1 / z by Smith's algorithm (R. L. Smith, "Algorithm 116: Complex
+// division", CACM 5(8), 1962), which never squares |z|.
+__device__ __forceinline__ cplx recip_smith(cplx z) {
+  if (fabs(z.x) >= fabs(z.y)) {
+    const double r = z.y / z.x, t = 1.0 / (z.x + z.y * r);
+    return make_double2(t, -r * t);
+  }
+  const double r = z.x / z.y, t = 1.0 / (z.y + z.x * r);
+  return make_double2(r * t, -t);
+}
+
+// Smallest |beta| handled without rescaling: the underflow threshold divided
+// by the machine epsilon (LAPACK zlarfg's SAFMIN = dlamch('S') / dlamch('E')).
+constexpr double kSafeMin = 2.2250738585072014e-308 / 1.1102230246251565e-16;
+
 // Apply (I - V T' V^H) to the mp x cw column slice C (shared, ld = mp), where
 // V (mp x jb, unit lower trapezoidal) and T (jb x jb) are in global memory
 // and T' = T^H (conjT = true, for Q^H A) or T (for Q E).  W is jb x cw shared.
@@ -122,29 +177,45 @@ __global__ void __launch_bounds__(QR_THREADS) qr_factor_kernel(QrParams p) {
       }
       __syncthreads();
       for (int c = 0; c < jb; c++) {
-        // reflector of column c, rows c..mp-1
-        double part = 0.0;
-        for (int r = c + 1 + threadIdx.x; r < mp; r += blockDim.x) part += cabs2(P[r + c * mp]);
-        double xn2 = block_sum(part, red);
+        // reflector of column c, rows c..mp-1 (block-uniform control flow:
+        // every thread holds the same norms, alpha and beta)
+        cplx* x = P + (c + 1) + c * mp;
+        const int nx = mp - c - 1;
+        double xnorm = block_scaled_norm(nx, x, red);
         cplx alpha = P[c + c * mp];
         cplx tau, scale;
-        bool ident = (xn2 == 0.0 && alpha.y == 0.0);
+        bool ident = (xnorm == 0.0 && alpha.y == 0.0);
         double beta = 0.0;
         if (ident) {
           tau = make_double2(0.0, 0.0);
           scale = make_double2(0.0, 0.0);
         } else {
-          double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+          double nrm = hypot3(alpha.x, alpha.y, xnorm);
           beta = alpha.x >= 0.0 ? -nrm : nrm;
+          // |beta| below kSafeMin: scale the column up (at most 20 times)
+          // so that 1 / (alpha - beta) stays finite; beta is scaled back
+          // at the end, tau and v are scale-invariant
+          int knt = 0;
+          while (fabs(beta) < kSafeMin && knt < 20) {
+            __syncthreads();
+            for (int r = threadIdx.x; r < nx; r += blockDim.x) x[r] = cscale(x[r], 1.0 / kSafeMin);
+            beta /= kSafeMin;
+            alpha = cscale(alpha, 1.0 / kSafeMin);
+            knt++;
+          }
+          if (knt > 0) {
+            __syncthreads();
+            xnorm = block_scaled_norm(nx, x, red);
+            nrm = hypot3(alpha.x, alpha.y, xnorm);
+            beta = alpha.x >= 0.0 ? -nrm : nrm;
+          }
           tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-          // scale = 1 / (alpha - beta)
-          cplx den = make_double2(alpha.x - beta, alpha.y);
-          double dd = cabs2(den);
-          scale = make_double2(den.x / dd, -den.y / dd);
+          scale = recip_smith(make_double2(alpha.x - beta, alpha.y));
+          for (int k = 0; k < knt; k++) beta *= kSafeMin;
         }
         __syncthreads();
         if (!ident) {
-          for (int r = c + 1 + threadIdx.x; r < mp; r += blockDim.x) P[r + c * mp] = cmul(P[r + c * mp], scale);
+          for (int r = threadIdx.x; r < nx; r += blockDim.x) x[r] = cmul(x[r], scale);
         }
         __syncthreads();
         if (threadIdx.x == 0) {

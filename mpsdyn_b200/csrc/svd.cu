@@ -95,11 +95,24 @@ __global__ void __launch_bounds__(JT) jacobi_sv_kernel(int m, int n, cplx* A, do
     if (!rotated) break;
     __syncthreads();
   }
+  // column norms with the largest magnitude factored out, so that singular
+  // values below 1e-154 (squares below the FP64 normal range) keep their
+  // relative accuracy
   for (int col = warp; col < n; col += nw) {
+    const cplx* a = A + (long long)col * m;
+    double mx = 0.0;
+    for (int r = lane; r < m; r += 32) mx = fmax(mx, fmax(fabs(a[r].x), fabs(a[r].y)));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     double s = 0.0;
-    for (int r = lane; r < m; r += 32) s += cabs2(A[(long long)col * m + r]);
+    if (mx > 0.0) {
+      const double inv = 1.0 / mx;
+      for (int r = lane; r < m; r += 32) {
+        const double u = a[r].x * inv, v = a[r].y * inv;
+        s += u * u + v * v;
+      }
+    }
     s = warp_sumd(s);
-    if (lane == 0) out[col] = sqrt(s);
+    if (lane == 0) out[col] = mx * sqrt(s);
   }
   if (threadIdx.x == 0) status[0] = sweep < MAX_SWEEPS ? sweep + 1 : MAX_SWEEPS + 1;
 }

@@ -165,6 +165,40 @@ def test_quench_entropy_matches_reference(ctx, golden):
     np.testing.assert_allclose(ent, golden["ising_L8_D8_quench_entropy"], rtol=0, atol=1e-8)
 
 
+def test_zero_padded_gauge_matches_oracle(ctx):
+    # a product state zero-padded to D=64 (what optimize sees for a D=1 start)
+    m = mo.product_mps(16, 2, 1)
+    mo.increase_bond_dimension(m, 64)
+    s = ctx.mps(m.sites)
+    ref = m.copy()
+    for d_ in ("R", "L"):
+        s.gauge(d_)
+        mo.gauge_cond_all(ref, d_, True)
+        sites, _ = s.download()
+        for k, (a, b) in enumerate(zip(sites, ref.sites)):
+            assert a.shape == b.shape, (d_, k)
+            assert np.all(np.isfinite(a)), (d_, k)
+            assert np.abs(a - b).max() < 1e-12, (d_, k, np.abs(a - b).max())
+
+
+def test_quench_from_product_state_D64_vs_oracle(ctx):
+    # the optimised sites are rank-deficient: their LQ meets trailing columns
+    # with entries far below 1e-154, whose plain squares underflow
+    L, D = 16, 64
+    U = ctx.mpo(mo.ising_umpo(L, 1, 1.0, 0.1, 0.01, False))
+    st = ctx.mps(mo.product_mps(L, 2, 1).sites)
+    ref = mo.product_mps(L, 2, 1)
+    Ur = mo.ising_umpo(L, 1, 1.0, 0.1, 0.01, False)
+    o = ctx.options(convtol=1e-10)
+    for _ in range(2):
+        aux = st.copy()
+        ctx.optimize(U, aux, st, D, o)
+        aux.free()
+        raux = ref.copy()
+        mo.optimize(Ur, raux, ref, D, convtol=1e-10)
+        assert abs(ctx.expectation_local(st, mo.SIGX)[L // 2] - mo.expectation_values(ref, mo.SIGX)[L // 2]) < 1e-8
+
+
 def test_expectation_values_vs_oracle(ctx):
     m = mo.random_mps(9, 2, 6, 21)
     s = ctx.mps(m.sites)
