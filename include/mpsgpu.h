@@ -123,6 +123,12 @@ mpsgpu_status mpsgpu_mps_upload(mpsgpu_context* ctx, int L, const int* dims,
  * counter stream (entry i of the chain uses draws 2i, 2i+1, Box-Muller). */
 mpsgpu_status mpsgpu_mps_random(mpsgpu_context* ctx, int L, int d, int D,
                                 uint64_t seed, mpsgpu_mps** out);
+/* The same sites right-gauged one after another as MPS::setRandomState
+ * does (src/core/cpp/MPS.cpp:282-294): a normalised chain of random
+ * isometries, safe from overflow at any L (the raw Gaussian chain above
+ * grows like (d D)^(L/2)). */
+mpsgpu_status mpsgpu_mps_random_state(mpsgpu_context* ctx, int L, int d, int D,
+                                      uint64_t seed, mpsgpu_mps** out);
 /* MPS(L,D,d) of the reference (src/core/cpp/MPS.cpp:15-35): element (0,0,0)
  * of every site is 1, bonds D (D=1: the product state |0...0>). */
 mpsgpu_status mpsgpu_mps_product(mpsgpu_context* ctx, int L, int d, int D,
@@ -136,6 +142,24 @@ mpsgpu_status mpsgpu_mps_download(mpsgpu_context* ctx, const mpsgpu_mps* mps,
 mpsgpu_status mpsgpu_mps_free(mpsgpu_context* ctx, mpsgpu_mps* mps);
 /* MPS::gaugeCond(dir, normal=true) (src/core/cpp/MPS.cpp:306-364). */
 mpsgpu_status mpsgpu_mps_gauge(mpsgpu_context* ctx, mpsgpu_mps* mps, char dir);
+/* MPS(const MPS& src, int D) (src/core/cpp/MPS.cpp:761-772): a copy cut to
+ * bond dimension D by right-to-left SVDs (gaugeCond('L', 0, D), Site::gaugeL
+ * with cutD, wrapper::svd with tol 0: zero singular values are dropped too).
+ * The norm stays in normfact.  discarded (nullable) receives the sum over
+ * the cut bonds of the squares of the dropped singular values, which the
+ * reference does not report. */
+mpsgpu_status mpsgpu_mps_approximate(mpsgpu_context* ctx, const mpsgpu_mps* src,
+                                     int D, mpsgpu_mps** out, double* discarded);
+/* MPO applied to an MPS site by site with an SVD gauge move after each site
+ * (src/core/cpp/MPS.cpp:858-936, Site::reduceDimLOp/ROp, Site.cpp:303-402):
+ * D <= 0 is MPS::applyExactly(ops, dagger, dir) (no cut beyond dropping
+ * zero singular values), D > 0 is MPS::truncate(ops, src, D, dagger, dir) /
+ * MPS::approximate.  dagger applies ops^dagger; dir 'L' sweeps from the
+ * right end (result right-gauged), 'R' from the left end. */
+mpsgpu_status mpsgpu_mps_apply_mpo(mpsgpu_context* ctx, const mpsgpu_mpo* ops,
+                                   const mpsgpu_mps* src, int D, int dagger,
+                                   char dir, mpsgpu_mps** out,
+                                   double* discarded);
 
 /* ---- Contractor (src/core/headers/Contractor.h:46-604) ------------------- */
 /* findGroundState(ops, D, &lambda, init, offset) (Contractor.cpp:1352-1533). */
@@ -192,7 +216,7 @@ typedef struct {
   int L;             /* sites */
   int D;             /* bond dimension */
   double p0, p1, p2; /* Ising: J, g, h.  Schwinger: mu, x, alpha (l0 = 0) */
-  uint64_t seed;     /* initial MPS: mpsgpu_mps_random(L, 2, D, seed) */
+  uint64_t seed;     /* initial MPS: mpsgpu_mps_random_state(L, 2, D, seed) */
   double convtol;    /* 0 = 1e-10 */
 } mpsgpu_request;
 

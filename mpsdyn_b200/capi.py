@@ -23,9 +23,9 @@ EXPORTS = [
     "mpsgpu_last_error", "mpsgpu_launch_count", "mpsgpu_synchronize", "mpsgpu_get_stream",
     "mpsgpu_profile_begin", "mpsgpu_profile_end", "mpsgpu_mpo_upload",
     "mpsgpu_mpo_free", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger",
-    "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_product",
+    "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_random_state", "mpsgpu_mps_product",
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
-    "mpsgpu_mps_gauge", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
+    "mpsgpu_mps_gauge", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_expectation_local", "mpsgpu_entropy",
     "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped",
     "mpsgpu_env_left", "mpsgpu_env_right",
@@ -78,6 +78,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         lib.mpsgpu_launch_count.argtypes = [P]
         lib.mpsgpu_default_options.argtypes = [C.POINTER(Options)]
         lib.mpsgpu_mps_random.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]
+        lib.mpsgpu_mps_random_state.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]
         lib.mpsgpu_find_ground_state.argtypes = [P, P, C.c_int, C.c_double, C.POINTER(Options), P,
                                                  C.POINTER(C.c_double), C.POINTER(Stats)]
         lib.mpsgpu_find_next_excited_state.argtypes = [P, P, C.c_int, C.POINTER(P), C.c_int, C.c_double,
@@ -89,6 +90,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         lib.mpsgpu_heff_matvec.argtypes = [P, P, P, P, P, P, P, P, P, C.c_double, C.c_int]
         lib.mpsgpu_entropy.argtypes = [P, P, C.c_int, C.POINTER(C.c_double)]
         lib.mpsgpu_mps_gauge.argtypes = [P, P, C.c_char]
+        lib.mpsgpu_mps_approximate.argtypes = [P, P, C.c_int, C.POINTER(P), C.POINTER(C.c_double)]
+        lib.mpsgpu_mps_apply_mpo.argtypes = [P, P, P, C.c_int, C.c_int, C.c_char, C.POINTER(P),
+                                             C.POINTER(C.c_double)]
         D_ = C.c_double
         lib.mpsgpu_mpo_ising.argtypes = [P, C.c_int, D_, D_, D_, C.POINTER(P)]
         lib.mpsgpu_mpo_ising_evolution.argtypes = [P, C.c_int, D_, D_, D_, D_, C.c_int, C.POINTER(P)]
@@ -191,6 +195,12 @@ class Context:
     def mps_random(self, L: int, d: int, D: int, seed: int) -> "DeviceMPS":
         h = C.c_void_p()
         self._check(self.lib.mpsgpu_mps_random(self.h, L, d, D, C.c_uint64(seed), C.byref(h)))
+        return DeviceMPS(self, h)
+
+    def mps_random_state(self, L: int, d: int, D: int, seed: int) -> "DeviceMPS":
+        """MPS::setRandomState: the random sites right-gauged, norm 1."""
+        h = C.c_void_p()
+        self._check(self.lib.mpsgpu_mps_random_state(self.h, L, d, D, C.c_uint64(seed), C.byref(h)))
         return DeviceMPS(self, h)
 
     def mps_product(self, L: int, d: int, D: int) -> "DeviceMPS":
@@ -337,6 +347,20 @@ class DeviceMPS:
 
     def gauge(self, direction: str) -> None:
         self.ctx._check(self.ctx.lib.mpsgpu_mps_gauge(self.ctx.h, self.h, direction.encode()))
+
+    def approximate(self, D: int):
+        """MPS(self, D): a copy cut to bond D; returns (DeviceMPS, discarded weight)."""
+        h, disc = C.c_void_p(), C.c_double()
+        self.ctx._check(self.ctx.lib.mpsgpu_mps_approximate(self.ctx.h, self.h, D, C.byref(h), C.byref(disc)))
+        return DeviceMPS(self.ctx, h), disc.value
+
+    def apply_mpo(self, ops: "DeviceMPO", D: int = 0, dagger: bool = False, direction: str = "L"):
+        """ops|self> applied exactly (D <= 0) or cut to D (MPS::truncate);
+        returns (DeviceMPS, discarded weight)."""
+        h, disc = C.c_void_p(), C.c_double()
+        self.ctx._check(self.ctx.lib.mpsgpu_mps_apply_mpo(self.ctx.h, ops.h, self.h, D, int(dagger),
+                                                          direction.encode(), C.byref(h), C.byref(disc)))
+        return DeviceMPS(self.ctx, h), disc.value
 
     def free(self) -> None:
         if self.h:

@@ -174,7 +174,7 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   if (!ctx) return MPSGPU_INVALID;
   Context& c = ctx->c;
   cudaSetDevice(c.device);
-  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lanV, &c.lanW}) dbuf_free(c, *b);
+  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lanV, &c.lanW, &c.lanT, &c.lanQ}) dbuf_free(c, *b);
   c.scratch.release();
   c.qrws.release();
   if (c.stream) cudaStreamSynchronize(c.stream);
@@ -321,6 +321,11 @@ mpsgpu_status mpsgpu_mps_random(mpsgpu_context* ctx, int L, int d, int D, uint64
   return new_mps(ctx, out, [&](MpsDev& s) { mps_random(ctx->c, s, L, d, D, seed); });
 }
 
+mpsgpu_status mpsgpu_mps_random_state(mpsgpu_context* ctx, int L, int d, int D, uint64_t seed,
+                                      mpsgpu_mps** out) {
+  return new_mps(ctx, out, [&](MpsDev& s) { mps_random_state(ctx->c, s, L, d, D, seed); });
+}
+
 mpsgpu_status mpsgpu_mps_product(mpsgpu_context* ctx, int L, int d, int D, mpsgpu_mps** out) {
   return new_mps(ctx, out, [&](MpsDev& s) { mps_product(ctx->c, s, L, d, D); });
 }
@@ -358,6 +363,30 @@ mpsgpu_status mpsgpu_mps_gauge(mpsgpu_context* ctx, mpsgpu_mps* mps, char dir) {
   return guarded(ctx, [&] {
     mps_gauge_all(ctx->c, mps->s, d, true);
     MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+mpsgpu_status mpsgpu_mps_approximate(mpsgpu_context* ctx, const mpsgpu_mps* src, int D, mpsgpu_mps** out,
+                                     double* discarded) {
+  if (!src || D <= 0) return MPSGPU_INVALID;
+  return new_mps(ctx, out, [&](MpsDev& s) {
+    double disc = 0.0;
+    mps_approximate(ctx->c, src->s, s, D, &disc);
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    if (discarded) *discarded = disc;
+  });
+}
+
+mpsgpu_status mpsgpu_mps_apply_mpo(mpsgpu_context* ctx, const mpsgpu_mpo* ops, const mpsgpu_mps* src, int D,
+                                   int dagger, char dir, mpsgpu_mps** out, double* discarded) {
+  if (!ops || !src) return MPSGPU_INVALID;
+  const char d = (dir == 'r' || dir == 'R') ? 'R' : (dir == 'l' || dir == 'L') ? 'L' : 0;
+  if (!d) return MPSGPU_INVALID;
+  return new_mps(ctx, out, [&](MpsDev& s) {
+    double disc = 0.0;
+    mps_apply_mpo(ctx->c, ops->m, src->s, s, D, dagger != 0, d, &disc);
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    if (discarded) *discarded = disc;
   });
 }
 

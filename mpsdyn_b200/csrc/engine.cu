@@ -168,6 +168,16 @@ void mps_random(Context& c, MpsDev& s, int L, int d, int D, uint64_t seed) {
   s.bond = s.max_bond();
 }
 
+// MPS::setRandomState (src/core/cpp/MPS.cpp:282-294): random sites, each
+// right-gauged in turn; the R factor moves on only where the bond shrinks,
+// so the state is a chain of random isometries with norm 1 whatever L.
+void mps_random_state(Context& c, MpsDev& s, int L, int d, int D, uint64_t seed) {
+  mps_random(c, s, L, d, D, seed);
+  for (int k = 0; k < L; k++) mps_gauge_site(c, s, k, 'R', false, nullptr);
+  s.normfact = 1.0;
+  s.gauge = 2;
+}
+
 void mps_product(Context& c, MpsDev& s, int L, int d, int D) {
   s.L = L;
   s.dims.resize(L);
@@ -227,7 +237,12 @@ void mps_free(Context& c, MpsDev& s) {
 // Move the norm of site pos into a factor: dir 'R' -> site = Q (left
 // isometry), factor R (K x Dr) left in c.matR (ld K); dir 'L' -> site = Q^H
 // rows (right isometry), factor R' (K x Dl) with L = R'^H.  Returns K.
-static int site_factor(Context& c, MpsDev& s, int pos, char dir, cplx* r00) {
+// cutD > 0 replaces the QR by the SVD cut of Site::gaugeR/gaugeL with cutD
+// (Site.cpp:186-193, :218-224): Q = U[:, :K], R = diag(s) V^H, K = the
+// number of values > 0 among the cutD largest; the sum of the squares of
+// the dropped values is added to *disc.
+static int site_factor(Context& c, MpsDev& s, int pos, char dir, cplx* r00, int cutD = 0,
+                       double* disc = nullptr) {
   const int d = s.dims[pos][0], Dl = s.dims[pos][1], Dr = s.dims[pos][2];
   int m, n;
   View2 v;
@@ -240,12 +255,19 @@ static int site_factor(Context& c, MpsDev& s, int pos, char dir, cplx* r00) {
     m = d * Dr; n = Dl;
     v.rd = 1; v.r0 = 0; v.r1 = Dl; v.cd = 1; v.c0 = 0; v.c1 = 1; v.conj = true;
   }
-  const int K = std::min(m, n);
+  int K = std::min(m, n);
   dbuf_reserve(c, c.matA, (long long)m * n);
   dbuf_reserve(c, c.matQ, (long long)m * K);
   dbuf_reserve(c, c.matR, (long long)K * n);
   gather2(c.st(), m, n, s.A[pos].p, v, c.matA.p);
-  householder_qr_inplace(c.st(), m, n, c.matA.p, c.matQ.p, m, c.matR.p, K, c.qrws);
+  if (cutD > 0) {
+    std::vector<double> sv;
+    K = svd_cut(c.st(), m, n, c.matA.p, m, cutD, c.matQ.p, c.matR.p, sv, c.scratch);
+    if (disc)
+      for (size_t j = K; j < sv.size(); j++) *disc += sv[j] * sv[j];
+  } else {
+    householder_qr_inplace(c.st(), m, n, c.matA.p, c.matQ.p, m, c.matR.p, K, c.qrws);
+  }
   // write the isometry back into the site
   View2 w;
   if (dir == 'R') {
@@ -304,11 +326,12 @@ static void absorb(Context& c, MpsDev& s, int target, char dir, int K, int n) {
 // QR/LQ of site pos; when the factor is the 1x1 of a bond of dimension 1
 // the phase goes into the site and |factor| is returned (else -1, factor
 // left in c.matR).  Site::gaugeR / gaugeL, Site.cpp:199-207 and :229-237.
-static int gauge_factor(Context& c, MpsDev& s, int pos, char dir, double* scalar, Counters* cnt) {
+static int gauge_factor(Context& c, MpsDev& s, int pos, char dir, double* scalar, Counters* cnt, int cutD = 0,
+                        double* disc = nullptr) {
   const auto old = s.dims[pos];
   const int n = dir == 'R' ? old[2] : old[1];
   cplx r00 = make_double2(0.0, 0.0);
-  const int K = site_factor(c, s, pos, dir, &r00);
+  const int K = site_factor(c, s, pos, dir, &r00, cutD, disc);
   *scalar = -1.0;
   if (K == 1 && n == 1) *scalar = edge_phase(c, s, pos, dir, r00);
   if (cnt) {
@@ -352,15 +375,16 @@ void mps_gauge_site(Context& c, MpsDev& s, int pos, char dir, bool next, Counter
   s.gauge = 0;
 }
 
-// MPS::gaugeCond(dir, normal) (MPS.cpp:306-364): a full QR (or LQ) sweep
-// carrying the factor along; the final scalar becomes the norm factor.
-void mps_gauge_all(Context& c, MpsDev& s, char dir, bool normal) {
+// MPS::gaugeCond(dir, normal, cutD) (MPS.cpp:306-364): a full QR (or LQ)
+// sweep carrying the factor along, or with cutD > 0 an SVD sweep that cuts
+// every bond to at most cutD; the final scalar becomes the norm factor.
+void mps_gauge_all(Context& c, MpsDev& s, char dir, bool normal, int cutD, double* disc) {
   double last = 1.0;
   if (dir == 'R') {
     for (int pos = 0; pos < s.L; pos++) {
       const int n = s.dims[pos][2];
       double scalar = -1.0;
-      const int K = gauge_factor(c, s, pos, 'R', &scalar, nullptr);
+      const int K = gauge_factor(c, s, pos, 'R', &scalar, nullptr, cutD, disc);
       if (pos < s.L - 1) pass_factor(c, s, pos + 1, 'R', K, n, scalar);
       else last = scalar;
     }
@@ -369,7 +393,7 @@ void mps_gauge_all(Context& c, MpsDev& s, char dir, bool normal) {
     for (int pos = s.L - 1; pos >= 0; pos--) {
       const int n = s.dims[pos][1];
       double scalar = -1.0;
-      const int K = gauge_factor(c, s, pos, 'L', &scalar, nullptr);
+      const int K = gauge_factor(c, s, pos, 'L', &scalar, nullptr, cutD, disc);
       if (pos > 0) pass_factor(c, s, pos - 1, 'L', K, n, scalar);
       else last = scalar;
     }
@@ -668,7 +692,6 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
   std::vector<double> a, b, s;
   double theta = 0.0;
   int total = 0;
-  const int max_restarts = 60;
   TridiagLowest tri;
   // Iteration j: matvec, fused reorthogonalisation, async copy of
   // (alpha_j, beta_j) to pinned memory, event.  The host enqueues iteration
@@ -685,12 +708,31 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
     MPSGPU_CUDA(cudaEventRecord(c.iter_ev[j], c.stream));
     total++;
   };
+  // Ritz vector of the current tridiagonal (k x k) into x, normalised
+  auto ritz_vector = [&](int k) {
+    MPSGPU_CUDA(cudaMemcpyAsync(c.dS, s.data(), k * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    combine_real(st, N, k, V, N, c.dS, x);
+    dznrm2(st, N, x, d_tmp, c.scratch);
+    zscal_inv(st, N, x, d_tmp, x);
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    if (iters) *iters = total;
+  };
+  // Thick-restarted Lanczos: after m steps the factorisation is compressed
+  // to about m/2 vectors spanning the lowest Ritz vectors, in tridiagonal
+  // form (ThickRestart), so the fused reorthogonalisation continues
+  // unchanged from index r.  Keeping many Ritz vectors preserves the
+  // convergence of the lowest pair when it is nearly degenerate, where a
+  // one-vector restart stalls.
+  const int keep = std::max(1, m / 2);
+  // budget of about 3840 matvecs (60 cycles of a 64-vector space), whatever m
+  const int max_restarts = std::max(60, 3840 / std::max(1, m - keep));
+  ThickRestart thick;
+  std::vector<double> gq;
+  std::vector<cplx> gqc;
+  int j0 = 0;
   for (int restart = 0; restart < max_restarts; restart++) {
-    a.clear();
-    b.clear();
-    bool conv = false;
-    enqueue(0);
-    for (int j = 0; j < m; j++) {
+    enqueue(j0);
+    for (int j = j0; j < m; j++) {
       if (j + 1 < m) enqueue(j + 1);
       MPSGPU_CUDA(cudaEventSynchronize(c.iter_ev[j]));
       const double alpha = c.hsc->alpha[j];
@@ -703,21 +745,45 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
       const double res = beta * std::fabs(s[j]);
       const double scale = std::max(normT, std::fabs(theta));
       if (res <= tol * scale || beta <= 1e-14 * scale || j + 1 == N) {
-        conv = true;
-        break;
+        ritz_vector(j + 1);
+        return theta;
       }
     }
-    const int k = (int)a.size();
-    MPSGPU_CUDA(cudaMemcpyAsync(c.dS, s.data(), k * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    combine_real(st, N, k, V, N, c.dS, x);
-    dznrm2(st, N, x, d_tmp, c.scratch);
-    zscal_inv(st, N, x, d_tmp, V);  // V[:,0] = normalised Ritz vector (restart vector)
-    zcopy(st, N, V, x);
-    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
-    if (conv) {
-      if (iters) *iters = total;
+    if (keep >= m) {
+      // no room to keep more than one vector: restart from the Ritz vector
+      ritz_vector(m);
+      zcopy(st, N, x, V);
+      a.clear();
+      b.clear();
+      j0 = 0;
+      continue;
+    }
+    // compress: V[:, 0..r) <- V G; V[:, r] = f / |f| with f = w, the
+    // orthogonalised (not normalised) residual of step m-1
+    const double fnorm = b[m - 1];
+    const int r = thick.compress(a, b, m, keep, fnorm, gq);
+    gqc.resize(gq.size());
+    for (size_t i = 0; i < gq.size(); i++) gqc[i] = make_double2(gq[i], 0.0);
+    dbuf_reserve(c, c.lanQ, (long long)gqc.size());
+    dbuf_reserve(c, c.lanT, (long long)N * r);
+    MPSGPU_CUDA(cudaMemcpyAsync(c.lanQ.p, gqc.data(), gqc.size() * sizeof(cplx), cudaMemcpyHostToDevice,
+                                c.stream));
+    GemmArgs g;
+    g.M = N; g.N = r; g.K = m;
+    g.A = V; g.lda = N;
+    g.B = c.lanQ.p; g.ldb = m;
+    g.C = c.lanT.p; g.ldc = N;
+    zgemm(st, g, c.scratch);
+    MPSGPU_CUDA(cudaMemcpyAsync(V, c.lanT.p, (size_t)N * r * sizeof(cplx), cudaMemcpyDeviceToDevice, c.stream));
+    double normT = 0.0;
+    tri.solve(a, b, r, theta, s, normT);
+    const double scale = std::max(normT, std::fabs(theta));
+    if (b[r - 1] * std::fabs(s[r - 1]) <= tol * scale || b[r - 1] <= 1e-14 * scale) {
+      ritz_vector(r);  // converged within the kept space
       return theta;
     }
+    zscal_inv(st, N, w, &c.dsc->beta[m - 1], V + (long long)r * N);  // beta[m-1] = |f| on the device
+    j0 = r;
   }
   if (iters) *iters = total;
   throw Error(MPSGPU_NOT_CONVERGED, "lanczos: no convergence");
@@ -727,11 +793,188 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
 // findGroundState (Contractor.cpp:1352-1533)
 // ---------------------------------------------------------------------------
 
+// MPS(const MPS&, int D) (MPS.cpp:761-772): copy, then gaugeCond('L', 0, D),
+// right-to-left SVD cuts to at most D that keep the norm in normfact.
+void mps_approximate(Context& c, const MpsDev& src, MpsDev& dst, int D, double* disc) {
+  MPSGPU_CHECK(D > 0, MPSGPU_INVALID, "approximate: D must be positive");
+  mps_copy(c, src, dst);
+  if (disc) *disc = 0.0;
+  mps_gauge_all(c, dst, 'L', false, D, disc);
+  dst.bond = dst.max_bond();
+}
+
+// MPO applied exactly to an MPS, site by site, with an SVD gauge move after
+// every site: MPS::applyExactly (cutD <= 0: no cut beyond dropping zero
+// singular values) and MPS::truncate / approximate (cutD > 0), MPS.cpp:
+// 858-936, with Site::reduceDimLOp / reduceDimROp (Site.cpp:303-402).
+// dir 'L' sweeps L-1 -> 0 (right-isometric result), 'R' sweeps 0 -> L-1.
+// The carried factor ("link") is kept as (r, w, beta) with r fastest for
+// 'L' and as (beta, w, a) with beta fastest for 'R', which is the layout
+// the factor of the gauge move comes out in.
+void mps_apply_mpo(Context& c, const MpoDev& ops, const MpsDev& src, MpsDev& dst, int cutD, bool dagger, char dir,
+                   double* disc) {
+  const int L = src.L;
+  MPSGPU_CHECK(ops.L == L, MPSGPU_BAD_SHAPE, "apply MPO: lengths differ");
+  MPSGPU_CHECK(dir == 'L' || dir == 'R', MPSGPU_INVALID, "apply MPO: direction must be 'L' or 'R'");
+  for (int k = 0; k < L; k++) {
+    const auto& w = ops.dims[k];
+    MPSGPU_CHECK(src.dims[k][0] == (dagger ? w[0] : w[2]), MPSGPU_BAD_SHAPE, "apply MPO: physical dimensions");
+  }
+  MPSGPU_CHECK(ops.dims[0][1] == 1 && ops.dims[L - 1][3] == 1, MPSGPU_BAD_SHAPE, "apply MPO: open boundary bonds");
+  mps_copy(c, src, dst);
+  if (disc) *disc = 0.0;
+  DBuf link, nlink, Wt;
+  int lr = 1, lw = 1, lb = 1;  // link dims: 'L' (r, w, beta), 'R' (beta, w, a)
+  dbuf_reserve(c, link, 1);
+  const cplx one = make_double2(1.0, 0.0);
+  MPSGPU_CUDA(cudaMemcpyAsync(link.p, &one, sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+  double last = 1.0;
+  try {
+    for (int step = 0; step < L; step++) {
+      const int pos = dir == 'L' ? L - 1 - step : step;
+      const auto od = dst.dims[pos];
+      const int d = od[0], Dl = od[1], Dr = od[2];
+      const auto& w4 = ops.dims[pos];
+      const int du = dagger ? w4[2] : w4[0], wl = w4[1], wr = w4[3];
+      // operator as the matrices the two directions need, conjugate-transposed
+      // on the physical legs when dagger (W^dag(u, b, s, c) = conj(W(s, b, u, c)))
+      const cplx* Wsrc = ops.W[pos].p;
+      const long long su = 1, sb = w4[0], ss = (long long)w4[0] * wl, sc = (long long)w4[0] * wl * w4[2];
+      const long long s_u = dagger ? ss : su, s_s = dagger ? su : ss;  // strides of (u, s) in W
+      View2 v;
+      v.conj = dagger;
+      GemmArgs g;
+      if (dir == 'L') {
+        MPSGPU_CHECK(lr == Dr && lw == wr, MPSGPU_BAD_SHAPE, "apply MPO: link mismatch");
+        // T1(a, s, c, beta) = X(a s x r) . link(r x c beta)
+        dbuf_reserve(c, c.t1, (long long)Dl * d * wr * lb);
+        g = GemmArgs();
+        g.M = Dl * d; g.N = wr * lb; g.K = Dr;
+        g.A = dst.A[pos].p; g.lda = (long long)Dl * d;
+        g.B = link.p; g.ldb = Dr;
+        g.C = c.t1.p; g.ldc = (long long)Dl * d;
+        zgemm(c.st(), g, c.scratch);
+        // P(s, c, a, beta)
+        dbuf_reserve(c, c.t2, (long long)d * wr * Dl * lb);
+        View2 p;
+        p.rd = d; p.r0 = Dl; p.r1 = (long long)Dl * d; p.cd = Dl; p.c0 = 1; p.c1 = (long long)Dl * d * wr;
+        gather2(c.st(), d * wr, Dl * lb, c.t1.p, p, c.t2.p);
+        // Wm(u b x s c)
+        dbuf_reserve(c, Wt, (long long)du * wl * d * wr);
+        v.rd = du; v.r0 = s_u; v.r1 = sb; v.cd = d; v.c0 = s_s; v.c1 = sc;
+        gather2(c.st(), du * wl, d * wr, Wsrc, v, Wt.p);
+        // T2(u, b, a, beta) = Wm . P
+        dbuf_reserve(c, c.t4, (long long)du * wl * Dl * lb);
+        g = GemmArgs();
+        g.M = du * wl; g.N = Dl * lb; g.K = d * wr;
+        g.A = Wt.p; g.lda = (long long)du * wl;
+        g.B = c.t2.p; g.ldb = (long long)d * wr;
+        g.C = c.t4.p; g.ldc = (long long)du * wl;
+        zgemm(c.st(), g, c.scratch);
+        // new site X'(b a, u, beta): left bond b + wl a
+        dst.dims[pos] = {du, wl * Dl, lb};
+        dbuf_reserve(c, dst.A[pos], nel(dst.dims[pos]));
+        View2 q;
+        q.rd = wl; q.r0 = du; q.r1 = (long long)du * wl; q.cd = du; q.c0 = 1; q.c1 = (long long)du * wl * Dl;
+        gather2(c.st(), wl * Dl, du * lb, c.t4.p, q, dst.A[pos].p);
+        const int n = wl * Dl;
+        double scalar = -1.0;
+        const int K = gauge_factor(c, dst, pos, 'L', &scalar, nullptr, cutD > 0 ? cutD : Dl * wl, disc);
+        if (scalar >= 0.0) {
+          const cplx sc1 = make_double2(scalar, 0.0);
+          dbuf_reserve(c, nlink, 1);
+          MPSGPU_CUDA(cudaMemcpyAsync(nlink.p, &sc1, sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+          MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+          last = scalar;
+          lr = 1; lw = 1; lb = 1;
+        } else {
+          // link'(a, b, k) = conj(R'(k, b + wl a)), R' in c.matR (ld K)
+          dbuf_reserve(c, nlink, (long long)n * K);
+          View2 r;
+          r.rd = Dl; r.r0 = (long long)K * wl; r.r1 = K; r.cd = 1; r.c0 = 0; r.c1 = 1; r.conj = true;
+          gather2(c.st(), n, K, c.matR.p, r, nlink.p);
+          lr = Dl; lw = wl; lb = K;
+        }
+      } else {
+        MPSGPU_CHECK(lr == Dl && lw == wl, MPSGPU_BAD_SHAPE, "apply MPO: link mismatch");
+        // T1(beta, b, s, r) = link(beta b x a) . X(a x s r)
+        dbuf_reserve(c, c.t1, (long long)lb * wl * d * Dr);
+        g = GemmArgs();
+        g.M = lb * wl; g.N = d * Dr; g.K = Dl;
+        g.A = link.p; g.lda = (long long)lb * wl;
+        g.B = dst.A[pos].p; g.ldb = Dl;
+        g.C = c.t1.p; g.ldc = (long long)lb * wl;
+        zgemm(c.st(), g, c.scratch);
+        // P(b, s, beta, r)
+        dbuf_reserve(c, c.t2, (long long)wl * d * lb * Dr);
+        View2 p;
+        p.rd = wl; p.r0 = lb; p.r1 = (long long)lb * wl; p.cd = lb; p.c0 = 1; p.c1 = (long long)lb * wl * d;
+        gather2(c.st(), wl * d, lb * Dr, c.t1.p, p, c.t2.p);
+        // Wm(u c x b s)
+        dbuf_reserve(c, Wt, (long long)du * wr * wl * d);
+        v.rd = du; v.r0 = s_u; v.r1 = sc; v.cd = wl; v.c0 = sb; v.c1 = s_s;
+        gather2(c.st(), du * wr, wl * d, Wsrc, v, Wt.p);
+        // T2(u, c, beta, r) = Wm . P
+        dbuf_reserve(c, c.t4, (long long)du * wr * lb * Dr);
+        g = GemmArgs();
+        g.M = du * wr; g.N = lb * Dr; g.K = wl * d;
+        g.A = Wt.p; g.lda = (long long)du * wr;
+        g.B = c.t2.p; g.ldb = (long long)wl * d;
+        g.C = c.t4.p; g.ldc = (long long)du * wr;
+        zgemm(c.st(), g, c.scratch);
+        // new site X'(beta, u, c r): right bond c + wr r
+        dst.dims[pos] = {du, lb, wr * Dr};
+        dbuf_reserve(c, dst.A[pos], nel(dst.dims[pos]));
+        View2 q;
+        q.rd = lb; q.r0 = (long long)du * wr; q.r1 = 1; q.cd = wr; q.c0 = du; q.c1 = (long long)du * wr * lb;
+        gather2(c.st(), lb * du, wr * Dr, c.t4.p, q, dst.A[pos].p);
+        const int n = wr * Dr;
+        double scalar = -1.0;
+        const int K = gauge_factor(c, dst, pos, 'R', &scalar, nullptr, cutD > 0 ? cutD : Dr * wr, disc);
+        if (scalar >= 0.0) {
+          const cplx sc1 = make_double2(scalar, 0.0);
+          dbuf_reserve(c, nlink, 1);
+          MPSGPU_CUDA(cudaMemcpyAsync(nlink.p, &sc1, sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+          MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+          last = scalar;
+          lr = 1; lw = 1; lb = 1;
+        } else {
+          // link'(k, c, r) = R(k, c + wr r): the factor as it stands
+          dbuf_reserve(c, nlink, (long long)K * n);
+          zcopy(c.st(), K * n, c.matR.p, nlink.p);
+          lr = Dr; lw = wr; lb = K;
+        }
+      }
+      std::swap(link, nlink);
+    }
+    MPSGPU_CHECK(lr == 1 && lw == 1 && lb == 1, MPSGPU_BAD_SHAPE, "apply MPO: final factor is not a scalar");
+  } catch (...) {
+    dbuf_free(c, link);
+    dbuf_free(c, nlink);
+    dbuf_free(c, Wt);
+    throw;
+  }
+  dbuf_free(c, link);
+  dbuf_free(c, nlink);
+  dbuf_free(c, Wt);
+  dst.normfact = src.normfact * last;
+  dst.gauge = dir == 'L' ? 1 : 2;
+  // applyExactly leaves the bond field alone; truncate lowers it to the
+  // largest bond present (MPS.cpp:919,934)
+  if (cutD > 0) dst.bond = std::min(src.bond > 0 ? src.bond : dst.max_bond(), dst.max_bond());
+}
+
+// Prologue of findGroundState / optimize (Contractor.cpp:1362-1373): pad the
+// bonds up to D, or cut the state down to D (init = MPS(init, D)), then
+// gauge to the right and back to the left.
 static void prepare_init(Context& c, MpsDev& init, int D) {
   if (D > 0) {
-    if (D > init.bond) mps_increase_bond(c, init, D);
-    else MPSGPU_CHECK(D >= init.bond, MPSGPU_BAD_SHAPE,
-                      "D smaller than the initial bond (truncation of the initial state is not supported)");
+    if (D > init.bond) {
+      mps_increase_bond(c, init, D);
+    } else if (D < init.bond) {
+      mps_gauge_all(c, init, 'L', false, D, nullptr);
+      init.bond = init.max_bond();
+    }
   }
   mps_gauge_all(c, init, 'R', true);
   mps_gauge_all(c, init, 'L', true);

@@ -54,6 +54,7 @@ struct Context {
   // reusable workspaces (complex elements)
   DBuf t1, t2, t3, t4, matA, matQ, matR;
   DBuf lanV, lanW;     // Lanczos basis and work vector
+  DBuf lanT, lanQ;     // thick restart: V G product and the restart matrix G
   double* dscal = nullptr;     // device scalars (alpha, beta, norms)
   cplx* dcplx = nullptr;       // device complex scalars (dots)
   double* hscal = nullptr;     // pinned host mirror
@@ -117,11 +118,15 @@ void mpo_upload(Context& c, MpoDev& m, int L, const int* dims, const double* con
 void mpo_free(Context& c, MpoDev& m);
 void mps_upload(Context& c, MpsDev& s, int L, const int* dims, const double* const* data, double nf);
 void mps_random(Context& c, MpsDev& s, int L, int d, int D, uint64_t seed);
+void mps_random_state(Context& c, MpsDev& s, int L, int d, int D, uint64_t seed);
 void mps_product(Context& c, MpsDev& s, int L, int d, int D);
 void mps_copy(Context& c, const MpsDev& src, MpsDev& dst);
 void mps_download(Context& c, const MpsDev& s, double* const* data);
 void mps_free(Context& c, MpsDev& s);
-void mps_gauge_all(Context& c, MpsDev& s, char dir, bool normal);
+void mps_gauge_all(Context& c, MpsDev& s, char dir, bool normal, int cutD = 0, double* disc = nullptr);
+void mps_approximate(Context& c, const MpsDev& src, MpsDev& dst, int D, double* disc);
+void mps_apply_mpo(Context& c, const MpoDev& ops, const MpsDev& src, MpsDev& dst, int cutD, bool dagger, char dir,
+                   double* disc);
 void mps_gauge_site(Context& c, MpsDev& s, int pos, char dir, bool next, Counters* cnt);
 void mps_increase_bond(Context& c, MpsDev& s, int D);
 

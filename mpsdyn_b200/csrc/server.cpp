@@ -124,7 +124,7 @@ struct mpsgpu_server {
     if (r.model == MPSGPU_MODEL_ISING) st = mpsgpu_mpo_ising(ctx, r.L, r.p0, r.p1, r.p2, &mpo);
     else if (r.model == MPSGPU_MODEL_SCHWINGER) st = mpsgpu_mpo_schwinger(ctx, r.L, r.p0, r.p1, 0.0, r.p2, &mpo);
     else st = MPSGPU_INVALID;
-    if (st == MPSGPU_OK) st = mpsgpu_mps_random(ctx, r.L, 2, r.D, r.seed, &mps);
+    if (st == MPSGPU_OK) st = mpsgpu_mps_random_state(ctx, r.L, 2, r.D, r.seed, &mps);
     if (st == MPSGPU_OK) {
       mpsgpu_options opt;
       mpsgpu_default_options(&opt);

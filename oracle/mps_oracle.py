@@ -158,6 +158,20 @@ def random_mps(L: int, d: int, D: int, seed: int) -> MPS:
     return MPS(sites, 1.0, 0, max(bonds))
 
 
+def random_state(L: int, d: int, D: int, seed: int) -> MPS:
+    """MPS::setRandomState (core/cpp/MPS.cpp:282-294) on the sites of
+    random_mps: each site right-gauged in turn, the R factor passed on only
+    where the bond shrinks (Site::gaugeR + reduceDimR)."""
+    m = random_mps(L, d, D, seed)
+    for k in range(L):
+        old = m.sites[k].shape
+        m.sites[k], tmp = site_gauge_r(m.sites[k])
+        if k < L - 1 and m.sites[k].shape[2] != old[2]:
+            m.sites[k + 1] = site_reduce_r(m.sites[k + 1], tmp)
+    m.gauge = 2
+    return m
+
+
 def product_mps(L: int, d: int, D: int) -> MPS:
     """MPS(L,D,d) of the reference: dims (d,1,D),(d,D,D)...,(d,D,1), each site
     with element (0,0,0)=1 (core/cpp/MPS.cpp:15-35, core/cpp/Site.cpp:16-21)."""
@@ -991,6 +1005,10 @@ def svd_cut(M: np.ndarray, cutD: int):
     discarded weight sum_{i>=cut} s_i^2 (not returned by the reference)."""
     U, s, Vh = np.linalg.svd(M, full_matrices=False)
     nr = min(cutD, s.size) if cutD > 0 else s.size
+    # tol = 0: values that are not > 0 are cut as well (svd.cpp:95-101)
+    nr = int(np.sum(s[:nr] > 0.0))
+    if nr == 0:
+        raise ValueError("svd: no singular value above 0")
     disc = float(np.sum(s[nr:] ** 2))
     return U[:, :nr], s[:nr], Vh[:nr, :], disc
 
@@ -1022,6 +1040,92 @@ def truncate_mps(mps: MPS, D: int):
     out.normfact = out.normfact * abs(tmp.reshape(-1)[0])
     out.discarded = disc[::-1]
     return out
+
+
+def _gauge_l_cut(A: np.ndarray, cutD: int):
+    """Site::gaugeL with cutD > 0 (Site.cpp:210-238) on an already reduced
+    site: SVD of A as (Dl x d Dr); returns (new site, leftterm, discarded)."""
+    d, Dl, Dr = A.shape
+    M = A.transpose(1, 0, 2).reshape(Dl, d * Dr, order="F")
+    U, sv, Vh, w = svd_cut(M, cutD)
+    left = U * sv[None, :]
+    K = Vh.shape[0]
+    A = Vh.reshape(K, d, Dr, order="F").transpose(1, 0, 2)
+    if K == 1 and left.shape[0] == 1:
+        aux = left[0, 0]
+        phase = aux / abs(aux) if abs(aux) != 0 else 1.0
+        A = A * phase
+        left = np.array([[abs(aux)]], dtype=np.complex128)
+    return np.ascontiguousarray(A), left, w
+
+
+def _gauge_r_cut(A: np.ndarray, cutD: int):
+    """Site::gaugeR with cutD > 0 (Site.cpp:179-208): SVD of A as (d Dl x Dr);
+    returns (new site, rightterm, discarded)."""
+    d, Dl, Dr = A.shape
+    U, sv, Vh, w = svd_cut(A.reshape(d * Dl, Dr, order="F"), cutD)
+    right = sv[:, None] * Vh
+    K = U.shape[1]
+    A = U.reshape(d, Dl, K, order="F")
+    if K == 1 and right.shape[1] == 1:
+        aux = right[0, 0]
+        phase = aux / abs(aux) if abs(aux) != 0 else 1.0
+        A = A * phase
+        right = np.array([[abs(aux)]], dtype=np.complex128)
+    return np.ascontiguousarray(A), right, w
+
+
+def apply_mpo(ops: list, mps: MPS, cutD: int = 0, dagger: bool = False, direction: str = "L") -> MPS:
+    """MPS::applyExactly (cutD <= 0) and MPS::truncate(ops, mps, cutD, dagger,
+    dir) (MPS.cpp:858-936): each site contracted with its operator and the
+    carried factor (Site::reduceDimLOp / reduceDimROp, Site.cpp:303-402),
+    then gauged by an SVD cut (applyExactly cuts at the full dimension,
+    Dl*w or Dr*w, which only drops zero values).  Returns a new MPS with
+    attribute ``discarded`` (sum of dropped squares)."""
+    out = mps.copy()
+    L = out.L
+    tmp = np.ones((1, 1), dtype=np.complex128)
+    disc = 0.0
+    order = range(L - 1, -1, -1) if direction == "L" else range(L)
+    for pos in order:
+        W = ops[pos]
+        if dagger:
+            W = W.transpose(2, 1, 0, 3).conj()
+        du, wl, dd, wr = W.shape
+        A = out.sites[pos]
+        d, Dl, Dr = A.shape
+        if direction == "L":
+            cut = cutD if cutD > 0 else Dl * wl
+            t = tmp.reshape(wr, Dr, -1, order="F")                  # (c, r, beta)
+            An = np.einsum("ubsc,sar,crq->ubaq", W, A, t)           # (u, b, a, beta)
+            An = An.reshape(du, wl * Dl, t.shape[2], order="F")     # left index b + wl a
+            out.sites[pos], tmp, w = _gauge_l_cut(An, cut)
+        else:
+            cut = cutD if cutD > 0 else Dr * wr
+            t = tmp.reshape(-1, wl, Dl, order="F")                  # (beta, b, a)
+            An = np.einsum("qba,ubsc,sar->uqcr", t, W, A)           # (u, beta, c, r)
+            An = An.reshape(du, t.shape[0], wr * Dr, order="F")     # right index c + wr r
+            out.sites[pos], tmp, w = _gauge_r_cut(An, cut)
+        disc += w
+    if tmp.size != 1:
+        raise ValueError("apply_mpo: final factor is not a scalar")
+    out.normfact = mps.normfact * abs(tmp.reshape(-1)[0])
+    out.gauge = 1 if direction == "L" else 2
+    # applyExactly leaves the bond field alone; truncate lowers it to the
+    # largest bond present (MPS.cpp:919,934)
+    if cutD > 0:
+        out.bond = min(mps.bond or out.max_bond(), out.max_bond())
+    out.discarded = disc
+    return out
+
+
+def mps_to_vector(mps: MPS) -> np.ndarray:
+    """Dense state vector (normfact included), index s_0 + d s_1 + d^2 s_2 ...
+    (small L only)."""
+    v = mps.sites[0][:, 0, :]                                      # (s0, r)
+    for A in mps.sites[1:]:
+        v = np.einsum("xa,sar->xsr", v, A).reshape(-1, A.shape[2], order="F")
+    return mps.normfact * v[:, 0]
 
 
 def expectation_values(mps: MPS, op2: np.ndarray) -> np.ndarray:

@@ -34,6 +34,9 @@
  *   entropy mps pos                Contractor::getEntropy             (Contractor.cpp:2045-2076)
  *   schmidt mps pos                Contractor::getSchmidtValues       (Contractor.cpp:2243-2270)
  *   truncate mps D out             MPS(mps, D) (SVD cut, MPS.cpp:761-772)
+ *   applympo model delta imag D dagger dir mps out
+ *                                  U-MPO of getUMPO applied to mps: MPS::applyExactly (D = 0) or
+ *                                  MPS::approximate (D > 0), MPS.cpp:853-936
  *   profile model D eigtol init n  timed sample: n site steps of the ground-state sweep
  *                                  around the chain centre (CPU baseline of the bench)
  *   gauge mps dir out              MPS::gaugeCond(dir, true)          (MPS.cpp:306-364)
@@ -313,6 +316,20 @@ int main(int argc, const char* argv[]) {
     s.importMPS(argv[2]);
     MPS t(s, atoi(argv[3]));
     t.exportMPS(argv[4]);
+    print_json({{"bond", (double)t.getBond()}, {"normfact", t.getNormFact()}});
+  } else if (cmd == "applympo") {
+    Model m = make_model(argv[2]);
+    MPO U(m.L);
+    m.ising->getUMPO(U, atof(argv[3]), 0., atoi(argv[4]) != 0, 2);
+    const int D = atoi(argv[5]);
+    const bool dagger = atoi(argv[6]) != 0;
+    const char dir = argv[7][0];
+    MPS s;
+    s.importMPS(argv[8]);
+    MPS t(s);
+    if (D > 0) t.approximate(U, s, D, dagger ? 'U' : 'D', dir);
+    else t.applyExactly(U, dagger, dir);
+    t.exportMPS(argv[9]);
     print_json({{"bond", (double)t.getBond()}, {"normfact", t.getNormFact()}});
   } else if (cmd == "gauge") {
     MPS s;

@@ -34,6 +34,12 @@ def mpo_npz():
 
 
 @pytest.fixture(scope="session")
+def trunc_npz():
+    import numpy as np
+    return np.load(os.path.join(ROOT, "tests", "golden", "truncation.npz"))
+
+
+@pytest.fixture(scope="session")
 def ctx():
     """One library context on cuda:0 for the GPU tests (fails loudly when the
     library or the GPU is missing: there is no fallback)."""

@@ -120,6 +120,32 @@ def main() -> None:
     golden["ising_L8_D8_quench_energies"] = r["energies"]
     golden["ising_L8_D8_quench_entropy"] = r["entropy_center"]
 
+    # SVD truncation MPS(mps, D) and MPO application (exact and cut), as
+    # dense state vectors (gauge-invariant) with the site dimensions
+    trunc = {}
+    fi, fo = os.path.join(tmp, "t_in.mps"), os.path.join(tmp, "t_out.mps")
+    mo.write_mps(fi, mo.random_mps(10, 2, 16, 21))
+    run("truncate", fi, 5, fo)
+    t = mo.read_mps(fo)
+    trunc["trunc_L10_D16_seed21_to5_vec"] = mo.mps_to_vector(t)
+    trunc["trunc_L10_D16_seed21_to5_dims"] = np.array([a.shape for a in t.sites])
+    mo.write_mps(fi, mo.random_mps(8, 2, 6, 5))
+    for D in (0, 4):
+        for dg in (0, 1):
+            for dr in "LR":
+                run("applympo", "ising:8:1:1.1:0.2", 0.05, 0, D, dg, dr, fi, fo)
+                t = mo.read_mps(fo)
+                tag = f"apply_L8_D6_seed5_ureal005_cut{D}_dag{dg}_{dr}"
+                trunc[tag + "_vec"] = mo.mps_to_vector(t)
+                trunc[tag + "_dims"] = np.array([a.shape for a in t.sites])
+    np.savez_compressed(os.path.join(HERE, "truncation.npz"), **trunc)
+    # ground state from an initial MPS with a larger bond than D (the
+    # prologue cuts it with MPS(init, D))
+    fg = os.path.join(tmp, "g_in.mps")
+    mo.write_mps(fg, mo.random_mps(12, 2, 16, 4))
+    golden["ising_L12_init16_D6_seed4_E0"] = run("gs", "ising:12:1:1:0", 6, 1e-10, 0, fg,
+                                                 os.path.join(tmp, "g_out.mps"))["E0"]
+
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print(json.dumps({k: (v if not isinstance(v, list) else v[:3]) for k, v in golden.items()}, indent=1))

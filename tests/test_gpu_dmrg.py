@@ -204,3 +204,35 @@ def test_expectation_values_vs_oracle(ctx):
     s = ctx.mps(m.sites)
     for op in (mo.SIGX, mo.SIGZ, mo.SIGY):
         np.testing.assert_allclose(ctx.expectation_local(s, op), mo.expectation_values(m, op), rtol=0, atol=1e-12)
+
+
+def test_random_state_matches_oracle(ctx):
+    s = ctx.mps_random_state(12, 2, 8, 5)
+    sites, nf = s.download()
+    ref = mo.random_state(12, 2, 8, 5)
+    assert nf == 1.0
+    for a, b in zip(sites, ref.sites):
+        assert a.shape == b.shape
+        assert np.abs(a - b).max() < 1e-12
+    assert abs(ctx.contract(s, None, s).real - 1.0) < 1e-12
+
+
+def test_gs_long_chain_from_random_state(ctx):
+    # L = 240: the raw Gaussian chain would overflow (norm ~ (d D)^(L/2));
+    # the gauged random state does not.  Gapped TFIM, exact energy by free fermions.
+    L, D, g = 240, 16, 2.0
+    m = ctx.mpo_ising(L, 1.0, g, 0.0)
+    s = ctx.mps_random_state(L, 2, D, 3)
+    e, st = ctx.find_ground_state(m, D, s, 0.0, ctx.options(convtol=1e-10))
+    exact = mo.tfim_open_energy(L, 1.0, g)
+    assert abs(e - exact) < 1e-9 * abs(exact), (e, exact)
+
+
+@pytest.mark.parametrize("krylov", [6, 16])
+def test_gs_with_small_krylov_space_restarts(ctx, golden, krylov):
+    # a short Krylov space forces many thick restarts per site
+    ops = ctx.mpo(mo.ising_hmpo(20, 1, 1, 0))
+    s = ctx.mps(mo.random_mps(20, 2, 20, 0).sites)
+    e, st = ctx.find_ground_state(ops, 20, s, 0.0, ctx.options(convtol=1e-10, max_krylov=krylov))
+    ref = golden["ising_L20_D20_seed0_E0"]
+    assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)

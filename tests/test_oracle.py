@@ -161,3 +161,38 @@ def test_qr_lq_conventions_match_lapack():
     Lm, Q2 = mo.lq_reduced(A.T.copy())
     np.testing.assert_allclose(Lm @ Q2, A.T, atol=1e-13)
     np.testing.assert_allclose(Q2 @ Q2.conj().T, np.eye(5), atol=1e-13)
+
+
+def test_random_state_is_normalised_isometry_chain():
+    m = mo.random_state(10, 2, 6, 3)
+    assert abs(mo.contract_overlap(m, m).real - 1.0) < 1e-12
+    for a in m.sites:
+        d, Dl, Dr = a.shape
+        M = a.reshape(d * Dl, Dr, order="F")
+        assert np.abs(M.conj().T @ M - np.eye(Dr)).max() < 1e-13
+
+
+def test_truncation_matches_reference(trunc_npz):
+    t = mo.truncate_mps(mo.random_mps(10, 2, 16, 21), 5)
+    np.testing.assert_array_equal(np.array([a.shape for a in t.sites]), trunc_npz["trunc_L10_D16_seed21_to5_dims"])
+    ref = trunc_npz["trunc_L10_D16_seed21_to5_vec"]
+    assert np.abs(mo.mps_to_vector(t) - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("cut", [0, 4])
+@pytest.mark.parametrize("dagger", [0, 1])
+@pytest.mark.parametrize("direction", ["L", "R"])
+def test_apply_mpo_matches_reference(trunc_npz, cut, dagger, direction):
+    U = mo.ising_umpo(8, 1.0, 1.1, 0.2, 0.05, False)
+    t = mo.apply_mpo(U, mo.random_mps(8, 2, 6, 5), cut, bool(dagger), direction)
+    tag = f"apply_L8_D6_seed5_ureal005_cut{cut}_dag{dagger}_{direction}"
+    np.testing.assert_array_equal(np.array([a.shape for a in t.sites]), trunc_npz[tag + "_dims"])
+    ref = trunc_npz[tag + "_vec"]
+    assert np.abs(mo.mps_to_vector(t) - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+def test_gs_prologue_truncates_large_initial_bond(golden):
+    m = mo.random_mps(12, 2, 16, 4)
+    e = mo.find_ground_state(mo.ising_hmpo(12, 1, 1, 0), 6, m, convtol=1e-10)
+    ref = golden["ising_L12_init16_D6_seed4_E0"]
+    assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
