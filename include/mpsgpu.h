@@ -300,8 +300,8 @@ mpsgpu_status mpsgpu_lq(mpsgpu_context* ctx, int m, int n, const double* A,
 /* QR of a device-resident m x n matrix that allocates nothing.  No
  * counterpart in the reference: it is a variant of mpsgpu_qr for callers that
  * cannot allocate device memory when they need a gauge move (a serving
- * process whose allocator owns the whole HBM, a caller recording a CUDA
- * graph, a loop that must not fail on allocation mid-sweep).
+ * process whose allocator owns the whole HBM, a loop that must not fail on
+ * an allocation half way through a sweep).
  *   A: m x n column-major complex128 on the device (read only);
  *   Q: m x K (ld m), R: K x n (ld K), K = min(m, n), on the device; either may
  *      be null.  Same results as mpsgpu_qr (LAPACK zgeqrf/zungqr conventions).

@@ -398,9 +398,8 @@ void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, lo
 //
 // Some callers cannot allocate device memory at the moment they need a gauge
 // move: a serving process whose memory manager has reserved the whole HBM
-// for its request slots, a caller recording work into a CUDA graph (no
-// allocation may happen while a stream is being captured), or a real-time
-// loop that must not meet an allocation failure half way through a sweep.
+// for its request slots, or a real-time loop that must not meet an
+// allocation failure half way through a sweep.
 // For them this variant keeps every byte of its working memory in one
 // file-scope device array: the working copy of A (factored in place), the
 // block-reflector factors T and the scalars tau.  The array is reserved when

@@ -2,8 +2,8 @@
 nothing (its working memory is a fixed device array inside the library).
 
 It is meant for callers that cannot allocate device memory when they need a
-gauge move: a serving process whose allocator owns the whole HBM, a caller
-recording a CUDA graph, a loop that must not fail on an allocation.  The test
+gauge move: a serving process whose allocator owns the whole HBM, or a loop
+that must not fail on an allocation half way through a sweep.  The test
 calls it twice in a row through the C ABI on device buffers (allocated here
 by the test with torch) and checks both results against the allocating entry
 point mpsgpu_qr, within the tolerance of the other QR tests.  It lives in a
