@@ -101,6 +101,13 @@ mpsgpu_status mpsgpu_profile_end(mpsgpu_context* ctx, double* gemm_ms, double* g
 mpsgpu_status mpsgpu_mpo_upload(mpsgpu_context* ctx, int L, const int* dims,
                                 const double* const* data, mpsgpu_mpo** out);
 mpsgpu_status mpsgpu_mpo_free(mpsgpu_context* ctx, mpsgpu_mpo* mpo);
+/* Length and dims[4k..4k+3] = (du, Dl, dd, Dr) of an uploaded MPO (either
+ * output may be null), and its tensors back to host buffers (data[k] holds
+ * du*Dl*dd*Dr complex128, column-major), as MPO::getOpData returns them. */
+mpsgpu_status mpsgpu_mpo_info(mpsgpu_context* ctx, const mpsgpu_mpo* mpo, int* L,
+                              int* dims);
+mpsgpu_status mpsgpu_mpo_download(mpsgpu_context* ctx, const mpsgpu_mpo* mpo,
+                                  double* const* data);
 /* Model MPOs built by the library (host tensors as the reference builds
  * them, then uploaded):
  *   IsingHamiltonian(L, 2, J, g, h).getHMPO() (models/cpp/IsingHamiltonian.cpp:70-121)
@@ -142,6 +149,20 @@ mpsgpu_status mpsgpu_mps_download(mpsgpu_context* ctx, const mpsgpu_mps* mps,
 mpsgpu_status mpsgpu_mps_free(mpsgpu_context* ctx, mpsgpu_mps* mps);
 /* MPS::gaugeCond(dir, normal=true) (src/core/cpp/MPS.cpp:306-364). */
 mpsgpu_status mpsgpu_mps_gauge(mpsgpu_context* ctx, mpsgpu_mps* mps, char dir);
+/* MPS::gaugeCond(dir, normalize, cutD) (src/core/cpp/MPS.cpp:306-364): QR
+ * (cutD = 0) or SVD-cut (cutD > 0, bonds <= cutD) sweep; normalize = 0 keeps
+ * the norm in normfact.  discarded (nullable): sum of dropped squares. */
+mpsgpu_status mpsgpu_mps_gauge_cond(mpsgpu_context* ctx, mpsgpu_mps* mps, char dir,
+                                    int normalize, int cutD, double* discarded);
+/* MPS::increaseBondDimension(D) (src/core/cpp/MPS.cpp:650-719): integer bond
+ * schedule and zero padding. */
+mpsgpu_status mpsgpu_mps_increase_bond(mpsgpu_context* ctx, mpsgpu_mps* mps, int D);
+/* The bond field and the gauge tag (0 none, 1 left, 2 right) the reference
+ * keeps beside the tensors (MPS::getBond, MPS.h:62-70), and the norm factor
+ * setter (MPS::setNormFact). */
+mpsgpu_status mpsgpu_mps_bond(mpsgpu_context* ctx, const mpsgpu_mps* mps, int* bond,
+                              int* gauge);
+mpsgpu_status mpsgpu_mps_set_normfact(mpsgpu_context* ctx, mpsgpu_mps* mps, double normfact);
 /* MPS(const MPS& src, int D) (src/core/cpp/MPS.cpp:761-772): a copy cut to
  * bond dimension D by right-to-left SVDs (gaugeCond('L', 0, D), Site::gaugeL
  * with cutD, wrapper::svd with tol 0: zero singular values are dropped too).
@@ -177,7 +198,9 @@ mpsgpu_status mpsgpu_find_next_excited_state(mpsgpu_context* ctx,
                                              mpsgpu_mps* init, double* lambda,
                                              mpsgpu_stats* stats);
 /* optimize(ops, orig, init, D, errN, errT) (Contractor.cpp:77-278): the
- * variational MPO.MPS product used for time evolution.  errN may be null. */
+ * variational MPO.MPS product used for time evolution.  errN (nullable)
+ * receives <orig|ops^dag ops|orig> + <init|init> - 2 Re <init|ops|orig> and
+ * errT (used only with errN) the first term (Contractor.cpp:263-276). */
 mpsgpu_status mpsgpu_optimize(mpsgpu_context* ctx, const mpsgpu_mpo* ops,
                               const mpsgpu_mps* orig, mpsgpu_mps* init, int D,
                               const mpsgpu_options* opt, double* errN,
@@ -187,6 +210,11 @@ mpsgpu_status mpsgpu_optimize(mpsgpu_context* ctx, const mpsgpu_mpo* ops,
 mpsgpu_status mpsgpu_contract(mpsgpu_context* ctx, const mpsgpu_mps* ket,
                               const mpsgpu_mpo* ops, const mpsgpu_mps* bra,
                               double* re, double* im);
+/* contract2(bra, ops, ket) = <bra|ops^dag ops|ket> (Contractor.cpp:634-718);
+ * bra may be null for contract2(ops, ket) = <ket|ops^dag ops|ket>. */
+mpsgpu_status mpsgpu_contract2(mpsgpu_context* ctx, const mpsgpu_mpo* ops,
+                               const mpsgpu_mps* ket, const mpsgpu_mps* bra,
+                               double* re, double* im);
 /* <op_k> / <psi|psi> for every site k, op a d x d column-major matrix
  * (programs/banulsm/curved/flatIsing.cpp:258-282). out has L entries. */
 mpsgpu_status mpsgpu_expectation_local(mpsgpu_context* ctx, const mpsgpu_mps* mps,

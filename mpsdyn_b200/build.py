@@ -3,7 +3,9 @@
     python -m mpsdyn_b200.build        # or: python mpsdyn_b200/build.py
 
 Objects go to mpsdyn_b200/_build/, the shared library to
-mpsdyn_b200/libmpsgpu.so (found by mpsdyn_b200.capi).
+mpsdyn_b200/libmpsgpu.so (found by mpsdyn_b200.capi).  The C++ facade with
+the reference's class names (mpsdyn_b200/cpp) is built next to it as
+mpsdyn_b200/libmpsdyn_facade.so (g++, links libmpsgpu.so, rpath $ORIGIN).
 """
 from __future__ import annotations
 
@@ -17,6 +19,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmpsgpu.so")
+FACADE_DIR = os.path.join(HERE, "cpp")
+FACADE_INC = os.path.join(FACADE_DIR, "include")
+FACADE_LIB = os.path.join(HERE, "libmpsdyn_facade.so")
 
 SOURCES = ["zgemm.cu", "blas1.cu", "lanczos.cu", "qr.cu", "svd.cu", "grouped.cu", "engine.cu", "capi.cu", "models.cpp", "server.cpp"]
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -51,15 +56,32 @@ def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(_compile, SOURCES))
-    if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
-        return LIB
-    cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB, *objs]
+    if not (os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs)):
+        cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB, *objs]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+        if verbose:
+            print("built", LIB)
+    build_facade(verbose)
+    return LIB
+
+
+def build_facade(verbose: bool = False) -> str:
+    src = os.path.join(FACADE_DIR, "facade.cpp")
+    deps = [src, LIB, os.path.join(ROOT, "include", "mpsgpu.h")] + [
+        os.path.join(FACADE_INC, h) for h in os.listdir(FACADE_INC)]
+    if os.path.exists(FACADE_LIB) and os.path.getmtime(FACADE_LIB) >= max(os.path.getmtime(d) for d in deps):
+        return FACADE_LIB
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall",
+           "-I" + FACADE_INC, "-I" + os.path.join(ROOT, "include"), src, "-o", FACADE_LIB,
+           "-L" + HERE, "-lmpsgpu", "-Wl,-rpath,$ORIGIN"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("facade build failed:\n" + r.stdout + r.stderr)
     if verbose:
-        print("built", LIB)
-    return LIB
+        print("built", FACADE_LIB)
+    return FACADE_LIB
 
 
 if __name__ == "__main__":

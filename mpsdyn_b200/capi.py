@@ -22,11 +22,11 @@ EXPORTS = [
     "mpsgpu_default_options", "mpsgpu_create", "mpsgpu_destroy", "mpsgpu_status_string",
     "mpsgpu_last_error", "mpsgpu_launch_count", "mpsgpu_synchronize", "mpsgpu_get_stream",
     "mpsgpu_profile_begin", "mpsgpu_profile_end", "mpsgpu_mpo_upload",
-    "mpsgpu_mpo_free", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger",
+    "mpsgpu_mpo_free", "mpsgpu_mpo_info", "mpsgpu_mpo_download", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger",
     "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_random_state", "mpsgpu_mps_product",
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
-    "mpsgpu_mps_gauge", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
-    "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_expectation_local", "mpsgpu_entropy",
+    "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
+    "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_contract2", "mpsgpu_expectation_local", "mpsgpu_entropy",
     "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped",
     "mpsgpu_env_left", "mpsgpu_env_right",
     "mpsgpu_qr", "mpsgpu_lq", "mpsgpu_qr_device_noalloc",
@@ -245,6 +245,13 @@ class Context:
         re, im = C.c_double(), C.c_double()
         self._check(self.lib.mpsgpu_contract(self.h, ket.h, ops.h if ops is not None else None, bra.h,
                                              C.byref(re), C.byref(im)))
+        return complex(re.value, im.value)
+
+    def contract2(self, ops, ket, bra=None) -> complex:
+        """<bra|ops^dag ops|ket> (bra defaults to ket)."""
+        re, im = C.c_double(), C.c_double()
+        self._check(self.lib.mpsgpu_contract2(self.h, ops.h, ket.h, bra.h if bra is not None else None,
+                                              C.byref(re), C.byref(im)))
         return complex(re.value, im.value)
 
     def expectation_local(self, mps, op2) -> np.ndarray:

@@ -64,6 +64,36 @@ __global__ void wcontract_kernel(WContractArgs a) {
   }
 }
 
+// Same contraction for leg products above WMAX (the doubled operator O^dag O
+// of contract2 has w^2 legs): the inputs are read from global memory (L1)
+// for every output instead of being held in registers.
+__global__ void wcontract_wide_kernel(WContractArgs a) {
+  extern __shared__ double wsm[];
+  cplx* wm = reinterpret_cast<cplx*>(wsm);
+  const int nin = a.n_i0 * a.n_i1, nout = a.n_o0 * a.n_o1;
+  for (int t = threadIdx.x; t < nin * nout; t += blockDim.x) wm[t] = a.Wm[t];
+  __syncthreads();
+  const long long npix = (long long)a.nx * a.ny;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(p % a.nx), y = (int)(p / a.nx);
+    const cplx* ib = a.in + x * a.ix + y * a.iy;
+    cplx* ob = a.out + x * a.ox + y * a.oy;
+    for (int o = 0; o < nout; o++) {
+      const int o0 = o % a.n_o0, o1 = o / a.n_o0;
+      cplx s = make_double2(0.0, 0.0);
+      for (int i = 0; i < nin; i++) {
+        const int i0 = i % a.n_i0, i1 = i / a.n_i0;
+        const cplx v = ib[i0 * a.si0 + i1 * a.si1];
+        const cplx w = wm[o + nout * i];
+        s.x += w.x * v.x - w.y * v.y;
+        s.y += w.x * v.y + w.y * v.x;
+      }
+      ob[o0 * a.so0 + o1 * a.so1] = s;
+    }
+  }
+}
+
 // ---- Gram-Schmidt projections ----------------------------------------------
 constexpr int DOT_CHUNK = 4096;
 
@@ -279,12 +309,17 @@ __global__ void scatter2_kernel(int m, int n, const cplx* __restrict__ src, cplx
 
 void wcontract(const Stream& st, const WContractArgs& a) {
   const int nin = a.n_i0 * a.n_i1, nout = a.n_o0 * a.n_o1;
-  MPSGPU_CHECK(nin <= WMAX && nout <= WMAX, MPSGPU_BAD_SHAPE,
-               "wcontract: MPO leg product too large (d*w <= 32)");
   long long npix = (long long)a.nx * a.ny;
   if (npix <= 0) return;
   const size_t smem = (size_t)nin * nout * sizeof(cplx);
   const int grid = grid_for(npix, 128);
+  if (nin > WMAX || nout > WMAX) {
+    MPSGPU_CHECK(smem <= 48 * 1024, MPSGPU_BAD_SHAPE,
+                 "wcontract: MPO leg product too large (nin * nout <= 3072)");
+    wcontract_wide_kernel<<<grid, 128, smem, st.s>>>(a);
+    after_launch(st);
+    return;
+  }
   if (nin <= 4) wcontract_kernel<4><<<grid, 128, smem, st.s>>>(a);
   else if (nin <= 8) wcontract_kernel<8><<<grid, 128, smem, st.s>>>(a);
   else if (nin <= 16) wcontract_kernel<16><<<grid, 128, smem, st.s>>>(a);

@@ -296,6 +296,28 @@ mpsgpu_status mpsgpu_mpo_free(mpsgpu_context* ctx, mpsgpu_mpo* mpo) {
   return MPSGPU_OK;
 }
 
+mpsgpu_status mpsgpu_mpo_info(mpsgpu_context* ctx, const mpsgpu_mpo* mpo, int* L, int* dims) {
+  if (!ctx || !mpo) return MPSGPU_INVALID;
+  if (L) *L = mpo->m.L;
+  if (dims)
+    for (int k = 0; k < mpo->m.L; k++)
+      for (int j = 0; j < 4; j++) dims[4 * k + j] = mpo->m.dims[k][j];
+  return MPSGPU_OK;
+}
+
+mpsgpu_status mpsgpu_mpo_download(mpsgpu_context* ctx, const mpsgpu_mpo* mpo, double* const* data) {
+  if (!ctx || !mpo || !data) return MPSGPU_INVALID;
+  return guarded(ctx, [&] {
+    for (int k = 0; k < mpo->m.L; k++) {
+      const auto& d = mpo->m.dims[k];
+      const size_t n = (size_t)d[0] * d[1] * d[2] * d[3];
+      MPSGPU_CUDA(cudaMemcpyAsync(data[k], mpo->m.W[k].p, n * sizeof(cplx), cudaMemcpyDeviceToHost,
+                                  ctx->c.stream));
+    }
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
 static mpsgpu_status new_mps(mpsgpu_context* ctx, mpsgpu_mps** out, const std::function<void(MpsDev&)>& f) {
   if (!ctx || !out) return MPSGPU_INVALID;
   *out = nullptr;
@@ -364,6 +386,39 @@ mpsgpu_status mpsgpu_mps_gauge(mpsgpu_context* ctx, mpsgpu_mps* mps, char dir) {
     mps_gauge_all(ctx->c, mps->s, d, true);
     MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
   });
+}
+
+mpsgpu_status mpsgpu_mps_gauge_cond(mpsgpu_context* ctx, mpsgpu_mps* mps, char dir, int normalize, int cutD,
+                                    double* discarded) {
+  const char d = (dir == 'r' || dir == 'R') ? 'R' : (dir == 'l' || dir == 'L') ? 'L' : 0;
+  if (!ctx || !mps || !d || cutD < 0) return MPSGPU_INVALID;
+  return guarded(ctx, [&] {
+    double disc = 0.0;
+    mps_gauge_all(ctx->c, mps->s, d, normalize != 0, cutD, &disc);
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    if (discarded) *discarded = disc;
+  });
+}
+
+mpsgpu_status mpsgpu_mps_increase_bond(mpsgpu_context* ctx, mpsgpu_mps* mps, int D) {
+  if (!ctx || !mps || D <= 0) return MPSGPU_INVALID;
+  return guarded(ctx, [&] {
+    mps_increase_bond(ctx->c, mps->s, D);
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+mpsgpu_status mpsgpu_mps_bond(mpsgpu_context* ctx, const mpsgpu_mps* mps, int* bond, int* gauge) {
+  if (!ctx || !mps) return MPSGPU_INVALID;
+  if (bond) *bond = mps->s.bond > 0 ? mps->s.bond : mps->s.max_bond();
+  if (gauge) *gauge = mps->s.gauge;
+  return MPSGPU_OK;
+}
+
+mpsgpu_status mpsgpu_mps_set_normfact(mpsgpu_context* ctx, mpsgpu_mps* mps, double normfact) {
+  if (!ctx || !mps) return MPSGPU_INVALID;
+  mps->s.normfact = normfact;
+  return MPSGPU_OK;
 }
 
 mpsgpu_status mpsgpu_mps_approximate(mpsgpu_context* ctx, const mpsgpu_mps* src, int D, mpsgpu_mps** out,
@@ -449,6 +504,16 @@ mpsgpu_status mpsgpu_contract(mpsgpu_context* ctx, const mpsgpu_mps* ket, const 
   if (!ctx || !ket || !bra) return MPSGPU_INVALID;
   return guarded(ctx, [&] {
     cplx r = contract(ctx->c, ket->s, ops ? &ops->m : nullptr, bra->s);
+    if (re) *re = r.x;
+    if (im) *im = r.y;
+  });
+}
+
+mpsgpu_status mpsgpu_contract2(mpsgpu_context* ctx, const mpsgpu_mpo* ops, const mpsgpu_mps* ket,
+                               const mpsgpu_mps* bra, double* re, double* im) {
+  if (!ctx || !ops || !ket) return MPSGPU_INVALID;
+  return guarded(ctx, [&] {
+    cplx r = contract2(ctx->c, ops->m, ket->s, bra ? bra->s : ket->s);
     if (re) *re = r.x;
     if (im) *im = r.y;
   });

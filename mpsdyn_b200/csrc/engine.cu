@@ -66,8 +66,8 @@ void mpo_upload(Context& c, MpoDev& m, int L, const int* dims, const double* con
   for (int k = 0; k < L; k++) {
     const int du = dims[4 * k], wl = dims[4 * k + 1], dd = dims[4 * k + 2], wr = dims[4 * k + 3];
     MPSGPU_CHECK(du > 0 && wl > 0 && dd > 0 && wr > 0, MPSGPU_BAD_SHAPE, "mpo: non-positive dimension");
-    MPSGPU_CHECK(du * wr <= 32 && wl * dd <= 32 && wl * du <= 32 && dd * wr <= 32, MPSGPU_BAD_SHAPE,
-                 "mpo: d*w must not exceed 32");
+    MPSGPU_CHECK(du * wr <= 64 && wl * dd <= 64 && wl * du <= 64 && dd * wr <= 64, MPSGPU_BAD_SHAPE,
+                 "mpo: d*w must not exceed 64");
     if (k > 0) MPSGPU_CHECK(m.dims[k - 1][3] == wl, MPSGPU_BAD_SHAPE, "mpo: bond mismatch");
     m.dims[k] = {du, wl, dd, wr};
     const long long n = (long long)du * wl * dd * wr;
@@ -659,6 +659,52 @@ cplx contract(Context& c, const MpsDev& ket, const MpoDev* ops, const MpsDev& br
   dbuf_free(c, a);
   dbuf_free(c, b);
   return cscale(r, ket.normfact * bra.normfact);
+}
+
+// Contractor::contract2(bra, ops, ket) = <bra|ops^dag ops|ket>
+// (Contractor.cpp:634-718, Operator::contractL2): the doubled operator
+// (O^dag O)(s', b1 b2, s, c1 c2) = sum_t conj(O(t, b1, s', c1)) O(t, b2, s, c2)
+// (bond index b1 + wl b2) is formed on the host from the device copy of O
+// and contracted like any MPO.
+cplx contract2(Context& c, const MpoDev& ops, const MpsDev& ket, const MpsDev& bra) {
+  const int L = ops.L;
+  MPSGPU_CHECK(ket.L == L && bra.L == L, MPSGPU_BAD_SHAPE, "contract2: lengths");
+  std::vector<std::vector<cplx>> dbl(L);
+  std::vector<int> dims(4 * L);
+  std::vector<const double*> ptrs(L);
+  for (int k = 0; k < L; k++) {
+    const auto& w = ops.dims[k];
+    const int du = w[0], wl = w[1], dd = w[2], wr = w[3];
+    std::vector<cplx> W((size_t)du * wl * dd * wr);
+    MPSGPU_CUDA(cudaMemcpyAsync(W.data(), ops.W[k].p, W.size() * sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    auto at = [&](int t, int b, int s, int cc) { return W[t + du * (b + wl * (s + dd * cc))]; };
+    const int WL = wl * wl, WR = wr * wr;
+    dbl[k].assign((size_t)dd * WL * dd * WR, make_double2(0.0, 0.0));
+    for (int sp = 0; sp < dd; sp++)
+      for (int b1 = 0; b1 < wl; b1++)
+        for (int b2 = 0; b2 < wl; b2++)
+          for (int s = 0; s < dd; s++)
+            for (int c1 = 0; c1 < wr; c1++)
+              for (int c2 = 0; c2 < wr; c2++) {
+                cplx acc = make_double2(0.0, 0.0);
+                for (int t = 0; t < du; t++) acc = cadd(acc, ccmul(at(t, b1, sp, c1), at(t, b2, s, c2)));
+                dbl[k][sp + dd * ((b1 + wl * b2) + WL * (s + dd * (c1 + wr * c2)))] = acc;
+              }
+    dims[4 * k] = dd; dims[4 * k + 1] = WL; dims[4 * k + 2] = dd; dims[4 * k + 3] = WR;
+    ptrs[k] = reinterpret_cast<const double*>(dbl[k].data());
+  }
+  MpoDev two;
+  mpo_upload(c, two, L, dims.data(), ptrs.data(), false);
+  cplx r;
+  try {
+    r = contract(c, ket, &two, bra);
+  } catch (...) {
+    mpo_free(c, two);
+    throw;
+  }
+  mpo_free(c, two);
+  return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -1280,10 +1326,6 @@ void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, i
               double* errN, double* errT, Counters& cnt) {
   const int L = orig.L;
   MPSGPU_CHECK(ops.L == L && init.L == L, MPSGPU_BAD_SHAPE, "optimize: lengths");
-  // errN = <orig|ops^dag ops|orig> + <init|init> - 2 Re <init|ops|orig>
-  // (Contractor.cpp:263-276) needs the doubled operator of
-  // Contractor::contract2, which this library does not provide yet.
-  MPSGPU_CHECK(errN == nullptr, MPSGPU_INVALID, "optimize: errN is not provided (pass null)");
   prepare_init(c, init, D);
   EnvCache E;
   E.init(c, L);
@@ -1360,7 +1402,15 @@ void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, i
   init.normfact = c2.x / c1.x;
   init.normfact *= orig.normfact;
   cnt.rounds += round;
-  (void)errT;
+  // errN = <orig|ops^dag ops|orig> + <init|init> - 2 Re <init|ops|orig>,
+  // errT = the first term (Contractor.cpp:263-276)
+  if (errN) {
+    const double norm0 = contract2(c, ops, orig, orig).x;
+    const double norm1 = contract(c, init, nullptr, init).x;
+    const cplx cross = contract(c, orig, &ops, init);
+    *errN = norm0 + norm1 - 2.0 * cross.x;
+    if (errT) *errT = norm0;
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -151,6 +151,7 @@ double find_next_excited_state(Context& c, const MpoDev& ops, int D,
 void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, int D,
               const SolveOptions& opt, double* errN, double* errT, Counters& cnt);
 cplx contract(Context& c, const MpsDev& ket, const MpoDev* ops, const MpsDev& bra);
+cplx contract2(Context& c, const MpoDev& ops, const MpsDev& ket, const MpsDev& bra);
 void expectation_local(Context& c, const MpsDev& s, const double* op, double* out);
 void schmidt_values(Context& c, const MpsDev& s, int pos, std::vector<double>& vals);
 double entropy(Context& c, const MpsDev& s, int pos);

@@ -458,6 +458,31 @@ def contract_overlap(ket: MPS, bra: MPS) -> complex:
     return complex(ket.normfact * bra.normfact * E.reshape(-1)[0])
 
 
+def doubled_mpo(ops: list) -> list:
+    """The operator O^dag O as an MPO: (O^dag O)(s', b1 b2, s, c1 c2) =
+    sum_t conj(O(t, b1, s', c1)) O(t, b2, s, c2), bond index b1 + wl b2."""
+    out = []
+    for W in ops:
+        du, wl, dd, wr = W.shape
+        X = np.einsum("tbpc,tqse->pbqsce", W.conj(), W)           # (s', b1, b2, s, c1, c2)
+        out.append(X.reshape(dd, wl * wl, dd, wr * wr, order="F"))
+    return out
+
+
+def contract2(ops: list, ket: MPS, bra: MPS = None) -> complex:
+    """Contractor::contract2(bra, ops, ket) = <bra|ops^dag ops|ket>
+    (Contractor.cpp:634-718; contract2(ops, ket) when bra is ket)."""
+    return contract_op(ket, doubled_mpo(ops), bra if bra is not None else ket)
+
+
+def optimize_error(ops: list, orig: MPS, init: MPS):
+    """errN and errT of Contractor::optimize (Contractor.cpp:263-276)."""
+    norm0 = contract2(ops, orig).real
+    norm1 = contract_overlap(init, init).real
+    cross = contract_op(orig, ops, init)
+    return norm0 + norm1 - 2 * cross.real, norm0
+
+
 # ---------------------------------------------------------------------------
 # QR / LQ gauge moves (core/cpp/Site.cpp:179-283, core/cpp/MPS.cpp:306-419)
 # ---------------------------------------------------------------------------

@@ -34,6 +34,8 @@
  *   entropy mps pos                Contractor::getEntropy             (Contractor.cpp:2045-2076)
  *   schmidt mps pos                Contractor::getSchmidtValues       (Contractor.cpp:2243-2270)
  *   truncate mps D out             MPS(mps, D) (SVD cut, MPS.cpp:761-772)
+ *   contract2 model mps            Contractor::contract2(H, mps) = <mps|H^dag H|mps> (Contractor.cpp:634-653)
+ *   opterr model delta imag D mps  one Contractor::optimize step with errN, errT (Contractor.cpp:263-276)
  *   applympo model delta imag D dagger dir mps out
  *                                  U-MPO of getUMPO applied to mps: MPS::applyExactly (D = 0) or
  *                                  MPS::approximate (D > 0), MPS.cpp:853-936
@@ -222,6 +224,23 @@ int main(int argc, const char* argv[]) {
     complex_t e = contractor.contract(s, m.H(), s);
     complex_t n = contractor.contract(s, s);
     print_json({{"E_re", e.re}, {"E_im", e.im}, {"norm_re", n.re}});
+  } else if (cmd == "contract2") {
+    Model m = make_model(argv[2]);
+    MPS s;
+    s.importMPS(argv[3]);
+    complex_t v = contractor.contract2(m.H(), s);
+    print_json({{"re", v.re}, {"im", v.im}});
+  } else if (cmd == "opterr") {
+    Model m = make_model(argv[2]);
+    MPO U(m.L);
+    m.ising->getUMPO(U, atof(argv[3]), 0., atoi(argv[4]) != 0, 2);
+    contractor.setConvTol(1e-10);
+    MPS orig;
+    orig.importMPS(argv[6]);
+    MPS init(orig);
+    double errN = 0., errT = 0.;
+    contractor.optimize(U, orig, init, atoi(argv[5]), &errN, &errT);
+    print_json({{"errN", errN}, {"errT", errT}, {"normfact", init.getNormFact()}});
   } else if (cmd == "gs") {
     Model m = make_model(argv[2]);
     int D = atoi(argv[3]);

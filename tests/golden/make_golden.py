@@ -146,6 +146,16 @@ def main() -> None:
     golden["ising_L12_init16_D6_seed4_E0"] = run("gs", "ising:12:1:1:0", 6, 1e-10, 0, fg,
                                                  os.path.join(tmp, "g_out.mps"))["E0"]
 
+    # <psi|H^dag H|psi> (Contractor::contract2) and the errN / errT of one
+    # optimize step
+    fc = os.path.join(tmp, "c2.mps")
+    mo.write_mps(fc, mo.random_mps(8, 2, 6, 7))
+    golden["contract2_ising_L8_D6_seed7"] = run("contract2", "ising:8:1:1.1:0.2", fc)["re"]
+    golden["contract2_schwinger_N8_D6_seed7"] = run("contract2", "schwinger:8:2.5:100:0:0", fc)["re"]
+    mo.write_mps(fc, mo.random_state(8, 2, 6, 9))
+    r = run("opterr", "ising:8:1:1.1:0.2", 0.05, 0, 6, fc)
+    golden["opterr_ising_L8_D6_state9_ureal005"] = [r["errN"], r["errT"], r["normfact"]]
+
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print(json.dumps({k: (v if not isinstance(v, list) else v[:3]) for k, v in golden.items()}, indent=1))

@@ -236,3 +236,21 @@ def test_gs_with_small_krylov_space_restarts(ctx, golden, krylov):
     e, st = ctx.find_ground_state(ops, 20, s, 0.0, ctx.options(convtol=1e-10, max_krylov=krylov))
     ref = golden["ising_L20_D20_seed0_E0"]
     assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
+
+
+def test_contract2_matches_reference(ctx, golden):
+    s = ctx.mps(mo.random_mps(8, 2, 6, 7).sites)
+    for key, H in (("contract2_ising_L8_D6_seed7", mo.ising_hmpo(8, 1, 1.1, 0.2)),
+                   ("contract2_schwinger_N8_D6_seed7", mo.schwinger_hmpo(8, 2.5, 100.0))):
+        v = ctx.contract2(ctx.mpo(H), s)
+        assert abs(v.real - golden[key]) < 1e-12 * abs(golden[key]), (key, v)
+
+
+def test_optimize_error_matches_reference(ctx, golden):
+    orig = ctx.mps_random_state(8, 2, 6, 9)
+    init = orig.copy()
+    U = ctx.mpo(mo.ising_umpo(8, 1.0, 1.1, 0.2, 0.05, False))
+    errN, errT, _ = ctx.optimize(U, orig, init, 6, ctx.options(convtol=1e-10), want_err=True)
+    rN, rT, rnf = golden["opterr_ising_L8_D6_state9_ureal005"]
+    assert abs(errN - rN) < 1e-11 and abs(errT - rT) < 1e-12
+    assert abs(init.info()[2] - rnf) < 1e-12

@@ -196,3 +196,21 @@ def test_gs_prologue_truncates_large_initial_bond(golden):
     e = mo.find_ground_state(mo.ising_hmpo(12, 1, 1, 0), 6, m, convtol=1e-10)
     ref = golden["ising_L12_init16_D6_seed4_E0"]
     assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
+
+
+def test_contract2_matches_reference(golden):
+    m = mo.random_mps(8, 2, 6, 7)
+    for key, H in (("contract2_ising_L8_D6_seed7", mo.ising_hmpo(8, 1, 1.1, 0.2)),
+                   ("contract2_schwinger_N8_D6_seed7", mo.schwinger_hmpo(8, 2.5, 100.0))):
+        v = mo.contract2(H, m)
+        assert abs(v.real - golden[key]) < 1e-12 * abs(golden[key]), (key, v)
+
+
+def test_optimize_error_matches_reference(golden):
+    orig = mo.random_state(8, 2, 6, 9)
+    init = orig.copy()
+    U = mo.ising_umpo(8, 1.0, 1.1, 0.2, 0.05, False)
+    mo.optimize(U, orig, init, 6, convtol=1e-10)
+    errN, errT = mo.optimize_error(U, orig, init)
+    rN, rT, rnf = golden["opterr_ising_L8_D6_state9_ureal005"]
+    assert abs(errN - rN) < 1e-11 and abs(errT - rT) < 1e-12 and abs(init.normfact - rnf) < 1e-12
