@@ -188,6 +188,19 @@ mpsgpu_status mpsgpu_find_ground_state(mpsgpu_context* ctx, const mpsgpu_mpo* op
                                        int D, double offset,
                                        const mpsgpu_options* opt, mpsgpu_mps* init,
                                        double* lambda, mpsgpu_stats* stats);
+/* Two-site DMRG ground state.  No counterpart in the reference (its sweeps
+ * are single-site): each bond (k, k+1) is optimised as one two-site tensor
+ * with the same thick-restart Lanczos, then split by an SVD cut to at most D
+ * (singular values moved in the sweep direction), so bonds grow from the
+ * initial state up to D.  Convergence as findGroundState: |E_old - E_new| <
+ * convtol |E + offset| at the chain ends.  max_discarded (nullable): the
+ * largest relative discarded weight sum_{i>=K} s_i^2 / sum s_i^2 of any cut
+ * in the run.  init is overwritten with the result (normalised). */
+mpsgpu_status mpsgpu_find_ground_state_two_site(mpsgpu_context* ctx, const mpsgpu_mpo* ops,
+                                                int D, double offset,
+                                                const mpsgpu_options* opt, mpsgpu_mps* init,
+                                                double* lambda, double* max_discarded,
+                                                mpsgpu_stats* stats);
 /* findNextExcitedState(ops, D, levels, &lambda, init, offset)
  * (Contractor.cpp:2676-2727 -> findGroundStateWithProjectorPenalty :2739-2956). */
 mpsgpu_status mpsgpu_find_next_excited_state(mpsgpu_context* ctx,

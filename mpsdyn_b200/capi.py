@@ -25,7 +25,7 @@ EXPORTS = [
     "mpsgpu_mpo_free", "mpsgpu_mpo_info", "mpsgpu_mpo_download", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger",
     "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_random_state", "mpsgpu_mps_product",
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
-    "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_next_excited_state",
+    "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_ground_state_two_site", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_contract2", "mpsgpu_expectation_local", "mpsgpu_entropy",
     "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped",
     "mpsgpu_env_left", "mpsgpu_env_right",
@@ -81,6 +81,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         lib.mpsgpu_mps_random_state.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(P)]
         lib.mpsgpu_find_ground_state.argtypes = [P, P, C.c_int, C.c_double, C.POINTER(Options), P,
                                                  C.POINTER(C.c_double), C.POINTER(Stats)]
+        lib.mpsgpu_find_ground_state_two_site.argtypes = [P, P, C.c_int, C.c_double, C.POINTER(Options), P,
+                                                          C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(Stats)]
         lib.mpsgpu_find_next_excited_state.argtypes = [P, P, C.c_int, C.POINTER(P), C.c_int, C.c_double,
                                                        C.POINTER(Options), P, C.POINTER(C.c_double),
                                                        C.POINTER(Stats)]
@@ -222,6 +224,16 @@ class Context:
         self._check(self.lib.mpsgpu_find_ground_state(self.h, ops.h, D, offset, C.byref(o), init.h,
                                                       C.byref(e), C.byref(st)))
         return e.value, st.as_dict()
+
+    def find_ground_state_two_site(self, ops: "DeviceMPO", D: int, init: "DeviceMPS", offset: float = 0.0,
+                                   opts: Options = None):
+        """Two-site DMRG; returns (energy, max relative discarded weight, stats)."""
+        e, dw = C.c_double(), C.c_double()
+        st = Stats()
+        o = opts or self.options()
+        self._check(self.lib.mpsgpu_find_ground_state_two_site(self.h, ops.h, D, offset, C.byref(o), init.h,
+                                                               C.byref(e), C.byref(dw), C.byref(st)))
+        return e.value, dw.value, st.as_dict()
 
     def find_next_excited_state(self, ops, D, levels, init, offset=0.0, opts=None):
         e = C.c_double()

@@ -461,6 +461,23 @@ mpsgpu_status mpsgpu_find_ground_state(mpsgpu_context* ctx, const mpsgpu_mpo* op
   return st;
 }
 
+mpsgpu_status mpsgpu_find_ground_state_two_site(mpsgpu_context* ctx, const mpsgpu_mpo* ops, int D, double offset,
+                                                const mpsgpu_options* opt, mpsgpu_mps* init, double* lambda,
+                                                double* max_discarded, mpsgpu_stats* stats) {
+  if (!ctx || !ops || !init || !lambda) return MPSGPU_INVALID;
+  Counters cnt;
+  double t0 = now_s();
+  mpsgpu_status st = guarded(ctx, [&] {
+    mpsgpu_options dflt;
+    mpsgpu_default_options(&dflt);
+    *lambda = find_ground_state_two_site(ctx->c, ops->m, D, init->s, offset, to_opts(opt ? opt : &dflt), cnt,
+                                         max_discarded);
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+  fill_stats(stats, cnt, now_s() - t0);
+  return st;
+}
+
 mpsgpu_status mpsgpu_find_next_excited_state(mpsgpu_context* ctx, const mpsgpu_mpo* ops, int D,
                                              const mpsgpu_mps* const* levels, int nlevels, double offset,
                                              const mpsgpu_options* opt, mpsgpu_mps* init, double* lambda,

@@ -1110,6 +1110,170 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
   return energy;
 }
 
+// ---------------------------------------------------------------------------
+// Two-site DMRG (no counterpart in the reference, whose sweeps are single
+// site): the bond between sites k and k+1 is optimised as one tensor
+// Theta(a, s1, s2, r) and split by a cut SVD, so bonds grow up to D and the
+// discarded weight of every cut is known.
+// ---------------------------------------------------------------------------
+
+// y = L W_k W_{k+1} R x for x = Theta (device layout a, s1, s2, r):
+//   T1[(a',b),(s1,s2,r)] = L . X                          GEMM
+//   T2[a',s1',c,(s2,r)]  = sum_{b,s1} W_k[s1',b,s1,c] T1    leg kernel
+//   T3[(a',s1'),s2',r,e] = sum_{c,s2} W_k+1[s2',c,s2,e] T2  leg kernel
+//   Y[(a',s1',s2'),r']   = T3 . Rt + offset X              GEMM
+static void heff2_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpoDev& m, int k,
+                        const cplx* Rt, const std::array<int, 3>& rd, const cplx* x, cplx* y, cplx offset,
+                        Counters* cnt) {
+  const auto& w1 = m.dims[k];
+  const auto& w2 = m.dims[k + 1];
+  const int du1 = w1[0], wl = w1[1], d1 = w1[2], wc = w1[3];
+  const int du2 = w2[0], d2 = w2[2], we = w2[3];
+  const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
+  MPSGPU_CHECK(ld[1] == wl && rd[1] == we && w2[1] == wc, MPSGPU_BAD_SHAPE, "heff2: MPO bond mismatch");
+  dbuf_reserve(c, c.t1, (long long)Dlb * wl * d1 * d2 * Drk);
+  GemmArgs g;
+  g.M = Dlb * wl; g.N = d1 * d2 * Drk; g.K = Dlk;
+  g.A = Le; g.lda = (long long)Dlb * wl;
+  g.B = x; g.ldb = Dlk;
+  g.C = c.t1.p; g.ldc = (long long)Dlb * wl;
+  zgemm(c.st(), g, c.scratch);
+  dbuf_reserve(c, c.t2, (long long)Dlb * du1 * wc * d2 * Drk);
+  WContractArgs a1;
+  a1.nx = Dlb; a1.ny = d2 * Drk;
+  a1.in = c.t1.p; a1.ix = 1; a1.iy = (long long)Dlb * wl * d1; a1.si0 = Dlb; a1.si1 = (long long)Dlb * wl;
+  a1.n_i0 = wl; a1.n_i1 = d1;
+  a1.out = c.t2.p; a1.ox = 1; a1.oy = (long long)Dlb * du1 * wc; a1.so0 = Dlb; a1.so1 = (long long)Dlb * du1;
+  a1.n_o0 = du1; a1.n_o1 = wc;
+  a1.Wm = m.Wlr[k].p;
+  wcontract(c.st(), a1);
+  dbuf_reserve(c, c.t3, (long long)Dlb * du1 * du2 * Drk * we);
+  WContractArgs a2;
+  a2.nx = Dlb * du1; a2.ny = Drk;
+  a2.in = c.t2.p; a2.ix = 1; a2.iy = (long long)Dlb * du1 * wc * d2;
+  a2.si0 = (long long)Dlb * du1; a2.si1 = (long long)Dlb * du1 * wc;
+  a2.n_i0 = wc; a2.n_i1 = d2;
+  a2.out = c.t3.p; a2.ox = 1; a2.oy = (long long)Dlb * du1 * du2;
+  a2.so0 = (long long)Dlb * du1; a2.so1 = (long long)Dlb * du1 * du2 * Drk;
+  a2.n_o0 = du2; a2.n_o1 = we;
+  a2.Wm = m.Wlr[k + 1].p;
+  wcontract(c.st(), a2);
+  GemmArgs h;
+  h.M = Dlb * du1 * du2; h.N = Drb; h.K = Drk * we;
+  h.A = c.t3.p; h.lda = (long long)Dlb * du1 * du2;
+  h.B = Rt; h.ldb = (long long)Drk * we;
+  h.C = y; h.ldc = (long long)Dlb * du1 * du2;
+  if (offset.x != 0.0 || offset.y != 0.0) {
+    h.Cin = x; h.ldcin = (long long)Dlb * du1 * du2; h.beta = offset;
+  }
+  zgemm(c.st(), h, c.scratch);
+  if (cnt) {
+    cnt->matvecs++;
+    cnt->flops += 8.0 * ((double)Dlb * wl * Dlk * d1 * d2 * Drk + (double)Dlb * du1 * wc * wl * d1 * d2 * Drk +
+                         (double)Dlb * du1 * du2 * we * wc * d2 * Drk + (double)Dlb * du1 * du2 * Drk * we * Drb);
+  }
+}
+
+double find_ground_state_two_site(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
+                                  const SolveOptions& opt, Counters& cnt, double* max_discarded) {
+  const int L = ops.L;
+  MPSGPU_CHECK(L >= 2 && init.L == L, MPSGPU_BAD_SHAPE, "two-site DMRG: lengths");
+  MPSGPU_CHECK(D > 0, MPSGPU_INVALID, "two-site DMRG: D must be positive");
+  for (int k = 0; k < L; k++)
+    MPSGPU_CHECK(init.dims[k][0] == ops.dims[k][2] && ops.dims[k][0] == ops.dims[k][2], MPSGPU_BAD_SHAPE,
+                 "two-site DMRG: physical dimensions differ");
+  // start from a normalised right-canonical state; the cut SVDs set the bonds
+  if (init.bond > D) {
+    mps_gauge_all(c, init, 'L', false, D, nullptr);
+    init.bond = init.max_bond();
+  }
+  mps_gauge_all(c, init, 'R', true);
+  mps_gauge_all(c, init, 'L', true);
+  EnvCache E;
+  E.init(c, L);
+  DBuf th;
+  double energy = contract(c, init, &ops, init).x;
+  double val = energy, dmax = 0.0;
+  bool right = true, done = false;
+  int pos = 0, round = 0;
+  const double tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
+  const cplx off = make_double2(offset, 0.0);
+  try {
+    while (!done) {
+      opt.check_cancel();
+      calc_left(c, E, pos, &ops, init, init, &cnt);
+      calc_right(c, E, pos + 1, &ops, init, init, &cnt);
+      const auto da = init.dims[pos], db = init.dims[pos + 1];
+      const int Dl = da[1], d1 = da[0], mid = da[2], d2 = db[0], Dr = db[2];
+      MPSGPU_CHECK(db[1] == mid, MPSGPU_BAD_SHAPE, "two-site DMRG: bond mismatch");
+      const long long N = (long long)Dl * d1 * d2 * Dr;
+      dbuf_reserve(c, th, N);
+      GemmArgs g;
+      g.M = Dl * d1; g.N = d2 * Dr; g.K = mid;
+      g.A = init.A[pos].p; g.lda = (long long)Dl * d1;
+      g.B = init.A[pos + 1].p; g.ldb = mid;
+      g.C = th.p; g.ldc = (long long)Dl * d1;
+      zgemm(c.st(), g, c.scratch);
+      const cplx* Le = E.Le[pos].p;
+      const cplx* Rt = E.Re[pos + 1].p;
+      const auto ld = E.ldims[pos];
+      const auto rd = E.rdims[pos + 1];
+      auto apply = [&](const cplx* xin, cplx* yout) { heff2_apply(c, Le, ld, ops, pos, Rt, rd, xin, yout, off, &cnt); };
+      int its = 0;
+      const double theta = lanczos_lowest(c, (int)N, apply, th.p, tol, opt.max_krylov, &its);
+      cnt.site_solves++;
+      val = theta - offset;
+      // split Theta (Dl d1 x d2 Dr) = U S V^H, cut to D; the singular values
+      // go right on a right move and left on a left move
+      const int m = Dl * d1, n = d2 * Dr;
+      const int Kmax = std::min(m, n);
+      dbuf_reserve(c, c.matQ, (long long)m * Kmax);
+      dbuf_reserve(c, c.matR, (long long)Kmax * n);
+      std::vector<double> sv;
+      const int K = svd_cut(c.st(), m, n, th.p, m, D, c.matQ.p, c.matR.p, sv, c.scratch, !right);
+      double dw = 0.0, tot = 0.0;
+      for (size_t j = 0; j < sv.size(); j++) {
+        tot += sv[j] * sv[j];
+        if ((int)j >= K) dw += sv[j] * sv[j];
+      }
+      if (tot > 0) dmax = std::max(dmax, dw / tot);
+      init.dims[pos] = {d1, Dl, K};
+      init.dims[pos + 1] = {d2, K, Dr};
+      dbuf_reserve(c, init.A[pos], (long long)m * K);
+      dbuf_reserve(c, init.A[pos + 1], (long long)K * n);
+      zcopy(c.st(), m * K, c.matQ.p, init.A[pos].p);
+      zcopy(c.st(), K * n, c.matR.p, init.A[pos + 1].p);
+      for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
+      for (int l = pos; l >= 0; l--) E.outofdate_r(l);
+      const bool at_end = (right && pos == L - 2) || (!right && pos == 0);
+      if (at_end) {
+        done = std::fabs(energy - val) < opt.convtol * std::fabs(energy + offset);
+        if (!done && std::fabs(val) < 1e-13) done = true;
+        energy = val;
+        if (opt.verbose) printf("mpsgpu: two-site round %d energy %.15g max discarded %.3g\n", round, val, dmax);
+        right = !right;  // the same bond is solved again in the new direction
+        round++;
+        if (!done && round >= opt.max_rounds)
+          throw Error(MPSGPU_NOT_CONVERGED, "two-site DMRG: round limit reached");
+      } else {
+        pos += right ? 1 : -1;
+      }
+    }
+  } catch (...) {
+    E.release(c);
+    dbuf_free(c, th);
+    throw;
+  }
+  E.release(c);
+  dbuf_free(c, th);
+  init.bond = init.max_bond();
+  init.gauge = 0;
+  init.normfact = 1.0;
+  cnt.rounds += round;
+  if (max_discarded) *max_discarded = dmax;
+  return energy;
+}
+
 }  // namespace mpsgpu
 
 namespace mpsgpu {

@@ -145,6 +145,8 @@ void env_right_update(Context& c, const cplx* Rt, const std::array<int, 3>& rd, 
 // ---- algorithms (Contractor) ----
 double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
                          const SolveOptions& opt, Counters& cnt);
+double find_ground_state_two_site(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
+                                  const SolveOptions& opt, Counters& cnt, double* max_discarded);
 double find_next_excited_state(Context& c, const MpoDev& ops, int D,
                                const std::vector<const MpsDev*>& levels, MpsDev& init,
                                double offset, const SolveOptions& opt, Counters& cnt);

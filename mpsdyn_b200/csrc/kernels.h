@@ -166,7 +166,7 @@ std::vector<double> singular_values(const Stream& st, int m, int n, const cplx* 
 // Thin SVD with the cut of wrapper::svd(A, 0, cut): U (m x keep, ld m),
 // diag(s) V^H (keep x n, ld keep); all min(m, n) values in sv; returns keep.
 int svd_cut(const Stream& st, int m, int n, const cplx* A, long long lda, int cut, cplx* U, cplx* SVh,
-            std::vector<double>& sv, Scratch& scratch);
+            std::vector<double>& sv, Scratch& scratch, bool left_s = false);
 
 // ---- Householder QR (LAPACK zgeqrf/zungqr conventions) ----
 // Factor the m x n column-major matrix A (ld = m; overwritten by R above and

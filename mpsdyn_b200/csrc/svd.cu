@@ -165,9 +165,10 @@ namespace {
 // j-th largest value).  Not transposed (m >= n, W = A V): U[:, j] =
 // W[:, idx_j] / s_j, SVh[j, :] = s_j V[:, idx_j]^H.  Transposed (W = A^H V'):
 // A = V' S U'^H, so U[:, j] = V'[:, idx_j] and SVh[j, :] = W[:, idx_j]^H.
+// left_s moves diag(s) to the left factor: U diag(s) and V^H.
 __global__ void svd_finish_kernel(int m, int n, int rows, int cols, bool tr, const cplx* __restrict__ W,
                                   const cplx* __restrict__ V, const int* __restrict__ idx,
-                                  const double* __restrict__ sig, int keep, cplx* __restrict__ U,
+                                  const double* __restrict__ sig, int keep, bool left_s, cplx* __restrict__ U,
                                   cplx* __restrict__ SVh) {
   const long long totU = (long long)m * keep, totS = (long long)keep * n;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < totU + totS;
@@ -175,12 +176,15 @@ __global__ void svd_finish_kernel(int m, int n, int rows, int cols, bool tr, con
     if (t < totU) {
       const int i = (int)(t % m), j = (int)(t / m);
       const int c = idx[j];
-      U[t] = tr ? V[i + (long long)c * cols] : cscale(W[i + (long long)c * rows], 1.0 / sig[c]);
+      cplx u = tr ? V[i + (long long)c * cols] : cscale(W[i + (long long)c * rows], 1.0 / sig[c]);
+      if (left_s) u = cscale(u, sig[c]);
+      U[t] = u;
     } else {
-      const long long u = t - totU;
-      const int j = (int)(u % keep), k = (int)(u / keep);
+      const long long q = t - totU;
+      const int j = (int)(q % keep), k = (int)(q / keep);
       const int c = idx[j];
-      const cplx x = tr ? W[k + (long long)c * rows] : cscale(V[k + (long long)c * cols], sig[c]);
+      cplx x = tr ? W[k + (long long)c * rows] : cscale(V[k + (long long)c * cols], sig[c]);
+      if (left_s) x = cscale(x, 1.0 / sig[c]);
       SVh[j + (long long)k * keep] = make_double2(x.x, -x.y);
     }
   }
@@ -197,9 +201,10 @@ __global__ void identity_kernel(int n, cplx* __restrict__ V) {
 // Thin SVD with the cut of wrapper::svd(A, tol = 0, Xi = cut) (svd.cpp:23-118):
 // keep = min(cut, min(m, n)) (cut <= 0: all), then only the values > 0 among
 // those.  A (m x n, ld m) is not modified.  Writes U (m x keep, ld m) and
-// diag(s) V^H (keep x n, ld keep); sv gets all min(m, n) values descending.
+// diag(s) V^H (keep x n, ld keep) -- or, with left_s, U diag(s) and V^H;
+// sv gets all min(m, n) values descending.
 int svd_cut(const Stream& st, int m, int n, const cplx* A, long long lda, int cut, cplx* U, cplx* SVh,
-            std::vector<double>& sv, Scratch& scratch) {
+            std::vector<double>& sv, Scratch& scratch, bool left_s) {
   MPSGPU_CHECK(m > 0 && n > 0, MPSGPU_BAD_SHAPE, "svd: empty matrix");
   const bool tr = n > m;
   const int rows = tr ? n : m;
@@ -242,7 +247,7 @@ int svd_cut(const Stream& st, int m, int n, const cplx* A, long long lda, int cu
   MPSGPU_CUDA(cudaMemcpyAsync(d_idx, idx.data(), keep * sizeof(int), cudaMemcpyHostToDevice, st.s));
   const long long tot = (long long)m * keep + (long long)keep * n;
   svd_finish_kernel<<<std::min(ceil_div(tot, 256), 1184), 256, 0, st.s>>>(m, n, rows, colsp, tr, W, V, d_idx,
-                                                                           d_sig, keep, U, SVh);
+                                                                           d_sig, keep, left_s, U, SVh);
   after_launch(st);
   // idx is a host vector: wait for its copy before it goes out of scope
   MPSGPU_CUDA(cudaStreamSynchronize(st.s));

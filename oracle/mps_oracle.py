@@ -818,6 +818,88 @@ def find_ground_state(ops: list, D: int, mps: MPS, offset: float = 0.0,
     return energy
 
 
+def heff2_apply(L: np.ndarray, W1: np.ndarray, W2: np.ndarray, R: np.ndarray, T: np.ndarray) -> np.ndarray:
+    """Two-site effective Hamiltonian on Theta[s1, s2, a, r]:
+    y[s1',s2',a',r'] = sum L[a',b,a] W1[s1',b,s1,c] W2[s2',c,s2,e] R[r',e,r] T[s1,s2,a,r]."""
+    return np.einsum("pba,ubsc,vcte,qer,star->uvpq", L, W1, W2, R, T, optimize=True)
+
+
+def find_ground_state_two_site(ops: list, D: int, mps: MPS, offset: float = 0.0, convtol: float = 1e-5,
+                               eigtol: float = 0.0, stats: SweepStats = None):
+    """Two-site DMRG as the library runs it (no counterpart in the reference,
+    whose sweeps are single site): start from gaugeCond('R',1) then
+    gaugeCond('L',1) (after a cut to D if the state is larger), optimise the
+    bond (pos, pos+1) with the lowest eigenpair of the two-site H_eff, split
+    by svd_cut(Theta, D) with the singular values moved in the sweep
+    direction, and at a chain end solve the same bond again in the other
+    direction.  Convergence |E_old - E_new| < convtol |E + offset| at the
+    ends.  Returns (energy, max relative discarded weight)."""
+    st = stats if stats is not None else SweepStats()
+    L = mps.L
+    if D < mps.bond:
+        t = truncate_mps(mps, D)
+        mps.sites, mps.normfact = t.sites, t.normfact
+        mps.bond = t.max_bond()
+    gauge_cond_all(mps, "R", True)
+    gauge_cond_all(mps, "L", True)
+    cache = EnvCache(L)
+    energy = contract_op(mps, ops, mps).real
+    val, dmax = energy, 0.0
+    right, pos, rnd, done = True, 0, 0, False
+    tol = eigtol if eigtol > 0 else 1e-12
+    while not done:
+        Lenv = cache.left(pos, ops, mps, mps)
+        Renv = cache.right(pos + 1, ops, mps, mps)
+        A1, A2 = mps.sites[pos], mps.sites[pos + 1]
+        d1, Dl, _ = A1.shape
+        d2, _, Dr = A2.shape
+        T = np.einsum("sam,tmr->star", A1, A2)
+        shape = T.shape
+        n = T.size
+
+        def mv(v, L_=Lenv, R_=Renv, W1=ops[pos], W2=ops[pos + 1]):
+            st.matvecs += 1
+            return (heff2_apply(L_, W1, W2, R_, v.reshape(shape, order="F")).ravel(order="F")
+                    + offset * v)
+
+        def dense():
+            return np.array([mv(e) for e in np.eye(n, dtype=np.complex128)]).T
+
+        theta, x = lowest_eigpair(mv, n, T.ravel(order="F"), dense=dense if n <= 128 else None, tol=tol)
+        st.site_solves += 1
+        val = theta - offset
+        T = x.reshape(shape, order="F")
+        M = T.transpose(0, 2, 1, 3).reshape(d1 * Dl, d2 * Dr, order="F")      # rows (s1, a), cols (s2, r)
+        U, s, Vh, w = svd_cut(M, D)
+        tot = float(np.sum(np.linalg.svd(M, compute_uv=False) ** 2))
+        dmax = max(dmax, w / tot if tot > 0 else 0.0)
+        K = s.size
+        if right:
+            left, rightf = U, s[:, None] * Vh
+        else:
+            left, rightf = U * s[None, :], Vh
+        mps.sites[pos] = np.ascontiguousarray(left.reshape(d1, Dl, K, order="F"))
+        mps.sites[pos + 1] = np.ascontiguousarray(
+            rightf.reshape(K, d2, Dr, order="F").transpose(1, 0, 2))
+        for l in range(pos + 1, L):
+            cache.outofdate_l(l)
+        for l in range(pos, -1, -1):
+            cache.outofdate_r(l)
+        if (right and pos == L - 2) or (not right and pos == 0):
+            done = abs(energy - val) < convtol * abs(energy + offset)
+            if not done and abs(val) < 1e-13:
+                done = True
+            energy = val
+            right = not right
+            rnd += 1
+        else:
+            pos += 1 if right else -1
+    st.rounds += rnd
+    mps.normfact = 1.0
+    mps.bond = mps.max_bond()
+    return energy, dmax
+
+
 def find_next_excited_state(ops: list, D: int, levels: list, mps: MPS, offset: float = 0.0,
                             convtol: float = 1e-5, eigtol: float = 0.0, excorthtol: float = 0.0,
                             stats: SweepStats = None):

@@ -214,3 +214,11 @@ def test_optimize_error_matches_reference(golden):
     errN, errT = mo.optimize_error(U, orig, init)
     rN, rT, rnf = golden["opterr_ising_L8_D6_state9_ureal005"]
     assert abs(errN - rN) < 1e-11 and abs(errT - rT) < 1e-12 and abs(init.normfact - rnf) < 1e-12
+
+
+def test_two_site_oracle_exact_tfim():
+    L, g = 8, 1.3
+    m = mo.product_mps(L, 2, 1)
+    e, dw = mo.find_ground_state_two_site(mo.ising_hmpo(L, 1, g, 0), 16, m, convtol=1e-10)
+    exact = mo.tfim_open_energy(L, 1, g)
+    assert abs(e - exact) <= 1e-10 * abs(exact) and dw == 0.0
