@@ -111,6 +111,10 @@ def main() -> None:
     # Imaginary-time evolution from MPS(L, D, d) (testIsing.cpp:106-138)
     r = run("imag", "ising:10:1:1:0", 6, 20, 0.05, 1e-10)
     golden["ising_L10_D6_imag_dt005_energies"] = r["energies"]
+    # the full imaginary-time phase of the L=20 Ising configuration
+    # (testIsing.cpp with M = 200, delta = 0.01, D = 20)
+    r = run("imag", "ising:20:1:1:0", 20, 200, 0.01, 1e-10)
+    golden["ising_L20_D20_imag_dt001_M200_energies"] = r["energies"]
 
     # Real-time quench from |0...0> with D=1 initial bonds
     fq = os.path.join(tmp, "q.mps")

@@ -254,3 +254,21 @@ def test_optimize_error_matches_reference(ctx, golden):
     rN, rT, rnf = golden["opterr_ising_L8_D6_state9_ureal005"]
     assert abs(errN - rN) < 1e-11 and abs(errT - rT) < 1e-12
     assert abs(init.info()[2] - rnf) < 1e-12
+
+
+def test_imaginary_time_L20_config_matches_reference(ctx, golden):
+    # testIsing.cpp's imaginary-time phase at L = 20, D = 20: 200 steps of
+    # delta = 0.01 from MPS(L, D, d)
+    L, D = 20, 20
+    H = ctx.mpo(mo.ising_hmpo(L, 1, 1, 0))
+    U = ctx.mpo(mo.ising_umpo(L, 1, 1, 0, 0.01, True))
+    st = ctx.mps_product(L, 2, D)
+    o = ctx.options(convtol=1e-10)
+    es = []
+    for _ in range(200):
+        aux = st.copy()
+        ctx.optimize(U, aux, st, D, o)
+        aux.free()
+        st.gauge("R")
+        es.append(ctx.contract(st, H, st).real)
+    np.testing.assert_allclose(es, golden["ising_L20_D20_imag_dt001_M200_energies"], rtol=1e-10, atol=0)

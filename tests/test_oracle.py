@@ -222,3 +222,16 @@ def test_two_site_oracle_exact_tfim():
     e, dw = mo.find_ground_state_two_site(mo.ising_hmpo(L, 1, g, 0), 16, m, convtol=1e-10)
     exact = mo.tfim_open_energy(L, 1, g)
     assert abs(e - exact) <= 1e-10 * abs(exact) and dw == 0.0
+
+
+def test_imaginary_time_L20_config(golden):
+    L, D = 20, 20
+    H, U = mo.ising_hmpo(L, 1, 1, 0), mo.ising_umpo(L, 1, 1, 0, 0.01, True)
+    st = mo.product_mps(L, 2, D)
+    es = []
+    for _ in range(200):
+        aux = st.copy()
+        mo.optimize(U, aux, st, D, convtol=1e-10)
+        mo.gauge_cond_all(st, "R", True)
+        es.append(mo.contract_op(st, H, st).real)
+    np.testing.assert_allclose(es, golden["ising_L20_D20_imag_dt001_M200_energies"], rtol=1e-10, atol=0)
