@@ -156,9 +156,14 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
     MPSGPU_CUDA(cudaEventCreate(&c.mv0));
     MPSGPU_CUDA(cudaEventCreate(&c.mv1));
     MPSGPU_CUDA(cudaMalloc((void**)&c.dsc, sizeof(LanczosScalars)));
-    MPSGPU_CUDA(cudaMallocHost((void**)&c.hsc, sizeof(LanczosScalars)));
-    MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 64 * sizeof(unsigned)));
-    MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 64 * sizeof(unsigned)));
+    // pinned and mapped: the fused Lanczos kernels write alpha_j, beta_j
+    // straight into it (no copy per iteration); the host reads them after
+    // the iteration's event
+    MPSGPU_CUDA(cudaHostAlloc((void**)&c.hsc, sizeof(LanczosScalars), cudaHostAllocMapped));
+    MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.hsc_dev, c.hsc, 0));
+    MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 128 * sizeof(unsigned)));
+    MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 128 * sizeof(unsigned)));
+    MPSGPU_CUDA(cudaMemset(c.dsc, 0, sizeof(LanczosScalars)));
     c.iter_ev.resize(257);
     for (auto& e : c.iter_ev) MPSGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   });

@@ -710,13 +710,15 @@ cplx contract2(Context& c, const MpoDev& ops, const MpsDev& ket, const MpsDev& b
 // ---------------------------------------------------------------------------
 // Lanczos for the lowest eigenpair (replaces the PRIMME call of
 // Contractor::solveEigs, Contractor.cpp:3067-3138; and its dense branch).
-// Restarted Lanczos with full (twice classical Gram-Schmidt)
-// reorthogonalisation, FP64; convergence ||r|| <= tol * max|Ritz|.
+// Restarted Lanczos with full reorthogonalisation (lanczos.cu), FP64;
+// convergence ||r|| <= tol * max|Ritz|.  apply(x, y, sigma) must compute
+// y = (H - sigma) x; sigma follows the latest Ritz value (shift0 before the
+// first one is known), which keeps the Gram-Schmidt passes well conditioned.
 // ---------------------------------------------------------------------------
 
 template <class Op>
 static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, int max_krylov,
-                             int* iters) {
+                             int* iters, double shift0) {
   const int m = std::min(N, std::max(2, std::min(max_krylov, 200)));
   dbuf_reserve(c, c.lanV, (long long)N * (m + 1));
   dbuf_reserve(c, c.lanW, N);
@@ -737,20 +739,18 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
   zscal_inv(st, N, x, d_tmp, V);
   std::vector<double> a, b, s;
   double theta = 0.0;
+  double sigma = std::isfinite(shift0) ? shift0 : 0.0;
   int total = 0;
   TridiagLowest tri;
-  // Iteration j: matvec, fused reorthogonalisation, async copy of
-  // (alpha_j, beta_j) to pinned memory, event.  The host enqueues iteration
+  // Iteration j: matvec, fused reorthogonalisation (which also writes
+  // alpha_j, beta_j into mapped pinned memory), event.  The host enqueues iteration
   // j+1 before it waits for j, so the convergence test (tridiagonal
   // eigenpair on the host) overlaps the device work; a speculative iteration
   // after convergence is discarded (it only writes V[:, j+2] and w).
   auto enqueue = [&](int j) {
-    apply(V + (long long)j * N, w);
-    lanczos_orthonormalize(st, N, j, V, N, w, j + 1 < m, c.dsc, h1, h2, c.dcounter, c.scratch);
-    MPSGPU_CUDA(cudaMemcpyAsync(&c.hsc->alpha[j], &c.dsc->alpha[j], sizeof(double), cudaMemcpyDeviceToHost,
-                                c.stream));
-    MPSGPU_CUDA(cudaMemcpyAsync(&c.hsc->beta[j], &c.dsc->beta[j], sizeof(double), cudaMemcpyDeviceToHost,
-                                c.stream));
+    apply(V + (long long)j * N, w, sigma);
+    lanczos_orthonormalize(st, N, j, V, N, w, j + 1 < m, sigma, c.dsc, c.hsc_dev, h1, h2, c.dcounter,
+                           c.scratch);
     MPSGPU_CUDA(cudaEventRecord(c.iter_ev[j], c.stream));
     total++;
   };
@@ -788,6 +788,7 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
       b.push_back(beta);
       double normT = 0.0;
       tri.solve(a, b, (int)a.size(), theta, s, normT);
+      sigma = theta;
       const double res = beta * std::fabs(s[j]);
       const double scale = std::max(normT, std::fabs(theta));
       if (res <= tol * scale || beta <= 1e-14 * scale || j + 1 == N) {
@@ -829,6 +830,9 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
       return theta;
     }
     zscal_inv(st, N, w, &c.dsc->beta[m - 1], V + (long long)r * N);  // beta[m-1] = |f| on the device
+    // the coupling of V[:, r-1] to the new V[:, r], used by the next step
+    MPSGPU_CUDA(cudaMemcpyAsync(&c.dsc->beta[r - 1], &b[r - 1], sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    sigma = theta;
     j0 = r;
   }
   if (iters) *iters = total;
@@ -1053,11 +1057,11 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
       const cplx* Rt = E.Re[pos].p;
       auto ld = E.ldims[pos];
       auto rd = E.rdims[pos];
-      auto apply = [&](const cplx* xin, cplx* yout) {
-        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, off, &cnt);
+      auto apply = [&](const cplx* xin, cplx* yout, double sg) {
+        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(off.x - sg, off.y), &cnt);
       };
       int its = 0;
-      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, tol, opt.max_krylov, &its);
+      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, tol, opt.max_krylov, &its, val + offset);
       cnt.site_solves++;
       val = theta - offset;
       if ((val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
@@ -1218,9 +1222,11 @@ double find_ground_state_two_site(Context& c, const MpoDev& ops, int D, MpsDev& 
       const cplx* Rt = E.Re[pos + 1].p;
       const auto ld = E.ldims[pos];
       const auto rd = E.rdims[pos + 1];
-      auto apply = [&](const cplx* xin, cplx* yout) { heff2_apply(c, Le, ld, ops, pos, Rt, rd, xin, yout, off, &cnt); };
+      auto apply = [&](const cplx* xin, cplx* yout, double sg) {
+        heff2_apply(c, Le, ld, ops, pos, Rt, rd, xin, yout, make_double2(off.x - sg, off.y), &cnt);
+      };
       int its = 0;
-      const double theta = lanczos_lowest(c, (int)N, apply, th.p, tol, opt.max_krylov, &its);
+      const double theta = lanczos_lowest(c, (int)N, apply, th.p, tol, opt.max_krylov, &its, val + offset);
       cnt.site_solves++;
       val = theta - offset;
       // split Theta (Dl d1 x d2 Dr) = U S V^H, cut to D; the singular values
@@ -1386,17 +1392,17 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
       cplx* dots = c.dcplx + 512;
       const cplx* Le = E.Le[pos].p;
       const cplx* Rt = E.Re[pos].p;
-      auto apply = [&](const cplx* xin, cplx* yout) {
+      auto apply = [&](const cplx* xin, cplx* yout, double sg) {
         heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(0.0, 0.0), &cnt);
         heff_apply(c, Lh.p, ld, ops, pos, true, Rth.p, rd, xin, y2.p, make_double2(0.0, 0.0), &cnt);
         cnt.matvecs--;  // the pair counts as one product of the Hermitian multiplier
         zaxpby(c.st(), N, make_double2(0.5, 0.0), y2.p, make_double2(0.5, 0.0), yout);
-        if (offset != 0.0) zaxpby(c.st(), N, make_double2(offset, 0.0), xin, make_double2(1.0, 0.0), yout);
+        if (offset - sg != 0.0) zaxpby(c.st(), N, make_double2(offset - sg, 0.0), xin, make_double2(1.0, 0.0), yout);
         cgemv_c(c.st(), N, nk, U.p, N, xin, dots, c.scratch);
         cgemv_n_sub(c.st(), N, nk, U.p, N, dots, yout, 1.0);
       };
       int its = 0;
-      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, tol, opt.max_krylov, &its);
+      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, tol, opt.max_krylov, &its, val + offset);
       cnt.site_solves++;
       val = theta - offset;
       if ((val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {

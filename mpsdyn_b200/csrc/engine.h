@@ -61,7 +61,8 @@ struct Context {
   cplx* hcplx = nullptr;
   double* dS = nullptr;        // Ritz coefficients on device
   LanczosScalars* dsc = nullptr;  // alpha/beta written by the fused kernels
-  LanczosScalars* hsc = nullptr;  // pinned host mirror
+  LanczosScalars* hsc = nullptr;  // pinned, mapped host mirror
+  LanczosScalars* hsc_dev = nullptr;  // its device address
   unsigned* dcounter = nullptr;   // last-block ticket of the fused reductions
   std::vector<cudaEvent_t> iter_ev;  // one per Lanczos iteration in flight
   cudaEvent_t ev = nullptr;

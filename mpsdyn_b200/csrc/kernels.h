@@ -122,16 +122,23 @@ void cgemv_n_sub(const Stream& st, int n, int k, const cplx* V, long long ldv, c
 struct LanczosScalars {
   double alpha[256];
   double beta[256];
+  cplx loc;    // v_j^H w after the beta_{j-1} v_{j-1} subtraction (local step)
+  double nb2;  // |w'|^2 before the first Gram-Schmidt pass
+  double ap;   // first-pass Re h_j, while a second pass is pending
+  int flag;    // second pass needed
 };
 // One reorthogonalised Lanczos step after the matvec (lanczos.cu): with
-// k = j+1 basis vectors V[:, 0..j] and w = H v_j,
-//   w <- w - V (V^H w) twice (classical Gram-Schmidt, two passes),
-//   sc->alpha[j] = Re(v_j^H H v_j), sc->beta[j] = ||w||,
+// k = j+1 basis vectors V[:, 0..j] and w = (H - sigma) v_j,
+//   w <- w - beta_{j-1} v_{j-1} - a v_j (the local three-term step),
+//   w <- w - V (V^H w) (classical Gram-Schmidt, a second pass when the norm
+//        drops below 1/sqrt(2) of its value),
+//   sc->alpha[j] = sigma + Re(v_j^H w), sc->beta[j] = ||w|| (and the same in
+//   mirror, mapped host memory, when non-null),
 //   V[:, j+1] = w / beta_j when write_next.
-// counter: one device unsigned, zero on entry, left zero.
+// counters: 67 device unsigneds, zero on entry, left zero.
 void lanczos_orthonormalize(const Stream& st, int n, int j, cplx* V, long long ldv, cplx* w,
-                            bool write_next, LanczosScalars* sc, cplx* h1, cplx* h2,
-                            unsigned* counter, Scratch& scratch);
+                            bool write_next, double sigma, LanczosScalars* sc, LanczosScalars* mirror, cplx* h1,
+                            cplx* h2, unsigned* counters, Scratch& scratch);
 // out[0] = ||x||_2 (deterministic two-stage reduction)
 void dznrm2(const Stream& st, int n, const cplx* x, double* out, Scratch& scratch);
 // y = x / (*nrm)   (device scalar)

@@ -1,17 +1,25 @@
 // Fused Lanczos kernels: one iteration of the reorthogonalised Lanczos
-// recurrence (after the matvec) in four launches.
+// recurrence after the matvec, for the basis V[:, 0..j] (k = j+1 vectors)
+// and w = (H - sigma) v_j, sigma the caller's latest Ritz value.  The local
+// three-term step removes the large components along v_j and v_{j-1}
+// first, so that one classical Gram-Schmidt pass over V usually suffices.
 //
-//   stage 1   h1 = V^H w                                   (dots)
-//   stage 2   w -= V h1 ; h2 = V^H w                       (update + dots)
-//   stage 3   w -= V h2 ; beta_j = ||w|| ; alpha_j = Re(h1_j + h2_j)
-//   stage 4   V[:, j+1] = w / beta_j
+//   local       w = w - beta_{j-1} v_{j-1} ; a = v_j^H w
+//   dots<1>     h = V^H w',  w' = w - a v_j                  (|w'|^2 too)
+//   update<1>   w = w' - V h ; beta^2 = |w|^2 ; if beta^2 < |w'|^2 / 2 a
+//               second pass is flagged (Daniel, Gragg, Kaufman, Stewart
+//               1976), else alpha_j = sigma + Re(a + h_j), beta_j are final
+//   dots<2>     h2 = V^H w                   (returns at once unless flagged)
+//   update<2>   w -= V h2 ; beta_j = |w| ; alpha_j += Re h2_j   (idem)
+//   scale       V[:, j+1] = w / beta_j
 //
-// Stages 1-3 split the rows into blocks of 256; every block writes partial
-// sums, and the last block to finish (ticket counter, __threadfence) reduces
-// the partials in a fixed order, so results are deterministic.  The
-// classical Gram-Schmidt pass is applied twice ("twice is enough",
-// Giraud, Langou, Rozloznik 2005), the full reorthogonalisation that the
-// restarted Lanczos of engine.cu relies on.
+// The dot kernels run on a 2-D grid (row blocks x groups of 8 basis vectors)
+// so that many independent loads are in flight; every block writes partial
+// sums and the last block of each group (ticket counter, __threadfence)
+// reduces them, one warp per vector with lane-strided loads and a shuffle
+// tree, in a fixed order: results are deterministic.  alpha_j and beta_j
+// are also written to a mapped host mirror, read by the host after the
+// iteration's event.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -19,99 +27,227 @@ namespace mpsgpu {
 
 namespace {
 
-constexpr int ROWS = 128;     // rows per block (= threads per block)
-constexpr int KMAX = 256;     // Krylov vectors
+constexpr int RB = 256;           // rows per block (one per thread)
+constexpr int NW = RB / 32;       // warps per block
+constexpr int JG = 8;             // basis vectors per block of the dot kernels (== NW)
+constexpr int KMAX = 256;         // Krylov vectors
+constexpr double DGKS2 = 0.5;     // second pass when |w_after|^2 < 0.5 |w_before|^2
+static_assert(JG == NW, "one warp per vector in the group reduction");
 
-__device__ __forceinline__ bool last_block(unsigned* counter) {
+struct LzArgs {
+  int n, k, j, nrb;
+  const cplx* V;
+  long long ldv;
+  cplx* w;
+  cplx* part;          // k x nrb partial dots
+  double* pnorm;       // nrb partial squared norms
+  cplx* h;             // first-pass coefficients (k)
+  cplx* h2;            // second-pass coefficients (k)
+  LanczosScalars* sc;
+  LanczosScalars* mirror;
+  unsigned* counters;  // [0, 32) first-pass groups, [32, 64) second-pass groups, 64, 65 updates, 66 local
+  double sigma;
+};
+
+__device__ __forceinline__ cplx warp_sum(cplx s) {
+  for (int o = 16; o > 0; o >>= 1) {
+    s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+    s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+  }
+  return s;
+}
+
+__device__ __forceinline__ double warp_sumd(double s) {
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// true in the last block (of gridDim.x blocks) to pass the ticket counter
+__device__ __forceinline__ bool last_block(unsigned* counter, unsigned nblocks) {
   __shared__ bool is_last;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned t = atomicAdd(counter, 1u);
-    is_last = (t == gridDim.x - 1);
-  }
+  if (threadIdx.x == 0) is_last = (atomicAdd(counter, 1u) == nblocks - 1);
   __syncthreads();
   return is_last;
 }
 
-// MODE 0: dots only; MODE 1: update then dots; MODE 2: update then norm.
-template <int MODE>
-__global__ void __launch_bounds__(ROWS)
-gs_stage_kernel(int n, int k, const cplx* __restrict__ V, long long ldv, const cplx* __restrict__ h,
-                cplx* __restrict__ w, cplx* __restrict__ part, double* __restrict__ partr,
-                cplx* __restrict__ out, LanczosScalars* sc, const cplx* __restrict__ h1, int j,
-                unsigned* counter) {
-  __shared__ cplx hs[KMAX];
-  __shared__ cplx ws[ROWS];
-  __shared__ double red[ROWS / 32];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = ROWS / 32;
-  const int b = blockIdx.x, nblk = gridDim.x;
-  const long long r0 = (long long)b * ROWS;
-  const long long i = r0 + tid;
-  const bool valid = i < n;
-  if (MODE >= 1)
-    for (int t = tid; t < k; t += ROWS) hs[t] = h[t];
-  __syncthreads();
-  cplx wi = valid ? w[i] : make_double2(0.0, 0.0);
-  if (MODE >= 1 && valid) {
-    cplx s = make_double2(0.0, 0.0);
-    // four independent accumulators keep several loads of V in flight
-    cplx s1 = make_double2(0.0, 0.0), s2 = s1, s3 = s1;
-    int jj = 0;
-    for (; jj + 4 <= k; jj += 4) {
-      const cplx v0 = V[i + jj * ldv], v1 = V[i + (jj + 1) * ldv];
-      const cplx v2 = V[i + (jj + 2) * ldv], v3 = V[i + (jj + 3) * ldv];
-      s = cadd(s, cmul(v0, hs[jj]));
-      s1 = cadd(s1, cmul(v1, hs[jj + 1]));
-      s2 = cadd(s2, cmul(v2, hs[jj + 2]));
-      s3 = cadd(s3, cmul(v3, hs[jj + 3]));
+__global__ void __launch_bounds__(RB) lz_local_kernel(LzArgs a) {
+  __shared__ cplx red[NW];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long i = (long long)blockIdx.x * RB + tid;
+  cplx acc = make_double2(0.0, 0.0);
+  if (i < a.n) {
+    cplx wi = a.w[i];
+    if (a.j > 0) {
+      wi = csub(wi, cscale(a.V[i + (long long)(a.j - 1) * a.ldv], a.sc->beta[a.j - 1]));
+      a.w[i] = wi;
     }
-    for (; jj < k; jj++) s = cadd(s, cmul(V[i + jj * ldv], hs[jj]));
-    s = cadd(cadd(s, s1), cadd(s2, s3));
-    wi = csub(wi, s);
-    w[i] = wi;
+    acc = ccmul(a.V[i + (long long)a.j * a.ldv], wi);
   }
-  ws[tid] = wi;
+  acc = warp_sum(acc);
+  if (lane == 0) red[warp] = acc;
   __syncthreads();
-  const int rows = (int)min((long long)ROWS, (long long)n - r0);
-  if (MODE <= 1) {
-    // part[jj * nblk + b] = sum over the block's rows of conj(V[:, jj]) w
-    for (int jj = warp; jj < k; jj += nw) {
-      const cplx* v = V + jj * ldv + r0;
-      cplx s = make_double2(0.0, 0.0);
-      for (int r = lane; r < rows; r += 32) s = cadd(s, ccmul(v[r], ws[r]));
-      for (int o = 16; o > 0; o >>= 1) {
-        s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-        s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-      }
-      if (lane == 0) part[(long long)jj * nblk + b] = s;
-    }
-    if (last_block(counter)) {
-      for (int jj = tid; jj < k; jj += ROWS) {
-        cplx s = make_double2(0.0, 0.0);
-        for (int q = 0; q < nblk; q++) s = cadd(s, __ldcg(&part[(long long)jj * nblk + q]));
-        out[jj] = s;
-      }
-      if (tid == 0) *counter = 0u;
-    }
-  } else {
-    double s = cabs2(ws[tid]);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (tid == 0) {
+    cplx s = make_double2(0.0, 0.0);
+    for (int q = 0; q < NW; q++) s = cadd(s, red[q]);
+    a.part[blockIdx.x] = s;
+  }
+  if (last_block(a.counters + 66, gridDim.x)) {
+    cplx s = make_double2(0.0, 0.0);
+    for (int q = tid; q < a.nrb; q += RB) s = cadd(s, __ldcg(&a.part[q]));
+    s = warp_sum(s);
+    __syncthreads();
     if (lane == 0) red[warp] = s;
     __syncthreads();
     if (tid == 0) {
-      double t = 0.0;
-      for (int q = 0; q < nw; q++) t += red[q];
-      partr[b] = t;
+      cplx t = make_double2(0.0, 0.0);
+      for (int q = 0; q < NW; q++) t = cadd(t, red[q]);
+      a.sc->loc = t;
+      a.counters[66] = 0u;
     }
-    if (last_block(counter)) {
-      if (tid == 0) {
-        double t = 0.0;
-        for (int q = 0; q < nblk; q++) t += __ldcg(&partr[q]);
-        sc->beta[j] = sqrt(t);
-        sc->alpha[j] = __ldcg(&h1[j].x) + __ldcg(&h[j].x);
-        *counter = 0u;
+  }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(RB) lz_dots_kernel(LzArgs a) {
+  if (PASS == 2 && a.sc->flag == 0) return;  // written by update<1> (earlier kernel)
+  __shared__ cplx red[NW][JG];
+  __shared__ double rn[NW];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int rb = blockIdx.x, g = blockIdx.y;
+  const long long i = (long long)rb * RB + tid;
+  const bool valid = i < a.n;
+  cplx wi = valid ? a.w[i] : make_double2(0.0, 0.0);
+  if (PASS == 1 && valid) wi = csub(wi, cmul(a.V[i + (long long)a.j * a.ldv], a.sc->loc));
+  const int j0 = g * JG;
+  cplx acc[JG];
+#pragma unroll
+  for (int u = 0; u < JG; u++) {
+    const int jj = j0 + u;
+    acc[u] = (valid && jj < a.k) ? ccmul(a.V[i + (long long)jj * a.ldv], wi) : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int u = 0; u < JG; u++) acc[u] = warp_sum(acc[u]);
+  if (lane == 0) {
+#pragma unroll
+    for (int u = 0; u < JG; u++) red[warp][u] = acc[u];
+  }
+  const bool with_norm = (PASS == 1 && g == 0);
+  if (with_norm) {
+    const double s = warp_sumd(cabs2(wi));
+    if (lane == 0) rn[warp] = s;
+  }
+  __syncthreads();
+  if (tid < JG && j0 + tid < a.k) {
+    cplx s = make_double2(0.0, 0.0);
+    for (int q = 0; q < NW; q++) s = cadd(s, red[q][tid]);
+    a.part[(long long)(j0 + tid) * a.nrb + rb] = s;
+  }
+  if (with_norm && tid == 0) {
+    double s = 0.0;
+    for (int q = 0; q < NW; q++) s += rn[q];
+    a.pnorm[rb] = s;
+  }
+  unsigned* counter = a.counters + (PASS == 1 ? 0 : 32) + g;
+  if (last_block(counter, gridDim.x)) {
+    cplx* out = PASS == 1 ? a.h : a.h2;
+    const int jj = j0 + warp;
+    if (jj < a.k) {
+      const cplx* pj = a.part + (long long)jj * a.nrb;
+      cplx s = make_double2(0.0, 0.0);
+      for (int q = lane; q < a.nrb; q += 32) s = cadd(s, __ldcg(&pj[q]));
+      s = warp_sum(s);
+      if (lane == 0) out[jj] = s;
+    }
+    if (with_norm && warp == 0) {
+      double s = 0.0;
+      for (int q = lane; q < a.nrb; q += 32) s += __ldcg(&a.pnorm[q]);
+      s = warp_sumd(s);
+      if (lane == 0) a.sc->nb2 = s;
+    }
+    if (tid == 0) *counter = 0u;
+  }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(RB) lz_update_kernel(LzArgs a) {
+  if (PASS == 2 && a.sc->flag == 0) return;
+  __shared__ cplx hs[KMAX];
+  __shared__ double rn[NW];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const cplx* h = PASS == 1 ? a.h : a.h2;
+  for (int t = tid; t < a.k; t += RB) hs[t] = h[t];
+  __syncthreads();
+  const long long i = (long long)blockIdx.x * RB + tid;
+  const bool valid = i < a.n;
+  double nrm = 0.0;
+  if (valid) {
+    cplx wi = a.w[i];
+    if (PASS == 1) wi = csub(wi, cmul(a.V[i + (long long)a.j * a.ldv], a.sc->loc));
+    // eight independent accumulators keep eight loads of V in flight
+    cplx s[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) s[u] = make_double2(0.0, 0.0);
+    int jj = 0;
+    for (; jj + 8 <= a.k; jj += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; u++) s[u] = cadd(s[u], cmul(a.V[i + (long long)(jj + u) * a.ldv], hs[jj + u]));
+    }
+    for (; jj < a.k; jj++) s[0] = cadd(s[0], cmul(a.V[i + (long long)jj * a.ldv], hs[jj]));
+    cplx t = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int u = 0; u < 8; u++) t = cadd(t, s[u]);
+    wi = csub(wi, t);
+    a.w[i] = wi;
+    nrm = cabs2(wi);
+  }
+  nrm = warp_sumd(nrm);
+  if (lane == 0) rn[warp] = nrm;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+    for (int q = 0; q < NW; q++) s += rn[q];
+    a.pnorm[blockIdx.x] = s;
+  }
+  unsigned* counter = a.counters + 63 + PASS;
+  if (last_block(counter, gridDim.x)) {
+    double s = 0.0;
+    for (int q = tid; q < a.nrb; q += RB) s += __ldcg(&a.pnorm[q]);
+    s = warp_sumd(s);
+    __syncthreads();
+    if (lane == 0) rn[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+      double b2 = 0.0;
+      for (int q = 0; q < NW; q++) b2 += rn[q];
+      LanczosScalars* sc = a.sc;
+      const int j = a.j;
+      bool final_now = true;
+      double alpha;
+      if (PASS == 1) {
+        const double ap = sc->loc.x + __ldcg(&a.h[j].x);
+        if (b2 < DGKS2 * sc->nb2) {
+          sc->flag = 1;
+          sc->ap = ap;
+          final_now = false;
+        } else {
+          sc->flag = 0;
+        }
+        alpha = a.sigma + ap;
+      } else {
+        alpha = a.sigma + sc->ap + __ldcg(&a.h2[j].x);
       }
+      if (final_now) {
+        const double beta = sqrt(b2);
+        sc->alpha[j] = alpha;
+        sc->beta[j] = beta;
+        if (a.mirror) {  // mapped host memory: visible to the host once the kernel is complete
+          a.mirror->alpha[j] = alpha;
+          a.mirror->beta[j] = beta;
+        }
+      }
+      *counter = 0u;
     }
   }
 }
@@ -127,18 +263,30 @@ __global__ void scale_next_kernel(int n, const cplx* __restrict__ w, const Lancz
 }  // namespace
 
 void lanczos_orthonormalize(const Stream& st, int n, int j, cplx* V, long long ldv, cplx* w, bool write_next,
-                            LanczosScalars* sc, cplx* h1, cplx* h2, unsigned* counter, Scratch& scratch) {
+                            double sigma, LanczosScalars* sc, LanczosScalars* mirror, cplx* h1, cplx* h2,
+                            unsigned* counters, Scratch& scratch) {
   MPSGPU_CHECK(j + 1 <= KMAX, MPSGPU_BAD_SHAPE, "lanczos: more than 256 Krylov vectors");
-  const int k = j + 1;
-  const int nblk = ceil_div(n, ROWS);
-  char* ws = (char*)scratch.get((size_t)nblk * KMAX * sizeof(cplx) + (size_t)nblk * sizeof(double) + 256);
-  cplx* part = (cplx*)ws;
-  double* partr = (double*)(ws + (size_t)nblk * KMAX * sizeof(cplx));
-  gs_stage_kernel<0><<<nblk, ROWS, 0, st.s>>>(n, k, V, ldv, nullptr, w, part, partr, h1, sc, nullptr, j, counter);
+  LzArgs a;
+  a.n = n; a.k = j + 1; a.j = j;
+  a.nrb = ceil_div(n, RB);
+  a.V = V; a.ldv = ldv; a.w = w;
+  char* ws = (char*)scratch.get((size_t)a.nrb * a.k * sizeof(cplx) + (size_t)a.nrb * sizeof(double) + 256);
+  a.part = (cplx*)ws;
+  a.pnorm = (double*)(ws + (size_t)a.nrb * a.k * sizeof(cplx));
+  a.h = h1; a.h2 = h2;
+  a.sc = sc; a.mirror = mirror;
+  a.counters = counters;
+  a.sigma = sigma;
+  const dim3 g2(a.nrb, ceil_div(a.k, JG));
+  lz_local_kernel<<<a.nrb, RB, 0, st.s>>>(a);
   after_launch(st);
-  gs_stage_kernel<1><<<nblk, ROWS, 0, st.s>>>(n, k, V, ldv, h1, w, part, partr, h2, sc, nullptr, j, counter);
+  lz_dots_kernel<1><<<g2, RB, 0, st.s>>>(a);
   after_launch(st);
-  gs_stage_kernel<2><<<nblk, ROWS, 0, st.s>>>(n, k, V, ldv, h2, w, part, partr, nullptr, sc, h1, j, counter);
+  lz_update_kernel<1><<<a.nrb, RB, 0, st.s>>>(a);
+  after_launch(st);
+  lz_dots_kernel<2><<<g2, RB, 0, st.s>>>(a);
+  after_launch(st);
+  lz_update_kernel<2><<<a.nrb, RB, 0, st.s>>>(a);
   after_launch(st);
   if (write_next) {
     const int g = std::min(ceil_div(n, 256), 148 * 8);
