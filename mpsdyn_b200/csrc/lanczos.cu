@@ -27,7 +27,9 @@ namespace mpsgpu {
 
 namespace {
 
-constexpr int RB = 256;           // rows per block (one per thread)
+constexpr int RB = 256;           // rows per block (one per thread) of the local and dot kernels
+constexpr int UR = 64;            // rows per block of the update kernels
+constexpr int UP = RB / UR;       // threads per row there (each takes every UP-th basis vector)
 constexpr int NW = RB / 32;       // warps per block
 constexpr int JG = 8;             // basis vectors per block of the dot kernels (== NW)
 constexpr int KMAX = 256;         // Krylov vectors
@@ -176,28 +178,37 @@ __global__ void __launch_bounds__(RB) lz_update_kernel(LzArgs a) {
   __shared__ cplx hs[KMAX];
   __shared__ double rn[NW];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ cplx sp[UP][UR];
   const cplx* h = PASS == 1 ? a.h : a.h2;
   for (int t = tid; t < a.k; t += RB) hs[t] = h[t];
   __syncthreads();
-  const long long i = (long long)blockIdx.x * RB + tid;
+  // UP threads per row: thread (r, p) sums V[i, jj] h[jj] over jj = p mod UP
+  // with four independent accumulators, so that each row has 4 * UP loads
+  // of V in flight and the grid has UP times more warps
+  const int r = tid % UR, p = tid / UR;
+  const long long i = (long long)blockIdx.x * UR + r;
   const bool valid = i < a.n;
+  {
+    cplx s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
+    if (valid) {
+      int jj = p;
+      for (; jj + 3 * UP < a.k; jj += 4 * UP) {
+        s0 = cadd(s0, cmul(a.V[i + (long long)jj * a.ldv], hs[jj]));
+        s1 = cadd(s1, cmul(a.V[i + (long long)(jj + UP) * a.ldv], hs[jj + UP]));
+        s2 = cadd(s2, cmul(a.V[i + (long long)(jj + 2 * UP) * a.ldv], hs[jj + 2 * UP]));
+        s3 = cadd(s3, cmul(a.V[i + (long long)(jj + 3 * UP) * a.ldv], hs[jj + 3 * UP]));
+      }
+      for (; jj < a.k; jj += UP) s0 = cadd(s0, cmul(a.V[i + (long long)jj * a.ldv], hs[jj]));
+    }
+    sp[p][r] = cadd(cadd(s0, s1), cadd(s2, s3));
+  }
+  __syncthreads();
   double nrm = 0.0;
-  if (valid) {
+  if (p == 0 && valid) {
     cplx wi = a.w[i];
     if (PASS == 1) wi = csub(wi, cmul(a.V[i + (long long)a.j * a.ldv], a.sc->loc));
-    // eight independent accumulators keep eight loads of V in flight
-    cplx s[8];
-#pragma unroll
-    for (int u = 0; u < 8; u++) s[u] = make_double2(0.0, 0.0);
-    int jj = 0;
-    for (; jj + 8 <= a.k; jj += 8) {
-#pragma unroll
-      for (int u = 0; u < 8; u++) s[u] = cadd(s[u], cmul(a.V[i + (long long)(jj + u) * a.ldv], hs[jj + u]));
-    }
-    for (; jj < a.k; jj++) s[0] = cadd(s[0], cmul(a.V[i + (long long)jj * a.ldv], hs[jj]));
-    cplx t = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int u = 0; u < 8; u++) t = cadd(t, s[u]);
+    cplx t = sp[0][r];
+    for (int q = 1; q < UP; q++) t = cadd(t, sp[q][r]);
     wi = csub(wi, t);
     a.w[i] = wi;
     nrm = cabs2(wi);
@@ -213,7 +224,7 @@ __global__ void __launch_bounds__(RB) lz_update_kernel(LzArgs a) {
   unsigned* counter = a.counters + 63 + PASS;
   if (last_block(counter, gridDim.x)) {
     double s = 0.0;
-    for (int q = tid; q < a.nrb; q += RB) s += __ldcg(&a.pnorm[q]);
+    for (int q = tid; q < (int)gridDim.x; q += RB) s += __ldcg(&a.pnorm[q]);
     s = warp_sumd(s);
     __syncthreads();
     if (lane == 0) rn[warp] = s;
@@ -270,7 +281,8 @@ void lanczos_orthonormalize(const Stream& st, int n, int j, cplx* V, long long l
   a.n = n; a.k = j + 1; a.j = j;
   a.nrb = ceil_div(n, RB);
   a.V = V; a.ldv = ldv; a.w = w;
-  char* ws = (char*)scratch.get((size_t)a.nrb * a.k * sizeof(cplx) + (size_t)a.nrb * sizeof(double) + 256);
+  const int nub = ceil_div(n, UR);  // blocks of the update kernels
+  char* ws = (char*)scratch.get((size_t)a.nrb * a.k * sizeof(cplx) + (size_t)nub * sizeof(double) + 256);
   a.part = (cplx*)ws;
   a.pnorm = (double*)(ws + (size_t)a.nrb * a.k * sizeof(cplx));
   a.h = h1; a.h2 = h2;
@@ -282,11 +294,11 @@ void lanczos_orthonormalize(const Stream& st, int n, int j, cplx* V, long long l
   after_launch(st);
   lz_dots_kernel<1><<<g2, RB, 0, st.s>>>(a);
   after_launch(st);
-  lz_update_kernel<1><<<a.nrb, RB, 0, st.s>>>(a);
+  lz_update_kernel<1><<<nub, RB, 0, st.s>>>(a);
   after_launch(st);
   lz_dots_kernel<2><<<g2, RB, 0, st.s>>>(a);
   after_launch(st);
-  lz_update_kernel<2><<<a.nrb, RB, 0, st.s>>>(a);
+  lz_update_kernel<2><<<nub, RB, 0, st.s>>>(a);
   after_launch(st);
   if (write_next) {
     const int g = std::min(ceil_div(n, 256), 148 * 8);
