@@ -117,39 +117,43 @@ __global__ void __launch_bounds__(RB) lz_dots_kernel(LzArgs a) {
   __shared__ cplx red[NW][JG];
   __shared__ double rn[NW];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int rb = blockIdx.x, g = blockIdx.y;
-  const long long i = (long long)rb * RB + tid;
-  const bool valid = i < a.n;
-  cplx wi = valid ? a.w[i] : make_double2(0.0, 0.0);
-  if (PASS == 1 && valid) wi = csub(wi, cmul(a.V[i + (long long)a.j * a.ldv], a.sc->loc));
+  const int g = blockIdx.y;
   const int j0 = g * JG;
-  cplx acc[JG];
-#pragma unroll
-  for (int u = 0; u < JG; u++) {
-    const int jj = j0 + u;
-    acc[u] = (valid && jj < a.k) ? ccmul(a.V[i + (long long)jj * a.ldv], wi) : make_double2(0.0, 0.0);
-  }
-#pragma unroll
-  for (int u = 0; u < JG; u++) acc[u] = warp_sum(acc[u]);
-  if (lane == 0) {
-#pragma unroll
-    for (int u = 0; u < JG; u++) red[warp][u] = acc[u];
-  }
   const bool with_norm = (PASS == 1 && g == 0);
-  if (with_norm) {
-    const double s = warp_sumd(cabs2(wi));
-    if (lane == 0) rn[warp] = s;
-  }
-  __syncthreads();
-  if (tid < JG && j0 + tid < a.k) {
-    cplx s = make_double2(0.0, 0.0);
-    for (int q = 0; q < NW; q++) s = cadd(s, red[q][tid]);
-    a.part[(long long)(j0 + tid) * a.nrb + rb] = s;
-  }
-  if (with_norm && tid == 0) {
-    double s = 0.0;
-    for (int q = 0; q < NW; q++) s += rn[q];
-    a.pnorm[rb] = s;
+  // row blocks in grid-stride order (the second pass launches fewer blocks)
+  for (int rb = blockIdx.x; rb < a.nrb; rb += gridDim.x) {
+    const long long i = (long long)rb * RB + tid;
+    const bool valid = i < a.n;
+    cplx wi = valid ? a.w[i] : make_double2(0.0, 0.0);
+    if (PASS == 1 && valid) wi = csub(wi, cmul(a.V[i + (long long)a.j * a.ldv], a.sc->loc));
+    cplx acc[JG];
+#pragma unroll
+    for (int u = 0; u < JG; u++) {
+      const int jj = j0 + u;
+      acc[u] = (valid && jj < a.k) ? ccmul(a.V[i + (long long)jj * a.ldv], wi) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < JG; u++) acc[u] = warp_sum(acc[u]);
+    if (lane == 0) {
+#pragma unroll
+      for (int u = 0; u < JG; u++) red[warp][u] = acc[u];
+    }
+    if (with_norm) {
+      const double s = warp_sumd(cabs2(wi));
+      if (lane == 0) rn[warp] = s;
+    }
+    __syncthreads();
+    if (tid < JG && j0 + tid < a.k) {
+      cplx s = make_double2(0.0, 0.0);
+      for (int q = 0; q < NW; q++) s = cadd(s, red[q][tid]);
+      a.part[(long long)(j0 + tid) * a.nrb + rb] = s;
+    }
+    if (with_norm && tid == 0) {
+      double s = 0.0;
+      for (int q = 0; q < NW; q++) s += rn[q];
+      a.pnorm[rb] = s;
+    }
+    __syncthreads();
   }
   unsigned* counter = a.counters + (PASS == 1 ? 0 : 32) + g;
   if (last_block(counter, gridDim.x)) {
@@ -186,41 +190,44 @@ __global__ void __launch_bounds__(RB) lz_update_kernel(LzArgs a) {
   // with four independent accumulators, so that each row has 4 * UP loads
   // of V in flight and the grid has UP times more warps
   const int r = tid % UR, p = tid / UR;
-  const long long i = (long long)blockIdx.x * UR + r;
-  const bool valid = i < a.n;
-  {
-    cplx s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
-    if (valid) {
-      int jj = p;
-      for (; jj + 3 * UP < a.k; jj += 4 * UP) {
-        s0 = cadd(s0, cmul(a.V[i + (long long)jj * a.ldv], hs[jj]));
-        s1 = cadd(s1, cmul(a.V[i + (long long)(jj + UP) * a.ldv], hs[jj + UP]));
-        s2 = cadd(s2, cmul(a.V[i + (long long)(jj + 2 * UP) * a.ldv], hs[jj + 2 * UP]));
-        s3 = cadd(s3, cmul(a.V[i + (long long)(jj + 3 * UP) * a.ldv], hs[jj + 3 * UP]));
+  const int nub = (a.n + UR - 1) / UR;
+  double bsum = 0.0;  // this block's sum of squares (thread 0)
+  for (int ub = blockIdx.x; ub < nub; ub += gridDim.x) {
+    const long long i = (long long)ub * UR + r;
+    const bool valid = i < a.n;
+    {
+      cplx s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
+      if (valid) {
+        int jj = p;
+        for (; jj + 3 * UP < a.k; jj += 4 * UP) {
+          s0 = cadd(s0, cmul(a.V[i + (long long)jj * a.ldv], hs[jj]));
+          s1 = cadd(s1, cmul(a.V[i + (long long)(jj + UP) * a.ldv], hs[jj + UP]));
+          s2 = cadd(s2, cmul(a.V[i + (long long)(jj + 2 * UP) * a.ldv], hs[jj + 2 * UP]));
+          s3 = cadd(s3, cmul(a.V[i + (long long)(jj + 3 * UP) * a.ldv], hs[jj + 3 * UP]));
+        }
+        for (; jj < a.k; jj += UP) s0 = cadd(s0, cmul(a.V[i + (long long)jj * a.ldv], hs[jj]));
       }
-      for (; jj < a.k; jj += UP) s0 = cadd(s0, cmul(a.V[i + (long long)jj * a.ldv], hs[jj]));
+      sp[p][r] = cadd(cadd(s0, s1), cadd(s2, s3));
     }
-    sp[p][r] = cadd(cadd(s0, s1), cadd(s2, s3));
+    __syncthreads();
+    double nrm = 0.0;
+    if (p == 0 && valid) {
+      cplx wi = a.w[i];
+      if (PASS == 1) wi = csub(wi, cmul(a.V[i + (long long)a.j * a.ldv], a.sc->loc));
+      cplx t = sp[0][r];
+      for (int q = 1; q < UP; q++) t = cadd(t, sp[q][r]);
+      wi = csub(wi, t);
+      a.w[i] = wi;
+      nrm = cabs2(wi);
+    }
+    nrm = warp_sumd(nrm);
+    if (lane == 0) rn[warp] = nrm;
+    __syncthreads();
+    if (tid == 0)
+      for (int q = 0; q < NW; q++) bsum += rn[q];
+    __syncthreads();
   }
-  __syncthreads();
-  double nrm = 0.0;
-  if (p == 0 && valid) {
-    cplx wi = a.w[i];
-    if (PASS == 1) wi = csub(wi, cmul(a.V[i + (long long)a.j * a.ldv], a.sc->loc));
-    cplx t = sp[0][r];
-    for (int q = 1; q < UP; q++) t = cadd(t, sp[q][r]);
-    wi = csub(wi, t);
-    a.w[i] = wi;
-    nrm = cabs2(wi);
-  }
-  nrm = warp_sumd(nrm);
-  if (lane == 0) rn[warp] = nrm;
-  __syncthreads();
-  if (tid == 0) {
-    double s = 0.0;
-    for (int q = 0; q < NW; q++) s += rn[q];
-    a.pnorm[blockIdx.x] = s;
-  }
+  if (tid == 0) a.pnorm[blockIdx.x] = bsum;
   unsigned* counter = a.counters + 63 + PASS;
   if (last_block(counter, gridDim.x)) {
     double s = 0.0;
@@ -296,9 +303,11 @@ void lanczos_orthonormalize(const Stream& st, int n, int j, cplx* V, long long l
   after_launch(st);
   lz_update_kernel<1><<<nub, RB, 0, st.s>>>(a);
   after_launch(st);
-  lz_dots_kernel<2><<<g2, RB, 0, st.s>>>(a);
+  // the second pass is usually skipped (flag clear): few blocks, grid-stride
+  const dim3 g2b(std::min(a.nrb, 16), ceil_div(a.k, JG));
+  lz_dots_kernel<2><<<g2b, RB, 0, st.s>>>(a);
   after_launch(st);
-  lz_update_kernel<2><<<nub, RB, 0, st.s>>>(a);
+  lz_update_kernel<2><<<std::min(nub, 64), RB, 0, st.s>>>(a);
   after_launch(st);
   if (write_next) {
     const int g = std::min(ceil_div(n, 256), 148 * 8);
