@@ -119,6 +119,12 @@ mpsgpu_status mpsgpu_mpo_ising_evolution(mpsgpu_context* ctx, int L, double J, d
                                          double h, double delta, int imag, mpsgpu_mpo** out);
 mpsgpu_status mpsgpu_mpo_schwinger(mpsgpu_context* ctx, int N, double mu, double x, double l0,
                                    double alpha, mpsgpu_mpo** out);
+/* HeisenbergHamiltonian(L, Jx, Jy, Jz, hx, hy, hz, 2, offset).getHMPO()
+ * (models/cpp/HeisenbergHamiltonian.cpp:266-331): spin-1/2 XYZ chain with
+ * uniform couplings and fields, MPO bond 5. */
+mpsgpu_status mpsgpu_mpo_heisenberg(mpsgpu_context* ctx, int L, double Jx, double Jy, double Jz,
+                                    double hx, double hy, double hz, double offset,
+                                    mpsgpu_mpo** out);
 
 /* ---- MPS (replaces MPS / Site storage, src/core/headers/MPS.h) ------------
  * dims[3k..3k+2] = (d, Dl, Dr) of site k; data[k] column-major complex128. */

@@ -22,7 +22,7 @@ EXPORTS = [
     "mpsgpu_default_options", "mpsgpu_create", "mpsgpu_destroy", "mpsgpu_status_string",
     "mpsgpu_last_error", "mpsgpu_launch_count", "mpsgpu_synchronize", "mpsgpu_get_stream",
     "mpsgpu_profile_begin", "mpsgpu_profile_end", "mpsgpu_mpo_upload",
-    "mpsgpu_mpo_free", "mpsgpu_mpo_info", "mpsgpu_mpo_download", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger",
+    "mpsgpu_mpo_free", "mpsgpu_mpo_info", "mpsgpu_mpo_download", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger", "mpsgpu_mpo_heisenberg",
     "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_random_state", "mpsgpu_mps_product",
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
     "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_ground_state_two_site", "mpsgpu_find_next_excited_state",
@@ -99,6 +99,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         lib.mpsgpu_mpo_ising.argtypes = [P, C.c_int, D_, D_, D_, C.POINTER(P)]
         lib.mpsgpu_mpo_ising_evolution.argtypes = [P, C.c_int, D_, D_, D_, D_, C.c_int, C.POINTER(P)]
         lib.mpsgpu_mpo_schwinger.argtypes = [P, C.c_int, D_, D_, D_, D_, C.POINTER(P)]
+        lib.mpsgpu_mpo_heisenberg.argtypes = [P, C.c_int, D_, D_, D_, D_, D_, D_, D_, C.POINTER(P)]
         _lib = lib
     return _lib
 
@@ -185,6 +186,12 @@ class Context:
         h_ = C.c_void_p()
         self._check(self.lib.mpsgpu_mpo_schwinger(self.h, N, mu, x, l0, alpha, C.byref(h_)))
         return DeviceMPO(self, h_, N)
+
+    def mpo_heisenberg(self, L: int, Jx: float, Jy: float, Jz: float, hx: float = 0.0, hy: float = 0.0,
+                       hz: float = 0.0, offset: float = 0.0) -> "DeviceMPO":
+        h_ = C.c_void_p()
+        self._check(self.lib.mpsgpu_mpo_heisenberg(self.h, L, Jx, Jy, Jz, hx, hy, hz, offset, C.byref(h_)))
+        return DeviceMPO(self, h_, L)
 
     def mps(self, sites: list, normfact: float = 1.0) -> "DeviceMPS":
         arrs = [_fortran(a) for a in sites]
@@ -333,6 +340,17 @@ class Context:
 class DeviceMPO:
     def __init__(self, ctx: Context, h, L: int):
         self.ctx, self.h, self.L = ctx, h, L
+
+    def download(self) -> list:
+        """The operator tensors W(du, Dl, dd, Dr) back on the host."""
+        L = C.c_int()
+        self.ctx._check(self.ctx.lib.mpsgpu_mpo_info(self.ctx.h, self.h, C.byref(L), None))
+        dims = np.zeros(4 * L.value, dtype=np.int32)
+        self.ctx._check(self.ctx.lib.mpsgpu_mpo_info(self.ctx.h, self.h, C.byref(L), _ptr(dims)))
+        ws = [np.zeros(tuple(d), dtype=np.complex128, order="F") for d in dims.reshape(L.value, 4)]
+        ptrs = (C.c_void_p * L.value)(*[w.ctypes.data for w in ws])
+        self.ctx._check(self.ctx.lib.mpsgpu_mpo_download(self.ctx.h, self.h, ptrs))
+        return ws
 
     def free(self) -> None:
         if self.h:

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "Contractor.h"
+#include "HeisenbergHamiltonian.h"
 #include "IsingHamiltonian.h"
 #include "MPO.h"
 #include "MPS.h"
@@ -744,5 +745,24 @@ SchwingerHamiltonian::SchwingerHamiltonian(int N, double mu, double x, double l0
     Contractor::check(MPSGPU_INVALID, "SchwingerHamiltonian: offset = nu = 0 and y = 1 only");
   mpsgpu_mpo* m = nullptr;
   Contractor::check(mpsgpu_mpo_schwinger(ctx(), N, mu, x, l0, alpha, &m), "SchwingerHamiltonian");
+  hamil.setFromDevice(m);
+}
+
+HeisenbergHamiltonian::HeisenbergHamiltonian(int L, double Jx, double Jy, double Jz, double h, int d, double offset, int,
+                                             double penalty) {
+  build(L, Jx, Jy, Jz, 0.0, 0.0, h, d, offset, penalty);
+}
+
+HeisenbergHamiltonian::HeisenbergHamiltonian(int L, double Jx, double Jy, double Jz, double hx, double hy, double hz,
+                                             int d, double offset, int, double penalty) {
+  build(L, Jx, Jy, Jz, hx, hy, hz, d, offset, penalty);
+}
+
+void HeisenbergHamiltonian::build(int L, double Jx, double Jy, double Jz, double hx, double hy, double hz, int d,
+                                  double offset, double penalty) {
+  if (d != 2 || penalty != 0.0)
+    Contractor::check(MPSGPU_INVALID, "HeisenbergHamiltonian: d = 2 and no Sz penalty only");
+  mpsgpu_mpo* m = nullptr;
+  Contractor::check(mpsgpu_mpo_heisenberg(ctx(), L, Jx, Jy, Jz, hx, hy, hz, offset, &m), "HeisenbergHamiltonian");
   hamil.setFromDevice(m);
 }

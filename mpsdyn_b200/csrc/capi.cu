@@ -294,6 +294,11 @@ mpsgpu_status mpsgpu_mpo_schwinger(mpsgpu_context* ctx, int N, double mu, double
   return upload_host_mpo(ctx, [&] { return schwinger_hmpo(N, mu, x, l0, alpha); }, out);
 }
 
+mpsgpu_status mpsgpu_mpo_heisenberg(mpsgpu_context* ctx, int L, double Jx, double Jy, double Jz, double hx,
+                                    double hy, double hz, double offset, mpsgpu_mpo** out) {
+  return upload_host_mpo(ctx, [&] { return heisenberg_hmpo(L, Jx, Jy, Jz, hx, hy, hz, offset); }, out);
+}
+
 mpsgpu_status mpsgpu_mpo_free(mpsgpu_context* ctx, mpsgpu_mpo* mpo) {
   if (!ctx || !mpo) return MPSGPU_INVALID;
   mpo_free(ctx->c, mpo->m);

@@ -198,4 +198,41 @@ HostMPO schwinger_hmpo(int N, double mu, double x, double l0, double alpha, doub
   return m;
 }
 
+HostMPO heisenberg_hmpo(int L, double Jx, double Jy, double Jz, double hx, double hy, double hz, double offset) {
+  if (L < 2) throw std::invalid_argument("heisenberg_hmpo: L < 2");
+  // spin-1/2 operators: identity, S_x, S_y = [[0, -i/2], [i/2, 0]], S_z
+  // (HeisenbergHamiltonian.cpp:266-284 fills them column-major)
+  const std::array<cd, 4> S0 = SIG0;
+  const std::array<cd, 4> SX = {cd(0, 0), cd(0.5, 0), cd(0.5, 0), cd(0, 0)};
+  const std::array<cd, 4> SY = {cd(0, 0), cd(0, 0.5), cd(0, -0.5), cd(0, 0)};
+  const std::array<cd, 4> SZ = {cd(0.5, 0), cd(0, 0), cd(0, 0), cd(-0.5, 0)};
+  const std::vector<std::array<cd, 4>> Z = {S0, SX, SY, SZ};
+  const int D = 5;
+  HostMPO m;
+  for (int k = 0; k < L; k++) {
+    const int Dl = k == 0 ? 1 : D, Dr = k == L - 1 ? 1 : D;
+    std::vector<cd> C((size_t)Dl * Dr * 4, cd(0, 0));
+    auto at = [&](int l, int r, int op) -> cd& { return C[l + Dl * (r + Dr * op)]; };
+    if (k != L - 1) {
+      at(0, 0, 0) = 1.0;
+      at(0, 1, 1) = Jx;
+      at(0, 2, 2) = Jy;
+      at(0, 3, 3) = Jz;
+    }
+    if (k != 0) {
+      at(Dl - 1, Dr - 1, 0) = 1.0;
+      at(1, Dr - 1, 1) = 1.0;
+      at(2, Dr - 1, 2) = 1.0;
+      at(3, Dr - 1, 3) = 1.0;
+    }
+    at(0, Dr - 1, 3) = hz;
+    if (hx != 0) at(0, Dr - 1, 1) = hx;
+    if (hy != 0) at(0, Dr - 1, 2) = hy;
+    if (offset != 0) at(0, Dr - 1, 0) = offset / L;
+    m.dims.push_back({2, Dl, 2, Dr});
+    m.W.push_back(contract_coeffs(C, Dl, Dr, 4, Z));
+  }
+  return m;
+}
+
 }  // namespace mpsgpu

@@ -25,5 +25,10 @@ HostMPO ising_umpo(int L, double J, double g, double h, double delta, bool imag)
 // spin formulation, staggered fermions, gauge field integrated out, MPO bond 5.
 HostMPO schwinger_hmpo(int N, double mu, double x, double l0, double alpha, double offset = 0.0,
                        double nu = 0.0, double y = 1.0);
+// HeisenbergHamiltonian::initHMPO (models/cpp/HeisenbergHamiltonian.cpp:266-331)
+// with uniform couplings, d = 2 and no Sz penalty: H = sum (Jx SxSx + Jy SySy
+// + Jz SzSz) + sum (hx Sx + hy Sy + hz Sz) + offset, S = sigma / 2, bond 5.
+HostMPO heisenberg_hmpo(int L, double Jx, double Jy, double Jz, double hx, double hy, double hz,
+                        double offset = 0.0);
 
 }  // namespace mpsgpu

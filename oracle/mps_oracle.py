@@ -239,6 +239,37 @@ def ising_hmpo(L: int, J: float, g: float, h: float, K: float = 0.0) -> list:
     return ops
 
 
+def heisenberg_hmpo(L: int, Jx: float, Jy: float, Jz: float, hx: float = 0.0, hy: float = 0.0,
+                    hz: float = 0.0, offset: float = 0.0) -> list:
+    """HeisenbergHamiltonian::initHMPO (HeisenbergHamiltonian.cpp:266-331)
+    for uniform couplings, d = 2, no Sz penalty: H = sum_k (Jx Sx Sx + Jy Sy Sy
+    + Jz Sz Sz)_(k,k+1) + sum_k (hx Sx + hy Sy + hz Sz)_k + offset, spin-1/2
+    operators S = sigma / 2; MPO bond 5."""
+    Z = np.zeros((4, 2, 2), dtype=np.complex128)
+    Z[0], Z[1], Z[2], Z[3] = SIG0, 0.5 * SIGX, 0.5 * SIGY, 0.5 * SIGZ
+    D = 5
+    ops = []
+    for k in range(L):
+        Dl = 1 if k == 0 else D
+        Dr = 1 if k == L - 1 else D
+        C = np.zeros((Dl, Dr, 4), dtype=np.complex128)
+        if k != L - 1:
+            C[0, 0, 0] = 1.0
+            C[0, 1, 1], C[0, 2, 2], C[0, 3, 3] = Jx, Jy, Jz
+        if k != 0:
+            C[Dl - 1, Dr - 1, 0] = 1.0
+            C[1, Dr - 1, 1] = C[2, Dr - 1, 2] = C[3, Dr - 1, 3] = 1.0
+        C[0, Dr - 1, 3] = hz
+        if hx != 0:
+            C[0, Dr - 1, 1] = hx
+        if hy != 0:
+            C[0, Dr - 1, 2] = hy
+        if offset != 0:
+            C[0, Dr - 1, 0] = offset / L
+        ops.append(_w_from_coeffs(C, Z))
+    return ops
+
+
 def _ising_u1(eps: complex, g: float, h: float) -> np.ndarray:
     """isingU1MPO (IsingHamiltonian.cpp:203-218): exp(eps (g sx + h sz))."""
     norm = math.sqrt(g * g + h * h)

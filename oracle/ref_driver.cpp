@@ -46,6 +46,7 @@
 #include "Contractor.h"
 #include "IsingHamiltonian.h"
 #include "SchwingerHamiltonian.h"
+#include "HeisenbergHamiltonian.h"
 #include "MPS.h"
 #include "MPO.h"
 #include "Operator.h"
@@ -94,8 +95,9 @@ vector<string> split(const string& s, char c) {
 struct Model {
   IsingHamiltonian* ising = nullptr;
   SchwingerHamiltonian* schw = nullptr;
+  HeisenbergHamiltonian* heis = nullptr;
   int L = 0;
-  const MPO& H() { return ising ? ising->getHMPO(0.) : schw->getHMPO(); }
+  const MPO& H() { return ising ? ising->getHMPO(0.) : heis ? heis->getHMPO() : schw->getHMPO(); }
 };
 
 Model make_model(const char* spec) {
@@ -109,6 +111,12 @@ Model make_model(const char* spec) {
     m.L = atoi(p[1].c_str());
     m.schw = new SchwingerHamiltonian(m.L, atof(p[2].c_str()), atof(p[3].c_str()),
                                       atof(p[4].c_str()), atof(p[5].c_str()));
+  } else if (p[0] == "heis") {
+    // heis:L:Jx:Jy:Jz:hx:hy:hz:offset  (HeisenbergHamiltonian.cpp, d = 2)
+    m.L = atoi(p[1].c_str());
+    m.heis = new HeisenbergHamiltonian(m.L, atof(p[2].c_str()), atof(p[3].c_str()), atof(p[4].c_str()),
+                                       atof(p[5].c_str()), atof(p[6].c_str()), atof(p[7].c_str()), 2,
+                                       atof(p[8].c_str()));
   } else {
     cerr << "unknown model " << spec << endl;
     exit(3);

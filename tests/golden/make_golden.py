@@ -45,7 +45,8 @@ def main() -> None:
 
     # MPO builders (bit-exact targets)
     mpos = {}
-    for name, spec in [("ising6", "ising:6:1:1:0.3"), ("schwinger6", "schwinger:6:2.5:100:0:0")]:
+    for name, spec in [("ising6", "ising:6:1:1:0.3"), ("schwinger6", "schwinger:6:2.5:100:0:0"),
+                       ("heis6", "heis:6:1:0.8:1.2:0.3:0.1:0.5:0.7")]:
         run("mpo", spec, os.path.join(tmp, name + "_"))
         for k in range(6):
             mpos[f"{name}_{k}"] = mo.load_array(os.path.join(tmp, f"{name}_{k}.bin"))
@@ -98,6 +99,8 @@ def main() -> None:
     golden["ising_L12_D16_h01_seed3_E0"] = gs("ising:12:1:0.8:0.1", 12, 16, 3)
     mu = 2 * 0.125 * np.sqrt(100.0)
     golden["schwinger_N16_D24_seed1_E0"] = gs(f"schwinger:16:{mu}:100:0:0", 16, 24, 1)
+    golden["heisenberg_L10_D16_seed0_E0"] = gs("heis:10:1:1:1:0:0:0:0", 10, 16, 0)
+    golden["xxz_L12_D20_fields_seed5_E0"] = gs("heis:12:1:0.7:1.3:0.2:0.1:0.4:0", 12, 20, 5)
 
     # Excited state (penalty L/2 = 5 is above the N=10 gap)
     f0 = os.path.join(tmp, "e0.mps")

@@ -235,3 +235,15 @@ def test_imaginary_time_L20_config(golden):
         mo.gauge_cond_all(st, "R", True)
         es.append(mo.contract_op(st, H, st).real)
     np.testing.assert_allclose(es, golden["ising_L20_D20_imag_dt001_M200_energies"], rtol=1e-10, atol=0)
+
+
+def test_heisenberg_mpo_bit_exact(mpo_npz):
+    ops = mo.heisenberg_hmpo(6, 1, 0.8, 1.2, 0.3, 0.1, 0.5, 0.7)
+    for k in range(6):
+        np.testing.assert_array_equal(ops[k], mpo_npz[f"heis6_{k}"])
+
+
+def test_heisenberg_gs_matches_reference(golden):
+    e = mo.find_ground_state(mo.heisenberg_hmpo(10, 1, 1, 1), 16, mo.random_mps(10, 2, 16, 0), convtol=1e-10)
+    ref = golden["heisenberg_L10_D16_seed0_E0"]
+    assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
