@@ -324,6 +324,19 @@ typedef struct {
 mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgpu_heff_instance* inst,
                                          int repeats, double* ms_per_run, double* flops);
 
+/* Split-precision complex GEMM C = A B (column-major, complex interleaved,
+ * host buffers; m x k times k x n) on the tcgen05 tensor cores: every FP64
+ * real is split into three BF16 limbs and the limb products with combined
+ * order <= 2 are accumulated in FP32, so C carries about 1e-7 relative error
+ * of |A||B| entrywise.  No counterpart in the reference (which multiplies in
+ * complex FP64 through zgemm, wrapper.cpp); it is the product the
+ * split-precision sweep mode runs on.  With repeats > 0, *ms_total gets the
+ * device time of operand preparation plus product and *ms_mma the product
+ * alone, each averaged over `repeats` runs. */
+mpsgpu_status mpsgpu_zgemm_split(mpsgpu_context* ctx, int m, int n, int k, const double* A, int lda,
+                                 const double* B, int ldb, double* C, int ldc, int repeats,
+                                 double* ms_total, double* ms_mma);
+
 /* Operator::contractL / contractR (Operator.cpp:273-398): out gets
  * (Dr_bra, wr, Dr_ket) resp. (Dl_bra, wl, Dl_ket). */
 mpsgpu_status mpsgpu_env_left(mpsgpu_context* ctx, const int* tdims,

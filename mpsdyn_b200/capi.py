@@ -27,7 +27,7 @@ EXPORTS = [
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
     "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_ground_state_two_site", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_contract2", "mpsgpu_expectation_local", "mpsgpu_entropy",
-    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped",
+    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped", "mpsgpu_zgemm_split",
     "mpsgpu_env_left", "mpsgpu_env_right",
     "mpsgpu_qr", "mpsgpu_lq", "mpsgpu_qr_device_noalloc",
     "mpsgpu_server_create", "mpsgpu_server_submit", "mpsgpu_server_poll", "mpsgpu_server_cancel",
@@ -436,6 +436,28 @@ def heff_matvec_grouped(ctx: "Context", instances: list, repeats: int = 0):
     ms, fl = C.c_double(), C.c_double()
     ctx._check(lib.mpsgpu_heff_matvec_grouped(ctx.h, len(instances), arr, repeats, C.byref(ms), C.byref(fl)))
     return (ms.value if repeats > 0 else None), fl.value
+
+
+def zgemm_split(ctx: "Context", A: np.ndarray, B: np.ndarray, repeats: int = 0):
+    """mpsgpu_zgemm_split: A @ B (complex) in split precision on the tensor
+    cores.  Returns (C, ms_total or None, ms_mma or None)."""
+    lib = ctx.lib
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    lib.mpsgpu_zgemm_split.argtypes = [P, C.c_int, C.c_int, C.c_int, D, C.c_int, D, C.c_int, D, C.c_int,
+                                       C.c_int, D, D]
+    A = np.asfortranarray(A, dtype=np.complex128)
+    B = np.asfortranarray(B, dtype=np.complex128)
+    m, k = A.shape
+    k2, n = B.shape
+    if k != k2:
+        raise ValueError("inner dimensions differ")
+    out = np.zeros((m, n), dtype=np.complex128, order="F")
+    dp = lambda a: a.ctypes.data_as(D)
+    t1, t2 = C.c_double(), C.c_double()
+    ctx._check(lib.mpsgpu_zgemm_split(ctx.h, m, n, k, dp(A), m, dp(B), k, dp(out), m, repeats,
+                                      C.byref(t1), C.byref(t2)))
+    return out, (t1.value if repeats > 0 else None), (t2.value if repeats > 0 else None)
 
 
 class Request(C.Structure):

@@ -683,6 +683,57 @@ mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgp
   });
 }
 
+mpsgpu_status mpsgpu_zgemm_split(mpsgpu_context* ctx, int m, int n, int k, const double* A, int lda,
+                                 const double* B, int ldb, double* C, int ldc, int repeats, double* ms_total,
+                                 double* ms_mma) {
+  if (!ctx || m <= 0 || n <= 0 || k <= 0 || !A || !B || !C || lda < m || ldb < k || ldc < m || repeats < 0)
+    return MPSGPU_INVALID;
+  return guarded(ctx, [&] {
+    Context& c = ctx->c;
+    const Stream st = c.st();
+    TmpDev tmp(c);
+    cplx* dA = tmp.upload(A, (long long)lda * k);
+    cplx* dB = tmp.upload(B, (long long)ldb * n);
+    cplx* dC = tmp.alloc((long long)ldc * n);
+    int nsm = 148;
+    MPSGPU_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
+    const SplitPlan pl = split_plan(m, n, k, nsm);
+    uint8_t* Ap = (uint8_t*)tmp.alloc((split_operand_bytes(m, k, 128) + 15) / 16);
+    uint8_t* Bp = (uint8_t*)tmp.alloc((split_operand_bytes(n, k, pl.BN) + 15) / 16);
+    cplx* part = pl.splits > 1 ? tmp.alloc((long long)pl.splits * m * n) : nullptr;
+    int* err = (int*)tmp.alloc(1);
+    MPSGPU_CUDA(cudaMemsetAsync(err, 0, sizeof(int), c.stream));
+    auto run = [&](bool prepare) {
+      if (prepare) {
+        split_prepare(st, m, k, dA, 1, lda, 128, Ap);
+        split_prepare(st, n, k, dB, ldb, 1, pl.BN, Bp);
+      }
+      zgemm_split_prepared(st, pl, Ap, Bp, dC, ldc, cmake(1.0, 0.0), nullptr, 0, cmake(0.0, 0.0), part, err);
+    };
+    run(true);
+    if (repeats > 0) {
+      float ms = 0.f;
+      MPSGPU_CUDA(cudaEventRecord(c.mv0, c.stream));
+      for (int r = 0; r < repeats; r++) run(true);
+      MPSGPU_CUDA(cudaEventRecord(c.mv1, c.stream));
+      MPSGPU_CUDA(cudaEventSynchronize(c.mv1));
+      MPSGPU_CUDA(cudaEventElapsedTime(&ms, c.mv0, c.mv1));
+      if (ms_total) *ms_total = ms / repeats;
+      MPSGPU_CUDA(cudaEventRecord(c.mv0, c.stream));
+      for (int r = 0; r < repeats; r++) run(false);
+      MPSGPU_CUDA(cudaEventRecord(c.mv1, c.stream));
+      MPSGPU_CUDA(cudaEventSynchronize(c.mv1));
+      MPSGPU_CUDA(cudaEventElapsedTime(&ms, c.mv0, c.mv1));
+      if (ms_mma) *ms_mma = ms / repeats;
+    }
+    int herr = 0;
+    MPSGPU_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    MPSGPU_CUDA(cudaMemcpyAsync(C, dC, (size_t)ldc * n * sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    MPSGPU_CHECK(herr == 0, MPSGPU_TIMEOUT, "zgemm_split: a bounded wait in the tensor-core kernel ran out");
+  });
+}
+
 static mpsgpu_status env_common(mpsgpu_context* ctx, bool left, const int* tdims, const double* T,
                                 const int* kdims, const double* ket, const int* wdims, const double* W,
                                 const int* bdims, const double* bra, double* out) {

@@ -61,6 +61,29 @@ long long grouped_tiles(GroupedGemm* descs, int n);
 // All tiles of n GEMMs (descriptors in device memory) in one persistent launch of `ctas` CTAs.
 void zgemm_grouped(const Stream& st, const GroupedGemm* d_descs, int n, long long total_tiles, int ctas);
 
+// ---- split-precision complex GEMM (umma.cu): BF16 limbs on tcgen05 ----
+// Tiling of C = A B (M x N, inner K): 128-row A tiles, BN-column B tiles,
+// k-steps of 16, K split over `splits` CTAs of ks_per_split k-steps each.
+struct SplitPlan {
+  int M = 0, N = 0, K = 0, KS = 0;
+  int BN = 128, mtiles = 0, ntiles = 0;
+  int splits = 1, ks_per_split = 0;
+};
+SplitPlan split_plan(int M, int N, int K, int nsm);
+// Bytes of a prepared operand of `rows` rows and inner dimension K, row tile RT.
+long long split_operand_bytes(int rows, int K, int RT);
+// Six BF16 limb planes of X (rows x K, entry (r, k) at X[r*rs + k*ks]),
+// tiled for the tensor cores with row tile RT (128 for A, plan.BN for B,
+// whose rows are the columns of C); out is 16-byte aligned.
+void split_prepare(const Stream& st, int rows, int K, const cplx* X, long long rs, long long ks, int RT,
+                   uint8_t* out);
+// C = alpha A B + beta Cin from prepared operands; part holds
+// splits * M * N complex partial products when splits > 1; *err is set when
+// a bounded wait inside the kernel ran out.
+void zgemm_split_prepared(const Stream& st, const SplitPlan& pl, const uint8_t* Ap, const uint8_t* Bp, cplx* C,
+                          long long ldc, cplx alpha, const cplx* Cin, long long ldcin, cplx beta, cplx* part,
+                          int* err);
+
 // ---- grouped effective-Hamiltonian matvec (grouped.cu) ----
 // One instance in device layouts: L (Dl, wl, Dl) = (bra, w, ket); W
 // (d, wl, d, wr) as the reference stores it; Rt (Dr, wr, Dr) = (ket, w, bra);
