@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(workload="schwinger_N100_D128_gs+gap", N=100, x=100.0, mg=0.125, D=128,
                 seed_gs=1, seed_exc=11, convtol=1e-10, d=2, mpo_bond=5)
 MU = 2 * WORKLOAD["mg"] * np.sqrt(WORKLOAD["x"])
-METRIC = "DMRG solves/s (Schwinger N=100 D=128, E0 + first gap, FP64, |dE/E|<=1e-10)"
+METRIC = "DMRG solves/s (Schwinger N=100 D=128, E0 + first gap, |dE/E|<=1e-10)"
 UNIT = "solves/s"
 # Algorithmic flops of one solve of this workload as counted by the library
 # (GS + excited state); used by the reference arm to turn its measured flop
@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--batch", type=int, default=8, help="concurrent solves per step")
     p.add_argument("--plain", type=int, default=1, help="also time one solve alone (the plain form)")
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                   help="mixed: split-precision products until the energy settles, then FP64")
     p.add_argument("--workload", default="schwinger", choices=["schwinger", "grouped", "serving", "quench"],
                    help="schwinger: the headline line; the others time the secondary workloads")
     p.add_argument("--instances", type=int, default=512, help="grouped: matvec instances")
@@ -219,7 +221,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     ctxs = [capi.Context(local_rank) for _ in range(B)]
     exts = [torch.cuda.ExternalStream(c.stream) for c in ctxs]
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    opts = ctxs[0].options(convtol=W["convtol"])
+    mixed = args.precision == "mixed"
+    opts = ctxs[0].options(convtol=W["convtol"], precision=1 if mixed else 0)
+    opts64 = ctxs[0].options(convtol=W["convtol"], precision=0)
     mpos = [c.mpo_schwinger(W["N"], MU, W["x"]) for c in ctxs]
     seeds = [(W["seed_gs"] + 1000 * (rank * B + i), W["seed_exc"] + 1000 * (rank * B + i)) for i in range(B)]
     inits = [(c.mps_random(W["N"], 2, W["D"], sg), c.mps_random(W["N"], 2, W["D"], se))
@@ -229,11 +233,12 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     mpo_bytes = 16 * (2 * 1 * 2 * 5 + 2 * 5 * 2 * 1 + (W["N"] - 2) * 2 * 5 * 2 * 5)
     results = [None] * B
 
-    def solve_resident(i):
+    def solve_resident(i, o=None):
+        o = o or opts
         c = ctxs[i]
         g, x = inits[i][0].copy(), inits[i][1].copy()
-        e0, s0 = c.find_ground_state(mpos[i], W["D"], g, 0.0, opts)
-        e1, s1 = c.find_next_excited_state(mpos[i], W["D"], [g], x, 0.0, opts)
+        e0, s0 = c.find_ground_state(mpos[i], W["D"], g, 0.0, o)
+        e1, s1 = c.find_next_excited_state(mpos[i], W["D"], [g], x, 0.0, o)
         g.free()
         x.free()
         results[i] = {"E0": e0, "E1": e1, "gs": s0, "exc": s1}
@@ -320,7 +325,25 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     e2e_total = allreduce(float(sum(e2e_ms)), torch.distributed.ReduceOp.MAX if dist else None)
     e2e_value = solves / (e2e_total * 1e-3)
 
-    # ---- the plain form: one solve alone on the GPU, with the library's
+    # ---- the same batch in FP64 throughout (the comparison of the mixed
+    # form): same seeds, so the energies compare instance by instance ----
+    fp64 = None
+    if mixed:
+        barrier()
+        spans64 = []
+        energies64 = []
+        for _ in range(args.steps):
+            flush_l2()
+            span, _ = run_batch(lambda i: solve_resident(i, opts64))
+            spans64.append(span)
+            energies64.append([(r["E0"], r["E1"]) for r in results])
+        t64 = allreduce(float(sum(spans64)), torch.distributed.ReduceOp.MAX if dist else None)
+        dE = max(max(abs(a[0] - b[0]) / abs(b[0]), abs(a[1] - b[1]) / abs(b[1]))
+                 for sa, sb in zip(energies, energies64) for a, b in zip(sa, sb))
+        fp64 = {"value": solves / (t64 * 1e-3), "ms_per_step": t64 / args.steps,
+                "max_rel_dE_mixed_vs_fp64": dE}
+
+    # ---- the plain form: one FP64 solve alone on the GPU, with the library's
     # GEMM profiler on (events around 1 in 32 GEMM launches of its stream):
     # alone on the device, a launch's event time is its own duration ----
     plain_ms, prof = None, None
@@ -329,7 +352,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ctxs[0].profile_begin()
         ev0.record(exts[0])
-        solve_resident(0)
+        solve_resident(0, opts64)
         ev1.record(exts[0])
         ev1.synchronize()
         prof = ctxs[0].profile_end()
@@ -379,25 +402,33 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
 
     lat_s = np.array(lat) * 1e-3
     e0s = [e for step in energies for e in step]
+    plain_rate = 1e3 / plain_ms if plain_ms else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128/bf16x3" if mixed else "c128",
         "data": "synthetic (seeded complex Gaussian initial MPS, model MPO built in-library)",
-        "config": {**WORKLOAD, "mu": MU, "parallelism": f"replicas{world}", "precision": "fp64",
+        "config": {**WORKLOAD, "mu": MU, "parallelism": f"replicas{world}",
+                   "precision": ("mixed: split-precision (BF16-limb tcgen05) products until the half-sweep "
+                                 "energy changes < 1e-6, then FP64" if mixed else "fp64"),
                    "batch": B, "batch_form": "concurrent independent solves, one stream each",
                    "l2": "flushed between steps (256 MB write)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B * (h2d_mps + mpo_bytes),
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.steps},
         "latency_s": {"p50": float(np.percentile(lat_s, 50)), "p99": float(np.percentile(lat_s, 99))},
         "plain_single_solve_ms": plain_ms,
+        "plain_fp64_solves_per_s": plain_rate,
+        "vs_plain_fp64": (value / plain_rate) if plain_rate else None,
+        "fp64_batched": fp64,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
         "results": {"E0": e0s[0][0], "E1": e0s[0][1], "gap": e0s[0][1] - e0s[0][0],
-                    "gs": {k: s_gs[k] for k in ("rounds", "site_solves", "matvecs", "flops")},
-                    "exc": {k: s_ex[k] for k in ("rounds", "site_solves", "matvecs", "flops")}},
+                    "gs": {k: s_gs[k] for k in ("rounds", "site_solves", "matvecs", "split_rounds", "split_matvecs",
+                                                 "flops")},
+                    "exc": {k: s_ex[k] for k in ("rounds", "site_solves", "matvecs", "split_rounds", "split_matvecs",
+                                                  "flops")}},
     }
     print(json.dumps(line), flush=True)
     for c in ctxs:

@@ -56,7 +56,12 @@ typedef struct {
   double excorthtol;   /* setExcOrthTol (Contractor.h:229); 0 = no check */
   int max_rounds;      /* half-sweep cap; 0 = 1000 (MAX_ROUND_EXCTD, Contractor.cpp:26) */
   int max_krylov;      /* Lanczos vectors per restart; 0 = 64 */
-  int precision;       /* 0 = complex FP64 throughout */
+  int precision;       /* 0 = complex FP64 throughout; 1 = mixed: the
+                        * effective-Hamiltonian products of the single-site
+                        * ground-state sweep run in split precision (BF16
+                        * limbs on the tensor cores) until the half-sweep
+                        * energy change falls below 1e-6 relative, then in
+                        * FP64 to convtol (at least one full FP64 round) */
   int verbose;         /* 1 = one line per half-sweep on stdout */
   /* Optional: when *cancel_flag becomes non-zero (set by another host
    * thread), the sweep stops between two site steps with MPSGPU_CANCELLED. */
@@ -73,6 +78,8 @@ typedef struct {
   double flops;              /* algorithmic flops, all kernels */
   double seconds;            /* wall time of the call */
   double matvec_seconds;     /* device time spent in matvec kernels (events) */
+  long long split_matvecs;   /* products run in split precision (precision = 1) */
+  int split_rounds;          /* half-sweeps run in split precision */
 } mpsgpu_stats;
 
 /* ---- context ------------------------------------------------------------ */

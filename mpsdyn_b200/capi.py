@@ -48,6 +48,7 @@ class Stats(C.Structure):
         ("rounds", C.c_int), ("site_solves", C.c_longlong), ("matvecs", C.c_longlong),
         ("env_updates", C.c_longlong), ("qr_calls", C.c_longlong), ("flops", C.c_double),
         ("seconds", C.c_double), ("matvec_seconds", C.c_double),
+        ("split_matvecs", C.c_longlong), ("split_rounds", C.c_int),
     ]
 
     def as_dict(self) -> dict:

@@ -53,6 +53,7 @@ SolveOptions to_opts(const mpsgpu_options* o) {
     s.max_rounds = o->max_rounds > 0 ? o->max_rounds : 1000;
     s.max_krylov = o->max_krylov > 0 ? o->max_krylov : 64;
     s.verbose = o->verbose;
+    s.precision = o->precision;
     s.cancel = o->cancel_flag;
   }
   return s;
@@ -68,6 +69,8 @@ void fill_stats(mpsgpu_stats* st, const Counters& c, double secs) {
   st->flops = c.flops;
   st->seconds = secs;
   st->matvec_seconds = c.mv_ms * 1e-3;
+  st->split_matvecs = c.split_matvecs;
+  st->split_rounds = c.split_rounds;
 }
 
 double now_s() {
@@ -161,6 +164,9 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
     // the iteration's event
     MPSGPU_CUDA(cudaHostAlloc((void**)&c.hsc, sizeof(LanczosScalars), cudaHostAllocMapped));
     MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.hsc_dev, c.hsc, 0));
+    MPSGPU_CUDA(cudaHostAlloc((void**)&c.hsplit_err, sizeof(int), cudaHostAllocMapped));
+    MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dsplit_err, c.hsplit_err, 0));
+    *c.hsplit_err = 0;
     MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 128 * sizeof(unsigned)));
     MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 128 * sizeof(unsigned)));
     MPSGPU_CUDA(cudaMemset(c.dsc, 0, sizeof(LanczosScalars)));
@@ -179,7 +185,9 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   if (!ctx) return MPSGPU_INVALID;
   Context& c = ctx->c;
   cudaSetDevice(c.device);
-  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lanV, &c.lanW, &c.lanT, &c.lanQ}) dbuf_free(c, *b);
+  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lanV, &c.lanW, &c.lanT, &c.lanQ,
+                  &c.spX, &c.spT, &c.spPart})
+    dbuf_free(c, *b);
   c.scratch.release();
   c.qrws.release();
   if (c.stream) cudaStreamSynchronize(c.stream);
@@ -195,6 +203,7 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
     if (e) cudaEventDestroy(e);
   cudaFree(c.dsc);
   cudaFreeHost(c.hsc);
+  if (c.hsplit_err) cudaFreeHost(c.hsplit_err);
   cudaFree(c.dcounter);
   if (c.stream) cudaStreamDestroy(c.stream);
   delete ctx;

@@ -464,9 +464,61 @@ static double mv_flops(int d, int w1, int w2, int dl, int dr) {
   return 8.0 * (a + b + cc);
 }
 
+// Mixed-precision sweep: the split phase ends at the first half-sweep whose
+// energy change is below kSplitSwitchTol (relative); its Lanczos residual
+// tolerance and energy-increase margin sit above the products' error.
+constexpr double kSplitSwitchTol = 1e-6;
+constexpr double kSplitEigTol = 1e-6;
+constexpr double kSplitIncreaseTol = 1e-5;
+
+static int device_sms(Context& c) {
+  static int nsm = 0;
+  if (nsm == 0) {
+    int v = 148;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess) v = 148;
+    nsm = v;
+  }
+  return nsm;
+}
+
+static uint8_t* bytes_reserve(Context& c, DBuf& b, long long bytes) {
+  dbuf_reserve(c, b, (bytes + (long long)sizeof(cplx) - 1) / (long long)sizeof(cplx));
+  return reinterpret_cast<uint8_t*>(b.p);
+}
+
+void split_matvec_prepare(Context& c, SplitMatvec& s, const cplx* Le, const std::array<int, 3>& ld,
+                          const MpoDev& m, int k, const cplx* Rt, const std::array<int, 3>& rd) {
+  const auto& wd = m.dims[k];
+  const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
+  const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
+  const int nsm = device_sms(c);
+  s.p1 = split_plan(Dlb * wl, dd * Drk, Dlk, nsm);
+  s.p3 = split_plan(Dlb * du, Drb, Drk * wr, nsm);
+  const Stream st = c.st();
+  // L as the A operand of T1 = L . X: rows Dlb*wl, inner Dlk, column-major
+  split_prepare(st, Dlb * wl, Dlk, Le, 1, (long long)Dlb * wl, 128,
+                bytes_reserve(c, s.Lp, split_operand_bytes(Dlb * wl, Dlk, 128)));
+  // Rt as the B operand of Y = T2 . Rt: its columns (Drb) are the prepared rows
+  split_prepare(st, Drb, Drk * wr, Rt, (long long)Drk * wr, 1, s.p3.BN,
+                bytes_reserve(c, s.Rp, split_operand_bytes(Drb, Drk * wr, s.p3.BN)));
+  bytes_reserve(c, c.spX, split_operand_bytes(dd * Drk, Dlk, s.p1.BN));
+  bytes_reserve(c, c.spT, split_operand_bytes(Dlb * du, Drk * wr, 128));
+  long long part = 0;
+  if (s.p1.splits > 1) part = std::max(part, (long long)s.p1.splits * s.p1.M * s.p1.N);
+  if (s.p3.splits > 1) part = std::max(part, (long long)s.p3.splits * s.p3.M * s.p3.N);
+  if (part > 0) dbuf_reserve(c, c.spPart, part);
+  s.ready = true;
+}
+
+void split_matvec_release(Context& c, SplitMatvec& s) {
+  dbuf_free(c, s.Lp);
+  dbuf_free(c, s.Rp);
+  s.ready = false;
+}
+
 void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpoDev& m, int k,
                 bool adjoint, const cplx* Rt, const std::array<int, 3>& rd, const cplx* x, cplx* y,
-                cplx offset, Counters* cnt) {
+                cplx offset, Counters* cnt, const SplitMatvec* sp) {
   const auto& wd = m.dims[k];
   const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
   const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
@@ -479,7 +531,17 @@ void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const 
   g.A = Le; g.lda = (long long)Dlb * wl;
   g.B = x; g.ldb = Dlk;
   g.C = c.t1.p; g.ldc = (long long)Dlb * wl;
-  zgemm(c.st(), g, c.scratch);
+  // the caller prepared sp from the same Le and Rt (the adjoint ones for adjoint)
+  const bool split = sp && sp->ready;
+  if (split) {
+    // X as the B operand: its columns (dd*Drk) are the prepared rows
+    uint8_t* xp = reinterpret_cast<uint8_t*>(c.spX.p);
+    split_prepare(c.st(), dd * Drk, Dlk, x, Dlk, 1, sp->p1.BN, xp);
+    zgemm_split_prepared(c.st(), sp->p1, reinterpret_cast<const uint8_t*>(sp->Lp.p), xp, c.t1.p, g.ldc,
+                         make_double2(1.0, 0.0), nullptr, 0, make_double2(0.0, 0.0), c.spPart.p, c.dsplit_err);
+  } else {
+    zgemm(c.st(), g, c.scratch);
+  }
   // step 2: T2[a', s', r, c] = sum_{b,s} W[s',b,s,c] T1[a',b,s,r]
   const long long n2 = (long long)Dlb * du * Drk * wr;
   dbuf_reserve(c, c.t2, n2);
@@ -501,9 +563,17 @@ void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const 
   if (offset.x != 0.0 || offset.y != 0.0) {
     h.Cin = x; h.ldcin = (long long)Dlb * du; h.beta = offset;
   }
-  zgemm(c.st(), h, c.scratch);
+  if (split) {
+    uint8_t* tp = reinterpret_cast<uint8_t*>(c.spT.p);
+    split_prepare(c.st(), h.M, h.K, c.t2.p, 1, h.lda, 128, tp);
+    zgemm_split_prepared(c.st(), sp->p3, tp, reinterpret_cast<const uint8_t*>(sp->Rp.p), y, h.ldc,
+                         make_double2(1.0, 0.0), h.Cin, h.ldcin, h.beta, c.spPart.p, c.dsplit_err);
+  } else {
+    zgemm(c.st(), h, c.scratch);
+  }
   if (cnt) {
     cnt->matvecs++;
+    if (split) cnt->split_matvecs++;
     cnt->flops += mv_flops(dd, wl, wr, Dlb, Drb);
   }
 }
@@ -1046,6 +1116,17 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
   int pos = 0, round = 0;
   const double tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
   const cplx off = make_double2(offset, 0.0);
+  // Mixed precision (opt.precision == 1): split-precision products while the
+  // sweep is far from convergence, FP64 from the half-sweep after the energy
+  // change first falls below kSplitSwitchTol; the FP64 phase ends by the
+  // reference's test, after at least one full FP64 round.  Energies in the
+  // split phase carry the products' error (about 1e-7 relative), so its
+  // eigensolver tolerance and energy-increase margin are set at that level,
+  // and the first FP64 round is not tested for an increase.
+  bool split_phase = (opt.precision == 1);
+  bool first64 = false;
+  SplitMatvec smv;
+  if (split_phase) *c.hsplit_err = 0;
   try {
     while (!done) {
       opt.check_cancel();
@@ -1057,59 +1138,67 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
       const cplx* Rt = E.Re[pos].p;
       auto ld = E.ldims[pos];
       auto rd = E.rdims[pos];
+      smv.ready = false;
+      if (split_phase) split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
       auto apply = [&](const cplx* xin, cplx* yout, double sg) {
-        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(off.x - sg, off.y), &cnt);
+        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(off.x - sg, off.y), &cnt,
+                   split_phase ? &smv : nullptr);
       };
       int its = 0;
-      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, tol, opt.max_krylov, &its, val + offset);
+      const double etol = split_phase ? std::max(tol, kSplitEigTol) : tol;
+      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, etol, opt.max_krylov, &its, val + offset);
       cnt.site_solves++;
+      if (split_phase && *c.hsplit_err)
+        throw Error(MPSGPU_TIMEOUT, "findGroundState: a bounded wait in the tensor-core kernel ran out");
       val = theta - offset;
-      if ((val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
-        if (val - energy > std::fabs(energy + offset) * opt.convtol)
+      if (!first64 && (val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
+        const double margin = split_phase ? std::max(opt.convtol, kSplitIncreaseTol) : opt.convtol;
+        if (val - energy > std::fabs(energy + offset) * margin)
           throw Error(MPSGPU_ENERGY_INCREASE, "findGroundState: energy increasing");
       }
       mps_gauge_site(c, init, pos, right ? 'R' : 'L', true, &cnt);
       for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
       for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
-      if (right) {
-        if (pos == L - 1) {
-          right = false;
-          done = std::fabs(energy - val) < opt.convtol * std::fabs(energy + offset);
-          if (!done && std::fabs(val) < 1e-13) done = true;
-          energy = val;
-          if (opt.verbose) printf("mpsgpu: round %d energy %.15g\n", round, val);
-          if (!done) {
-            mps_gauge_site(c, init, pos, 'L', true, &cnt);
-            pos--;
+      const bool at_end = right ? (pos == L - 1) : (pos == 0);
+      if (at_end) {
+        const double change = std::fabs(energy - val);
+        const bool was_split = split_phase;
+        done = change < opt.convtol * std::fabs(energy + offset);
+        if (!done && std::fabs(val) < 1e-13) done = true;
+        if (split_phase) {
+          cnt.split_rounds++;
+          if (change < std::max(opt.convtol, kSplitSwitchTol) * std::fabs(energy + offset)) {
+            split_phase = false;
+            first64 = true;
           }
-          round++;
-        } else {
-          pos++;
+          done = false;
+        } else if (first64) {
+          // the first FP64 half-sweep was compared with a split-phase energy
+          first64 = false;
+          done = false;
         }
+        energy = val;
+        if (opt.verbose)
+          printf("mpsgpu: round %d energy %.15g%s\n", round, val, was_split ? " (split)" : "");
+        if (!done) {
+          mps_gauge_site(c, init, pos, right ? 'L' : 'R', true, &cnt);
+          pos += right ? -1 : 1;
+        }
+        right = !right;
+        round++;
       } else {
-        if (pos == 0) {
-          right = true;
-          done = std::fabs(energy - val) < opt.convtol * std::fabs(energy + offset);
-          if (!done && std::fabs(val) < 1e-13) done = true;
-          energy = val;
-          if (opt.verbose) printf("mpsgpu: round %d energy %.15g\n", round, val);
-          if (!done) {
-            mps_gauge_site(c, init, pos, 'R', true, &cnt);
-            pos++;
-          }
-          round++;
-        } else {
-          pos--;
-        }
+        pos += right ? 1 : -1;
       }
       if (!done && round >= opt.max_rounds)
         throw Error(MPSGPU_NOT_CONVERGED, "findGroundState: round limit reached");
     }
   } catch (...) {
     E.release(c);
+    split_matvec_release(c, smv);
     throw;
   }
   E.release(c);
+  split_matvec_release(c, smv);
   cnt.rounds += round;
   return energy;
 }
@@ -1325,10 +1414,19 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
   bool right = true, done = false;
   int pos = 0, round = 0;
   const double tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
+  // mixed precision as in find_ground_state: split-precision products of
+  // both halves of the Hermitian multiplier until the half-sweep energy
+  // settles, then FP64 (at least one full round)
+  bool split_phase = (opt.precision == 1);
+  bool first64 = false;
+  SplitMatvec smv, smvh;
+  if (split_phase) *c.hsplit_err = 0;
   auto cleanup = [&]() {
     E.release(c);
     for (auto& n : NC) n.release(c);
     for (DBuf* b : {&Lh, &Rth, &U, &y2, &sq}) dbuf_free(c, *b);
+    split_matvec_release(c, smv);
+    split_matvec_release(c, smvh);
   };
   try {
     while (!done) {
@@ -1392,21 +1490,33 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
       cplx* dots = c.dcplx + 512;
       const cplx* Le = E.Le[pos].p;
       const cplx* Rt = E.Re[pos].p;
+      smv.ready = smvh.ready = false;
+      if (split_phase) {
+        split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
+        split_matvec_prepare(c, smvh, Lh.p, ld, ops, pos, Rth.p, rd);
+      }
       auto apply = [&](const cplx* xin, cplx* yout, double sg) {
-        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(0.0, 0.0), &cnt);
-        heff_apply(c, Lh.p, ld, ops, pos, true, Rth.p, rd, xin, y2.p, make_double2(0.0, 0.0), &cnt);
+        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(0.0, 0.0), &cnt,
+                   split_phase ? &smv : nullptr);
+        heff_apply(c, Lh.p, ld, ops, pos, true, Rth.p, rd, xin, y2.p, make_double2(0.0, 0.0), &cnt,
+                   split_phase ? &smvh : nullptr);
         cnt.matvecs--;  // the pair counts as one product of the Hermitian multiplier
+        if (split_phase) cnt.split_matvecs--;
         zaxpby(c.st(), N, make_double2(0.5, 0.0), y2.p, make_double2(0.5, 0.0), yout);
         if (offset - sg != 0.0) zaxpby(c.st(), N, make_double2(offset - sg, 0.0), xin, make_double2(1.0, 0.0), yout);
         cgemv_c(c.st(), N, nk, U.p, N, xin, dots, c.scratch);
         cgemv_n_sub(c.st(), N, nk, U.p, N, dots, yout, 1.0);
       };
       int its = 0;
-      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, tol, opt.max_krylov, &its, val + offset);
+      const double etol = split_phase ? std::max(tol, kSplitEigTol) : tol;
+      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, etol, opt.max_krylov, &its, val + offset);
       cnt.site_solves++;
+      if (split_phase && *c.hsplit_err)
+        throw Error(MPSGPU_TIMEOUT, "findNextExcitedState: a bounded wait in the tensor-core kernel ran out");
       val = theta - offset;
-      if ((val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
-        if (val - energy > std::fabs(energy + offset) * 1e-6)
+      if (!first64 && (val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
+        const double margin = split_phase ? kSplitIncreaseTol : 1e-6;
+        if (val - energy > std::fabs(energy + offset) * margin)
           throw Error(MPSGPU_ENERGY_INCREASE, "findNextExcitedState: energy increasing");
       }
       mps_gauge_site(c, init, pos, right ? 'R' : 'L', true, &cnt);
@@ -1414,10 +1524,25 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
       for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
       const bool at_end = (right && pos == L - 1) || (!right && pos == 0);
       if (at_end) {
-        done = std::fabs(energy - val) < opt.convtol * std::fabs(energy + offset);
-        if (!done && (std::fabs(energy - val) < 1e-12 || round > MAX_ROUND_EXCTD)) done = true;
+        const double change = std::fabs(energy - val);
+        const bool was_split = split_phase;
+        done = change < opt.convtol * std::fabs(energy + offset);
+        if (!done && (change < 1e-12 || round > MAX_ROUND_EXCTD)) done = true;
+        if (split_phase) {
+          cnt.split_rounds++;
+          if (change < std::max(opt.convtol, kSplitSwitchTol) * std::fabs(energy + offset) ||
+              round > MAX_ROUND_EXCTD) {
+            split_phase = false;
+            first64 = true;
+          }
+          done = false;
+        } else if (first64) {
+          first64 = false;
+          done = false;
+        }
         energy = val;
-        if (opt.verbose) printf("mpsgpu: excited round %d energy %.15g\n", round, val);
+        if (opt.verbose)
+          printf("mpsgpu: excited round %d energy %.15g%s\n", round, val, was_split ? " (split)" : "");
         if (!done) {
           if (right) { mps_gauge_site(c, init, pos, 'L', true, &cnt); pos--; }
           else { mps_gauge_site(c, init, pos, 'R', true, &cnt); pos++; }

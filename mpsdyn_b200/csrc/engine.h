@@ -55,6 +55,10 @@ struct Context {
   DBuf t1, t2, t3, t4, matA, matQ, matR;
   DBuf lanV, lanW;     // Lanczos basis and work vector
   DBuf lanT, lanQ;     // thick restart: V G product and the restart matrix G
+  // split-precision matvec: prepared x and T2 (BF16 limb planes) and split-K partials
+  DBuf spX, spT, spPart;
+  int* hsplit_err = nullptr;   // pinned, mapped: set by a tensor-core kernel whose bounded wait ran out
+  int* dsplit_err = nullptr;   // its device address
   double* dscal = nullptr;     // device scalars (alpha, beta, norms)
   cplx* dcplx = nullptr;       // device complex scalars (dots)
   double* hscal = nullptr;     // pinned host mirror
@@ -100,11 +104,16 @@ struct Counters {
   double flops = 0.0;
   double mv_ms = 0.0;
   int rounds = 0;
+  long long split_matvecs = 0;  // products in split precision
+  int split_rounds = 0;         // half-sweeps in split precision
 };
 
 struct SolveOptions {
   double convtol = 1e-5, eigtol = 0.0, excorthtol = 0.0;
   int max_rounds = 1000, max_krylov = 64, verbose = 0;
+  // 0: complex FP64 throughout; 1: mixed (split-precision matvec products
+  // until the half-sweep energy settles to kSplitSwitchTol, then FP64 to convtol)
+  int precision = 0;
   // Raised by another host thread to stop a sweep between two site steps
   // (MPSGPU_CANCELLED); nothing is in flight on the device when it returns.
   const volatile int* cancel = nullptr;
@@ -132,9 +141,20 @@ void mps_gauge_site(Context& c, MpsDev& s, int pos, char dir, bool next, Counter
 void mps_increase_bond(Context& c, MpsDev& s, int D);
 
 // y = Heff x (+ offset x); environments in device layout.
+// Operands of one site's effective Hamiltonian prepared for the split-precision
+// products (BF16 limb planes of L and Rt, made once per site solve).
+struct SplitMatvec {
+  SplitPlan p1, p3;  // T1 = L . X and Y = T2 . Rt
+  DBuf Lp, Rp;       // prepared L and Rt (the per-product X and T2 planes live in the Context)
+  bool ready = false;
+};
+void split_matvec_prepare(Context& c, SplitMatvec& s, const cplx* Le, const std::array<int, 3>& ld,
+                          const MpoDev& m, int k, const cplx* Rt, const std::array<int, 3>& rd);
+void split_matvec_release(Context& c, SplitMatvec& s);
+// y = Heff x + offset x; in split precision when sp is non-null and ready.
 void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpoDev& m, int k,
                 bool adjoint, const cplx* Rt, const std::array<int, 3>& rd, const cplx* x,
-                cplx* y, cplx offset, Counters* cnt);
+                cplx* y, cplx offset, Counters* cnt, const SplitMatvec* sp = nullptr);
 // Left/right environment update (Operator::contractleftop / contractrightop).
 void env_left_update(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpsDev& ket,
                      const MpoDev* m, int k, const MpsDev& bra, DBuf& out,

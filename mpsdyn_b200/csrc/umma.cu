@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
       }
     }
     if (!ok) {
-      atomicExch(p.err, 1);
+      *(volatile int*)p.err = 1;
       aborted = 1;
       for (int t = kt; t < loaded; t++) mbar_wait(smem_u32(&full_bar[t % SP_STAGES]), (t / SP_STAGES) & 1);
     }
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
   }
   __syncthreads();
   const bool done = mbar_wait(smem_u32(&done_bar), 0);
-  if (!done && lane == 0) atomicExch(p.err, 1);
+  if (!done && lane == 0) *(volatile int*)p.err = 1;
   tc_fence_after();
   if (!aborted && __all_sync(0xffffffffu, done)) {
     const int row = mt * SP_BM + warp * 32 + lane;
