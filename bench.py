@@ -173,6 +173,16 @@ def run_reference(args, rank: int, world: int) -> None:
 # GPU arm
 # ---------------------------------------------------------------------------
 
+def bf16_peak() -> tuple:
+    """Dense BF16 tensor throughput measured on this pool (MEASURED_PEAKS.json,
+    burst figure), else the fallback measurement; returns (TFLOP/s, source)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops (measured, burst)"
+    except Exception:
+        return 1590.0, "fallback 1.59 PFLOP/s (earlier measurement on this pool)"
+
+
 def fp64_gemm_peak(torch) -> float:
     """Measured complex FP64 GEMM throughput of cuBLAS (torch.matmul on
     complex128, 4096^3, 8 n^3 flops), best of 5, TFLOP/s: the tensor-pipe
@@ -469,7 +479,9 @@ def run_grouped(args) -> None:
     ms, flops = capi.heff_matvec_grouped(ctx, inst, args.steps)
     # accuracy: relative error of a few instances against torch (cuBLAS) FP64
     errs = []
-    for k in list(range(min(n, 3))) + [int(np.argmax(Ds))]:
+    check = list(range(min(n, 3))) + [int(np.argmax(Ds))]
+    y64 = {k: keep[k][6].clone() for k in check}
+    for k in check:
         D, w, L, W, R, x, y = keep[k]
         Lm = L.view(D, w, D).permute(2, 1, 0)            # column-major (bra, w, ket) -> [a', b, a]
         Wm = W.view(w, 2, w, 2).permute(3, 2, 1, 0)      # [s', b, s, c]
@@ -482,15 +494,39 @@ def run_grouped(args) -> None:
         errs.append(float((Y - ref).abs().max() / ref.abs().max()))
     peak = fp64_gemm_peak(torch)
     tf = flops / (ms * 1e-3) / 1e12
-    line = {"metric": "grouped effective-Hamiltonian matvec TFLOP/s (512 instances, FP64)", "value": tf,
-            "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+    roof64 = {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+              "peak_source": "cuBLAS complex128 GEMM 4096^3 measured in this run"}
+    split = None
+    if args.precision == "mixed":
+        # the same products in split precision (tcgen05, BF16 limbs); the
+        # environments' limb planes are made once (ms_prepare), x and the
+        # intermediate in every product
+        ms_s, _, ms_prep = capi.heff_matvec_grouped_ex(ctx, inst, 1, args.steps)
+        torch.cuda.synchronize()
+        serr = max(float((keep[k][6] - y64[k]).abs().max() / y64[k].abs().max()) for k in check)
+        gemm_flops = sum(8.0 * (D * w * D * 2 * D + D * 2 * D * w * D) for D, w in zip(Ds.tolist(), ws.tolist()))
+        bpk, bsrc = bf16_peak()
+        bf16_rate = 6.0 * gemm_flops / (ms_s * 1e-3) / 1e12
+        split = {"ms_per_step": ms_s, "tflops_fp64_equivalent": flops / (ms_s * 1e-3) / 1e12,
+                 "env_prepare_ms_once": ms_prep, "rel_error_vs_fp64": serr,
+                 "speedup_vs_fp64": ms / ms_s,
+                 "roofline": {"bound": "tensor", "achieved": bf16_rate, "peak": bpk, "unit": "TFLOP/s",
+                              "frac": bf16_rate / bpk, "peak_source": bsrc,
+                              "note": ("BF16 tensor flops (24 limb MMAs per complex k-step = 6x the complex "
+                                       "GEMM flops) over the whole product time, prep and leg kernel included")}}
+    line = {"metric": "grouped effective-Hamiltonian matvec TFLOP/s (512 instances)",
+            "value": split["tflops_fp64_equivalent"] if split else tf,
+            "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": 1,
+            "ms_per_step": split["ms_per_step"] if split else ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128/bf16x3" if split else "c128",
             "data": "synthetic (complex N(0,1), torch generator seed 2)",
             "config": {"workload": "grouped_matvec_x512", "instances": n, "D": "U{32..1024}", "w": "U{3,5}",
-                       "graph": "3 grouped launches captured once, replayed", "l2": "inputs > 126 MB L2"},
-            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
-                         "peak_source": "cuBLAS complex128 GEMM 4096^3 measured in this run"},
-            "rel_error_vs_cublas_fp64": max(errs), "flops_per_step": flops}
+                       "precision": "split (BF16 limbs, tcgen05); value in FP64-equivalent flops" if split else "fp64",
+                       "graph": "grouped launches captured once, replayed", "l2": "inputs > 126 MB L2"},
+            "roofline": split["roofline"] if split else roof64,
+            "rel_error_vs_cublas_fp64": max(errs), "flops_per_step": flops,
+            "fp64": {"tflops": tf, "ms_per_step": ms, "roofline": roof64}, "split": split}
     print(json.dumps(line), flush=True)
     ctx.close()
 

@@ -330,6 +330,15 @@ typedef struct {
 } mpsgpu_heff_instance;
 mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgpu_heff_instance* inst,
                                          int repeats, double* ms_per_run, double* flops);
+/* The same with a precision choice: 0 = complex FP64 (as above); 1 = split
+ * precision, both GEMMs of every instance on the tcgen05 tensor cores with
+ * BF16 limbs (about 1e-7 relative error).  In split precision the limb
+ * planes of L and Rt are made once before the products (the environments
+ * of an eigensolve do not change between its products); *ms_prepare gets
+ * that device time, and every product prepares x and the intermediate. */
+mpsgpu_status mpsgpu_heff_matvec_grouped_ex(mpsgpu_context* ctx, int n, const mpsgpu_heff_instance* inst,
+                                            int precision, int repeats, double* ms_per_run, double* flops,
+                                            double* ms_prepare);
 
 /* Split-precision complex GEMM C = A B (column-major, complex interleaved,
  * host buffers; m x k times k x n) on the tcgen05 tensor cores: every FP64

@@ -27,7 +27,7 @@ EXPORTS = [
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
     "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_ground_state_two_site", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_contract2", "mpsgpu_expectation_local", "mpsgpu_entropy",
-    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped", "mpsgpu_zgemm_split",
+    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped", "mpsgpu_heff_matvec_grouped_ex", "mpsgpu_zgemm_split",
     "mpsgpu_env_left", "mpsgpu_env_right",
     "mpsgpu_qr", "mpsgpu_lq", "mpsgpu_qr_device_noalloc",
     "mpsgpu_server_create", "mpsgpu_server_submit", "mpsgpu_server_poll", "mpsgpu_server_cancel",
@@ -437,6 +437,22 @@ def heff_matvec_grouped(ctx: "Context", instances: list, repeats: int = 0):
     ms, fl = C.c_double(), C.c_double()
     ctx._check(lib.mpsgpu_heff_matvec_grouped(ctx.h, len(instances), arr, repeats, C.byref(ms), C.byref(fl)))
     return (ms.value if repeats > 0 else None), fl.value
+
+
+def heff_matvec_grouped_ex(ctx: "Context", instances: list, precision: int = 0, repeats: int = 0):
+    """mpsgpu_heff_matvec_grouped_ex: as heff_matvec_grouped with a precision
+    choice (0 FP64, 1 split).  Returns (ms_per_run or None, flops, ms_prepare)."""
+    lib = ctx.lib
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    lib.mpsgpu_heff_matvec_grouped_ex.argtypes = [P, C.c_int, C.POINTER(HeffInstance), C.c_int, C.c_int, D, D, D]
+    arr = (HeffInstance * len(instances))()
+    for i, s in enumerate(instances):
+        arr[i] = HeffInstance(s["d"], s["wl"], s["wr"], s["Dl"], s["Dr"], s["L"], s["W"], s["Rt"], s["x"], s["y"])
+    ms, fl, mp = C.c_double(), C.c_double(), C.c_double()
+    ctx._check(lib.mpsgpu_heff_matvec_grouped_ex(ctx.h, len(instances), arr, precision, repeats, C.byref(ms),
+                                                 C.byref(fl), C.byref(mp)))
+    return (ms.value if repeats > 0 else None), fl.value, mp.value
 
 
 def zgemm_split(ctx: "Context", A: np.ndarray, B: np.ndarray, repeats: int = 0):

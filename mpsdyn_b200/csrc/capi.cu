@@ -640,9 +640,10 @@ mpsgpu_status mpsgpu_heff_matvec(mpsgpu_context* ctx, const int* ldims, const do
   });
 }
 
-mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgpu_heff_instance* inst, int repeats,
-                                         double* ms_per_run, double* flops) {
-  if (!ctx || n <= 0 || !inst || repeats < 0) return MPSGPU_INVALID;
+mpsgpu_status mpsgpu_heff_matvec_grouped_ex(mpsgpu_context* ctx, int n, const mpsgpu_heff_instance* inst,
+                                            int precision, int repeats, double* ms_per_run, double* flops,
+                                            double* ms_prepare) {
+  if (!ctx || n <= 0 || !inst || repeats < 0 || (precision != 0 && precision != 1)) return MPSGPU_INVALID;
   return guarded(ctx, [&] {
     Context& c = ctx->c;
     std::vector<HeffInstance> v(n);
@@ -657,8 +658,21 @@ mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgp
     MPSGPU_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
     GroupedMatvecPlan plan;
     const Stream st = c.st();
-    grouped_matvec_plan(st, v, plan, nsm);
+    const bool split = precision == 1;
+    grouped_matvec_plan(st, v, plan, nsm, split);
+    const int per_run = split ? 6 : 4;  // launches of one grouped product
     try {
+      if (split) {
+        MPSGPU_CUDA(cudaEventRecord(c.mv0, c.stream));
+        grouped_matvec_prepare_env(st, plan);
+        MPSGPU_CUDA(cudaEventRecord(c.mv1, c.stream));
+        MPSGPU_CUDA(cudaEventSynchronize(c.mv1));
+        float ms = 0.f;
+        MPSGPU_CUDA(cudaEventElapsedTime(&ms, c.mv0, c.mv1));
+        if (ms_prepare) *ms_prepare = ms;
+      } else if (ms_prepare) {
+        *ms_prepare = 0.0;
+      }
       grouped_matvec_run(st, plan);
       if (flops) *flops = plan.flops;
       if (repeats > 0) {
@@ -678,11 +692,16 @@ mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgp
         float ms = 0.f;
         MPSGPU_CUDA(cudaEventElapsedTime(&ms, c.mv0, c.mv1));
         if (ms_per_run) *ms_per_run = ms / repeats;
-        c.launches += 4LL * (repeats + 1);
+        c.launches += (long long)per_run * (repeats + 1);
         cudaGraphExecDestroy(exec);
         cudaGraphDestroy(graph);
       }
       MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+      if (split) {
+        int herr = 0;
+        MPSGPU_CUDA(cudaMemcpy(&herr, plan.err, sizeof(int), cudaMemcpyDeviceToHost));
+        MPSGPU_CHECK(herr == 0, MPSGPU_TIMEOUT, "grouped matvec: a bounded wait in the tensor-core kernel ran out");
+      }
     } catch (...) {
       grouped_matvec_free(st, plan);
       throw;
@@ -690,6 +709,11 @@ mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgp
     grouped_matvec_free(st, plan);
     MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
   });
+}
+
+mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgpu_heff_instance* inst, int repeats,
+                                         double* ms_per_run, double* flops) {
+  return mpsgpu_heff_matvec_grouped_ex(ctx, n, inst, 0, repeats, ms_per_run, flops, nullptr);
 }
 
 mpsgpu_status mpsgpu_zgemm_split(mpsgpu_context* ctx, int m, int n, int k, const double* A, int lda,

@@ -85,7 +85,7 @@ __global__ void wcontract_grouped_kernel(const WGroup* __restrict__ g, int n, lo
 GroupedMatvecPlan::~GroupedMatvecPlan() {}
 
 void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst, GroupedMatvecPlan& plan,
-                         int nsm) {
+                         int nsm, bool split) {
   const int n = (int)inst.size();
   MPSGPU_CHECK(n > 0, MPSGPU_INVALID, "grouped matvec: no instances");
   // largest first
@@ -109,6 +109,16 @@ void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst
   std::vector<GroupedGemm> g1(n), g3(n);
   std::vector<WGroup> wg(n);
   std::vector<WPerm> wp(n);
+  // split form: byte offsets of every prepared operand in one buffer
+  std::vector<SplitProblem> s1(split ? n : 0), s3(split ? n : 0);
+  std::vector<SplitPrepJob> jenv(split ? 2 * n : 0), jx(split ? n : 0), jt(split ? n : 0);
+  std::vector<long long> offL(n), offX(n), offT(n), offR(n);
+  long long spb = 0;
+  auto take = [&](long long bytes) {
+    const long long o = spb;
+    spb += (bytes + 255) / 256 * 256;
+    return o;
+  };
   long long o1 = 0, ow = 0, pix = 0;
   int maxnin = 1;
   for (int q = 0; q < n; q++) {
@@ -141,6 +151,21 @@ void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst
     ow += (long long)d * wl * d * wr;
     pix += (long long)Dl * Dr;
     maxnin = std::max(maxnin, wl * d);
+    if (split) {
+      offL[q] = take(split_operand_bytes(Dl * wl, Dl, 128));
+      offX[q] = take(split_operand_bytes(d * Dr, Dl, 128));
+      offT[q] = take(split_operand_bytes(Dl * d, Dr * wr, 128));
+      offR[q] = take(split_operand_bytes(Dr, Dr * wr, 128));
+      // L as A (rows Dl*wl), x as B (rows = columns of T1), T2 as A, Rt as B
+      jenv[2 * q] = SplitPrepJob{Dl * wl, Dl, 0, h.L, 1, (long long)Dl * wl, nullptr, 0};
+      jenv[2 * q + 1] = SplitPrepJob{Dr, Dr * wr, 0, h.Rt, (long long)Dr * wr, 1, nullptr, 0};
+      jx[q] = SplitPrepJob{d * Dr, Dl, 0, h.x, Dl, 1, nullptr, 0};
+      jt[q] = SplitPrepJob{Dl * d, Dr * wr, 0, T2, 1, (long long)Dl * d, nullptr, 0};
+      s1[q].M = Dl * wl; s1[q].N = d * Dr; s1[q].K = Dl;
+      s1[q].C = T1; s1[q].ldc = (long long)Dl * wl;
+      s3[q].M = Dl * d; s3[q].N = Dr; s3[q].K = Dr * wr;
+      s3[q].C = h.y; s3[q].ldc = (long long)Dl * d;
+    }
     plan.flops += 8.0 * ((double)Dl * wl * Dl * d * Dr + (double)Dl * d * d * wl * wr * Dr +
                          (double)Dl * d * Dr * wr * Dr);
   }
@@ -163,6 +188,45 @@ void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst
   MPSGPU_CUDA(cudaMemcpyAsync(plan.d_wp, wp.data(), n * sizeof(WPerm), cudaMemcpyHostToDevice, st.s));
   MPSGPU_CUDA(cudaStreamSynchronize(st.s));
   plan.ctas = nsm;
+  plan.split = split;
+  if (split) {
+    dbuf_alloc(st, plan.sp, (spb + (long long)sizeof(cplx) - 1) / (long long)sizeof(cplx));
+    uint8_t* base = reinterpret_cast<uint8_t*>(plan.sp.p);
+    for (int q = 0; q < n; q++) {
+      jenv[2 * q].out = base + offL[q];
+      jenv[2 * q + 1].out = base + offR[q];
+      jx[q].out = base + offX[q];
+      jt[q].out = base + offT[q];
+      s1[q].Ap = base + offL[q]; s1[q].Bp = base + offX[q];
+      s3[q].Ap = base + offT[q]; s3[q].Bp = base + offR[q];
+    }
+    plan.stiles1 = split_group_tiles(s1.data(), n);
+    plan.stiles3 = split_group_tiles(s3.data(), n);
+    plan.thr_env = split_prepare_jobs(jenv.data(), 2 * n);
+    plan.thr_x = split_prepare_jobs(jx.data(), n);
+    plan.thr_t = split_prepare_jobs(jt.data(), n);
+    const size_t sbytes = 2 * n * sizeof(SplitProblem) + 4 * n * sizeof(SplitPrepJob) + 256;
+    MPSGPU_CUDA(cudaMallocAsync(&plan.sdesc, sbytes, st.s));
+    char* sq = (char*)plan.sdesc;
+    plan.d_s1 = (SplitProblem*)sq; sq += n * sizeof(SplitProblem);
+    plan.d_s3 = (SplitProblem*)sq; sq += n * sizeof(SplitProblem);
+    plan.d_jenv = (SplitPrepJob*)sq; sq += 2 * n * sizeof(SplitPrepJob);
+    plan.d_jx = (SplitPrepJob*)sq; sq += n * sizeof(SplitPrepJob);
+    plan.d_jt = (SplitPrepJob*)sq; sq += n * sizeof(SplitPrepJob);
+    plan.err = (int*)sq;
+    MPSGPU_CUDA(cudaMemcpyAsync(plan.d_s1, s1.data(), n * sizeof(SplitProblem), cudaMemcpyHostToDevice, st.s));
+    MPSGPU_CUDA(cudaMemcpyAsync(plan.d_s3, s3.data(), n * sizeof(SplitProblem), cudaMemcpyHostToDevice, st.s));
+    MPSGPU_CUDA(cudaMemcpyAsync(plan.d_jenv, jenv.data(), 2 * n * sizeof(SplitPrepJob), cudaMemcpyHostToDevice, st.s));
+    MPSGPU_CUDA(cudaMemcpyAsync(plan.d_jx, jx.data(), n * sizeof(SplitPrepJob), cudaMemcpyHostToDevice, st.s));
+    MPSGPU_CUDA(cudaMemcpyAsync(plan.d_jt, jt.data(), n * sizeof(SplitPrepJob), cudaMemcpyHostToDevice, st.s));
+    MPSGPU_CUDA(cudaMemsetAsync(plan.err, 0, sizeof(int), st.s));
+    MPSGPU_CUDA(cudaStreamSynchronize(st.s));
+  }
+}
+
+void grouped_matvec_prepare_env(const Stream& st, GroupedMatvecPlan& plan) {
+  MPSGPU_CHECK(plan.split, MPSGPU_INVALID, "grouped matvec: not planned in split precision");
+  split_prepare_grouped(st, plan.d_jenv, 2 * plan.n, plan.thr_env);
 }
 
 void grouped_matvec_run(const Stream& st, GroupedMatvecPlan& plan) {
@@ -170,19 +234,31 @@ void grouped_matvec_run(const Stream& st, GroupedMatvecPlan& plan) {
   wperm_kernel<<<std::min<long long>(ceil_div(plan.wel, 256), 4096), 256, 0, st.s>>>(
       (const WPerm*)plan.d_wp, plan.n, plan.wel);
   after_launch(st);
-  zgemm_grouped(st, plan.d_g1, plan.n, plan.tiles1, plan.ctas);
+  if (plan.split) {
+    split_prepare_grouped(st, plan.d_jx, plan.n, plan.thr_x);
+    zgemm_split_grouped(st, plan.d_s1, plan.n, plan.stiles1, plan.err);
+  } else {
+    zgemm_grouped(st, plan.d_g1, plan.n, plan.tiles1, plan.ctas);
+  }
   const int g = (int)std::min<long long>(ceil_div(plan.pixels, 128), 148LL * 16);
   if (plan.maxnin <= 8) wcontract_grouped_kernel<8><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
   else if (plan.maxnin <= 16) wcontract_grouped_kernel<16><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
   else wcontract_grouped_kernel<32><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
   after_launch(st);
-  zgemm_grouped(st, plan.d_g3, plan.n, plan.tiles3, plan.ctas);
+  if (plan.split) {
+    split_prepare_grouped(st, plan.d_jt, plan.n, plan.thr_t);
+    zgemm_split_grouped(st, plan.d_s3, plan.n, plan.stiles3, plan.err);
+  } else {
+    zgemm_grouped(st, plan.d_g3, plan.n, plan.tiles3, plan.ctas);
+  }
 }
 
 void grouped_matvec_free(const Stream& st, GroupedMatvecPlan& plan) {
   if (plan.desc) cudaFreeAsync(plan.desc, st.s);
   plan.desc = nullptr;
-  for (DevMem* b : {&plan.t1, &plan.t2, &plan.wm})
+  if (plan.sdesc) cudaFreeAsync(plan.sdesc, st.s);
+  plan.sdesc = nullptr;
+  for (DevMem* b : {&plan.t1, &plan.t2, &plan.wm, &plan.sp})
     if (b->p) {
       cudaFreeAsync(b->p, st.s);
       b->p = nullptr;

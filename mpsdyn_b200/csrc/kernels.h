@@ -83,6 +83,31 @@ void split_prepare(const Stream& st, int rows, int K, const cplx* X, long long r
 void zgemm_split_prepared(const Stream& st, const SplitPlan& pl, const uint8_t* Ap, const uint8_t* Bp, cplx* C,
                           long long ldc, cplx alpha, const cplx* Cin, long long ldcin, cplx beta, cplx* part,
                           int* err);
+// Grouped form: every operand prepared with 128-row tiles (split_prepare
+// with RT = 128, or the grouped preparation below); one launch computes all
+// C_q = A_q B_q (M_q x N_q, inner K_q), one CTA per 128 x 128 tile.
+struct SplitProblem {
+  int M = 0, N = 0, K = 0;
+  int KS = 0, mtiles = 0;  // filled by split_group_tiles
+  const uint8_t* Ap = nullptr;
+  const uint8_t* Bp = nullptr;
+  cplx* C = nullptr;
+  long long ldc = 0;
+  long long tile_begin = 0;
+};
+long long split_group_tiles(SplitProblem* probs, int n);
+void zgemm_split_grouped(const Stream& st, const SplitProblem* d_probs, int n, long long tiles, int* err);
+// One preparation job per operand (rows x K, entry (r, k) at X[r*rs + k*ks]).
+struct SplitPrepJob {
+  int rows = 0, K = 0;
+  int KS = 0;  // filled by split_prepare_jobs
+  const cplx* X = nullptr;
+  long long rs = 0, ks = 0;
+  uint8_t* out = nullptr;
+  long long thread_begin = 0;  // filled by split_prepare_jobs
+};
+long long split_prepare_jobs(SplitPrepJob* jobs, int n);
+void split_prepare_grouped(const Stream& st, const SplitPrepJob* d_jobs, int n, long long threads);
 
 // ---- grouped effective-Hamiltonian matvec (grouped.cu) ----
 // One instance in device layouts: L (Dl, wl, Dl) = (bra, w, ket); W
@@ -115,10 +140,25 @@ struct GroupedMatvecPlan {
   long long tiles1 = 0, tiles3 = 0, pixels = 0, wel = 0;
   int maxnin = 1, ctas = 148;
   double flops = 0.0;  // algorithmic flops of one grouped product
+  // split precision: BF16 limb planes of L, Rt (prepared once by
+  // grouped_matvec_prepare_env), x and T2 (prepared in every product)
+  bool split = false;
+  DevMem sp;                                  // all prepared planes
+  void* sdesc = nullptr;                      // device tables below
+  SplitProblem* d_s1 = nullptr;               // T1 = L . x
+  SplitProblem* d_s3 = nullptr;               // y = T2 . Rt
+  SplitPrepJob* d_jenv = nullptr;             // L and Rt, 2n jobs
+  SplitPrepJob* d_jx = nullptr;               // x, n jobs
+  SplitPrepJob* d_jt = nullptr;               // T2, n jobs
+  long long stiles1 = 0, stiles3 = 0, thr_env = 0, thr_x = 0, thr_t = 0;
+  int* err = nullptr;                         // set by a tensor-core kernel whose bounded wait ran out
   ~GroupedMatvecPlan();
 };
+// split = true plans the split-precision form (tcgen05, BF16 limbs).
 void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst, GroupedMatvecPlan& plan,
-                         int nsm);
+                         int nsm, bool split = false);
+// Split form: the limb planes of the environments, made once per set of instances.
+void grouped_matvec_prepare_env(const Stream& st, GroupedMatvecPlan& plan);
 void grouped_matvec_run(const Stream& st, GroupedMatvecPlan& plan);
 void grouped_matvec_free(const Stream& st, GroupedMatvecPlan& plan);
 

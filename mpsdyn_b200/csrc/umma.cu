@@ -42,6 +42,7 @@ constexpr int SP_BK = 16;        // K of one BF16 MMA = one pipeline stage
 constexpr int SP_PLANES = 6;     // re h/m/l, im h/m/l
 constexpr int SP_STAGES = 4;
 constexpr int SP_THREADS = 128;
+constexpr int SP_GROUP_BN = 128;  // column tile of grouped launches
 constexpr unsigned long long SP_WAIT_NS = 2000000000ULL;
 
 __host__ __device__ constexpr int sp_plane_bytes(int rows) { return rows * SP_BK * 2; }
@@ -201,8 +202,16 @@ struct SplitGemmParams {
   int* err;
 };
 
-template <int BN>
-__global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmParams p) {
+// Grouped launches: one CTA per 128 x BN tile of any of n independent GEMMs
+// C_q = A_q B_q (no split K; the tiles of many products fill the SMs).
+struct SplitGroupParams {
+  const SplitProblem* probs;  // tile_begin ascending
+  int n;
+  int* err;
+};
+
+template <int BN, bool GROUPED>
+__global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmParams p, SplitGroupParams gp) {
   constexpr int A_STAGE = SP_PLANES * sp_plane_bytes(SP_BM);
   constexpr int B_STAGE = SP_PLANES * sp_plane_bytes(BN);
   constexpr int STAGE = A_STAGE + B_STAGE;
@@ -217,9 +226,41 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
   // 128-byte aligned ring of SP_STAGES stages (the launch adds 128 bytes of slack)
   const uint32_t ring = (smem_u32(smem_dyn) + 127u) & ~127u;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int mt = blockIdx.x, nt = blockIdx.y, sp = blockIdx.z;
-  const int k0 = sp * p.ks_per_split;
-  const int nk = min(p.KS - k0, p.ks_per_split);
+  int mt, nt, sp, k0, nk;
+  if constexpr (GROUPED) {
+    // the problem whose tile range holds this CTA (last tile_begin <= blockIdx.x)
+    const long long t = blockIdx.x;
+    int lo = 0, hi = gp.n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (gp.probs[mid].tile_begin <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const SplitProblem q = gp.probs[lo];
+    const long long local = t - q.tile_begin;
+    mt = (int)(local % q.mtiles);
+    nt = (int)(local / q.mtiles);
+    sp = 0;
+    k0 = 0;
+    nk = q.KS;
+    p.M = q.M;
+    p.N = q.N;
+    p.KS = q.KS;
+    p.Ap = q.Ap;
+    p.Bp = q.Bp;
+    p.C = q.C;
+    p.ldc = q.ldc;
+    p.alpha = cmake(1.0, 0.0);
+    p.Cin = nullptr;
+    p.part = nullptr;
+    p.err = gp.err;
+  } else {
+    mt = blockIdx.x;
+    nt = blockIdx.y;
+    sp = blockIdx.z;
+    k0 = sp * p.ks_per_split;
+    nk = min(p.KS - k0, p.ks_per_split);
+  }
 
   if (tid == 0) {
     for (int s = 0; s < SP_STAGES; s++) {
@@ -365,16 +406,61 @@ constexpr int split_smem_bytes() {
   return SP_STAGES * (SP_PLANES * sp_plane_bytes(SP_BM) + SP_PLANES * sp_plane_bytes(BN)) + 128;
 }
 
-template <int BN>
-void launch_split(const Stream& st, const SplitGemmParams& p, int mtiles, int ntiles, int splits) {
+template <int BN, bool GROUPED>
+void launch_split(const Stream& st, const SplitGemmParams& p, const SplitGroupParams& gp, dim3 grid) {
   constexpr int smem = split_smem_bytes<BN>();
   static bool attr = false;
   if (!attr) {
-    MPSGPU_CUDA(cudaFuncSetAttribute(zgemm_split_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    MPSGPU_CUDA(cudaFuncSetAttribute(zgemm_split_kernel<BN, GROUPED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     smem));
     attr = true;
   }
-  zgemm_split_kernel<BN><<<dim3(mtiles, ntiles, splits), SP_THREADS, smem, st.s>>>(p);
+  zgemm_split_kernel<BN, GROUPED><<<grid, SP_THREADS, smem, st.s>>>(p, gp);
   after_launch(st);
+}
+
+// Grouped operand preparation: job j covers threads [thread_begin, next);
+// every operand is tiled with 128-row tiles.
+__global__ void split_prepare_grouped_kernel(const SplitPrepJob* __restrict__ jobs, int n, long long total) {
+  constexpr int RT = SP_BM;
+  constexpr int groups = RT / 8;
+  constexpr int plane = sp_plane_bytes(RT);
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].thread_begin <= idx) lo = mid;
+      else hi = mid - 1;
+    }
+    const SplitPrepJob& jb = jobs[lo];
+    const long long li = idx - jb.thread_begin;
+    const int r = (int)(li & 7);
+    long long q = li >> 3;
+    const int g = (int)(q % groups);
+    q /= groups;
+    const int kg = (int)(q & 1);
+    q >>= 1;
+    const int ks = (int)(q % jb.KS);
+    const long long rt = q / jb.KS;
+    const long long row = rt * RT + g * 8 + r;
+    const int k0 = ks * SP_BK + kg * 8;
+    union {
+      __nv_bfloat16 h[8];
+      uint4 u;
+    } pk[SP_PLANES];
+#pragma unroll
+    for (int kk = 0; kk < 8; kk++) {
+      const int k = k0 + kk;
+      cplx x = cmake(0.0, 0.0);
+      if (row < jb.rows && k < jb.K) x = jb.X[row * jb.rs + (long long)k * jb.ks];
+      split3(x.x, pk[0].h[kk], pk[1].h[kk], pk[2].h[kk]);
+      split3(x.y, pk[3].h[kk], pk[4].h[kk], pk[5].h[kk]);
+    }
+    uint8_t* base = jb.out + ((rt * jb.KS + ks) * SP_PLANES) * plane + (long long)kg * (RT * 16) + g * 128 + r * 16;
+#pragma unroll
+    for (int p = 0; p < SP_PLANES; p++) *reinterpret_cast<uint4*>(base + (long long)p * plane) = pk[p].u;
+  }
 }
 
 }  // namespace
@@ -435,16 +521,54 @@ void zgemm_split_prepared(const Stream& st, const SplitPlan& pl, const uint8_t* 
   p.beta = beta;
   p.part = pl.splits > 1 ? part : nullptr;
   p.err = err;
+  const SplitGroupParams none{nullptr, 0, nullptr};
+  const dim3 grid(pl.mtiles, pl.ntiles, pl.splits);
   if (pl.BN == 128)
-    launch_split<128>(st, p, pl.mtiles, pl.ntiles, pl.splits);
+    launch_split<128, false>(st, p, none, grid);
   else
-    launch_split<64>(st, p, pl.mtiles, pl.ntiles, pl.splits);
+    launch_split<64, false>(st, p, none, grid);
   if (pl.splits > 1) {
     const long long total = (long long)pl.M * pl.N;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
     split_reduce_kernel<<<blocks, 256, 0, st.s>>>(pl.M, pl.N, pl.splits, part, C, ldc, alpha, Cin, ldcin, beta);
     after_launch(st);
   }
+}
+
+long long split_group_tiles(SplitProblem* probs, int n) {
+  long long t = 0;
+  for (int i = 0; i < n; i++) {
+    SplitProblem& q = probs[i];
+    q.KS = (q.K + SP_BK - 1) / SP_BK;
+    q.mtiles = (q.M + SP_BM - 1) / SP_BM;
+    q.tile_begin = t;
+    t += (long long)q.mtiles * ((q.N + SP_GROUP_BN - 1) / SP_GROUP_BN);
+  }
+  return t;
+}
+
+void zgemm_split_grouped(const Stream& st, const SplitProblem* d_probs, int n, long long tiles, int* err) {
+  MPSGPU_CHECK(tiles > 0 && tiles < (1LL << 31), MPSGPU_INVALID, "zgemm_split_grouped: tile count");
+  SplitGemmParams p{};
+  const SplitGroupParams gp{d_probs, n, err};
+  launch_split<SP_GROUP_BN, true>(st, p, gp, dim3((unsigned)tiles));
+}
+
+long long split_prepare_jobs(SplitPrepJob* jobs, int n) {
+  long long t = 0;
+  for (int i = 0; i < n; i++) {
+    SplitPrepJob& j = jobs[i];
+    j.KS = (j.K + SP_BK - 1) / SP_BK;
+    j.thread_begin = t;
+    t += (long long)((j.rows + SP_BM - 1) / SP_BM) * ((j.K + SP_BK - 1) / SP_BK) * 2 * SP_BM;
+  }
+  return t;
+}
+
+void split_prepare_grouped(const Stream& st, const SplitPrepJob* d_jobs, int n, long long threads) {
+  const int blocks = (int)std::min<long long>((threads + 255) / 256, 148LL * 16);
+  split_prepare_grouped_kernel<<<blocks, 256, 0, st.s>>>(d_jobs, n, threads);
+  after_launch(st);
 }
 
 }  // namespace mpsgpu
