@@ -547,30 +547,50 @@ def run_serving(args) -> None:
     gaps = rs.exponential(1.0 / args.rate, size=n)
     free, total = torch.cuda.mem_get_info(0)
     budget = int(free * 0.85)
-    with capi.Server(0, slots=args.batch, hbm_budget_bytes=budget) as srv:
-        t0 = time.perf_counter()
-        nxt = t0
-        for i in range(n):
-            nxt += gaps[i]
-            dt = nxt - time.perf_counter()
-            if dt > 0:
-                time.sleep(dt)
-            srv.submit(0, int(Ls[i]), int(Ds[i]), 1.0, float(gs[i]), float(hs[i]), i + 1)
-        srv.drain()
-        wall = time.perf_counter() - t0
-        res = srv.poll()
-    ok = [r for r in res if r["status"] == 0]
-    bad = [r["status"] for r in res if r["status"] != 0]
-    lat = np.array([r["t_end"] - r["t_submit"] for r in ok]) if ok else np.zeros(1)
-    span = max(r["t_end"] for r in res) - min(r["t_submit"] for r in res)
-    line = {"metric": "served DMRG solves/s (Ising mix, FP64)", "value": len(ok) / span, "unit": "solves/s",
+
+    def stream(precision):
+        with capi.Server(0, slots=args.batch, hbm_budget_bytes=budget) as srv:
+            t0 = time.perf_counter()
+            nxt = t0
+            for i in range(n):
+                nxt += gaps[i]
+                dt = nxt - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                srv.submit(0, int(Ls[i]), int(Ds[i]), 1.0, float(gs[i]), float(hs[i]), i + 1, 1e-10, precision)
+            srv.drain()
+            wall = time.perf_counter() - t0
+            res = srv.poll()
+        ok = [r for r in res if r["status"] == 0]
+        bad = [r["status"] for r in res if r["status"] != 0]
+        lat = np.array([r["t_end"] - r["t_submit"] for r in ok]) if ok else np.zeros(1)
+        span = max(r["t_end"] for r in res) - min(r["t_submit"] for r in res)
+        return {"value": len(ok) / span, "latency_s": {"p50": float(np.percentile(lat, 50)),
+                                                       "p99": float(np.percentile(lat, 99))},
+                "completed": len(ok), "failed": {str(k): bad.count(k) for k in sorted(set(bad))}, "wall_s": wall,
+                "flops_total": float(sum(r["flops"] for r in ok)),
+                "energies": {int(r["id"]): r["energy"] for r in ok}}
+
+    mixed = args.precision == "mixed"
+    main = stream(1 if mixed else 0)
+    fp64 = stream(0) if mixed else None
+    cmp = None
+    if fp64:
+        common = set(main["energies"]) & set(fp64["energies"])
+        cmp = {"value": fp64["value"], "latency_s": fp64["latency_s"], "completed": fp64["completed"],
+               "failed": fp64["failed"],
+               "max_rel_dE_mixed_vs_fp64": max((abs(main["energies"][k] - fp64["energies"][k]) /
+                                                abs(fp64["energies"][k]) for k in common), default=None),
+               "mixed_over_fp64": main["value"] / fp64["value"] if fp64["value"] else None}
+    line = {"metric": "served DMRG solves/s (Ising mix)", "value": main["value"], "unit": "solves/s",
             "n_gpus": 1, "steps": n, "warmup": 0, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic request stream (numpy seed 4)",
+            "vs_baseline": None, "dtype": "c128/bf16x3" if mixed else "c128",
+            "data": "synthetic request stream (numpy seed 4)",
             "config": {"workload": "serving_ising_poisson", "requests": n, "rate_req_s": args.rate,
-                       "slots": args.batch, "hbm_budget_bytes": budget, "L": "U[16,256]", "D": "U{32,64,128,256}"},
-            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-            "completed": len(ok), "failed": {str(k): bad.count(k) for k in sorted(set(bad))}, "wall_s": wall,
-            "flops_total": float(sum(r["flops"] for r in ok))}
+                       "slots": args.batch, "hbm_budget_bytes": budget, "L": "U[16,256]", "D": "U{32,64,128,256}",
+                       "precision": "mixed" if mixed else "fp64"},
+            "latency_s": main["latency_s"], "completed": main["completed"], "failed": main["failed"],
+            "wall_s": main["wall_s"], "flops_total": main["flops_total"], "fp64_stream": cmp}
     print(json.dumps(line), flush=True)
 
 

@@ -272,6 +272,7 @@ typedef struct {
   double p0, p1, p2; /* Ising: J, g, h.  Schwinger: mu, x, alpha (l0 = 0) */
   uint64_t seed;     /* initial MPS: mpsgpu_mps_random_state(L, 2, D, seed) */
   double convtol;    /* 0 = 1e-10 */
+  int precision;     /* mpsgpu_options.precision: 0 FP64, 1 mixed */
 } mpsgpu_request;
 
 typedef struct {

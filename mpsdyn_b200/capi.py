@@ -479,7 +479,7 @@ def zgemm_split(ctx: "Context", A: np.ndarray, B: np.ndarray, repeats: int = 0):
 
 class Request(C.Structure):
     _fields_ = [("model", C.c_int), ("L", C.c_int), ("D", C.c_int), ("p0", C.c_double), ("p1", C.c_double),
-                ("p2", C.c_double), ("seed", C.c_uint64), ("convtol", C.c_double)]
+                ("p2", C.c_double), ("seed", C.c_uint64), ("convtol", C.c_double), ("precision", C.c_int)]
 
 
 class Result(C.Structure):
@@ -515,8 +515,8 @@ class Server:
         self.h = h
 
     def submit(self, model: int, L: int, D: int, p0: float, p1: float, p2: float, seed: int,
-               convtol: float = 1e-10) -> int:
-        r = Request(model, L, D, p0, p1, p2, seed, convtol)
+               convtol: float = 1e-10, precision: int = 0) -> int:
+        r = Request(model, L, D, p0, p1, p2, seed, convtol, precision)
         rid = C.c_uint64()
         st = self.lib.mpsgpu_server_submit(self.h, C.byref(r), C.byref(rid))
         if st != 0:
@@ -524,7 +524,7 @@ class Server:
         return rid.value
 
     def footprint(self, model: int, L: int, D: int) -> int:
-        r = Request(model, L, D, 0, 0, 0, 0, 0)
+        r = Request(model, L, D, 0, 0, 0, 0, 0, 0)
         return int(self.lib.mpsgpu_request_footprint(C.byref(r)))
 
     def poll(self) -> list:

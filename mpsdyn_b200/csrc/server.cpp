@@ -129,6 +129,7 @@ struct mpsgpu_server {
       mpsgpu_options opt;
       mpsgpu_default_options(&opt);
       opt.convtol = r.convtol > 0 ? r.convtol : 1e-10;
+      opt.precision = r.precision == 1 ? 1 : 0;
       opt.cancel_flag = &job.cancel;
       mpsgpu_stats stats{};
       double e = 0.0;
