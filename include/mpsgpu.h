@@ -341,6 +341,17 @@ mpsgpu_status mpsgpu_heff_matvec_grouped_ex(mpsgpu_context* ctx, int n, const mp
                                             int precision, int repeats, double* ms_per_run, double* flops,
                                             double* ms_prepare);
 
+/* Autotuner of the complex FP64 GEMM's launch configuration (tile edge
+ * 32 or 64, 1 to 16 K slices).  The first GEMM of each shape (M, N, K,
+ * batch, ops, epilogue) times every candidate on its own operands into a
+ * scratch output and the fastest is used from then on, for all contexts of
+ * the process; no tuning while a stream is captured into a graph.  On by
+ * default (MPSGPU_AUTOTUNE=0 in the environment turns it off before the
+ * first GEMM); results of different configurations differ only by the order
+ * of the K-slice sums.  entries = shapes tuned so far. */
+void mpsgpu_set_autotune(int on);
+long long mpsgpu_autotune_entries(void);
+
 /* Split-precision complex GEMM C = A B (column-major, complex interleaved,
  * host buffers; m x k times k x n) on the tcgen05 tensor cores: every FP64
  * real is split into three BF16 limbs and the limb products with combined

@@ -27,7 +27,7 @@ EXPORTS = [
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
     "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_ground_state_two_site", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_contract2", "mpsgpu_expectation_local", "mpsgpu_entropy",
-    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped", "mpsgpu_heff_matvec_grouped_ex", "mpsgpu_zgemm_split",
+    "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped", "mpsgpu_heff_matvec_grouped_ex", "mpsgpu_zgemm_split", "mpsgpu_set_autotune", "mpsgpu_autotune_entries",
     "mpsgpu_env_left", "mpsgpu_env_right",
     "mpsgpu_qr", "mpsgpu_lq", "mpsgpu_qr_device_noalloc",
     "mpsgpu_server_create", "mpsgpu_server_submit", "mpsgpu_server_poll", "mpsgpu_server_cancel",
@@ -453,6 +453,19 @@ def heff_matvec_grouped_ex(ctx: "Context", instances: list, precision: int = 0, 
     ctx._check(lib.mpsgpu_heff_matvec_grouped_ex(ctx.h, len(instances), arr, precision, repeats, C.byref(ms),
                                                  C.byref(fl), C.byref(mp)))
     return (ms.value if repeats > 0 else None), fl.value, mp.value
+
+
+def set_autotune(on: bool) -> None:
+    """mpsgpu_set_autotune: the FP64 GEMM autotuner on or off (process-wide)."""
+    lib = load()
+    lib.mpsgpu_set_autotune.argtypes = [C.c_int]
+    lib.mpsgpu_set_autotune(1 if on else 0)
+
+
+def autotune_entries() -> int:
+    lib = load()
+    lib.mpsgpu_autotune_entries.restype = C.c_longlong
+    return int(lib.mpsgpu_autotune_entries())
 
 
 def zgemm_split(ctx: "Context", A: np.ndarray, B: np.ndarray, repeats: int = 0):

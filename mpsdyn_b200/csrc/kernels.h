@@ -45,6 +45,10 @@ struct GemmArgs {
 
 // C = alpha op(A) op(B) + beta Cin  (complex FP64, DMMA tensor pipe)
 void zgemm(const Stream& st, const GemmArgs& g, Scratch& scratch);
+// Autotuner of zgemm's launch configuration (tile edge, K slices): on by
+// default (environment MPSGPU_AUTOTUNE=0 turns it off); entries = shapes tuned.
+void set_gemm_autotune(int on);
+long long gemm_autotune_entries();
 
 // One GEMM C = A B (op N, N) of a grouped launch; tile_begin / tiles_m are
 // filled by grouped_tiles (64 x 64 tiles).

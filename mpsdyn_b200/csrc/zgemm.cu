@@ -21,6 +21,12 @@
 // that also applies the epilogue (deterministic order).  A grouped variant
 // runs the tiles of many independent GEMMs (different shapes) in one
 // persistent launch.
+#include <atomic>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -275,6 +281,138 @@ void launch_tiles(const Stream& st, const GemmArgs& g, int splits, int kchunk, c
 
 }  // namespace
 
+namespace {
+
+// Launch configuration of one GEMM: tile edge (32: 4 warps, 64: 8 warps) and
+// the number of K slices.
+struct GemmCfg {
+  int tile = 32;
+  int splits = 1;
+};
+
+// Default when no measurement is available: 64x64 tiles when they already
+// fill the GPU, otherwise 32x32 plus a split over K.
+GemmCfg heuristic_cfg(const GemmArgs& g) {
+  const long long target = 2 * 148;
+  const long long ctas64 = (long long)ceil_div(g.M, 64) * ceil_div(g.N, 64) * g.batch;
+  GemmCfg c;
+  c.tile = ctas64 >= target ? 64 : 32;
+  const long long ctas = (long long)ceil_div(g.M, c.tile) * ceil_div(g.N, c.tile) * g.batch;
+  while (c.splits < 8 && ctas * c.splits * 2 <= target && g.K / (c.splits * 2) >= 4 * BK) c.splits *= 2;
+  return c;
+}
+
+void run_cfg(const Stream& st, const GemmArgs& g, GemmCfg c, Scratch& scratch) {
+  int splits = c.splits;
+  const int kchunk = splits > 1 ? ceil_div(ceil_div(g.K, splits), BK) * BK : g.K;
+  if (splits > 1) splits = ceil_div(g.K, kchunk);
+  cplx* partial = nullptr;
+  if (splits > 1) partial = (cplx*)scratch.get((size_t)splits * g.batch * (size_t)g.M * g.N * sizeof(cplx));
+  if (c.tile == 64) launch_tiles<64, 64, 2, 4>(st, g, splits, kchunk, partial);
+  else launch_tiles<32, 32, 2, 2>(st, g, splits, kchunk, partial);
+  if (splits > 1) {
+    const long long total = (long long)g.M * g.N * g.batch;
+    splitk_reduce_kernel<<<std::min<long long>(ceil_div(total, 256), 4096), 256, 0, st.s>>>(g, splits, partial);
+    after_launch(st);
+  }
+}
+
+// ---- autotuner ----------------------------------------------------------
+// The first GEMM of every shape (M, N, K, batch, ops, epilogue) times the
+// candidate configurations on its own operands, writing to a scratch output
+// (C is never written twice, so aliasing of C with Cin is harmless), and the
+// fastest is kept in a process-wide table that every later GEMM of that shape
+// uses.  Skipped while the stream is being captured into a graph.
+struct TuneKey {
+  int M, N, K, batch, opA, opB, cin;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(M, N, K, batch, opA, opB, cin) < std::tie(o.M, o.N, o.K, o.batch, o.opA, o.opB, o.cin);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, GemmCfg> g_tune;
+std::atomic<int> g_tune_mode{-1};  // -1: not read yet, 0: off, 1: on
+
+bool autotune_enabled() {
+  int m = g_tune_mode.load();
+  if (m < 0) {
+    const char* e = std::getenv("MPSGPU_AUTOTUNE");
+    m = (e && e[0] == '0') ? 0 : 1;
+    g_tune_mode.store(m);
+  }
+  return m == 1;
+}
+
+GemmCfg tune(const Stream& st, const GemmArgs& g, Scratch& scratch) {
+  std::vector<GemmCfg> cands;
+  for (int tile : {32, 64})
+    for (int sp : {1, 2, 4, 8, 16}) {
+      if (sp > 1 && g.K / sp < 2 * BK) continue;
+      cands.push_back(GemmCfg{tile, sp});
+    }
+  GemmArgs t = g;
+  const long long nel = (long long)(g.batch - 1) * g.strideC + g.ldc * (long long)g.N;
+  cplx* tmp = nullptr;
+  MPSGPU_CUDA(cudaMallocAsync((void**)&tmp, std::max<long long>(nel, 1) * sizeof(cplx), st.s));
+  t.C = tmp;
+  Stream quiet = st;
+  quiet.prof = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  GemmCfg best = heuristic_cfg(g);
+  float best_ms = 1e30f;
+  try {
+    MPSGPU_CUDA(cudaEventCreate(&e0));
+    MPSGPU_CUDA(cudaEventCreate(&e1));
+    for (const GemmCfg& c : cands) {
+      run_cfg(quiet, t, c, scratch);  // warm (instruction cache, scratch size)
+      MPSGPU_CUDA(cudaEventRecord(e0, st.s));
+      for (int r = 0; r < 3; r++) run_cfg(quiet, t, c, scratch);
+      MPSGPU_CUDA(cudaEventRecord(e1, st.s));
+      MPSGPU_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      MPSGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+  } catch (...) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFreeAsync(tmp, st.s);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  MPSGPU_CUDA(cudaFreeAsync(tmp, st.s));
+  return best;
+}
+
+GemmCfg choose_cfg(const Stream& st, const GemmArgs& g, Scratch& scratch) {
+  if (!autotune_enabled()) return heuristic_cfg(g);
+  const TuneKey key{g.M, g.N, g.K, g.batch, g.opA, g.opB, g.Cin != nullptr ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st.s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return heuristic_cfg(g);
+  const GemmCfg c = tune(st, g, scratch);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = c;
+  return c;
+}
+
+}  // namespace
+
+void set_gemm_autotune(int on) { g_tune_mode.store(on ? 1 : 0); }
+
+long long gemm_autotune_entries() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return (long long)g_tune.size();
+}
+
 void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
   GemmArgs g = g0;
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
@@ -287,32 +425,13 @@ void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
     after_launch(st);
     return;
   }
-  // Tile choice: 64x64 (8 warps) when that already fills the GPU, otherwise
-  // 32x32 (4 warps) plus a split over K.
-  const long long target = 2 * 148;
-  long long ctas64 = (long long)ceil_div(g.M, 64) * ceil_div(g.N, 64) * g.batch;
-  bool big = ctas64 >= target;
-  int BMs = big ? 64 : 32;
-  long long ctas = (long long)ceil_div(g.M, BMs) * ceil_div(g.N, BMs) * g.batch;
-  int splits = 1;
-  while (splits < 8 && ctas * splits * 2 <= target && g.K / (splits * 2) >= 4 * BK) splits *= 2;
-  int kchunk = splits > 1 ? ceil_div(ceil_div(g.K, splits), BK) * BK : g.K;
-  if (splits > 1) splits = ceil_div(g.K, kchunk);
-  cplx* partial = nullptr;
-  if (splits > 1)
-    partial = (cplx*)scratch.get((size_t)splits * g.batch * (size_t)g.M * g.N * sizeof(cplx));
+  const GemmCfg cfg = choose_cfg(st, g, scratch);
   const bool prof = st.prof && st.prof->sample();
   if (prof) {
     cudaEvent_t e0 = st.prof->next();
     if (e0) cudaEventRecord(e0, st.s);
   }
-  if (big) launch_tiles<64, 64, 2, 4>(st, g, splits, kchunk, partial);
-  else launch_tiles<32, 32, 2, 2>(st, g, splits, kchunk, partial);
-  if (splits > 1) {
-    long long total = (long long)g.M * g.N * g.batch;
-    splitk_reduce_kernel<<<std::min<long long>(ceil_div(total, 256), 4096), 256, 0, st.s>>>(g, splits, partial);
-    after_launch(st);
-  }
+  run_cfg(st, g, cfg, scratch);
   if (prof) {
     cudaEvent_t e1 = st.prof->next();
     if (e1) cudaEventRecord(e1, st.s);

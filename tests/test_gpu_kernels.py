@@ -91,3 +91,25 @@ def test_lq_matches_lapack(ctx, m, n):
     Lr, Qr = mo.lq_reduced(A)
     assert np.abs(Lm @ Q - A).max() < 1e-13 * np.abs(A).max() * max(m, n) ** 0.5
     assert rel(Lm, Lr) < 1e-11 and rel(Q, Qr) < 1e-11
+
+
+def test_gemm_autotuner_same_energy_on_and_off(ctx):
+    """The GEMM autotuner only changes launch configurations: the sweep
+    reaches the same energy with it off and on, and it records the shapes
+    it tuned."""
+    from mpsdyn_b200 import capi
+    from oracle import mps_oracle as mo
+    H = mo.ising_hmpo(12, 1, 0.9, 0.1)
+    m = ctx.mpo(H)
+    o = ctx.options(convtol=1e-10)
+    energies = []
+    try:
+        for on in (False, True):
+            capi.set_autotune(on)
+            s = ctx.mps(mo.random_mps(12, 2, 16, 21).sites)
+            e, _ = ctx.find_ground_state(m, 16, s, 0.0, o)
+            energies.append(e)
+    finally:
+        capi.set_autotune(True)
+    assert abs(energies[0] - energies[1]) <= 1e-10 * abs(energies[0])
+    assert capi.autotune_entries() > 0
