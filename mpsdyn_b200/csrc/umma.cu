@@ -40,7 +40,9 @@ namespace {
 constexpr int SP_BM = 128;       // rows of an A tile = TMEM lanes of the accumulator
 constexpr int SP_BK = 16;        // K of one BF16 MMA = one pipeline stage
 constexpr int SP_PLANES = 6;     // re h/m/l, im h/m/l
-constexpr int SP_STAGES = 4;
+constexpr int SP_STAGES = 4;      // ring depth of the 64- and 128-column tiles
+// stages of the ring for a column tile: 128 x 256 tiles (72 KB a stage) fit three
+__host__ __device__ constexpr int sp_stages(int bn) { return bn == 256 ? 3 : SP_STAGES; }
 constexpr int SP_THREADS = 128;
 constexpr int SP_GROUP_BN = 128;  // column tile of grouped launches
 constexpr unsigned long long SP_WAIT_NS = 2000000000ULL;
@@ -215,7 +217,8 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
   constexpr int A_STAGE = SP_PLANES * sp_plane_bytes(SP_BM);
   constexpr int B_STAGE = SP_PLANES * sp_plane_bytes(BN);
   constexpr int STAGE = A_STAGE + B_STAGE;
-  constexpr uint32_t TMEM_COLS = 2 * BN;  // Cr in [0, BN), Ci in [BN, 2 BN)
+  constexpr int STAGES = sp_stages(BN);
+  constexpr uint32_t TMEM_COLS = 2 * BN;  // Cr in [0, BN), Ci in [BN, 2 BN); 512 = all of TMEM at BN = 256
   extern __shared__ uint8_t smem_dyn[];
   __shared__ __align__(8) uint64_t full_bar[SP_STAGES];
   __shared__ __align__(8) uint64_t empty_bar[SP_STAGES];
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
   __shared__ uint32_t tmem_slot;
   __shared__ int aborted;
 
-  // 128-byte aligned ring of SP_STAGES stages (the launch adds 128 bytes of slack)
+  // 128-byte aligned ring of STAGES stages (the launch adds 128 bytes of slack)
   const uint32_t ring = (smem_u32(smem_dyn) + 127u) & ~127u;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int mt, nt, sp, k0, nk;
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
   }
 
   if (tid == 0) {
-    for (int s = 0; s < SP_STAGES; s++) {
+    for (int s = 0; s < STAGES; s++) {
       mbar_init(smem_u32(&full_bar[s]), 1);
       mbar_init(smem_u32(&empty_bar[s]), 1);
     }
@@ -287,21 +290,21 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
     const uint8_t* a_src = p.Ap + ((size_t)mt * p.KS + k0) * A_STAGE;
     const uint8_t* b_src = p.Bp + ((size_t)nt * p.KS + k0) * B_STAGE;
     auto load = [&](int t) {
-      const int buf = t % SP_STAGES;
+      const int buf = t % STAGES;
       const uint32_t bar = smem_u32(&full_bar[buf]);
       const uint32_t dst = ring + buf * STAGE;
       mbar_expect_tx(bar, STAGE);
       bulk_g2s(dst, a_src + (size_t)t * A_STAGE, A_STAGE, bar);
       bulk_g2s(dst + A_STAGE, b_src + (size_t)t * B_STAGE, B_STAGE, bar);
     };
-    int loaded = min(SP_STAGES, nk);
+    int loaded = min(STAGES, nk);
     for (int t = 0; t < loaded; t++) load(t);
     const uint32_t id_pos = mma_idesc(BN, false), id_neg = mma_idesc(BN, true);
     bool ok = true;
     int kt = 0;
     for (; kt < nk; ++kt) {
-      const int buf = kt % SP_STAGES;
-      if (!mbar_wait(smem_u32(&full_bar[buf]), (kt / SP_STAGES) & 1)) {
+      const int buf = kt % STAGES;
+      if (!mbar_wait(smem_u32(&full_bar[buf]), (kt / STAGES) & 1)) {
         ok = false;
         break;
       }
@@ -326,21 +329,21 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
       mma_commit(smem_u32(&empty_bar[buf]));
       // refill the stage the previous k-step used once its MMAs are done,
       // keeping this step's MMAs queued behind them
-      if (kt >= 1 && kt - 1 + SP_STAGES < nk) {
+      if (kt >= 1 && kt - 1 + STAGES < nk) {
         const int j = kt - 1;
-        if (!mbar_wait(smem_u32(&empty_bar[j % SP_STAGES]), (j / SP_STAGES) & 1)) {
+        if (!mbar_wait(smem_u32(&empty_bar[j % STAGES]), (j / STAGES) & 1)) {
           ok = false;
           ++kt;
           break;
         }
-        load(j + SP_STAGES);
-        loaded = j + SP_STAGES + 1;
+        load(j + STAGES);
+        loaded = j + STAGES + 1;
       }
     }
     if (!ok) {
       *(volatile int*)p.err = 1;
       aborted = 1;
-      for (int t = kt; t < loaded; t++) mbar_wait(smem_u32(&full_bar[t % SP_STAGES]), (t / SP_STAGES) & 1);
+      for (int t = kt; t < loaded; t++) mbar_wait(smem_u32(&full_bar[t % STAGES]), (t / STAGES) & 1);
     }
     mma_commit(smem_u32(&done_bar));
   }
@@ -403,7 +406,7 @@ __global__ void split_reduce_kernel(int M, int N, int splits, const cplx* __rest
 
 template <int BN>
 constexpr int split_smem_bytes() {
-  return SP_STAGES * (SP_PLANES * sp_plane_bytes(SP_BM) + SP_PLANES * sp_plane_bytes(BN)) + 128;
+  return sp_stages(BN) * (SP_PLANES * sp_plane_bytes(SP_BM) + SP_PLANES * sp_plane_bytes(BN)) + 128;
 }
 
 template <int BN, bool GROUPED>
@@ -472,7 +475,8 @@ long long split_operand_bytes(int rows, int K, int RT) {
 
 void split_prepare(const Stream& st, int rows, int K, const cplx* X, long long rs, long long ks, int RT,
                    uint8_t* out) {
-  MPSGPU_CHECK(rows > 0 && K > 0 && (RT == 64 || RT == 128), MPSGPU_INVALID, "split_prepare: bad shape");
+  MPSGPU_CHECK(rows > 0 && K > 0 && (RT == 64 || RT == 128 || RT == 256), MPSGPU_INVALID,
+               "split_prepare: bad shape");
   MPSGPU_CHECK(((uintptr_t)out & 15) == 0, MPSGPU_INVALID, "split_prepare: output not 16-byte aligned");
   const int KS = (K + SP_BK - 1) / SP_BK;
   const long long total = (long long)((rows + RT - 1) / RT) * KS * 2 * RT;
@@ -489,8 +493,10 @@ SplitPlan split_plan(int M, int N, int K, int nsm) {
   pl.K = K;
   pl.KS = (K + SP_BK - 1) / SP_BK;
   pl.mtiles = (M + SP_BM - 1) / SP_BM;
-  // 128-column tiles unless that leaves most SMs idle
-  pl.BN = (pl.mtiles * ((N + 127) / 128) >= nsm / 2) ? 128 : 64;
+  // 256-column tiles when they alone fill the SMs (half the A traffic and
+  // tile overhead per flop), 128 unless that leaves most SMs idle, else 64
+  if (pl.mtiles * ((N + 255) / 256) >= nsm) pl.BN = 256;
+  else pl.BN = (pl.mtiles * ((N + 127) / 128) >= nsm / 2) ? 128 : 64;
   pl.ntiles = (N + pl.BN - 1) / pl.BN;
   const int tiles = pl.mtiles * pl.ntiles;
   // split K over CTAs while tiles do not fill the SMs, keeping >= 4 k-steps each
@@ -523,7 +529,9 @@ void zgemm_split_prepared(const Stream& st, const SplitPlan& pl, const uint8_t* 
   p.err = err;
   const SplitGroupParams none{nullptr, 0, nullptr};
   const dim3 grid(pl.mtiles, pl.ntiles, pl.splits);
-  if (pl.BN == 128)
+  if (pl.BN == 256)
+    launch_split<256, false>(st, p, none, grid);
+  else if (pl.BN == 128)
     launch_split<128, false>(st, p, none, grid);
   else
     launch_split<64, false>(st, p, none, grid);

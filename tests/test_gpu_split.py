@@ -26,6 +26,7 @@ def _crandn(rng, *shape, scale=1.0):
     (256, 128, 640),    # last GEMM of the same matvec (split K)
     (1024, 1024, 1024), # 64 k-steps through the four-stage ring
     (1280, 1280, 256),  # 128-column tiles
+    (2048, 4096, 72),   # 128 x 256 tiles (enough of them to fill the SMs), ragged K
     (8, 3, 5),          # smaller than one tile
 ])
 def test_split_gemm_accuracy(ctx, m, n, k):
