@@ -469,6 +469,11 @@ static double mv_flops(int d, int w1, int w2, int dl, int dr) {
 // tolerance and energy-increase margin sit above the products' error.
 constexpr double kSplitSwitchTol = 1e-6;
 constexpr double kSplitEigTol = 1e-6;
+// The first FP64 half-sweep after the split phase cannot end the solve (it is
+// compared with a split-phase energy), so its site solves stop at a residual
+// of 1e-9: the energy error is quadratic in the residual, and the half-sweeps
+// that decide convergence run at the full tolerance.
+constexpr double kFirst64EigTol = 1e-9;
 constexpr double kSplitIncreaseTol = 1e-5;
 
 static int device_sms(Context& c) {
@@ -1145,7 +1150,7 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
                    split_phase ? &smv : nullptr);
       };
       int its = 0;
-      const double etol = split_phase ? std::max(tol, kSplitEigTol) : tol;
+      const double etol = split_phase ? std::max(tol, kSplitEigTol) : first64 ? std::max(tol, kFirst64EigTol) : tol;
       double theta = lanczos_lowest(c, N, apply, init.A[pos].p, etol, opt.max_krylov, &its, val + offset);
       cnt.site_solves++;
       if (split_phase && *c.hsplit_err)
@@ -1508,7 +1513,7 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
         cgemv_n_sub(c.st(), N, nk, U.p, N, dots, yout, 1.0);
       };
       int its = 0;
-      const double etol = split_phase ? std::max(tol, kSplitEigTol) : tol;
+      const double etol = split_phase ? std::max(tol, kSplitEigTol) : first64 ? std::max(tol, kFirst64EigTol) : tol;
       double theta = lanczos_lowest(c, N, apply, init.A[pos].p, etol, opt.max_krylov, &its, val + offset);
       cnt.site_solves++;
       if (split_phase && *c.hsplit_err)
