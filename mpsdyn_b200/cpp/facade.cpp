@@ -295,9 +295,10 @@ namespace {
 
 mpsgpu_context* ctx() { return Contractor::theContractor().context(); }
 
-mpsgpu_options options_from(double convtol, double eigtol, double excorthtol) {
+mpsgpu_options options_from(double convtol, double eigtol, double excorthtol, int precision = 0) {
   mpsgpu_options o;
   mpsgpu_default_options(&o);
+  o.precision = precision;
   o.convtol = convtol;
   o.eigtol = eigtol;
   o.excorthtol = excorthtol;
@@ -339,7 +340,7 @@ void Contractor::check(int status, const char* what) {
 
 void Contractor::findGroundState(const MPO& ops, int D, double* lambda, MPS& init, double offset, int, const std::string&,
                                  int, bool) {
-  const mpsgpu_options o = options_from(convtol, eigtol, excorthtol);
+  const mpsgpu_options o = options_from(convtol, eigtol, excorthtol, precision);
   check(mpsgpu_find_ground_state(context(), ops.device(), D, offset, &o, init.device(), lambda, nullptr),
         "findGroundState");
   init.changed();
@@ -349,7 +350,7 @@ void Contractor::findNextExcitedState(const MPO& ops, int D, const std::vector<M
                                       MPS& init, double offset, int, const std::string&, int, bool) {
   std::vector<const mpsgpu_mps*> lv;
   for (const MPS* m : levels) lv.push_back(m->device());
-  const mpsgpu_options o = options_from(convtol, eigtol, excorthtol);
+  const mpsgpu_options o = options_from(convtol, eigtol, excorthtol, precision);
   check(mpsgpu_find_next_excited_state(context(), ops.device(), D, lv.data(), (int)lv.size(), offset, &o,
                                        init.device(), lambdak, nullptr),
         "findNextExcitedState");

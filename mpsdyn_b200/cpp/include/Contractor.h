@@ -40,6 +40,12 @@ class Contractor {
   void setEigenSolver(EigenSolver solver_ = arpack) { solver = solver_; }
   double getConvTol() const { return convtol; }
   double getEigTol() const { return eigtol; }
+  // Extension without a counterpart in the reference: 0 = complex FP64
+  // throughout (default), 1 = mixed precision for findGroundState and
+  // findNextExcitedState (split-precision products on the tensor cores until
+  // the half-sweep energy settles, then FP64 to the convergence tolerance).
+  void setPrecision(int value) { precision = value; }
+  int getPrecision() const { return precision; }
 
   void findGroundState(const MPO& ops, int D, double* lambda, MPS& resultMPS, double offset = 0.,
                        int nrLocalEig = 1, const std::string& tmpfile = "", int freqSv = 200, bool useLM = false);
@@ -65,6 +71,7 @@ class Contractor {
   Contractor(const Contractor&) = delete;
   Contractor& operator=(const Contractor&) = delete;
   double svdtol = 1e-8, convtol = 1e-5, eigtol = 0., excorthtol = 0.;
+  int precision = 0;
   EigenSolver solver = primme;
   mpsgpu_context* ctx_ = nullptr;
 };

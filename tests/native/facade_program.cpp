@@ -96,6 +96,19 @@ int main(int argc, const char* argv[]) {
     out.push_back("\"trunc_norm\": " + num(real(contractor.contract(cut, cut))));
   }
 
+  // the same ground state in mixed precision (facade extension setPrecision)
+  {
+    IsingHamiltonian hamI(10, 2, 1., 1., 0.);
+    const MPO& hamil = hamI.getHMPO(0.);
+    MPS gs;
+    gs.importMPS(argv[1]);
+    double E0 = 0.;
+    contractor.setPrecision(1);
+    contractor.findGroundState(hamil, 8, &E0, gs);
+    contractor.setPrecision(0);
+    out.push_back("\"mixed_gs_E0\": " + num(E0));
+  }
+
   // Schwinger MPO built by the library: energy of the product state
   {
     SchwingerHamiltonian hs(16, 2.5, 100., 0., 0.);

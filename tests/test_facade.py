@@ -73,6 +73,7 @@ def test_facade_program_reproduces_reference(tmp_path, golden):
     res = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
     ref = golden["ising_L10_D8_seed0_E0"]
     assert abs(res["gs_E0"] - ref) <= 1e-10 * abs(ref)
+    assert abs(res["mixed_gs_E0"] - ref) <= 1e-10 * abs(ref)
     assert abs(res["gs_norm"] - 1.0) < 1e-12
     assert abs(res["gs_H"] - res["gs_E0"]) < 1e-9 * abs(ref)
     # the ground state is an eigenstate: <H^2> = E^2
