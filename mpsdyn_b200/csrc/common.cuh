@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -106,5 +107,20 @@ inline void after_launch(const Stream& st) {
 }
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// One-time set-up per device (kernel attributes live in each device's
+// context): true until mark_device_done has recorded the current device.
+// The set-up is idempotent, so threads that race on the first use all do it
+// before any of them records it, and a thread that sees the mark knows the
+// set-up is complete.
+inline bool device_needs_setup(const std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+  return (done.load() & (1ull << dev)) == 0;
+}
+inline void mark_device_done(std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) done.fetch_or(1ull << dev);
+}
 
 }  // namespace mpsgpu

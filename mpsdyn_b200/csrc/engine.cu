@@ -477,13 +477,9 @@ constexpr double kFirst64EigTol = 1e-9;
 constexpr double kSplitIncreaseTol = 1e-5;
 
 static int device_sms(Context& c) {
-  static int nsm = 0;
-  if (nsm == 0) {
-    int v = 148;
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess) v = 148;
-    nsm = v;
-  }
-  return nsm;
+  int v = 148;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess) v = 148;
+  return v;
 }
 
 static uint8_t* bytes_reserve(Context& c, DBuf& b, long long bytes) {

@@ -369,11 +369,11 @@ void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, lo
   p.T = (cplx*)ws;
   p.tau = p.T + (size_t)p.npanel * nb * nb;
   size_t smem = (size_t)m * nb * sizeof(cplx);
-  static bool attr_done = false;
-  if (!attr_done) {
+  static std::atomic<unsigned long long> attr_done{0};
+  if (device_needs_setup(attr_done)) {
     MPSGPU_CUDA(cudaFuncSetAttribute(qr_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     MPSGPU_CUDA(cudaFuncSetAttribute(qr_form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr_done = true;
+    mark_device_done(attr_done);
   }
   int dev = 0, nsm = 148, per_sm = 1;
   MPSGPU_CUDA(cudaGetDevice(&dev));

@@ -412,11 +412,11 @@ constexpr int split_smem_bytes() {
 template <int BN, bool GROUPED>
 void launch_split(const Stream& st, const SplitGemmParams& p, const SplitGroupParams& gp, dim3 grid) {
   constexpr int smem = split_smem_bytes<BN>();
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<unsigned long long> attr{0};
+  if (device_needs_setup(attr)) {
     MPSGPU_CUDA(cudaFuncSetAttribute(zgemm_split_kernel<BN, GROUPED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      smem));
-    attr = true;
+    mark_device_done(attr);
   }
   zgemm_split_kernel<BN, GROUPED><<<grid, SP_THREADS, smem, st.s>>>(p, gp);
   after_launch(st);

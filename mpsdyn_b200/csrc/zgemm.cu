@@ -318,15 +318,16 @@ void run_cfg(const Stream& st, const GemmArgs& g, GemmCfg c, Scratch& scratch) {
 }
 
 // ---- autotuner ----------------------------------------------------------
-// The first GEMM of every shape (M, N, K, batch, ops, epilogue) times the
+// The first GEMM of every shape (device, M, N, K, batch, ops, epilogue) times the
 // candidate configurations on its own operands, writing to a scratch output
 // (C is never written twice, so aliasing of C with Cin is harmless), and the
 // fastest is kept in a process-wide table that every later GEMM of that shape
 // uses.  Skipped while the stream is being captured into a graph.
 struct TuneKey {
-  int M, N, K, batch, opA, opB, cin;
+  int dev, M, N, K, batch, opA, opB, cin;
   bool operator<(const TuneKey& o) const {
-    return std::tie(M, N, K, batch, opA, opB, cin) < std::tie(o.M, o.N, o.K, o.batch, o.opA, o.opB, o.cin);
+    return std::tie(dev, M, N, K, batch, opA, opB, cin) <
+           std::tie(o.dev, o.M, o.N, o.K, o.batch, o.opA, o.opB, o.cin);
   }
 };
 std::mutex g_tune_mu;
@@ -390,7 +391,9 @@ GemmCfg tune(const Stream& st, const GemmArgs& g, Scratch& scratch) {
 
 GemmCfg choose_cfg(const Stream& st, const GemmArgs& g, Scratch& scratch) {
   if (!autotune_enabled()) return heuristic_cfg(g);
-  const TuneKey key{g.M, g.N, g.K, g.batch, g.opA, g.opB, g.Cin != nullptr ? 1 : 0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  const TuneKey key{dev, g.M, g.N, g.K, g.batch, g.opA, g.opB, g.Cin != nullptr ? 1 : 0};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
