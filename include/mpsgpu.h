@@ -132,6 +132,13 @@ mpsgpu_status mpsgpu_mpo_schwinger(mpsgpu_context* ctx, int N, double mu, double
 mpsgpu_status mpsgpu_mpo_heisenberg(mpsgpu_context* ctx, int L, double Jx, double Jy, double Jz,
                                     double hx, double hy, double hz, double offset,
                                     mpsgpu_mpo** out);
+/* BoseHubbardHamiltonian(L, N, t, U, Ntarget, penN, V).getHMPO()
+ * (models/cpp/BoseHubbardHamiltonian.cpp:7-17, 73-160): bosons with at most
+ * N per site (d = N + 1), H = -t sum (b+_i b_i+1 + h.c.) + U/2 sum n_i(n_i-1)
+ * + V sum n_i + penN (sum n_i - Ntarget)^2, MPO bond 5; t >= 0
+ * (MPSGPU_INVALID otherwise). */
+mpsgpu_status mpsgpu_mpo_bosehubbard(mpsgpu_context* ctx, int L, int N, double t, double U, int Ntarget,
+                                     double penN, double V, mpsgpu_mpo** out);
 
 /* ---- MPS (replaces MPS / Site storage, src/core/headers/MPS.h) ------------
  * dims[3k..3k+2] = (d, Dl, Dr) of site k; data[k] column-major complex128. */

@@ -22,7 +22,7 @@ EXPORTS = [
     "mpsgpu_default_options", "mpsgpu_create", "mpsgpu_destroy", "mpsgpu_status_string",
     "mpsgpu_last_error", "mpsgpu_launch_count", "mpsgpu_synchronize", "mpsgpu_get_stream",
     "mpsgpu_profile_begin", "mpsgpu_profile_end", "mpsgpu_mpo_upload",
-    "mpsgpu_mpo_free", "mpsgpu_mpo_info", "mpsgpu_mpo_download", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger", "mpsgpu_mpo_heisenberg",
+    "mpsgpu_mpo_free", "mpsgpu_mpo_info", "mpsgpu_mpo_download", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger", "mpsgpu_mpo_heisenberg", "mpsgpu_mpo_bosehubbard",
     "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_random_state", "mpsgpu_mps_product",
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
     "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_ground_state_two_site", "mpsgpu_find_next_excited_state",
@@ -101,6 +101,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         lib.mpsgpu_mpo_ising_evolution.argtypes = [P, C.c_int, D_, D_, D_, D_, C.c_int, C.POINTER(P)]
         lib.mpsgpu_mpo_schwinger.argtypes = [P, C.c_int, D_, D_, D_, D_, C.POINTER(P)]
         lib.mpsgpu_mpo_heisenberg.argtypes = [P, C.c_int, D_, D_, D_, D_, D_, D_, D_, C.POINTER(P)]
+        lib.mpsgpu_mpo_bosehubbard.argtypes = [P, C.c_int, C.c_int, D_, D_, C.c_int, D_, D_, C.POINTER(P)]
         _lib = lib
     return _lib
 
@@ -192,6 +193,12 @@ class Context:
                        hz: float = 0.0, offset: float = 0.0) -> "DeviceMPO":
         h_ = C.c_void_p()
         self._check(self.lib.mpsgpu_mpo_heisenberg(self.h, L, Jx, Jy, Jz, hx, hy, hz, offset, C.byref(h_)))
+        return DeviceMPO(self, h_, L)
+
+    def mpo_bosehubbard(self, L: int, N: int, t: float, U: float, Ntarget: int, penN: float,
+                        V: float = 0.0) -> "DeviceMPO":
+        h_ = C.c_void_p()
+        self._check(self.lib.mpsgpu_mpo_bosehubbard(self.h, L, N, t, U, Ntarget, penN, V, C.byref(h_)))
         return DeviceMPO(self, h_, L)
 
     def mps(self, sites: list, normfact: float = 1.0) -> "DeviceMPS":

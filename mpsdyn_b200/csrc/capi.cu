@@ -308,6 +308,11 @@ mpsgpu_status mpsgpu_mpo_heisenberg(mpsgpu_context* ctx, int L, double Jx, doubl
   return upload_host_mpo(ctx, [&] { return heisenberg_hmpo(L, Jx, Jy, Jz, hx, hy, hz, offset); }, out);
 }
 
+mpsgpu_status mpsgpu_mpo_bosehubbard(mpsgpu_context* ctx, int L, int N, double t, double U, int Ntarget,
+                                     double penN, double V, mpsgpu_mpo** out) {
+  return upload_host_mpo(ctx, [&] { return bosehubbard_hmpo(L, N, t, U, Ntarget, penN, V); }, out);
+}
+
 mpsgpu_status mpsgpu_mpo_free(mpsgpu_context* ctx, mpsgpu_mpo* mpo) {
   if (!ctx || !mpo) return MPSGPU_INVALID;
   mpo_free(ctx->c, mpo->m);

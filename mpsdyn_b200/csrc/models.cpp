@@ -235,4 +235,71 @@ HostMPO heisenberg_hmpo(int L, double Jx, double Jy, double Jz, double hx, doubl
   return m;
 }
 
+namespace {
+
+// W[s', l, s, r] = sum_op C[l, r, op] Z[op][s', s] for a physical dimension d
+// (Z[op] column-major d x d); the ops are summed in order, as the
+// reference's C * Z product does.
+std::vector<cd> contract_coeffs_d(const std::vector<cd>& C, int Dl, int Dr, int nops,
+                                  const std::vector<std::vector<cd>>& Z, int d) {
+  std::vector<cd> W((size_t)d * Dl * d * Dr, cd(0, 0));
+  for (int l = 0; l < Dl; l++)
+    for (int r = 0; r < Dr; r++)
+      for (int op = 0; op < nops; op++) {
+        const cd c = C[l + Dl * (r + Dr * op)];
+        if (c == cd(0, 0)) continue;
+        for (int sp = 0; sp < d; sp++)
+          for (int s = 0; s < d; s++) W[sp + d * (l + Dl * (s + d * r))] += c * Z[op][sp + d * s];
+      }
+  return W;
+}
+
+}  // namespace
+
+HostMPO bosehubbard_hmpo(int L, int N, double t, double U, int Ntarget, double penN, double V) {
+  if (L < 2) throw std::invalid_argument("bosehubbard_hmpo: L < 2");
+  if (N < 1) throw std::invalid_argument("bosehubbard_hmpo: N < 1");
+  if (!(t >= 0)) throw std::invalid_argument("bosehubbard_hmpo: t < 0");
+  const int d = N + 1;
+  // local operators (initZ): 1, n(n-1), b+, b, n, n^2; entry (i1, i2) = <i1|op|i2>
+  std::vector<std::vector<cd>> Z(6, std::vector<cd>((size_t)d * d, cd(0, 0)));
+  for (int i = 0; i < d; i++) {
+    Z[0][i + d * i] = 1.0;
+    Z[1][i + d * i] = (double)(i * (i - 1));
+    if (i > 0) Z[2][i + d * (i - 1)] = std::sqrt((double)i);
+    if (i < N) Z[3][i + d * (i + 1)] = std::sqrt((double)(i + 1));
+    Z[4][i + d * i] = (double)i;
+    Z[5][i + d * i] = (double)(i * i);
+  }
+  const double half_u = 0.5 * U;  // the reference keeps U/2
+  const cd hop(0.0, std::sqrt(t));  // i sqrt(t) on each side of a hop
+  const int D = 5;
+  HostMPO m;
+  for (int k = 0; k < L; k++) {
+    const int Dl = k == 0 ? 1 : D, Dr = k == L - 1 ? 1 : D;
+    std::vector<cd> C((size_t)Dl * Dr * 6, cd(0, 0));
+    auto at = [&](int l, int r, int op) -> cd& { return C[l + Dl * (r + Dr * op)]; };
+    if (k != L - 1) {
+      at(0, 0, 0) = 1.0;
+      at(0, 1, 2) = hop;
+      at(0, 2, 3) = hop;
+      at(0, 3, 4) = 2 * penN;  // first half of the 2 pen n_i n_j pair term
+    }
+    if (k != 0 && k != L - 1) at(3, 3, 0) = 1.0;
+    at(0, Dr - 1, 1) = half_u;
+    at(0, Dr - 1, 4) = V - 2 * Ntarget * penN;
+    at(0, Dr - 1, 5) = penN;
+    at(0, Dr - 1, 0) = penN * Ntarget * Ntarget / L;  // constant share of pen Ntarget^2
+    if (k != 0) {
+      at(1, Dr - 1, 3) = hop;
+      at(2, Dr - 1, 2) = hop;
+      at(3, Dr - 1, 4) = 1.0;
+      at(Dl - 1, Dr - 1, 0) = 1.0;
+    }
+    m.dims.push_back({d, Dl, d, Dr});
+    m.W.push_back(contract_coeffs_d(C, Dl, Dr, 6, Z, d));
+  }
+  return m;
+}
+
 }  // namespace mpsgpu

@@ -30,5 +30,11 @@ HostMPO schwinger_hmpo(int N, double mu, double x, double l0, double alpha, doub
 // + Jz SzSz) + sum (hx Sx + hy Sy + hz Sz) + offset, S = sigma / 2, bond 5.
 HostMPO heisenberg_hmpo(int L, double Jx, double Jy, double Jz, double hx, double hy, double hz,
                         double offset = 0.0);
+// BoseHubbardHamiltonian(L, N, t, U, Ntarget, penaltyN, V) and its initZ /
+// initHMPO (models/cpp/BoseHubbardHamiltonian.cpp:7-17, 73-160): occupation
+// cut at N (d = N + 1), H = -t sum (b+_i b_i+1 + h.c.) + U/2 sum n_i (n_i - 1)
+// + V sum n_i + penaltyN (sum n_i - Ntarget)^2, bond 5.  t >= 0 (the
+// reference's uniform-coupling form takes sqrt(t) on both sides of a hop).
+HostMPO bosehubbard_hmpo(int L, int N, double t, double U, int Ntarget, double penN, double V = 0.0);
 
 }  // namespace mpsgpu

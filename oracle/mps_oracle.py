@@ -270,6 +270,53 @@ def heisenberg_hmpo(L: int, Jx: float, Jy: float, Jz: float, hx: float = 0.0, hy
     return ops
 
 
+def bosehubbard_hmpo(L: int, N: int, t: float, U: float, Ntarget: int, penN: float, V: float = 0.0) -> list:
+    """BoseHubbardHamiltonian(L, N, t, U, Ntarget, penN, V) with initZ / initHMPO
+    (models/cpp/BoseHubbardHamiltonian.cpp:7-17, 73-160): occupations 0..N
+    (d = N + 1), H = -t sum (b+_k b_k+1 + h.c.) + U/2 sum n_k (n_k - 1)
+    + V sum n_k + penN (sum n_k - Ntarget)^2, MPO bond 5; the hop is split as
+    i sqrt(t) on either side (uniform-coupling form, t >= 0)."""
+    if t < 0:
+        raise ValueError("bosehubbard_hmpo: t < 0")
+    d = N + 1
+    Z = np.zeros((6, d, d), dtype=np.complex128)
+    for i in range(d):
+        Z[0, i, i] = 1.0
+        Z[1, i, i] = i * (i - 1)
+        if i > 0:
+            Z[2, i, i - 1] = math.sqrt(i)      # b+
+        if i < N:
+            Z[3, i, i + 1] = math.sqrt(i + 1)  # b
+        Z[4, i, i] = i
+        Z[5, i, i] = i * i
+    half_u = 0.5 * U
+    hop = 1j * math.sqrt(t)
+    D = 5
+    ops = []
+    for k in range(L):
+        Dl = 1 if k == 0 else D
+        Dr = 1 if k == L - 1 else D
+        C = np.zeros((Dl, Dr, 6), dtype=np.complex128)
+        if k != L - 1:
+            C[0, 0, 0] = 1.0
+            C[0, 1, 2] = hop
+            C[0, 2, 3] = hop
+            C[0, 3, 4] = 2 * penN
+        if k != 0 and k != L - 1:
+            C[3, 3, 0] = 1.0
+        C[0, Dr - 1, 1] = half_u
+        C[0, Dr - 1, 4] = V - 2 * Ntarget * penN
+        C[0, Dr - 1, 5] = penN
+        C[0, Dr - 1, 0] = penN * Ntarget * Ntarget / L
+        if k != 0:
+            C[1, Dr - 1, 3] = hop
+            C[2, Dr - 1, 2] = hop
+            C[3, Dr - 1, 4] = 1.0
+            C[Dl - 1, Dr - 1, 0] = 1.0
+        ops.append(_w_from_coeffs(C, Z))
+    return ops
+
+
 def _ising_u1(eps: complex, g: float, h: float) -> np.ndarray:
     """isingU1MPO (IsingHamiltonian.cpp:203-218): exp(eps (g sx + h sz))."""
     norm = math.sqrt(g * g + h * h)

@@ -47,6 +47,7 @@
 #include "IsingHamiltonian.h"
 #include "SchwingerHamiltonian.h"
 #include "HeisenbergHamiltonian.h"
+#include "BoseHubbardHamiltonian.h"
 #include "MPS.h"
 #include "MPO.h"
 #include "Operator.h"
@@ -96,8 +97,11 @@ struct Model {
   IsingHamiltonian* ising = nullptr;
   SchwingerHamiltonian* schw = nullptr;
   HeisenbergHamiltonian* heis = nullptr;
+  BoseHubbardHamiltonian* bh = nullptr;
   int L = 0;
-  const MPO& H() { return ising ? ising->getHMPO(0.) : heis ? heis->getHMPO() : schw->getHMPO(); }
+  const MPO& H() {
+    return ising ? ising->getHMPO(0.) : heis ? heis->getHMPO() : bh ? bh->getHMPO() : schw->getHMPO();
+  }
 };
 
 Model make_model(const char* spec) {
@@ -117,6 +121,11 @@ Model make_model(const char* spec) {
     m.heis = new HeisenbergHamiltonian(m.L, atof(p[2].c_str()), atof(p[3].c_str()), atof(p[4].c_str()),
                                        atof(p[5].c_str()), atof(p[6].c_str()), atof(p[7].c_str()), 2,
                                        atof(p[8].c_str()));
+  } else if (p[0] == "bh") {
+    // bh:L:N:t:U:Ntarget:penN:V  (BoseHubbardHamiltonian.cpp, uniform couplings, d = N + 1)
+    m.L = atoi(p[1].c_str());
+    m.bh = new BoseHubbardHamiltonian(m.L, atoi(p[2].c_str()), atof(p[3].c_str()), atof(p[4].c_str()),
+                                      atoi(p[5].c_str()), atof(p[6].c_str()), atof(p[7].c_str()));
   } else {
     cerr << "unknown model " << spec << endl;
     exit(3);

@@ -46,7 +46,8 @@ def main() -> None:
     # MPO builders (bit-exact targets)
     mpos = {}
     for name, spec in [("ising6", "ising:6:1:1:0.3"), ("schwinger6", "schwinger:6:2.5:100:0:0"),
-                       ("heis6", "heis:6:1:0.8:1.2:0.3:0.1:0.5:0.7")]:
+                       ("heis6", "heis:6:1:0.8:1.2:0.3:0.1:0.5:0.7"),
+                       ("bh6", "bh:6:2:1:2:3:0.25:0.5"), ("bh6x", "bh:6:3:0.7:1.3:4:0.3:0.15")]:
         run("mpo", spec, os.path.join(tmp, name + "_"))
         for k in range(6):
             mpos[f"{name}_{k}"] = mo.load_array(os.path.join(tmp, f"{name}_{k}.bin"))
@@ -89,9 +90,9 @@ def main() -> None:
     np.savez_compressed(os.path.join(HERE, "kernels.npz"), **ker)
 
     # Sweeps from seeded initial states (generator: oracle.mps_oracle.random_mps)
-    def gs(spec, L, D, seed, convtol=1e-10):
+    def gs(spec, L, D, seed, convtol=1e-10, d=2):
         fn = os.path.join(tmp, f"init_{seed}.mps")
-        mo.write_mps(fn, mo.random_mps(L, 2, D, seed))
+        mo.write_mps(fn, mo.random_mps(L, d, D, seed))
         return run("gs", spec, D, convtol, 0, fn, os.path.join(tmp, "out.mps"))["E0"]
 
     golden["ising_L10_D8_seed0_E0"] = gs("ising:10:1:1:0", 10, 8, 0)
@@ -101,6 +102,7 @@ def main() -> None:
     golden["schwinger_N16_D24_seed1_E0"] = gs(f"schwinger:16:{mu}:100:0:0", 16, 24, 1)
     golden["heisenberg_L10_D16_seed0_E0"] = gs("heis:10:1:1:1:0:0:0:0", 10, 16, 0)
     golden["xxz_L12_D20_fields_seed5_E0"] = gs("heis:12:1:0.7:1.3:0.2:0.1:0.4:0", 12, 20, 5)
+    golden["bosehubbard_L8_N2_D12_seed6_E0"] = gs("bh:8:2:1:2:4:1:0", 8, 12, 6, d=3)
 
     # Excited state (penalty L/2 = 5 is above the N=10 gap)
     f0 = os.path.join(tmp, "e0.mps")

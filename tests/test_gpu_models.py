@@ -25,3 +25,17 @@ def test_heisenberg_gs_matches_reference(ctx, golden, key, L, D, seed, params):
     e, _ = ctx.find_ground_state(ops, D, s, 0.0, ctx.options(convtol=1e-10))
     ref = golden[key]
     assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
+
+
+def test_bosehubbard_mpo_and_ground_state(ctx, golden, mpo_npz):
+    """Bose-Hubbard chain with up to two bosons per site (d = 3): the
+    library's MPO equals the reference's tensors and the sweep from the
+    seeded initial state reaches the reference's energy."""
+    ws = ctx.mpo_bosehubbard(6, 2, 1.0, 2.0, 3, 0.25, 0.5).download()
+    for k in range(6):
+        np.testing.assert_array_equal(ws[k], mpo_npz[f"bh6_{k}"])
+    ops = ctx.mpo_bosehubbard(8, 2, 1.0, 2.0, 4, 1.0, 0.0)
+    s = ctx.mps(mo.random_mps(8, 3, 12, 6).sites)
+    e, _ = ctx.find_ground_state(ops, 12, s, 0.0, ctx.options(convtol=1e-10))
+    ref = golden["bosehubbard_L8_N2_D12_seed6_E0"]
+    assert abs(e - ref) <= 1e-10 * abs(ref), (e, ref)
