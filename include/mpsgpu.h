@@ -61,11 +61,29 @@ typedef struct {
                         * ground-state sweep run in split precision (BF16
                         * limbs on the tensor cores) until the half-sweep
                         * energy change falls below 1e-6 relative, then in
-                        * FP64 to convtol (at least one full FP64 round) */
+                        * FP64 to convtol (at least one full FP64 round);
+                        * 2 = the schedule of 1 (its eigensolver tolerances
+                        * and phases) with FP64 products, which separates
+                        * what the schedule saves from what the tensor
+                        * cores save */
   int verbose;         /* 1 = one line per half-sweep on stdout */
   /* Optional: when *cancel_flag becomes non-zero (set by another host
    * thread), the sweep stops between two site steps with MPSGPU_CANCELLED. */
   const volatile int* cancel_flag;
+  /* Checkpoints (the reference's tmpfile / freqSv / maxTime arguments of
+   * findGroundState, Contractor.h:255-257, and findNextExcitedState,
+   * Contractor.h:309-314): when checkpoint_file is non-null the state is
+   * written there in the reference's binary MPS format (MPS::exportMPS).
+   * Ground state: at the end of a half-sweep that does not converge, when
+   * the half-sweep count is a multiple of checkpoint_every (0 = 200), as
+   * Contractor.cpp:1526-1530.  Excited state: at the end of every half-sweep
+   * when checkpoint_seconds <= 0, else once at least checkpoint_seconds of
+   * wall time have passed since the last save (the reference counts CPU
+   * time, Contractor.cpp:2868-2883).  Restart by importing the file
+   * (mpsgpu_mps_import) and calling the solver again. */
+  const char* checkpoint_file;
+  int checkpoint_every;
+  double checkpoint_seconds;
 } mpsgpu_options;
 
 /* Counters of one solve (host-side; the flop count is algorithmic). */
@@ -108,6 +126,11 @@ mpsgpu_status mpsgpu_profile_end(mpsgpu_context* ctx, double* gemm_ms, double* g
 mpsgpu_status mpsgpu_mpo_upload(mpsgpu_context* ctx, int L, const int* dims,
                                 const double* const* data, mpsgpu_mpo** out);
 mpsgpu_status mpsgpu_mpo_free(mpsgpu_context* ctx, mpsgpu_mpo* mpo);
+/* MPO::saveMPO / loadMPO (src/core/cpp/MPO.cpp:214-231, 291-312): the
+ * reference's binary MPO file (int length, then every operator as an
+ * mwArray: int rank, int dims[rank], column-major complex128 data). */
+mpsgpu_status mpsgpu_mpo_save(mpsgpu_context* ctx, const mpsgpu_mpo* mpo, const char* filename);
+mpsgpu_status mpsgpu_mpo_load(mpsgpu_context* ctx, const char* filename, mpsgpu_mpo** out);
 /* Length and dims[4k..4k+3] = (du, Dl, dd, Dr) of an uploaded MPO (either
  * output may be null), and its tensors back to host buffers (data[k] holds
  * du*Dl*dd*Dr complex128, column-major), as MPO::getOpData returns them. */
@@ -167,6 +190,11 @@ mpsgpu_status mpsgpu_mps_info(mpsgpu_context* ctx, const mpsgpu_mps* mps,
 mpsgpu_status mpsgpu_mps_download(mpsgpu_context* ctx, const mpsgpu_mps* mps,
                                   double* const* data);
 mpsgpu_status mpsgpu_mps_free(mpsgpu_context* ctx, mpsgpu_mps* mps);
+/* MPS::exportMPS / importMPS (src/core/cpp/MPS.cpp:442-509): the
+ * reference's binary MPS file (int length, int bond, double normfact, int
+ * gauge, then per site int pos and the site as an mwArray (d, Dl, Dr)). */
+mpsgpu_status mpsgpu_mps_export(mpsgpu_context* ctx, const mpsgpu_mps* mps, const char* filename);
+mpsgpu_status mpsgpu_mps_import(mpsgpu_context* ctx, const char* filename, mpsgpu_mps** out);
 /* MPS::gaugeCond(dir, normal=true) (src/core/cpp/MPS.cpp:306-364). */
 mpsgpu_status mpsgpu_mps_gauge(mpsgpu_context* ctx, mpsgpu_mps* mps, char dir);
 /* MPS::gaugeCond(dir, normalize, cutD) (src/core/cpp/MPS.cpp:306-364): QR
@@ -238,6 +266,19 @@ mpsgpu_status mpsgpu_optimize(mpsgpu_context* ctx, const mpsgpu_mpo* ops,
                               const mpsgpu_mps* orig, mpsgpu_mps* init, int D,
                               const mpsgpu_options* opt, double* errN,
                               double* errT, mpsgpu_stats* stats);
+/* Contractor::optimizeSum (Contractor.cpp:2332-2477): init becomes the best
+ * MPS of bond D approximating sum_k beta_k |kets[k]>; beta holds n complex
+ * coefficients as (re, im) pairs.  Convergence by opt->convtol on the
+ * distance, as optimize.  Replaces the reference's random perturbation of an
+ * init without overlap (:2395-2405) by MPSGPU_INVALID. */
+mpsgpu_status mpsgpu_optimize_sum(mpsgpu_context* ctx, int n, const mpsgpu_mps* const* kets,
+                                  const double* beta, mpsgpu_mps* init, int D,
+                                  const mpsgpu_options* opt, mpsgpu_stats* stats);
+/* Contractor::optimizeMPS (Contractor.cpp:2319-2329): optimizeSum of one ket
+ * with beta = 1; err (may be null) = <ket|ket> + <init|init> - 2 Re <init|ket>. */
+mpsgpu_status mpsgpu_optimize_mps(mpsgpu_context* ctx, const mpsgpu_mps* ket, mpsgpu_mps* init,
+                                  int D, const mpsgpu_options* opt, double* err,
+                                  mpsgpu_stats* stats);
 /* contract(ket, ops, bra) = <bra|ops|ket> (Contractor.cpp:528-556); ops may be
  * null for contract(ket, bra) (Contractor.cpp:467-499). */
 mpsgpu_status mpsgpu_contract(mpsgpu_context* ctx, const mpsgpu_mps* ket,
@@ -261,25 +302,49 @@ mpsgpu_status mpsgpu_schmidt_values(mpsgpu_context* ctx, const mpsgpu_mps* mps,
                                     int pos, double* values, int cap, int* n);
 
 /* ---- solve server (continuous batching of independent requests) ---------
- * Requests are ground-state solves of model chains.  The server owns
- * `slots` worker threads, each with its own context (CUDA stream); a request
- * starts when a slot is free and its HBM footprint fits in what the running
- * requests leave of `hbm_budget_bytes` (admission in arrival order), so
- * requests that arrive while others run are admitted as slots and memory
- * free up and their device work overlaps.  State (MPO, MPS, environments,
- * Lanczos basis) stays on the device for the whole solve. */
+ * Requests are ground-state solves of model chains or time evolutions of
+ * Ising chains.  The server owns `slots` worker threads, each with its own
+ * context (CUDA stream); a request starts when a slot is free and its HBM
+ * footprint fits in what the running requests leave of `hbm_budget_bytes`.
+ * Admission is first fit in arrival order: the oldest queued request that
+ * fits starts, so one large request does not hold free slots idle, and a
+ * request that has been passed over 32 times is admitted before any later
+ * one (no starvation).  Requests that arrive while others run are admitted
+ * as slots and memory free up, and their device work overlaps.  State (MPO,
+ * MPS, environments, Lanczos basis) stays on the device for the whole
+ * request; the final state can be written to a file. */
 typedef struct mpsgpu_server mpsgpu_server;
 
 typedef enum { MPSGPU_MODEL_ISING = 0, MPSGPU_MODEL_SCHWINGER = 1 } mpsgpu_model;
+typedef enum { MPSGPU_REQUEST_GROUND_STATE = 0, MPSGPU_REQUEST_TIME_EVOLUTION = 1 } mpsgpu_request_kind;
 
 typedef struct {
   int model;         /* mpsgpu_model */
   int L;             /* sites */
-  int D;             /* bond dimension */
+  int D;             /* bond dimension (the maximum for a time evolution) */
   double p0, p1, p2; /* Ising: J, g, h.  Schwinger: mu, x, alpha (l0 = 0) */
   uint64_t seed;     /* initial MPS: mpsgpu_mps_random_state(L, 2, D, seed) */
   double convtol;    /* 0 = 1e-10 */
   int precision;     /* mpsgpu_options.precision: 0 FP64, 1 mixed */
+  /* ---- fields below: zero-initialise for a ground-state request ---- */
+  int kind;          /* mpsgpu_request_kind */
+  /* Time evolution (Ising only): `steps` steps of the second-order Trotter
+   * MPO of IsingHamiltonian::getUMPO (IsingHamiltonian.cpp:131-148) with
+   * time step dt, imaginary time when imag != 0, each applied by
+   * Contractor::optimize at bond D (Contractor.cpp:77-278), starting from
+   * the product state |0...0> (seed unused).  After every step
+   * obs_sx[step] = <sigma_x> on site L/2 and obs_entropy[step] = the
+   * entropy of the bond L/2 when those caller-owned arrays (length steps)
+   * are non-null; they must stay valid until the result is polled.  The
+   * result's energy is <H> of the final state. */
+  int steps;
+  double dt;
+  int imag;
+  double* obs_sx;
+  double* obs_entropy;
+  /* Non-null: the final state is written there (reference binary MPS format,
+   * MPS::exportMPS) before the result is reported; copied at submission. */
+  const char* result_file;
 } mpsgpu_request;
 
 typedef struct {
@@ -403,9 +468,12 @@ mpsgpu_status mpsgpu_lq(mpsgpu_context* ctx, int m, int n, const double* A,
  *   stream: the cudaStream_t to run on (null = default stream); the call is
  *      asynchronous on it and returns after enqueueing.
  * Limit: m, n <= 640 and m*n <= 131072; larger sizes return MPSGPU_BAD_SHAPE.
- * Working memory is one fixed 2.1 MiB device array inside the library,
- * reserved on every GPU that loads it until the process exits.  The first
- * call on a device looks up that array's address (cudaGetSymbolAddress):
+ * Working memory is one fixed 2.1 MiB device array inside the library.  CUDA
+ * places it on a GPU when the library's code is first loaded there:
+ * mpsgpu_create does that for its device (so create a context on the GPU,
+ * while allocation is still allowed, before relying on this call); it is then
+ * held until the process exits.  The first call on a device also looks up the
+ * array's address (cudaGetSymbolAddress) unless a context did it already:
  * make that first call before any stream capture.  All calls share the
  * array, so calls that overlap on the GPU (different streams, or concurrent
  * host threads) race; serialise them on one stream. */

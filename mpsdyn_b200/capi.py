@@ -25,6 +25,8 @@ EXPORTS = [
     "mpsgpu_mpo_free", "mpsgpu_mpo_info", "mpsgpu_mpo_download", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger", "mpsgpu_mpo_heisenberg", "mpsgpu_mpo_bosehubbard",
     "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_random_state", "mpsgpu_mps_product",
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
+    "mpsgpu_mps_export", "mpsgpu_mps_import", "mpsgpu_mpo_save", "mpsgpu_mpo_load",
+    "mpsgpu_optimize_sum", "mpsgpu_optimize_mps",
     "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_ground_state_two_site", "mpsgpu_find_next_excited_state",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_contract2", "mpsgpu_expectation_local", "mpsgpu_entropy",
     "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped", "mpsgpu_heff_matvec_grouped_ex", "mpsgpu_zgemm_split", "mpsgpu_set_autotune", "mpsgpu_autotune_entries",
@@ -40,6 +42,7 @@ class Options(C.Structure):
         ("convtol", C.c_double), ("eigtol", C.c_double), ("excorthtol", C.c_double),
         ("max_rounds", C.c_int), ("max_krylov", C.c_int), ("precision", C.c_int),
         ("verbose", C.c_int), ("cancel_flag", C.c_void_p),
+        ("checkpoint_file", C.c_char_p), ("checkpoint_every", C.c_int), ("checkpoint_seconds", C.c_double),
     ]
 
 
@@ -102,6 +105,13 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         lib.mpsgpu_mpo_schwinger.argtypes = [P, C.c_int, D_, D_, D_, D_, C.POINTER(P)]
         lib.mpsgpu_mpo_heisenberg.argtypes = [P, C.c_int, D_, D_, D_, D_, D_, D_, D_, C.POINTER(P)]
         lib.mpsgpu_mpo_bosehubbard.argtypes = [P, C.c_int, C.c_int, D_, D_, C.c_int, D_, D_, C.POINTER(P)]
+        lib.mpsgpu_mps_import.argtypes = [P, C.c_char_p, C.POINTER(P)]
+        lib.mpsgpu_mps_export.argtypes = [P, P, C.c_char_p]
+        lib.mpsgpu_mpo_load.argtypes = [P, C.c_char_p, C.POINTER(P)]
+        lib.mpsgpu_mpo_save.argtypes = [P, P, C.c_char_p]
+        lib.mpsgpu_optimize_sum.argtypes = [P, C.c_int, P, P, P, C.c_int, C.POINTER(Options), C.POINTER(Stats)]
+        lib.mpsgpu_optimize_mps.argtypes = [P, P, P, C.c_int, C.POINTER(Options), C.POINTER(C.c_double),
+                                            C.POINTER(Stats)]
         _lib = lib
     return _lib
 
@@ -227,8 +237,34 @@ class Context:
 
     @staticmethod
     def options(convtol=1e-5, eigtol=0.0, excorthtol=0.0, max_rounds=1000, max_krylov=64,
-                precision=0, verbose=0) -> Options:
-        return Options(convtol, eigtol, excorthtol, max_rounds, max_krylov, precision, verbose)
+                precision=0, verbose=0, checkpoint_file=None, checkpoint_every=200,
+                checkpoint_seconds=0.0) -> Options:
+        o = Options(convtol, eigtol, excorthtol, max_rounds, max_krylov, precision, verbose)
+        if checkpoint_file:
+            o._ckpt = str(checkpoint_file).encode()  # kept alive with the struct
+            o.checkpoint_file = o._ckpt
+        o.checkpoint_every = checkpoint_every
+        o.checkpoint_seconds = checkpoint_seconds
+        return o
+
+    # ---- files in the reference's binary formats ----
+    def mps_import(self, filename: str) -> "DeviceMPS":
+        h = C.c_void_p()
+        self._check(self.lib.mpsgpu_mps_import(self.h, str(filename).encode(), C.byref(h)))
+        return DeviceMPS(self, h)
+
+    def mps_export(self, mps: "DeviceMPS", filename: str) -> None:
+        self._check(self.lib.mpsgpu_mps_export(self.h, mps.h, str(filename).encode()))
+
+    def mpo_load(self, filename: str) -> "DeviceMPO":
+        h = C.c_void_p()
+        self._check(self.lib.mpsgpu_mpo_load(self.h, str(filename).encode(), C.byref(h)))
+        L = C.c_int()
+        self._check(self.lib.mpsgpu_mpo_info(self.h, h, C.byref(L), None))
+        return DeviceMPO(self, h, L.value)
+
+    def mpo_save(self, mpo: "DeviceMPO", filename: str) -> None:
+        self._check(self.lib.mpsgpu_mpo_save(self.h, mpo.h, str(filename).encode()))
 
     # ---- Contractor ----
     def find_ground_state(self, ops: "DeviceMPO", D: int, init: "DeviceMPS", offset: float = 0.0,
@@ -267,6 +303,22 @@ class Context:
                                              C.byref(en) if want_err else None,
                                              C.byref(et) if want_err else None, C.byref(st)))
         return (en.value, et.value, st.as_dict()) if want_err else st.as_dict()
+
+    def optimize_sum(self, kets: list, beta: list, init: "DeviceMPS", D: int = 0, opts: Options = None) -> dict:
+        n = len(kets)
+        arr = (C.c_void_p * n)(*[k.h for k in kets])
+        b = np.array([[complex(x).real, complex(x).imag] for x in beta], dtype=np.float64).ravel()
+        st = Stats()
+        o = opts or self.options()
+        self._check(self.lib.mpsgpu_optimize_sum(self.h, n, arr, _ptr(b), init.h, D, C.byref(o), C.byref(st)))
+        return st.as_dict()
+
+    def optimize_mps(self, ket: "DeviceMPS", init: "DeviceMPS", D: int = 0, opts: Options = None):
+        err = C.c_double()
+        st = Stats()
+        o = opts or self.options()
+        self._check(self.lib.mpsgpu_optimize_mps(self.h, ket.h, init.h, D, C.byref(o), C.byref(err), C.byref(st)))
+        return err.value, st.as_dict()
 
     def contract(self, ket, ops, bra) -> complex:
         re, im = C.c_double(), C.c_double()
@@ -499,7 +551,12 @@ def zgemm_split(ctx: "Context", A: np.ndarray, B: np.ndarray, repeats: int = 0):
 
 class Request(C.Structure):
     _fields_ = [("model", C.c_int), ("L", C.c_int), ("D", C.c_int), ("p0", C.c_double), ("p1", C.c_double),
-                ("p2", C.c_double), ("seed", C.c_uint64), ("convtol", C.c_double), ("precision", C.c_int)]
+                ("p2", C.c_double), ("seed", C.c_uint64), ("convtol", C.c_double), ("precision", C.c_int),
+                ("kind", C.c_int), ("steps", C.c_int), ("dt", C.c_double), ("imag", C.c_int),
+                ("obs_sx", C.c_void_p), ("obs_entropy", C.c_void_p), ("result_file", C.c_char_p)]
+
+
+KIND_GROUND_STATE, KIND_TIME_EVOLUTION = 0, 1
 
 
 class Result(C.Structure):
@@ -528,6 +585,7 @@ class Server:
         self.lib.mpsgpu_server_destroy.argtypes = [P]
         self.lib.mpsgpu_request_footprint.argtypes = [C.POINTER(Request)]
         self.lib.mpsgpu_request_footprint.restype = C.c_longlong
+        self._keep = []
         h = P()
         st = self.lib.mpsgpu_server_create(device, slots, hbm_budget_bytes, C.byref(h))
         if st != 0:
@@ -535,16 +593,40 @@ class Server:
         self.h = h
 
     def submit(self, model: int, L: int, D: int, p0: float, p1: float, p2: float, seed: int,
-               convtol: float = 1e-10, precision: int = 0) -> int:
+               convtol: float = 1e-10, precision: int = 0, result_file: str = None) -> int:
+        """A ground-state request (mpsgpu_request, kind 0)."""
         r = Request(model, L, D, p0, p1, p2, seed, convtol, precision)
+        return self._submit(r, result_file)
+
+    def submit_evolution(self, L: int, D: int, J: float, g: float, h: float, steps: int, dt: float,
+                         imag: bool = False, convtol: float = 1e-10, observe: bool = True,
+                         result_file: str = None) -> tuple:
+        """A time-evolution request (kind 1) of the open Ising chain from
+        |0...0>; returns (id, sx, entropy): arrays (length steps) the server
+        fills with <sigma_x> at site L/2 and the entropy of bond L/2 after
+        every step."""
+        r = Request(MODEL_ISING, L, D, J, g, h, 0, convtol, 0)
+        r.kind = KIND_TIME_EVOLUTION
+        r.steps, r.dt, r.imag = steps, dt, int(bool(imag))
+        sx = np.full(steps, np.nan)
+        ent = np.full(steps, np.nan)
+        if observe:
+            r.obs_sx, r.obs_entropy = sx.ctypes.data, ent.ctypes.data
+            self._keep.append((sx, ent))  # the server writes into them until the result is polled
+        return self._submit(r, result_file), sx, ent
+
+    def _submit(self, r: Request, result_file) -> int:
+        if result_file:
+            r.result_file = str(result_file).encode()
         rid = C.c_uint64()
         st = self.lib.mpsgpu_server_submit(self.h, C.byref(r), C.byref(rid))
         if st != 0:
             raise MpsgpuError(st, "mpsgpu_server_submit")
         return rid.value
 
-    def footprint(self, model: int, L: int, D: int) -> int:
-        r = Request(model, L, D, 0, 0, 0, 0, 0, 0)
+    def footprint(self, model: int, L: int, D: int, precision: int = 0, kind: int = 0) -> int:
+        r = Request(model, L, D, 0, 0, 0, 0, 0, precision)
+        r.kind = kind
         return int(self.lib.mpsgpu_request_footprint(C.byref(r)))
 
     def poll(self) -> list:

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <iostream>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -338,22 +339,68 @@ void Contractor::check(int status, const char* what) {
 #endif
 }
 
-void Contractor::findGroundState(const MPO& ops, int D, double* lambda, MPS& init, double offset, int, const std::string&,
-                                 int, bool) {
-  const mpsgpu_options o = options_from(convtol, eigtol, excorthtol, precision);
+// nrLocalEig: the reference asks the local eigensolver for knr pairs and
+// keeps the lowest (U.resize to the first column, Contractor.cpp:1410-1416);
+// the library computes that pair directly, so the result does not depend on
+// knr.  useLM (target the largest-magnitude local eigenvalue) has no
+// counterpart in the library: the call warns once and targets the lowest.
+static void warn_use_lm(bool useLM, const char* where) {
+  static bool warned = false;
+  if (useLM && !warned) {
+    std::cerr << "WARNING: " << where << ": useLM is not supported by the GPU library; "
+              << "the lowest local eigenvalue (SR) is targeted" << std::endl;
+    warned = true;
+  }
+}
+
+void Contractor::findGroundState(const MPO& ops, int D, double* lambda, MPS& init, double offset, int,
+                                 const std::string& tmpfile, int freqSv, bool useLM) {
+  warn_use_lm(useLM, "findGroundState");
+  mpsgpu_options o = options_from(convtol, eigtol, excorthtol, precision);
+  if (!tmpfile.empty()) {
+    o.checkpoint_file = tmpfile.c_str();
+    o.checkpoint_every = freqSv > 0 ? freqSv : 200;
+  }
   check(mpsgpu_find_ground_state(context(), ops.device(), D, offset, &o, init.device(), lambda, nullptr),
         "findGroundState");
   init.changed();
 }
 
 void Contractor::findNextExcitedState(const MPO& ops, int D, const std::vector<MPS*>& levels, double* lambdak,
-                                      MPS& init, double offset, int, const std::string&, int, bool) {
+                                      MPS& init, double offset, int, const std::string& tmpfile, int maxTime,
+                                      bool useLM) {
+  warn_use_lm(useLM, "findNextExcitedState");
   std::vector<const mpsgpu_mps*> lv;
   for (const MPS* m : levels) lv.push_back(m->device());
-  const mpsgpu_options o = options_from(convtol, eigtol, excorthtol, precision);
+  mpsgpu_options o = options_from(convtol, eigtol, excorthtol, precision);
+  if (!tmpfile.empty()) {
+    o.checkpoint_file = tmpfile.c_str();
+    o.checkpoint_seconds = maxTime;
+  }
   check(mpsgpu_find_next_excited_state(context(), ops.device(), D, lv.data(), (int)lv.size(), offset, &o,
                                        init.device(), lambdak, nullptr),
         "findNextExcitedState");
+  init.changed();
+}
+
+void Contractor::optimizeSum(std::vector<const MPS*> kets, std::vector<complex_t> beta, MPS& init, int D) {
+  if (kets.empty() || kets.size() != beta.size()) check(MPSGPU_INVALID, "optimizeSum: kets and beta differ");
+  std::vector<const mpsgpu_mps*> ks;
+  std::vector<double> b;
+  for (size_t k = 0; k < kets.size(); k++) {
+    ks.push_back(kets[k]->device());
+    b.push_back(beta[k].re);
+    b.push_back(beta[k].im);
+  }
+  const mpsgpu_options o = options_from(convtol, eigtol, excorthtol);
+  check(mpsgpu_optimize_sum(context(), (int)ks.size(), ks.data(), b.data(), init.device(), D, &o, nullptr),
+        "optimizeSum");
+  init.changed();
+}
+
+void Contractor::optimizeMPS(const MPS& ket, MPS& init, int D, double* err) {
+  const mpsgpu_options o = options_from(convtol, eigtol, excorthtol);
+  check(mpsgpu_optimize_mps(context(), ket.device(), init.device(), D, &o, err, nullptr), "optimizeMPS");
   init.changed();
 }
 
@@ -498,6 +545,16 @@ void MPO::setFromDevice(mpsgpu_mpo* h) {
   initLength(L);
   for (int k = 0; k < L; k++) setOp(k, new Operator(host[k]), true);
   dev_ = h;  // after setOp, which drops any previous device copy
+}
+
+void MPO::saveMPO(const char* filename) const {
+  Contractor::check(mpsgpu_mpo_save(ctx(), device(), filename), "MPO::saveMPO");
+}
+
+void MPO::loadMPO(const char* filename) {
+  mpsgpu_mpo* h = nullptr;
+  Contractor::check(mpsgpu_mpo_load(ctx(), filename, &h), "MPO::loadMPO");
+  setFromDevice(h);
 }
 
 // ---------------------------------------------------------------------------

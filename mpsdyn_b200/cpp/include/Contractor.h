@@ -53,6 +53,9 @@ class Contractor {
                             MPS& init, double offset = 0., int nrLocalEig = 1, const std::string& tmpfile = "",
                             int maxTime = 0, bool useLM = false);
   void optimize(const MPO& ops, const MPS& ket, MPS& init, int D = 0, double* errN = 0, double* errT = 0);
+  // Contractor.h:133-140 of the reference
+  void optimizeSum(std::vector<const MPS*> kets, std::vector<complex_t> beta, MPS& init, int D = 0);
+  void optimizeMPS(const MPS& ket, MPS& init, int D = 0, double* err = 0);
 
   complex_t contract(const MPS& ket, const MPS& bra, char dir = 'L');
   complex_t contract(const MPS& ket, const MPO& ops, const MPS& bra);

@@ -27,6 +27,9 @@ class MPO {
   void setOp(int pos, const Operator* op, bool myop = false);
   // physical (output) dimension of every site
   const std::vector<int> getDimensions() const;
+  // binary MPO file of the reference (MPO.cpp:214-231, 291-312)
+  void saveMPO(const char* filename) const;
+  void loadMPO(const char* filename);
 
   // The device copy (uploaded on demand), for the Contractor and MPS.
   mpsgpu_mpo* device() const;

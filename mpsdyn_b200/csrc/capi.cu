@@ -55,6 +55,9 @@ SolveOptions to_opts(const mpsgpu_options* o) {
     s.verbose = o->verbose;
     s.precision = o->precision;
     s.cancel = o->cancel_flag;
+    if (o->checkpoint_file) s.checkpoint = o->checkpoint_file;
+    s.checkpoint_every = o->checkpoint_every > 0 ? o->checkpoint_every : 200;
+    s.checkpoint_seconds = o->checkpoint_seconds;
   }
   return s;
 }
@@ -111,6 +114,9 @@ void mpsgpu_default_options(mpsgpu_options* opt) {
   opt->max_krylov = 64;
   opt->precision = 0;
   opt->verbose = 0;
+  opt->checkpoint_file = nullptr;
+  opt->checkpoint_every = 200;  // freqSv default of findGroundState (Contractor.h:255-257)
+  opt->checkpoint_seconds = 0.0;
 }
 
 const char* mpsgpu_status_string(mpsgpu_status s) {
@@ -142,6 +148,12 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
     Context& c = ctx->c;
     c.device = device;
     MPSGPU_CUDA(cudaSetDevice(device));
+    // the no-allocation QR's fixed array is placed now, while allocation is
+    // still allowed, not at that entry point's first call
+    {
+      const mpsgpu_status ns = noalloc_qr_prepare(device);
+      MPSGPU_CHECK(ns == MPSGPU_OK, ns, "create: placing the no-allocation QR scratch failed");
+    }
     MPSGPU_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     c.scratch.stream = c.stream;
     c.qrws.stream = c.stream;
@@ -167,6 +179,9 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
     MPSGPU_CUDA(cudaHostAlloc((void**)&c.hsplit_err, sizeof(int), cudaHostAllocMapped));
     MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dsplit_err, c.hsplit_err, 0));
     *c.hsplit_err = 0;
+    MPSGPU_CUDA(cudaHostAlloc((void**)&c.hlz_err, sizeof(int), cudaHostAllocMapped));
+    MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dlz_err, c.hlz_err, 0));
+    *c.hlz_err = 0;
     MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 128 * sizeof(unsigned)));
     MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 128 * sizeof(unsigned)));
     MPSGPU_CUDA(cudaMemset(c.dsc, 0, sizeof(LanczosScalars)));
@@ -186,7 +201,7 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   Context& c = ctx->c;
   cudaSetDevice(c.device);
   for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lanV, &c.lanW, &c.lanT, &c.lanQ,
-                  &c.spX, &c.spT, &c.spPart})
+                  &c.lzws, &c.spX, &c.spT, &c.spPart})
     dbuf_free(c, *b);
   c.scratch.release();
   c.qrws.release();
@@ -204,6 +219,7 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   cudaFree(c.dsc);
   cudaFreeHost(c.hsc);
   if (c.hsplit_err) cudaFreeHost(c.hsplit_err);
+  if (c.hlz_err) cudaFreeHost(c.hlz_err);
   cudaFree(c.dcounter);
   if (c.stream) cudaStreamDestroy(c.stream);
   delete ctx;
@@ -361,6 +377,36 @@ mpsgpu_status mpsgpu_mps_upload(mpsgpu_context* ctx, int L, const int* dims, con
                                 double normfact, mpsgpu_mps** out) {
   if (!dims || !data) return MPSGPU_INVALID;
   return new_mps(ctx, out, [&](MpsDev& s) { mps_upload(ctx->c, s, L, dims, data, normfact); });
+}
+
+mpsgpu_status mpsgpu_mps_import(mpsgpu_context* ctx, const char* filename, mpsgpu_mps** out) {
+  if (!filename) return MPSGPU_INVALID;
+  return new_mps(ctx, out, [&](MpsDev& s) { mps_import_file(ctx->c, filename, s); });
+}
+
+mpsgpu_status mpsgpu_mps_export(mpsgpu_context* ctx, const mpsgpu_mps* mps, const char* filename) {
+  if (!ctx || !mps || !filename) return MPSGPU_INVALID;
+  return guarded(ctx, [&] { mps_export_file(ctx->c, mps->s, filename); });
+}
+
+mpsgpu_status mpsgpu_mpo_save(mpsgpu_context* ctx, const mpsgpu_mpo* mpo, const char* filename) {
+  if (!ctx || !mpo || !filename) return MPSGPU_INVALID;
+  return guarded(ctx, [&] { mpo_save_file(ctx->c, mpo->m, filename); });
+}
+
+mpsgpu_status mpsgpu_mpo_load(mpsgpu_context* ctx, const char* filename, mpsgpu_mpo** out) {
+  if (!ctx || !filename || !out) return MPSGPU_INVALID;
+  *out = nullptr;
+  auto* h = new (std::nothrow) mpsgpu_mpo();
+  if (!h) return MPSGPU_OOM;
+  mpsgpu_status st = guarded(ctx, [&] { mpo_load_file(ctx->c, filename, h->m); });
+  if (st != MPSGPU_OK) {
+    mpo_free(ctx->c, h->m);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return MPSGPU_OK;
 }
 
 mpsgpu_status mpsgpu_mps_random(mpsgpu_context* ctx, int L, int d, int D, uint64_t seed, mpsgpu_mps** out) {
@@ -538,6 +584,44 @@ mpsgpu_status mpsgpu_optimize(mpsgpu_context* ctx, const mpsgpu_mpo* ops, const 
   });
   fill_stats(stats, cnt, now_s() - t0);
   return st;
+}
+
+mpsgpu_status mpsgpu_optimize_sum(mpsgpu_context* ctx, int n, const mpsgpu_mps* const* kets, const double* beta,
+                                  mpsgpu_mps* init, int D, const mpsgpu_options* opt, mpsgpu_stats* stats) {
+  if (!ctx || n < 1 || !kets || !beta || !init) return MPSGPU_INVALID;
+  for (int k = 0; k < n; k++)
+    if (!kets[k]) return MPSGPU_INVALID;
+  Counters cnt;
+  double t0 = now_s();
+  mpsgpu_status st = guarded(ctx, [&] {
+    mpsgpu_options dflt;
+    mpsgpu_default_options(&dflt);
+    std::vector<const MpsDev*> ks(n);
+    std::vector<cplx> b(n);
+    for (int k = 0; k < n; k++) {
+      ks[k] = &kets[k]->s;
+      b[k] = make_double2(beta[2 * k], beta[2 * k + 1]);
+    }
+    optimize_sum(ctx->c, ks, b, init->s, D, to_opts(opt ? opt : &dflt), cnt);
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+  fill_stats(stats, cnt, now_s() - t0);
+  return st;
+}
+
+mpsgpu_status mpsgpu_optimize_mps(mpsgpu_context* ctx, const mpsgpu_mps* ket, mpsgpu_mps* init, int D,
+                                  const mpsgpu_options* opt, double* err, mpsgpu_stats* stats) {
+  if (!ctx || !ket || !init) return MPSGPU_INVALID;
+  const double one[2] = {1.0, 0.0};
+  const mpsgpu_mps* kets[1] = {ket};
+  mpsgpu_status st = mpsgpu_optimize_sum(ctx, 1, kets, one, init, D, opt, stats);
+  if (st != MPSGPU_OK || !err) return st;
+  return guarded(ctx, [&] {
+    const double n0 = contract(ctx->c, ket->s, nullptr, ket->s).x;
+    const double n1 = contract(ctx->c, init->s, nullptr, init->s).x;
+    const cplx ov = contract(ctx->c, init->s, nullptr, ket->s);
+    *err = n0 + n1 - 2.0 * ov.x;
+  });
 }
 
 mpsgpu_status mpsgpu_contract(mpsgpu_context* ctx, const mpsgpu_mps* ket, const mpsgpu_mpo* ops,

@@ -511,6 +511,35 @@ void split_matvec_prepare(Context& c, SplitMatvec& s, const cplx* Le, const std:
   s.ready = true;
 }
 
+// First contraction of the matvec: T2[a', s', r, c] = sum_{a,b,s} W[s',b,s,c]
+// L[a',b,a] X[a,s,r] with L (Dlb, w, Dlk), X (Dlk, d, Drk) in device layout
+// and T2 (Dlb, du, Drk, wr) (a' fastest), the operand of the last product.
+Gemm1wDesc heff_first_desc(const cplx* Le, int Dlb, int Dlk, int wl, const cplx* x, int dd, int Drk, const cplx* Wm,
+                           int du, int wr, cplx* t2) {
+  Gemm1wDesc d;
+  d.A = Le; d.lda = (long long)Dlb * wl;
+  d.B = x; d.ldb = Dlk;
+  d.X = Dlb; d.Y = Drk; d.K = Dlk;
+  d.n_i0 = wl; d.n_i1 = dd; d.n_o0 = du; d.n_o1 = wr;
+  d.Wm = Wm;
+  d.out = t2; d.ox = 1; d.oy = (long long)Dlb * du; d.so0 = Dlb; d.so1 = (long long)Dlb * du * Drk;
+  return d;
+}
+
+// Last contraction: Y[(a',s'), r'] = T2((Dlb du) x (Drk wr)) . Rt((Drk wr) x Drb) + offset X.
+Gemm3Desc heff_last_desc(const cplx* t2, int M, const cplx* Rt, int K, int Drb, cplx* y, const cplx* x,
+                         cplx offset) {
+  Gemm3Desc d;
+  d.M = M; d.N = Drb; d.K1 = K;
+  d.A1 = t2; d.lda1 = M;
+  d.B1 = Rt; d.ldb1 = K;
+  d.C = y; d.ldc = M;
+  if (offset.x != 0.0 || offset.y != 0.0) {
+    d.Cin = x; d.ldcin = M; d.beta = offset;
+  }
+  return d;
+}
+
 void split_matvec_release(Context& c, SplitMatvec& s) {
   dbuf_free(c, s.Lp);
   dbuf_free(c, s.Rp);
@@ -524,7 +553,28 @@ void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const 
   const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
   const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
   MPSGPU_CHECK(ld[1] == wl && rd[1] == wr, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
-  // step 1: T1[(a',b),(s,r)] = L((Dlb*wl) x Dlk) . X(Dlk x dd*Drk)
+  const bool split = sp && sp->ready;
+  if (!split) {
+    // FP64: steps 1 and 2 in one kernel (the MPO legs applied in the epilogue
+    // of L . X), step 3 with the offset in the epilogue
+    const cplx* Wm = adjoint ? m.Wlr_h[k].p : m.Wlr[k].p;
+    MPSGPU_CHECK(Wm != nullptr, MPSGPU_BAD_SHAPE, "heff: adjoint needs du == dd");
+    dbuf_reserve(c, c.t2, (long long)Dlb * du * Drk * wr);
+    Gemm1wBatch g1;
+    g1.n = 1;
+    g1.d[0] = heff_first_desc(Le, Dlb, Dlk, wl, x, dd, Drk, Wm, du, wr, c.t2.p);
+    heff_gemm1w(c.st(), g1);
+    Gemm3Batch g3;
+    g3.n = 1;
+    g3.d[0] = heff_last_desc(c.t2.p, Dlb * du, Rt, Drk * wr, Drb, y, x, offset);
+    heff_gemm3(c.st(), g3);
+    if (cnt) {
+      cnt->matvecs++;
+      cnt->flops += mv_flops(dd, wl, wr, Dlb, Drb);
+    }
+    return;
+  }
+  // split precision: step 1: T1[(a',b),(s,r)] = L((Dlb*wl) x Dlk) . X(Dlk x dd*Drk)
   const long long n1 = (long long)Dlb * wl * dd * Drk;
   dbuf_reserve(c, c.t1, n1);
   GemmArgs g;
@@ -533,15 +583,12 @@ void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const 
   g.B = x; g.ldb = Dlk;
   g.C = c.t1.p; g.ldc = (long long)Dlb * wl;
   // the caller prepared sp from the same Le and Rt (the adjoint ones for adjoint)
-  const bool split = sp && sp->ready;
-  if (split) {
+  {
     // X as the B operand: its columns (dd*Drk) are the prepared rows
     uint8_t* xp = reinterpret_cast<uint8_t*>(c.spX.p);
     split_prepare(c.st(), dd * Drk, Dlk, x, Dlk, 1, sp->p1.BN, xp);
     zgemm_split_prepared(c.st(), sp->p1, reinterpret_cast<const uint8_t*>(sp->Lp.p), xp, c.t1.p, g.ldc,
                          make_double2(1.0, 0.0), nullptr, 0, make_double2(0.0, 0.0), c.spPart.p, c.dsplit_err);
-  } else {
-    zgemm(c.st(), g, c.scratch);
   }
   // step 2: T2[a', s', r, c] = sum_{b,s} W[s',b,s,c] T1[a',b,s,r]
   const long long n2 = (long long)Dlb * du * Drk * wr;
@@ -564,18 +611,67 @@ void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const 
   if (offset.x != 0.0 || offset.y != 0.0) {
     h.Cin = x; h.ldcin = (long long)Dlb * du; h.beta = offset;
   }
-  if (split) {
+  {
     uint8_t* tp = reinterpret_cast<uint8_t*>(c.spT.p);
     split_prepare(c.st(), h.M, h.K, c.t2.p, 1, h.lda, 128, tp);
     zgemm_split_prepared(c.st(), sp->p3, tp, reinterpret_cast<const uint8_t*>(sp->Rp.p), y, h.ldc,
                          make_double2(1.0, 0.0), h.Cin, h.ldcin, h.beta, c.spPart.p, c.dsplit_err);
-  } else {
-    zgemm(c.st(), h, c.scratch);
   }
   if (cnt) {
     cnt->matvecs++;
-    if (split) cnt->split_matvecs++;
+    cnt->split_matvecs++;
     cnt->flops += mv_flops(dd, wl, wr, Dlb, Drb);
+  }
+}
+
+// Hermitian part of the effective Hamiltonian, TensorMultiplierHermitian
+// (TensorMultiplierHermitian.cpp:37-70): y = 1/2 (H x + H^dag x) + offset x,
+// with H^dag from the adjoint environments (Lh, Rth) and MPO legs.  FP64:
+// both first contractions in one grouped launch, the two last ones as one
+// product with the two sources concatenated along K.
+void heff_apply_hermitian(Context& c, const cplx* Le, const cplx* Lh, const std::array<int, 3>& ld,
+                          const MpoDev& m, int k, const cplx* Rt, const cplx* Rth, const std::array<int, 3>& rd,
+                          const cplx* x, cplx* y, cplx offset, Counters* cnt, const SplitMatvec* sp,
+                          const SplitMatvec* sph) {
+  const auto& wd = m.dims[k];
+  const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
+  const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
+  MPSGPU_CHECK(m.Wlr_h[k].p != nullptr, MPSGPU_BAD_SHAPE, "heff: adjoint needs du == dd");
+  if (sp && sp->ready) {
+    const long long N = (long long)Dlb * du * Drb;
+    dbuf_reserve(c, c.t4, N);
+    heff_apply(c, Le, ld, m, k, false, Rt, rd, x, y, make_double2(0.0, 0.0), cnt, sp);
+    heff_apply(c, Lh, ld, m, k, true, Rth, rd, x, c.t4.p, make_double2(0.0, 0.0), cnt, sph);
+    if (cnt) {
+      cnt->matvecs--;  // the pair counts as one product of the Hermitian multiplier
+      cnt->split_matvecs--;
+    }
+    zaxpby(c.st(), (int)N, make_double2(0.5, 0.0), c.t4.p, make_double2(0.5, 0.0), y);
+    if (offset.x != 0.0 || offset.y != 0.0) zaxpby(c.st(), (int)N, offset, x, make_double2(1.0, 0.0), y);
+    return;
+  }
+  MPSGPU_CHECK(ld[1] == wl && rd[1] == wr, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
+  const long long n2 = (long long)Dlb * du * Drk * wr;
+  dbuf_reserve(c, c.t2, n2);
+  dbuf_reserve(c, c.t3, n2);
+  Gemm1wBatch g1;
+  g1.n = 2;
+  g1.d[0] = heff_first_desc(Le, Dlb, Dlk, wl, x, dd, Drk, m.Wlr[k].p, du, wr, c.t2.p);
+  g1.d[1] = heff_first_desc(Lh, Dlb, Dlk, wl, x, dd, Drk, m.Wlr_h[k].p, du, wr, c.t3.p);
+  heff_gemm1w(c.st(), g1);
+  Gemm3Batch g3;
+  g3.n = 1;
+  g3.d[0] = heff_last_desc(c.t2.p, Dlb * du, Rt, Drk * wr, Drb, y, x, offset);
+  g3.d[0].K2 = Drk * wr;
+  g3.d[0].A2 = c.t3.p;
+  g3.d[0].lda2 = (long long)Dlb * du;
+  g3.d[0].B2 = Rth;
+  g3.d[0].ldb2 = (long long)Drk * wr;
+  g3.d[0].alpha = make_double2(0.5, 0.0);
+  heff_gemm3(c.st(), g3);
+  if (cnt) {
+    cnt->matvecs++;
+    cnt->flops += 2.0 * mv_flops(dd, wl, wr, Dlb, Drb);
   }
 }
 
@@ -588,27 +684,31 @@ void env_left_update(Context& c, const cplx* Le, const std::array<int, 3>& ld, c
   const int du = bd[0], Dlb = bd[1], Drb = bd[2];
   const int wl = m ? m->dims[k][1] : 1, wr = m ? m->dims[k][3] : 1;
   MPSGPU_CHECK(ld[0] == Dlb && ld[2] == Dlk && ld[1] == wl, MPSGPU_BAD_SHAPE, "envL: dims");
-  // T1 = L . X_ket  -> [a', b, s, r']
-  dbuf_reserve(c, c.t1, (long long)Dlb * wl * dd * Drk);
-  GemmArgs g;
-  g.M = Dlb * wl; g.N = dd * Drk; g.K = Dlk;
-  g.A = Le; g.lda = (long long)Dlb * wl;
-  g.B = ket.A[k].p; g.ldb = Dlk;
-  g.C = c.t1.p; g.ldc = (long long)Dlb * wl;
-  zgemm(c.st(), g, c.scratch);
-  const cplx* T2 = c.t1.p;
+  const cplx* T2 = nullptr;
   if (m) {
-    // T2[a', t, c, r'] = sum W[t,b,s,c] T1[a',b,s,r']
+    // T2[a', t, c, r'] = sum_{a,b,s} W[t,b,s,c] L[a',b,a] X_ket[a,s,r'] (one kernel)
     dbuf_reserve(c, c.t2, (long long)Dlb * du * wr * Drk);
-    WContractArgs wa;
-    wa.nx = Dlb; wa.ny = Drk;
-    wa.in = c.t1.p; wa.ix = 1; wa.iy = (long long)Dlb * wl * dd; wa.si0 = Dlb; wa.si1 = (long long)Dlb * wl;
-    wa.n_i0 = wl; wa.n_i1 = dd;
-    wa.out = c.t2.p; wa.ox = 1; wa.oy = (long long)Dlb * du * wr; wa.so0 = Dlb; wa.so1 = (long long)Dlb * du;
-    wa.n_o0 = du; wa.n_o1 = wr;
-    wa.Wm = m->Wlr[k].p;
-    wcontract(c.st(), wa);
+    Gemm1wBatch g1;
+    g1.n = 1;
+    Gemm1wDesc& d = g1.d[0];
+    d.A = Le; d.lda = (long long)Dlb * wl;
+    d.B = ket.A[k].p; d.ldb = Dlk;
+    d.X = Dlb; d.Y = Drk; d.K = Dlk;
+    d.n_i0 = wl; d.n_i1 = dd; d.n_o0 = du; d.n_o1 = wr;
+    d.Wm = m->Wlr[k].p;
+    d.out = c.t2.p; d.ox = 1; d.oy = (long long)Dlb * du * wr; d.so0 = Dlb; d.so1 = (long long)Dlb * du;
+    heff_gemm1w(c.st(), g1);
     T2 = c.t2.p;
+  } else {
+    // T1 = L . X_ket  -> [a', s, r'] (w = 1)
+    dbuf_reserve(c, c.t1, (long long)Dlb * wl * dd * Drk);
+    GemmArgs g;
+    g.M = Dlb * wl; g.N = dd * Drk; g.K = Dlk;
+    g.A = Le; g.lda = (long long)Dlb * wl;
+    g.B = ket.A[k].p; g.ldb = Dlk;
+    g.C = c.t1.p; g.ldc = (long long)Dlb * wl;
+    zgemm(c.st(), g, c.scratch);
+    T2 = c.t1.p;
   }
   // Lnew[r, (c, r')] = X_bra^H . T2
   od = {Drb, wr, Drk};
@@ -634,27 +734,31 @@ void env_right_update(Context& c, const cplx* Rt, const std::array<int, 3>& rd, 
   const int du = bd[0], Dlb = bd[1], Drb = bd[2];
   const int wl = m ? m->dims[k][1] : 1, wr = m ? m->dims[k][3] : 1;
   MPSGPU_CHECK(rd[0] == Drk && rd[2] == Drb && rd[1] == wr, MPSGPU_BAD_SHAPE, "envR: dims");
-  // T1[(l', s), (c, r)] = X_ket((Dlk*dd) x Drk) . Rt(Drk x (wr*Drb))
-  dbuf_reserve(c, c.t1, (long long)Dlk * dd * wr * Drb);
-  GemmArgs g;
-  g.M = Dlk * dd; g.N = wr * Drb; g.K = Drk;
-  g.A = ket.A[k].p; g.lda = (long long)Dlk * dd;
-  g.B = Rt; g.ldb = Drk;
-  g.C = c.t1.p; g.ldc = (long long)Dlk * dd;
-  zgemm(c.st(), g, c.scratch);
-  const cplx* T2 = c.t1.p;
+  const cplx* T2 = nullptr;
   if (m) {
-    // T2[l', b, t, r] = sum_{s,c} W[t,b,s,c] T1[l', s, c, r]
+    // T2[l', b, t, r] = sum_{s,c,r''} W[t,b,s,c] X_ket[l',s,r''] Rt[r'',c,r] (one kernel)
     dbuf_reserve(c, c.t2, (long long)Dlk * wl * du * Drb);
-    WContractArgs wa;
-    wa.nx = Dlk; wa.ny = Drb;
-    wa.in = c.t1.p; wa.ix = 1; wa.iy = (long long)Dlk * dd * wr; wa.si0 = Dlk; wa.si1 = (long long)Dlk * dd;
-    wa.n_i0 = dd; wa.n_i1 = wr;
-    wa.out = c.t2.p; wa.ox = 1; wa.oy = (long long)Dlk * wl * du; wa.so0 = Dlk; wa.so1 = (long long)Dlk * wl;
-    wa.n_o0 = wl; wa.n_o1 = du;
-    wa.Wm = m->Wrl[k].p;
-    wcontract(c.st(), wa);
+    Gemm1wBatch g1;
+    g1.n = 1;
+    Gemm1wDesc& d = g1.d[0];
+    d.A = ket.A[k].p; d.lda = (long long)Dlk * dd;
+    d.B = Rt; d.ldb = Drk;
+    d.X = Dlk; d.Y = Drb; d.K = Drk;
+    d.n_i0 = dd; d.n_i1 = wr; d.n_o0 = wl; d.n_o1 = du;
+    d.Wm = m->Wrl[k].p;
+    d.out = c.t2.p; d.ox = 1; d.oy = (long long)Dlk * wl * du; d.so0 = Dlk; d.so1 = (long long)Dlk * wl;
+    heff_gemm1w(c.st(), g1);
     T2 = c.t2.p;
+  } else {
+    // T1[(l', s), r] = X_ket((Dlk*dd) x Drk) . Rt(Drk x Drb)  (w = 1)
+    dbuf_reserve(c, c.t1, (long long)Dlk * dd * wr * Drb);
+    GemmArgs g;
+    g.M = Dlk * dd; g.N = wr * Drb; g.K = Drk;
+    g.A = ket.A[k].p; g.lda = (long long)Dlk * dd;
+    g.B = Rt; g.ldb = Drk;
+    g.C = c.t1.p; g.ldc = (long long)Dlk * dd;
+    zgemm(c.st(), g, c.scratch);
+    T2 = c.t1.p;
   }
   // Rt_new[(l', b), l] = T2((Dlk*wl) x (du*Drb)) . X_bra^H  (X_bra as Dlb x (du*Drb))
   od = {Dlk, wl, Dlb};
@@ -781,15 +885,21 @@ cplx contract2(Context& c, const MpoDev& ops, const MpsDev& ket, const MpsDev& b
 // ---------------------------------------------------------------------------
 // Lanczos for the lowest eigenpair (replaces the PRIMME call of
 // Contractor::solveEigs, Contractor.cpp:3067-3138; and its dense branch).
-// Restarted Lanczos with full reorthogonalisation (lanczos.cu), FP64;
-// convergence ||r|| <= tol * max|Ritz|.  apply(x, y, sigma) must compute
-// y = (H - sigma) x; sigma follows the latest Ritz value (shift0 before the
-// first one is known), which keeps the Gram-Schmidt passes well conditioned.
+// Thick-restarted Lanczos with full reorthogonalisation, FP64; convergence
+// ||r|| <= tol * max|Ritz|.  apply(x, y, sigma) must compute y = (H - sigma) x
+// (the products of the excited-state multiplier without its projector);
+// sigma follows the latest Ritz value (shift0 before the first one is
+// known), which keeps the Gram-Schmidt passes well conditioned.  With nu > 0,
+// U (N x nu) holds the projector vectors with the square roots of the
+// penalties folded in, and the step adds U (U^H v_j) to every product
+// (TensorMultiplierProjMulti.cpp:81-90).  Each iteration is the product (two
+// launches in FP64) and one cooperative launch of the Lanczos step
+// (lzstep.cu), which writes alpha_j, beta_j into mapped host memory.
 // ---------------------------------------------------------------------------
 
 template <class Op>
-static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, int max_krylov,
-                             int* iters, double shift0) {
+static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, int max_krylov, int* iters,
+                             double shift0, const cplx* U = nullptr, int nu = 0) {
   const int m = std::min(N, std::max(2, std::min(max_krylov, 200)));
   dbuf_reserve(c, c.lanV, (long long)N * (m + 1));
   dbuf_reserve(c, c.lanW, N);
@@ -797,8 +907,28 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
   cplx* w = c.lanW.p;
   const Stream st = c.st();
   double* d_tmp = c.dscal + 512;
-  cplx* h1 = c.dcplx;
-  cplx* h2 = c.dcplx + 256;
+  // workspace of the step: partial dots (nrb x 256), two partial-norm
+  // arrays (nrb), the coefficients h, h2 (256 each)
+  const long long nrb = ceil_div(N, lanczos_step_rows_per_block());
+  dbuf_reserve(c, c.lzws, nrb * 256 + 512 + nrb + 8);
+  LzBatch b;
+  b.ninst = 1;
+  b.part = c.lzws.p;
+  b.h = c.lzws.p + nrb * 256;
+  b.h2 = b.h + 256;
+  b.pn1 = reinterpret_cast<double*>(b.h2 + 256);
+  b.pn2 = b.pn1 + nrb;
+  b.bar = c.dcounter + 96;
+  b.err = c.dlz_err;
+  LzInst& in = b.in[0];
+  in.n = N;
+  in.V = V;
+  in.ldv = N;
+  in.w = w;
+  in.U = U;
+  in.nu = nu;
+  in.sc = c.dsc;
+  in.mirror = c.hsc_dev;
   // v0 = x / ||x||
   dznrm2(st, N, x, d_tmp, c.scratch);
   MPSGPU_CUDA(cudaMemcpyAsync(c.hscal, d_tmp, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -808,22 +938,35 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
     dznrm2(st, N, x, d_tmp, c.scratch);
   }
   zscal_inv(st, N, x, d_tmp, V);
-  std::vector<double> a, b, s;
-  double theta = 0.0;
+  std::vector<double> a, b2v, s;
+  double theta = 0.0, step_hint = 0.0;
+  bool have_theta = false;
   double sigma = std::isfinite(shift0) ? shift0 : 0.0;
   int total = 0;
   TridiagLowest tri;
-  // Iteration j: matvec, fused reorthogonalisation (which also writes
-  // alpha_j, beta_j into mapped pinned memory), event.  The host enqueues iteration
+  // Iteration j: product, Lanczos step, event.  The host enqueues iteration
   // j+1 before it waits for j, so the convergence test (tridiagonal
-  // eigenpair on the host) overlaps the device work; a speculative iteration
-  // after convergence is discarded (it only writes V[:, j+2] and w).
+  // eigenpair on the host) overlaps the device work; a speculative
+  // iteration after convergence is discarded (it only writes V[:, j+2], w
+  // and the coefficients of step j+1).
   auto enqueue = [&](int j) {
     apply(V + (long long)j * N, w, sigma);
-    lanczos_orthonormalize(st, N, j, V, N, w, j + 1 < m, sigma, c.dsc, c.hsc_dev, h1, h2, c.dcounter,
-                           c.scratch);
+    in.j = j;
+    in.k = j + 1;
+    in.sigma = sigma;
+    in.write_next = j + 1 < m ? 1 : 0;
+    lanczos_step(st, b);
     MPSGPU_CUDA(cudaEventRecord(c.iter_ev[j], c.stream));
     total++;
+  };
+  auto check_step = [&]() {
+    if (*c.hlz_err) {
+      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+      MPSGPU_CUDA(cudaMemsetAsync(b.bar, 0, 2 * sizeof(unsigned), c.stream));
+      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+      *c.hlz_err = 0;
+      throw Error(MPSGPU_TIMEOUT, "lanczos: a bounded grid barrier of the Lanczos step ran out");
+    }
   };
   // Ritz vector of the current tridiagonal (k x k) into x, normalised
   auto ritz_vector = [&](int k) {
@@ -832,11 +975,12 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
     dznrm2(st, N, x, d_tmp, c.scratch);
     zscal_inv(st, N, x, d_tmp, x);
     MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    check_step();
     if (iters) *iters = total;
   };
   // Thick-restarted Lanczos: after m steps the factorisation is compressed
   // to about m/2 vectors spanning the lowest Ritz vectors, in tridiagonal
-  // form (ThickRestart), so the fused reorthogonalisation continues
+  // form (ThickRestart), so the reorthogonalised recurrence continues
   // unchanged from index r.  Keeping many Ritz vectors preserves the
   // convergence of the lowest pair when it is nearly degenerate, where a
   // one-vector restart stalls.
@@ -852,13 +996,20 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
     for (int j = j0; j < m; j++) {
       if (j + 1 < m) enqueue(j + 1);
       MPSGPU_CUDA(cudaEventSynchronize(c.iter_ev[j]));
+      check_step();
       const double alpha = c.hsc->alpha[j];
       const double beta = c.hsc->beta[j];
       MPSGPU_CHECK(std::isfinite(alpha) && std::isfinite(beta), MPSGPU_NAN, "lanczos: non-finite value");
       a.push_back(alpha);
-      b.push_back(beta);
+      b2v.push_back(beta);
       double normT = 0.0;
-      tri.solve(a, b, (int)a.size(), theta, s, normT);
+      const double th_old = theta;
+      if (have_theta)
+        tri.solve_from(a, b2v, (int)a.size(), th_old, 4.0 * step_hint, theta, s, normT);
+      else
+        tri.solve(a, b2v, (int)a.size(), theta, s, normT);
+      step_hint = have_theta ? std::fabs(th_old - theta) : 0.0;
+      have_theta = true;
       sigma = theta;
       const double res = beta * std::fabs(s[j]);
       const double scale = std::max(normT, std::fabs(theta));
@@ -872,14 +1023,14 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
       ritz_vector(m);
       zcopy(st, N, x, V);
       a.clear();
-      b.clear();
+      b2v.clear();
       j0 = 0;
       continue;
     }
     // compress: V[:, 0..r) <- V G; V[:, r] = f / |f| with f = w, the
     // orthogonalised (not normalised) residual of step m-1
-    const double fnorm = b[m - 1];
-    const int r = thick.compress(a, b, m, keep, fnorm, gq);
+    const double fnorm = b2v[m - 1];
+    const int r = thick.compress(a, b2v, m, keep, fnorm, gq);
     gqc.resize(gq.size());
     for (size_t i = 0; i < gq.size(); i++) gqc[i] = make_double2(gq[i], 0.0);
     dbuf_reserve(c, c.lanQ, (long long)gqc.size());
@@ -894,15 +1045,15 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
     zgemm(st, g, c.scratch);
     MPSGPU_CUDA(cudaMemcpyAsync(V, c.lanT.p, (size_t)N * r * sizeof(cplx), cudaMemcpyDeviceToDevice, c.stream));
     double normT = 0.0;
-    tri.solve(a, b, r, theta, s, normT);
+    tri.solve(a, b2v, r, theta, s, normT);
     const double scale = std::max(normT, std::fabs(theta));
-    if (b[r - 1] * std::fabs(s[r - 1]) <= tol * scale || b[r - 1] <= 1e-14 * scale) {
+    if (b2v[r - 1] * std::fabs(s[r - 1]) <= tol * scale || b2v[r - 1] <= 1e-14 * scale) {
       ritz_vector(r);  // converged within the kept space
       return theta;
     }
     zscal_inv(st, N, w, &c.dsc->beta[m - 1], V + (long long)r * N);  // beta[m-1] = |f| on the device
     // the coupling of V[:, r-1] to the new V[:, r], used by the next step
-    MPSGPU_CUDA(cudaMemcpyAsync(&c.dsc->beta[r - 1], &b[r - 1], sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    MPSGPU_CUDA(cudaMemcpyAsync(&c.dsc->beta[r - 1], &b2v[r - 1], sizeof(double), cudaMemcpyHostToDevice, c.stream));
     sigma = theta;
     j0 = r;
   }
@@ -1124,7 +1275,10 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
   // split phase carry the products' error (about 1e-7 relative), so its
   // eigensolver tolerance and energy-increase margin are set at that level,
   // and the first FP64 round is not tested for an increase.
-  bool split_phase = (opt.precision == 1);
+  // precision 2: the same schedule of tolerances with FP64 products (to
+  // separate what the schedule saves from what the tensor cores save)
+  bool split_phase = (opt.precision == 1 || opt.precision == 2);
+  const bool split_products = (opt.precision == 1);
   bool first64 = false;
   SplitMatvec smv;
   if (split_phase) *c.hsplit_err = 0;
@@ -1140,10 +1294,10 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
       auto ld = E.ldims[pos];
       auto rd = E.rdims[pos];
       smv.ready = false;
-      if (split_phase) split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
+      if (split_phase && split_products) split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
       auto apply = [&](const cplx* xin, cplx* yout, double sg) {
         heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(off.x - sg, off.y), &cnt,
-                   split_phase ? &smv : nullptr);
+                   split_phase && split_products ? &smv : nullptr);
       };
       int its = 0;
       const double etol = split_phase ? std::max(tol, kSplitEigTol) : first64 ? std::max(tol, kFirst64EigTol) : tol;
@@ -1187,6 +1341,9 @@ double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, dou
         }
         right = !right;
         round++;
+        // intermediate result every checkpoint_every half-sweeps (Contractor.cpp:1526-1530)
+        if (!done && !opt.checkpoint.empty() && round % std::max(1, opt.checkpoint_every) == 0)
+          mps_export_file(c, init, opt.checkpoint);
       } else {
         pos += right ? 1 : -1;
       }
@@ -1399,6 +1556,7 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
                                         const SolveOptions& opt, Counters& cnt) {
   const int L = ops.L;
   const int nk = (int)levels.size();
+  MPSGPU_CHECK(nk <= LZ_MAXU, MPSGPU_BAD_SHAPE, "findNextExcitedState: at most 8 computed levels");
   prepare_init(c, init, D);
   double energy = contract(c, init, &ops, init).x + offset;
   for (int k = 0; k < nk; k++) {
@@ -1418,10 +1576,12 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
   // mixed precision as in find_ground_state: split-precision products of
   // both halves of the Hermitian multiplier until the half-sweep energy
   // settles, then FP64 (at least one full round)
-  bool split_phase = (opt.precision == 1);
+  bool split_phase = (opt.precision == 1 || opt.precision == 2);
+  const bool split_products = (opt.precision == 1);
   bool first64 = false;
   SplitMatvec smv, smvh;
   if (split_phase) *c.hsplit_err = 0;
+  auto last_saved = std::chrono::steady_clock::now();
   auto cleanup = [&]() {
     E.release(c);
     for (auto& n : NC) n.release(c);
@@ -1487,30 +1647,23 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
         g2.alpha = make_double2(std::sqrt(pens[k]), 0.0);
         zgemm(c.st(), g2, c.scratch);
       }
-      dbuf_reserve(c, y2, N);
-      cplx* dots = c.dcplx + 512;
       const cplx* Le = E.Le[pos].p;
       const cplx* Rt = E.Re[pos].p;
       smv.ready = smvh.ready = false;
-      if (split_phase) {
+      if (split_phase && split_products) {
         split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
         split_matvec_prepare(c, smvh, Lh.p, ld, ops, pos, Rth.p, rd);
       }
+      // 1/2 (H + H^dag) x + (offset - sigma) x; the projector term
+      // sum_k pen_k u_k (u_k^H x) is added by the Lanczos step
       auto apply = [&](const cplx* xin, cplx* yout, double sg) {
-        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(0.0, 0.0), &cnt,
-                   split_phase ? &smv : nullptr);
-        heff_apply(c, Lh.p, ld, ops, pos, true, Rth.p, rd, xin, y2.p, make_double2(0.0, 0.0), &cnt,
-                   split_phase ? &smvh : nullptr);
-        cnt.matvecs--;  // the pair counts as one product of the Hermitian multiplier
-        if (split_phase) cnt.split_matvecs--;
-        zaxpby(c.st(), N, make_double2(0.5, 0.0), y2.p, make_double2(0.5, 0.0), yout);
-        if (offset - sg != 0.0) zaxpby(c.st(), N, make_double2(offset - sg, 0.0), xin, make_double2(1.0, 0.0), yout);
-        cgemv_c(c.st(), N, nk, U.p, N, xin, dots, c.scratch);
-        cgemv_n_sub(c.st(), N, nk, U.p, N, dots, yout, 1.0);
+        heff_apply_hermitian(c, Le, Lh.p, ld, ops, pos, Rt, Rth.p, rd, xin, yout, make_double2(offset - sg, 0.0),
+                             &cnt, split_phase && split_products ? &smv : nullptr,
+                             split_phase && split_products ? &smvh : nullptr);
       };
       int its = 0;
       const double etol = split_phase ? std::max(tol, kSplitEigTol) : first64 ? std::max(tol, kFirst64EigTol) : tol;
-      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, etol, opt.max_krylov, &its, val + offset);
+      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, etol, opt.max_krylov, &its, val + offset, U.p, nk);
       cnt.site_solves++;
       if (split_phase && *c.hsplit_err)
         throw Error(MPSGPU_TIMEOUT, "findNextExcitedState: a bounded wait in the tensor-core kernel ran out");
@@ -1524,6 +1677,16 @@ static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, co
       for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
       for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
       const bool at_end = (right && pos == L - 1) || (!right && pos == 0);
+      if (at_end && !opt.checkpoint.empty()) {
+        // save at the end of every half-sweep, or every checkpoint_seconds
+        // (Contractor.cpp:2868-2883)
+        const auto now = std::chrono::steady_clock::now();
+        if (opt.checkpoint_seconds <= 0.0 ||
+            std::chrono::duration<double>(now - last_saved).count() >= opt.checkpoint_seconds) {
+          mps_export_file(c, init, opt.checkpoint);
+          last_saved = now;
+        }
+      }
       if (at_end) {
         const double change = std::fabs(energy - val);
         const bool was_split = split_phase;
@@ -1707,6 +1870,139 @@ void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, i
     *errN = norm0 + norm1 - 2.0 * cross.x;
     if (errT) *errT = norm0;
   }
+}
+
+// ---------------------------------------------------------------------------
+// optimizeSum (Contractor.cpp:2332-2477): |init> ~ sum_k beta_k |ket_k> at
+// bond D, by the same sweep as optimize with w = 1 environments between
+// every ket and init (calculateL0 / calculateR0, :2272-2297) and the local
+// vector M = sum_k normfact_k beta_k L0_k ket_k R0_k (contractMketId,
+// :860-878).  The site becomes M / normfact(init) (solveSiteGauge and the
+// rescaling after it, :921-936, :2418-2420); the last site of a half-sweep
+// keeps the norm in normfact (gaugeCond(pos, dir, true)).  Convergence as in
+// optimize, with |M| as the norm of the target.  The initial distance is
+// distanceVectors (:2302-2316), including its |beta|^2 term written there as
+// re*re + im + im, so that the first convergence test sees the same value.
+// ---------------------------------------------------------------------------
+
+void optimize_sum(Context& c, const std::vector<const MpsDev*>& kets, const std::vector<cplx>& beta, MpsDev& init,
+                  int D, const SolveOptions& opt, Counters& cnt) {
+  const int nt = (int)kets.size();
+  MPSGPU_CHECK(nt >= 1 && (int)beta.size() == nt, MPSGPU_INVALID, "optimizeSum: kets and coefficients differ");
+  const int L = kets[0]->L;
+  for (auto* k : kets) MPSGPU_CHECK(k->L == L, MPSGPU_BAD_SHAPE, "optimizeSum: kets of different lengths");
+  MPSGPU_CHECK(init.L == L, MPSGPU_BAD_SHAPE, "optimizeSum: init length");
+  prepare_init(c, init, D);
+  std::vector<EnvCache> E(nt);
+  for (auto& e : E) e.init(c, L);
+  // distanceVectors
+  double distance;
+  {
+    cplx sum = make_double2(0.0, 0.0);
+    double sumNorms = 0.0;
+    for (int k = 0; k < nt; k++) {
+      sum = cadd(sum, cmul(beta[k], contract(c, *kets[k], nullptr, init)));
+      const double modBeta = beta[k].x * beta[k].x + beta[k].y + beta[k].y;
+      sumNorms += modBeta * contract(c, *kets[k], nullptr, *kets[k]).x;
+    }
+    distance = contract(c, init, nullptr, init).x - 2.0 * sum.x + sumNorms;
+  }
+  bool right = true, done = false;
+  int pos = 0, round = 1;
+  DBuf M, T;
+  auto cleanup = [&]() {
+    for (auto& e : E) e.release(c);
+    dbuf_free(c, M);
+    dbuf_free(c, T);
+  };
+  try {
+    while (!done) {
+      opt.check_cancel();
+      long long nM = 0;
+      std::array<int, 3> md = {0, 0, 0};
+      for (int k = 0; k < nt; k++) {
+        calc_left(c, E[k], pos, nullptr, *kets[k], init, &cnt);
+        calc_right(c, E[k], pos, nullptr, *kets[k], init, &cnt);
+        const auto kd = kets[k]->dims[pos];
+        const auto ld = E[k].ldims[pos];  // (Dinit_l, 1, Dket_l)
+        const auto rd = E[k].rdims[pos];  // (Dket_r, 1, Dinit_r)
+        MPSGPU_CHECK(ld[2] == kd[1] && rd[0] == kd[2], MPSGPU_BAD_SHAPE, "optimizeSum: dims");
+        const std::array<int, 3> mk = {kd[0], ld[0], rd[2]};
+        if (k == 0) {
+          md = mk;
+          nM = nel(md);
+          dbuf_reserve(c, M, nM);
+        } else {
+          MPSGPU_CHECK(mk == md, MPSGPU_BAD_SHAPE, "optimizeSum: kets disagree on the site shape");
+        }
+        // T[(a', s), r] = L0 (Dli x Dlk) . X_k (Dlk x d Drk)
+        dbuf_reserve(c, T, (long long)ld[0] * kd[0] * kd[2]);
+        GemmArgs g;
+        g.M = ld[0]; g.N = kd[0] * kd[2]; g.K = kd[1];
+        g.A = E[k].Le[pos].p; g.lda = ld[0];
+        g.B = kets[k]->A[pos].p; g.ldb = kd[1];
+        g.C = T.p; g.ldc = ld[0];
+        zgemm(c.st(), g, c.scratch);
+        // M (+)= normfact_k beta_k T (Dli d x Drk) . Rt0 (Drk x Dri)
+        GemmArgs h;
+        h.M = ld[0] * kd[0]; h.N = rd[2]; h.K = kd[2];
+        h.A = T.p; h.lda = (long long)ld[0] * kd[0];
+        h.B = E[k].Re[pos].p; h.ldb = kd[2];
+        h.C = M.p; h.ldc = (long long)ld[0] * kd[0];
+        h.alpha = cscale(beta[k], kets[k]->normfact);
+        if (k > 0) {
+          h.Cin = M.p; h.ldcin = h.ldc; h.beta = make_double2(1.0, 0.0);
+        }
+        zgemm(c.st(), h, c.scratch);
+      }
+      // |M| and the new site M / normfact(init)
+      double* dn = c.dscal + 600;
+      dznrm2(c.st(), (int)nM, M.p, dn, c.scratch);
+      MPSGPU_CUDA(cudaMemcpyAsync(c.hscal, dn, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+      const double normM = c.hscal[0];
+      if (pos == 0 && round == 1 && normM == 0.0)
+        throw Error(MPSGPU_INVALID,
+                    "optimizeSum: the initial state has no overlap with the target (the reference perturbs it "
+                    "randomly here)");
+      init.dims[pos] = md;
+      dbuf_reserve(c, init.A[pos], nM);
+      zaxpby(c.st(), (int)nM, make_double2(1.0 / init.normfact, 0.0), M.p, make_double2(0.0, 0.0),
+             init.A[pos].p);
+      const bool at_end = (right && pos == L - 1) || (!right && pos == 0);
+      mps_gauge_site(c, init, pos, right ? 'R' : 'L', at_end, &cnt);
+      for (int k = 0; k < nt; k++) {
+        for (int l = pos + 1; l < L; l++) E[k].outofdate_l(l);
+        for (int l = pos - 1; l >= 0; l--) E[k].outofdate_r(l);
+      }
+      if (at_end) {
+        // contr1 = <A|A>, contr2 = <A|M> with the gauged site
+        const auto nd = init.dims[pos];
+        MPSGPU_CHECK(nel(nd) == nM, MPSGPU_BAD_SHAPE, "optimizeSum: edge site changed shape");
+        cgemv_c(c.st(), (int)nM, 1, init.A[pos].p, nM, init.A[pos].p, c.dcplx + 700, c.scratch);
+        cgemv_c(c.st(), (int)nM, 1, init.A[pos].p, nM, M.p, c.dcplx + 701, c.scratch);
+        MPSGPU_CUDA(cudaMemcpyAsync(c.hcplx, c.dcplx + 700, 2 * sizeof(cplx), cudaMemcpyDeviceToHost, c.stream));
+        MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+        done = check_distance(distance, c.hcplx[0], c.hcplx[1], init.normfact, normM, opt.convtol);
+        if (opt.verbose) printf("mpsgpu: optimizeSum round %d distance %.17g\n", round, distance);
+        if (!done) {
+          if (right) { mps_gauge_site(c, init, pos, 'L', false, &cnt); pos--; }
+          else { mps_gauge_site(c, init, pos, 'R', false, &cnt); pos++; }
+          right = !right;
+          round++;
+          if (round >= opt.max_rounds) throw Error(MPSGPU_NOT_CONVERGED, "optimizeSum: round limit reached");
+        }
+      } else {
+        pos += right ? 1 : -1;
+      }
+    }
+  } catch (...) {
+    cleanup();
+    throw;
+  }
+  cleanup();
+  init.bond = init.max_bond();
+  cnt.rounds += round;
 }
 
 // ---------------------------------------------------------------------------

@@ -55,6 +55,9 @@ struct Context {
   DBuf t1, t2, t3, t4, matA, matQ, matR;
   DBuf lanV, lanW;     // Lanczos basis and work vector
   DBuf lanT, lanQ;     // thick restart: V G product and the restart matrix G
+  DBuf lzws;           // workspace of the fused Lanczos step (partial dots and norms)
+  int* hlz_err = nullptr;  // pinned, mapped: set when a grid barrier of the Lanczos step ran out
+  int* dlz_err = nullptr;  // its device address
   // split-precision matvec: prepared x and T2 (BF16 limb planes) and split-K partials
   DBuf spX, spT, spPart;
   int* hsplit_err = nullptr;   // pinned, mapped: set by a tensor-core kernel whose bounded wait ran out
@@ -118,8 +121,12 @@ struct SolveOptions {
   // (MPSGPU_CANCELLED); nothing is in flight on the device when it returns.
   const volatile int* cancel = nullptr;
   void check_cancel() const {
-    if (cancel && *cancel) throw Error(MPSGPU_CANCELLED, "solve cancelled");
+    if (cancel && __atomic_load_n(cancel, __ATOMIC_ACQUIRE)) throw Error(MPSGPU_CANCELLED, "solve cancelled");
   }
+  // checkpoints (tmpfile, freqSv, maxTime of the reference)
+  std::string checkpoint;
+  int checkpoint_every = 200;
+  double checkpoint_seconds = 0.0;
 };
 
 // ---- building blocks (device layout) ----
@@ -155,6 +162,17 @@ void split_matvec_release(Context& c, SplitMatvec& s);
 void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpoDev& m, int k,
                 bool adjoint, const cplx* Rt, const std::array<int, 3>& rd, const cplx* x,
                 cplx* y, cplx offset, Counters* cnt, const SplitMatvec* sp = nullptr);
+// y = 1/2 (H x + H^dag x) + offset x (TensorMultiplierHermitian); Lh, Rth the
+// adjoint environments; sp/sph the split operands of both halves, or null.
+void heff_apply_hermitian(Context& c, const cplx* Le, const cplx* Lh, const std::array<int, 3>& ld,
+                          const MpoDev& m, int k, const cplx* Rt, const cplx* Rth, const std::array<int, 3>& rd,
+                          const cplx* x, cplx* y, cplx offset, Counters* cnt, const SplitMatvec* sp = nullptr,
+                          const SplitMatvec* sph = nullptr);
+// Descriptors of the two FP64 contractions of one product (heff.cu).
+Gemm1wDesc heff_first_desc(const cplx* Le, int Dlb, int Dlk, int wl, const cplx* x, int dd, int Drk, const cplx* Wm,
+                           int du, int wr, cplx* t2);
+Gemm3Desc heff_last_desc(const cplx* t2, int M, const cplx* Rt, int K, int Drb, cplx* y, const cplx* x,
+                         cplx offset);
 // Left/right environment update (Operator::contractleftop / contractrightop).
 void env_left_update(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpsDev& ket,
                      const MpoDev* m, int k, const MpsDev& bra, DBuf& out,
@@ -162,6 +180,12 @@ void env_left_update(Context& c, const cplx* Le, const std::array<int, 3>& ld, c
 void env_right_update(Context& c, const cplx* Rt, const std::array<int, 3>& rd, const MpsDev& ket,
                       const MpoDev* m, int k, const MpsDev& bra, DBuf& out,
                       std::array<int, 3>& od, Counters* cnt);
+
+// ---- files in the reference's binary formats (mpsio.cpp) ----
+void mps_export_file(Context& c, const MpsDev& s, const std::string& fn);
+void mps_import_file(Context& c, const std::string& fn, MpsDev& s);
+void mpo_save_file(Context& c, const MpoDev& m, const std::string& fn);
+void mpo_load_file(Context& c, const std::string& fn, MpoDev& m);
 
 // ---- algorithms (Contractor) ----
 double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
@@ -173,6 +197,9 @@ double find_next_excited_state(Context& c, const MpoDev& ops, int D,
                                double offset, const SolveOptions& opt, Counters& cnt);
 void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, int D,
               const SolveOptions& opt, double* errN, double* errT, Counters& cnt);
+// optimizeSum: init ~ sum_k beta_k kets[k] at bond D (Contractor.cpp:2332-2477).
+void optimize_sum(Context& c, const std::vector<const MpsDev*>& kets, const std::vector<cplx>& beta, MpsDev& init,
+                  int D, const SolveOptions& opt, Counters& cnt);
 cplx contract(Context& c, const MpsDev& ket, const MpoDev* ops, const MpsDev& bra);
 cplx contract2(Context& c, const MpoDev& ops, const MpsDev& ket, const MpsDev& bra);
 void expectation_local(Context& c, const MpsDev& s, const double* op, double* out);

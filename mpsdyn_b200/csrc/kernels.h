@@ -178,6 +178,54 @@ struct WContractArgs {
 };
 void wcontract(const Stream& st, const WContractArgs& a);
 
+// ---- effective-Hamiltonian contractions (heff.cu), grouped ----
+constexpr int GEMM_MAXP = 16;  // problems per launch
+// T2 = Wm . (A B) per pixel: C = A B with A(row, k) = A[row + k lda],
+// B(k, col) = B[k + col ldb]; rows x + X i0 (i0 < n_i0), columns i1 + n_i1 y
+// (i1 < n_i1); for every pixel (x < X, y < Y)
+//   out[x ox + y oy + o0 so0 + o1 so1] = sum_{i0,i1} Wm[(o0 + n_o0 o1) + nout (i0 + n_i0 i1)] C[(x,i0),(i1,y)]
+// (Wm column-major nout x nin in device memory, nin = n_i0 n_i1 <= 1024).
+struct Gemm1wDesc {
+  const cplx* A = nullptr;
+  long long lda = 0;
+  const cplx* B = nullptr;
+  long long ldb = 0;
+  int X = 0, Y = 0, K = 0, n_i0 = 0, n_i1 = 0, n_o0 = 0, n_o1 = 0;
+  const cplx* Wm = nullptr;
+  cplx* out = nullptr;
+  long long ox = 0, oy = 0, so0 = 0, so1 = 0;
+  int tiles_x = 0, tiles_y = 0, tile_begin = 0;  // filled by heff_gemm1w
+};
+struct Gemm1wBatch {
+  int n = 0;
+  Gemm1wDesc d[GEMM_MAXP];
+};
+void heff_gemm1w(const Stream& st, Gemm1wBatch& b);
+// C = alpha (A1 B1 + A2 B2) + beta Cin, column-major, op N: A1 M x K1,
+// B1 K1 x N, and (K2 > 0) A2 M x K2, B2 K2 x N; Cin may be null.
+struct Gemm3Desc {
+  int M = 0, N = 0, K1 = 0, K2 = 0;
+  const cplx* A1 = nullptr;
+  long long lda1 = 0;
+  const cplx* B1 = nullptr;
+  long long ldb1 = 0;
+  const cplx* A2 = nullptr;
+  long long lda2 = 0;
+  const cplx* B2 = nullptr;
+  long long ldb2 = 0;
+  cplx alpha = {1.0, 0.0}, beta = {0.0, 0.0};
+  const cplx* Cin = nullptr;
+  long long ldcin = 0;
+  cplx* C = nullptr;
+  long long ldc = 0;
+  int tiles_m = 0, tiles_n = 0, tile_begin = 0;  // filled by heff_gemm3
+};
+struct Gemm3Batch {
+  int n = 0;
+  Gemm3Desc d[GEMM_MAXP];
+};
+void heff_gemm3(const Stream& st, Gemm3Batch& b);
+
 // ---- vector kernels (Lanczos, norms) ----
 // dots[j] = sum_i conj(V[i + j*ldv]) w[i], j < k   (two-stage, deterministic)
 void cgemv_c(const Stream& st, int n, int k, const cplx* V, long long ldv, const cplx* w,
@@ -206,6 +254,44 @@ struct LanczosScalars {
 void lanczos_orthonormalize(const Stream& st, int n, int j, cplx* V, long long ldv, cplx* w,
                             bool write_next, double sigma, LanczosScalars* sc, LanczosScalars* mirror, cplx* h1,
                             cplx* h2, unsigned* counters, Scratch& scratch);
+// One reorthogonalised Lanczos step (the recurrence above, with the local
+// three-term subtraction folded into the first Gram-Schmidt pass and an
+// optional projector) for a group of independent instances in one
+// cooperative launch (lzstep.cu).  Per instance: w = (H - sigma) v_j on
+// entry; on exit sc->alpha[j], sc->beta[j] (and the mirror) are set and, when
+// write_next, V[:, j+1] = w / beta_j.  With nu > 0, U (n x nu, ld n) holds the
+// projector vectors (sqrt of the penalty folded in) and w += U (U^H v_j)
+// first.  Workspaces: part nrb_total x 256 complex, pn1/pn2 nrb_total, h/h2
+// ninst x 256; bar two unsigned words that are zero at rest.
+constexpr int LZ_THREADS = 256;
+constexpr int LZ_MAXI = 16;  // instances per launch
+constexpr int LZ_MAXU = 8;   // projector vectors per instance
+struct LzInst {
+  int n = 0, j = 0, k = 0, nu = 0, write_next = 0;
+  int rb0 = 0, nrb = 0;  // row blocks, filled by lanczos_step
+  double sigma = 0.0;
+  cplx* V = nullptr;
+  long long ldv = 0;
+  cplx* w = nullptr;
+  const cplx* U = nullptr;
+  LanczosScalars* sc = nullptr;
+  LanczosScalars* mirror = nullptr;
+};
+struct LzBatch {
+  int ninst = 0, nrb_total = 0;
+  LzInst in[LZ_MAXI];
+  cplx* part = nullptr;
+  double* pn1 = nullptr;
+  double* pn2 = nullptr;
+  cplx* h = nullptr;
+  cplx* h2 = nullptr;
+  unsigned* bar = nullptr;
+  int* err = nullptr;  // set when a bounded grid barrier ran out
+};
+// Rows per row block (the unit of the workspaces' nrb counts).
+int lanczos_step_rows_per_block();
+void lanczos_step(const Stream& st, LzBatch& b);
+
 // out[0] = ||x||_2 (deterministic two-stage reduction)
 void dznrm2(const Stream& st, int n, const cplx* x, double* out, Scratch& scratch);
 // y = x / (*nrm)   (device scalar)
@@ -248,6 +334,9 @@ int svd_cut(const Stream& st, int m, int n, const cplx* A, long long lda, int cu
 // ld = ldr, zero below the diagonal) are written when non-null; K = min(m, n).
 void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, long long ldq,
                             cplx* R, long long ldr, Scratch& scratch);
+// Places the fixed scratch array of mpsgpu_qr_device_noalloc on device `dev`
+// (current) and sets its kernels' attributes; called when a context is created.
+mpsgpu_status noalloc_qr_prepare(int dev);
 
 // Two-level strided view: element (i, j) lives at
 //   (i % rd)*r0 + (i / rd)*r1 + (j % cd)*c0 + (j / cd)*c1, optionally conjugated.

@@ -1,0 +1,449 @@
+// One reorthogonalised Lanczos step for a group of independent local
+// eigenproblems, in a single cooperative launch (replaces the
+// orthogonalisation inside the PRIMME call of Contractor::solveEigs,
+// src/core/cpp/Contractor.cpp:3067-3138; the recurrence is the one of
+// lanczos.cu, organised for fewer launches).
+//
+// For every instance q, with k = j+1 basis vectors V[:, 0..j] and
+// w = (H - sigma) v_j computed by the matvec:
+//   projector  w += U (U^H v_j)        (excited states: U holds sqrt(pen) u_t)
+//   pass 1     w' = w - beta_{j-1} v_{j-1};  h = V^H w';  w'' = w' - V h
+//   pass 2     only when |w''|^2 < |w'|^2 / 2 (Daniel, Gragg, Kaufman,
+//              Stewart 1976): h2 = V^H w''; w''' = w'' - V h2
+//   alpha_j = sigma + Re(h_j + h2_j), beta_j = |w|, V[:, j+1] = w / beta_j.
+//
+// Rows of all instances are cut into row blocks of 256 (one per thread);
+// blocks are taken in grid-stride order by a grid that is resident all at
+// once (cooperative launch).  Partial sums per row block go to global
+// memory and are reduced in a fixed order, so the results are identical
+// from run to run and do not depend on the other instances of the group.
+// Grid barriers are bounded: a CTA that waits longer than 2 s sets the
+// error word and returns (the host reports MPSGPU_TIMEOUT and resets the
+// barrier words); the kernel has no copies in flight at any barrier.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mpsgpu {
+
+namespace {
+
+constexpr int T = LZ_THREADS;         // threads per CTA
+constexpr int RPT = 1;                // rows per thread per row block
+constexpr int RB = T * RPT;           // rows per row block
+constexpr int NW = T / 32;
+constexpr int KMAXS = 256;            // Krylov vectors
+constexpr double DGKS2 = 0.5;
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded grid barrier over gridDim.x co-resident CTAs: bar[0] counts the
+// arrivals, bar[1] is the generation the last arrival advances.  Returns
+// false (and sets *err) when the wait ran out.
+__device__ bool grid_barrier(unsigned* bar, int* err) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const unsigned long long t0 = gtimer();
+      while (*gen == g) {
+        __nanosleep(32);
+        if (gtimer() - t0 > 2000000000ull) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+__device__ __forceinline__ double warp_sumd(double s) {
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+__device__ __forceinline__ cplx warp_sumc(cplx s) {
+  for (int o = 16; o > 0; o >>= 1) {
+    s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+    s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+  }
+  return s;
+}
+
+// Sum of v[0..7] over the 32 lanes of a warp by a transposing butterfly:
+// afterwards lane L with (L & 3) == 0 holds the total of vector (L >> 2).
+__device__ __forceinline__ cplx warp_sum8(cplx (&v)[8]) {
+  const int lane = threadIdx.x & 31;
+  // xor 16: keep 4 of 8 (upper half of the lanes keeps vectors 4..7)
+  {
+    const bool up = lane & 16;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      cplx send = up ? v[i] : v[i + 4];
+      cplx keep = up ? v[i + 4] : v[i];
+      keep.x += __shfl_xor_sync(0xffffffffu, send.x, 16);
+      keep.y += __shfl_xor_sync(0xffffffffu, send.y, 16);
+      v[i] = keep;
+    }
+  }
+  {
+    const bool up = lane & 8;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      cplx send = up ? v[i] : v[i + 2];
+      cplx keep = up ? v[i + 2] : v[i];
+      keep.x += __shfl_xor_sync(0xffffffffu, send.x, 8);
+      keep.y += __shfl_xor_sync(0xffffffffu, send.y, 8);
+      v[i] = keep;
+    }
+  }
+  cplx r;
+  {
+    const bool up = lane & 4;
+    cplx send = up ? v[0] : v[1];
+    r = up ? v[1] : v[0];
+    r.x += __shfl_xor_sync(0xffffffffu, send.x, 4);
+    r.y += __shfl_xor_sync(0xffffffffu, send.y, 4);
+  }
+  r.x += __shfl_xor_sync(0xffffffffu, r.x, 2);
+  r.y += __shfl_xor_sync(0xffffffffu, r.y, 2);
+  r.x += __shfl_xor_sync(0xffffffffu, r.x, 1);
+  r.y += __shfl_xor_sync(0xffffffffu, r.y, 1);
+  // lane bits (4, 3, 2) select vector 4*b4 + 2*b3 + b2
+  return r;
+}
+__device__ __forceinline__ int sum8_vector_of_lane(int lane) {
+  return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+}
+
+// instance owning global row block rb (instances hold consecutive ranges)
+__device__ __forceinline__ int inst_of(const LzBatch& b, int rb) {
+  int q = 0;
+  while (q + 1 < b.ninst && b.in[q + 1].rb0 <= rb) q++;
+  return q;
+}
+
+// Partial dots over the rows [r0, r0 + RB) of an n-row instance:
+// part[rb * KMAXS + l] = sum_rows conj(V[:, l]) x for l < k (V with leading
+// dimension ldv), and the partial |x|^2 into pn[rb] when pn is non-null.
+__device__ void block_dots(const cplx* __restrict__ V, long long ldv, long long n, long long r0, int rb,
+                           const cplx* __restrict__ x, int k, cplx* part, double* pn, cplx (*red)[8],
+                           double* redn) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  long long rows[RPT];
+  bool ok[RPT];
+  cplx xv[RPT];
+#pragma unroll
+  for (int u = 0; u < RPT; u++) {
+    rows[u] = r0 + tid + u * T;
+    ok[u] = rows[u] < n;
+    xv[u] = ok[u] ? x[rows[u]] : make_double2(0.0, 0.0);
+  }
+  if (pn) {
+    double s = 0.0;
+#pragma unroll
+    for (int u = 0; u < RPT; u++) s += cabs2(xv[u]);
+    s = warp_sumd(s);
+    if (lane == 0) redn[warp] = s;
+  }
+  for (int l0 = 0; l0 < k; l0 += 8) {
+    cplx acc[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      const int l = l0 + t;
+      cplx s = make_double2(0.0, 0.0);
+      if (l < k) {
+        const cplx* col = V + (long long)l * ldv;
+#pragma unroll
+        for (int u = 0; u < RPT; u++)
+          if (ok[u]) s = cadd(s, ccmul(__ldcg(&col[rows[u]]), xv[u]));
+      }
+      acc[t] = s;
+    }
+    const cplx r = warp_sum8(acc);
+    if ((lane & 3) == 0) red[warp][sum8_vector_of_lane(lane)] = r;
+    __syncthreads();
+    if (tid < 8 && l0 + tid < k) {
+      cplx s = make_double2(0.0, 0.0);
+      for (int q = 0; q < NW; q++) s = cadd(s, red[q][tid]);
+      part[(long long)rb * KMAXS + l0 + tid] = s;
+    }
+    __syncthreads();
+  }
+  if (pn && tid == 0) {
+    double s = 0.0;
+    for (int q = 0; q < NW; q++) s += redn[q];
+    pn[rb] = s;
+  }
+}
+
+// x -= V h over the rows of row block rb (h in shared memory, k entries);
+// partial |x|^2 into pn[rb].
+__device__ void block_update(const LzInst& in, int rb, cplx* __restrict__ x, const cplx* hs, int k, double* pn,
+                             double* redn) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long r0 = (long long)(rb - in.rb0) * RB;
+  double s2 = 0.0;
+#pragma unroll
+  for (int u = 0; u < RPT; u++) {
+    const long long i = r0 + tid + u * T;
+    if (i < in.n) {
+      cplx a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
+      const cplx* v = in.V + i;
+      int l = 0;
+      for (; l + 3 < k; l += 4) {
+        a0 = cadd(a0, cmul(__ldcg(&v[(long long)l * in.ldv]), hs[l]));
+        a1 = cadd(a1, cmul(__ldcg(&v[(long long)(l + 1) * in.ldv]), hs[l + 1]));
+        a2 = cadd(a2, cmul(__ldcg(&v[(long long)(l + 2) * in.ldv]), hs[l + 2]));
+        a3 = cadd(a3, cmul(__ldcg(&v[(long long)(l + 3) * in.ldv]), hs[l + 3]));
+      }
+      for (; l < k; l++) a0 = cadd(a0, cmul(__ldcg(&v[(long long)l * in.ldv]), hs[l]));
+      const cplx xi = csub(x[i], cadd(cadd(a0, a1), cadd(a2, a3)));
+      x[i] = xi;
+      s2 += cabs2(xi);
+    }
+  }
+  s2 = warp_sumd(s2);
+  if (lane == 0) redn[warp] = s2;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+    for (int q = 0; q < NW; q++) s += redn[q];
+    pn[rb] = s;
+  }
+  __syncthreads();
+}
+
+// h[q][l] = sum over the row blocks of q of part[rb][l], one warp per (q, l),
+// for the instances selected by `sel` (bit q).
+__device__ void reduce_pairs(const LzBatch& b, const cplx* part, cplx* h, unsigned sel) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int npairs = 0;
+  for (int q = 0; q < b.ninst; q++) npairs += b.in[q].k;
+  for (int p = blockIdx.x * NW + warp; p < npairs; p += gridDim.x * NW) {
+    int q = 0, rem = p;
+    while (rem >= b.in[q].k) rem -= b.in[q].k, q++;
+    if (!((sel >> q) & 1u)) continue;
+    const LzInst& in = b.in[q];
+    cplx s = make_double2(0.0, 0.0);
+    for (int r = lane; r < in.nrb; r += 32) s = cadd(s, __ldcg(&part[(long long)(in.rb0 + r) * KMAXS + rem]));
+    s = warp_sumc(s);
+    if (lane == 0) h[q * KMAXS + rem] = s;
+  }
+}
+
+// sum over the row blocks of instance q of pn (fixed order; every CTA gets
+// the same value)
+__device__ double sum_norms(const LzInst& in, const double* pn, double* redn) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double s = 0.0;
+  for (int r = tid; r < in.nrb; r += T) s += __ldcg(&pn[in.rb0 + r]);
+  s = warp_sumd(s);
+  __syncthreads();
+  if (lane == 0) redn[warp] = s;
+  __syncthreads();
+  double t = 0.0;
+  for (int q = 0; q < NW; q++) t += redn[q];
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__ LzBatch b) {
+  __shared__ cplx red[NW][8];
+  __shared__ double redn[NW];
+  __shared__ cplx hs[KMAXS];
+  __shared__ cplx ucs[LZ_MAXU];
+  __shared__ unsigned flagged;
+  const int tid = threadIdx.x;
+
+  // ---- projector (excited states): c = U^H v_j, then w += U c ----
+  bool any_proj = false;
+  for (int q = 0; q < b.ninst; q++) any_proj |= b.in[q].nu > 0;
+  if (any_proj) {
+    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
+      const int q = inst_of(b, rb);
+      const LzInst& in = b.in[q];
+      if (in.nu == 0) continue;
+      // dots of the U columns with v_j
+      block_dots(in.U, in.n, in.n, (long long)(rb - in.rb0) * RB, rb, in.V + (long long)in.j * in.ldv, in.nu,
+                 b.part, nullptr, red, redn);
+    }
+    if (!grid_barrier(b.bar, b.err)) return;
+    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
+      const int q = inst_of(b, rb);
+      const LzInst& in = b.in[q];
+      if (in.nu == 0) continue;
+      // every CTA reduces the (few) coefficients of its instance itself
+      if (tid < 32) {
+        for (int t = 0; t < in.nu; t++) {
+          cplx s = make_double2(0.0, 0.0);
+          for (int r = tid; r < in.nrb; r += 32) s = cadd(s, __ldcg(&b.part[(long long)(in.rb0 + r) * KMAXS + t]));
+          s = warp_sumc(s);
+          if (tid == 0) ucs[t] = s;
+        }
+      }
+      __syncthreads();
+      const long long r0 = (long long)(rb - in.rb0) * RB;
+      for (int u = 0; u < RPT; u++) {
+        const long long i = r0 + tid + u * T;
+        if (i < in.n) {
+          cplx a = in.w[i];
+          for (int t = 0; t < in.nu; t++) a = cadd(a, cmul(in.U[i + (long long)t * in.n], ucs[t]));
+          in.w[i] = a;
+        }
+      }
+      __syncthreads();
+    }
+    // the dots below read other rows only through V, never w: no barrier needed
+  }
+
+  // ---- pass 1: w' = w - beta_{j-1} v_{j-1}; partial h = V^H w', |w'|^2 ----
+  for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
+    const int q = inst_of(b, rb);
+    const LzInst& in = b.in[q];
+    if (in.j > 0) {
+      const double bp = in.sc->beta[in.j - 1];
+      const cplx* vp = in.V + (long long)(in.j - 1) * in.ldv;
+      const long long r0 = (long long)(rb - in.rb0) * RB;
+#pragma unroll
+      for (int u = 0; u < RPT; u++) {
+        const long long i = r0 + tid + u * T;
+        if (i < in.n) in.w[i] = csub(in.w[i], cscale(__ldcg(&vp[i]), bp));
+      }
+      __syncthreads();
+    }
+    block_dots(in.V, in.ldv, in.n, (long long)(rb - in.rb0) * RB, rb, in.w, in.k, b.part, b.pn1, red, redn);
+  }
+  if (!grid_barrier(b.bar, b.err)) return;
+  reduce_pairs(b, b.part, b.h, 0xffffffffu);
+  if (!grid_barrier(b.bar, b.err)) return;
+  for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
+    const int q = inst_of(b, rb);
+    const LzInst& in = b.in[q];
+    for (int l = tid; l < in.k; l += T) hs[l] = __ldcg(&b.h[q * KMAXS + l]);
+    __syncthreads();
+    block_update(in, rb, in.w, hs, in.k, b.pn2, redn);
+  }
+  if (!grid_barrier(b.bar, b.err)) return;
+
+  // ---- DGKS test (every CTA decides the same) ----
+  if (tid == 0) flagged = 0u;
+  __syncthreads();
+  for (int q = 0; q < b.ninst; q++) {
+    const double nb2 = sum_norms(b.in[q], b.pn1, redn);
+    const double b2 = sum_norms(b.in[q], b.pn2, redn);
+    if (tid == 0 && b2 < DGKS2 * nb2) flagged |= 1u << q;
+  }
+  __syncthreads();
+  const unsigned fl = flagged;
+  if (fl) {
+    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
+      const int q = inst_of(b, rb);
+      if (!((fl >> q) & 1u)) continue;
+      const LzInst& in = b.in[q];
+      block_dots(in.V, in.ldv, in.n, (long long)(rb - in.rb0) * RB, rb, in.w, in.k, b.part, nullptr, red, redn);
+    }
+    if (!grid_barrier(b.bar, b.err)) return;
+    reduce_pairs(b, b.part, b.h2, fl);
+    if (!grid_barrier(b.bar, b.err)) return;
+    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
+      const int q = inst_of(b, rb);
+      if (!((fl >> q) & 1u)) continue;
+      const LzInst& in = b.in[q];
+      for (int l = tid; l < in.k; l += T) hs[l] = __ldcg(&b.h2[q * KMAXS + l]);
+      __syncthreads();
+      block_update(in, rb, in.w, hs, in.k, b.pn2, redn);
+    }
+    if (!grid_barrier(b.bar, b.err)) return;
+  }
+
+  // ---- alpha_j, beta_j; V[:, j+1] = w / beta_j ----
+  __shared__ double beta_s[LZ_MAXI];
+  for (int q = 0; q < b.ninst; q++) {
+    const double b2 = sum_norms(b.in[q], b.pn2, redn);
+    if (tid == 0) beta_s[q] = sqrt(b2);
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && tid < b.ninst) {
+    const LzInst& in = b.in[tid];
+    double alpha = in.sigma + __ldcg(&b.h[tid * KMAXS + in.j].x);
+    if ((fl >> tid) & 1u) alpha += __ldcg(&b.h2[tid * KMAXS + in.j].x);
+    const double beta = beta_s[tid];
+    in.sc->alpha[in.j] = alpha;
+    in.sc->beta[in.j] = beta;
+    in.sc->flag = (fl >> tid) & 1u;
+    if (in.mirror) {  // mapped host memory, read by the host after the launch's event
+      in.mirror->alpha[in.j] = alpha;
+      in.mirror->beta[in.j] = beta;
+    }
+  }
+  for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
+    const int q = inst_of(b, rb);
+    const LzInst& in = b.in[q];
+    if (!in.write_next) continue;
+    const double inv = 1.0 / beta_s[q];
+    cplx* vn = in.V + (long long)(in.j + 1) * in.ldv;
+    const long long r0 = (long long)(rb - in.rb0) * RB;
+#pragma unroll
+    for (int u = 0; u < RPT; u++) {
+      const long long i = r0 + tid + u * T;
+      if (i < in.n) vn[i] = cscale(in.w[i], inv);
+    }
+  }
+}
+
+std::atomic<unsigned long long> g_lz_setup{0};
+int g_lz_grid[64] = {0};
+
+}  // namespace
+
+int lanczos_step_rows_per_block() { return RB; }
+
+void lanczos_step(const Stream& st, LzBatch& b) {
+  MPSGPU_CHECK(b.ninst >= 1 && b.ninst <= LZ_MAXI, MPSGPU_BAD_SHAPE, "lanczos step: group size");
+  int rb = 0;
+  for (int q = 0; q < b.ninst; q++) {
+    LzInst& in = b.in[q];
+    MPSGPU_CHECK(in.k == in.j + 1 && in.k <= KMAXS && in.n > 0, MPSGPU_BAD_SHAPE, "lanczos step: basis size");
+    MPSGPU_CHECK(in.nu <= LZ_MAXU && in.nu <= KMAXS, MPSGPU_BAD_SHAPE, "lanczos step: projector size");
+    in.rb0 = rb;
+    in.nrb = ceil_div(in.n, RB);
+    rb += in.nrb;
+  }
+  b.nrb_total = rb;
+  int dev = 0;
+  MPSGPU_CUDA(cudaGetDevice(&dev));
+  if (device_needs_setup(g_lz_setup)) {
+    int nsm = 148, per = 1;
+    MPSGPU_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    MPSGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lanczos_step_kernel, T, 0));
+    MPSGPU_CHECK(per >= 1, MPSGPU_BAD_SHAPE, "lanczos step: kernel does not fit on an SM");
+    // one CTA per SM: room stays for the kernels of other streams (and for
+    // other cooperative launches) next to the step
+    g_lz_grid[dev] = nsm;
+    mark_device_done(g_lz_setup);
+  }
+  const int grid = std::max(1, std::min(g_lz_grid[dev], b.nrb_total));
+  void* args[] = {&b};
+  MPSGPU_CUDA(cudaLaunchCooperativeKernel((void*)lanczos_step_kernel, dim3(grid), dim3(T), args, 0, st.s));
+  after_launch(st);
+}
+
+}  // namespace mpsgpu

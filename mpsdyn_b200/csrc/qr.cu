@@ -32,49 +32,6 @@ namespace {
 
 constexpr int QR_THREADS = 512;
 
-__device__ double block_sum(double v, double* red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  double s = 0.0;
-  const int nw = blockDim.x >> 5;
-  for (int w = 0; w < nw; w++) s += red[w];
-  return s;
-}
-
-__device__ double block_max(double v, double* red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  double s = 0.0;
-  const int nw = blockDim.x >> 5;
-  for (int w = 0; w < nw; w++) s = fmax(s, red[w]);
-  return s;
-}
-
-// 2-norm of x[0..n) without underflow or overflow of the squares: the
-// entries are divided by the largest component magnitude before squaring
-// (the scaled sum of LAPACK's dznrm2).  Rank-deficient sites produce
-// trailing columns with entries far below 1e-154, whose plain squares
-// underflow to zero.  Every thread of the block gets the result.
-__device__ double block_scaled_norm(int n, const cplx* x, double* red) {
-  double mx = 0.0;
-  for (int r = threadIdx.x; r < n; r += blockDim.x) mx = fmax(mx, fmax(fabs(x[r].x), fabs(x[r].y)));
-  mx = block_max(mx, red);
-  if (mx == 0.0) return 0.0;
-  const double inv = 1.0 / mx;
-  double part = 0.0;
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
-    const double a = x[r].x * inv, b = x[r].y * inv;
-    part += a * a + b * b;
-  }
-  return mx * sqrt(block_sum(part, red));
-}
-
 // sqrt(a^2 + b^2 + c^2) with the largest magnitude factored out (dlapy3).
 __device__ __forceinline__ double hypot3(double a, double b, double c) {
   a = fabs(a); b = fabs(b); c = fabs(c);
@@ -99,50 +56,88 @@ __device__ __forceinline__ cplx recip_smith(cplx z) {
 // by the machine epsilon (LAPACK zlarfg's SAFMIN = dlamch('S') / dlamch('E')).
 constexpr double kSafeMin = 2.2250738585072014e-308 / 1.1102230246251565e-16;
 
-// Apply (I - V T' V^H) to the mp x cw column slice C (shared, ld = mp), where
-// V (mp x jb, unit lower trapezoidal) and T (jb x jb) are in global memory
-// and T' = T^H (conjT = true, for Q^H A) or T (for Q E).  W is jb x cw shared.
-__device__ void apply_block_reflector(int mp, int jb, int cw, const cplx* __restrict__ V,
-                                      long long ldv, const cplx* __restrict__ T, int ldt,
-                                      bool conjT, cplx* C, int ldc, cplx* W, cplx* W2) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  // W[l, q] = sum_r conj(V[r, l]) C[r, q]  (V[r,l] = 0 for r < l, 1 for r = l)
-  for (int t = warp; t < jb * cw; t += nw) {
-    int l = t % jb, q = t / jb;
+// Shared-memory plan of both kernels: the column slice C (mp x nb, ld mp),
+// a staging chunk of QR_CH rows of V, the block factor T (nb x nb), the
+// product W (nb x nb) and W2 (nb x nb, also the per-thread partial sums of
+// W: QR_THREADS entries).
+constexpr int QR_CH = 128;
+__host__ __device__ inline size_t qr_smem_bytes(int m, int nb) {
+  const size_t w2 = (size_t)nb * nb > (size_t)QR_THREADS ? (size_t)nb * nb : (size_t)QR_THREADS;
+  return ((size_t)m * nb + (size_t)QR_CH * nb + 2 * (size_t)nb * nb + w2) * sizeof(cplx);
+}
+constexpr int QR_SMEM_ATTR = 227 * 1024;
+
+// Apply (I - V T' V^H) to the mp x cw column slice C (shared, ld = ldc), where
+// V (mp x jb, unit lower trapezoidal: its upper triangle and diagonal are not
+// read) and T (jb x jb) are in global memory and T' = T^H (conjT = true, for
+// Q^H A) or T (for Q E).  V is staged through shared memory in chunks of
+// QR_CH rows (coalesced copies), T once; Vs, Ts, W, W2 are shared.
+__device__ void apply_block_reflector(int mp, int jb, int cw, const cplx* __restrict__ V, long long ldv,
+                                      const cplx* __restrict__ T, int ldt, bool conjT, cplx* C, int ldc,
+                                      cplx* Vs, cplx* Ts, cplx* W, cplx* W2) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int t = tid; t < jb * jb; t += nt) Ts[t] = T[(t % jb) + (long long)(t / jb) * ldt];
+  const int npair = jb * cw;
+  // W[l, q] = sum_r conj(V[r, l]) C[r, q]; threads own pairs (l, q), further
+  // groups of threads take every groups-th row when the block has threads to spare
+  const int groups = max(1, nt / max(1, npair));
+  const int pair = tid % max(1, npair), grp = tid / max(1, npair);
+  cplx acc = make_double2(0.0, 0.0);
+  for (int r0 = 0; r0 < mp; r0 += QR_CH) {
+    const int rows = min(QR_CH, mp - r0);
+    __syncthreads();
+    for (int t = tid; t < rows * jb; t += nt) {
+      const int r = t % rows, l = t / rows, gr = r0 + r;
+      cplx v = make_double2(0.0, 0.0);
+      if (gr > l) v = V[gr + (long long)l * ldv];
+      else if (gr == l) v = make_double2(1.0, 0.0);
+      Vs[r + l * QR_CH] = v;
+    }
+    __syncthreads();
+    if (pair < npair && grp < groups) {
+      const int l = pair % jb, q = pair / jb;
+      for (int r = grp; r < rows; r += groups) acc = cadd(acc, ccmul(Vs[r + l * QR_CH], C[r0 + r + q * ldc]));
+    }
+  }
+  __syncthreads();
+  // combine the row groups in a fixed order
+  if (pair < npair && grp < groups) W2[pair + grp * npair] = acc;  // W2 as scratch (groups * npair <= nt)
+  __syncthreads();
+  for (int t = tid; t < npair; t += nt) {
     cplx s = make_double2(0.0, 0.0);
-    for (int r = l + lane; r < mp; r += 32) {
-      cplx v = (r == l) ? make_double2(1.0, 0.0) : V[r + (long long)l * ldv];
-      s = cadd(s, ccmul(v, C[r + q * ldc]));
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-    }
-    if (lane == 0) W[l + q * jb] = s;
+    for (int g = 0; g < groups; g++) s = cadd(s, W2[t + g * npair]);
+    W[t] = s;
   }
   __syncthreads();
   // W2 = T' W  (T' = T^H lower triangular, or T upper triangular)
-  for (int t = threadIdx.x; t < jb * cw; t += blockDim.x) {
-    int i = t % jb, q = t / jb;
+  for (int t = tid; t < npair; t += nt) {
+    const int i = t % jb, q = t / jb;
     cplx s = make_double2(0.0, 0.0);
     if (conjT) {
-      for (int l = 0; l <= i; l++) s = cadd(s, ccmul(T[l + i * ldt], W[l + q * jb]));
+      for (int l = 0; l <= i; l++) s = cadd(s, ccmul(Ts[l + i * jb], W[l + q * jb]));
     } else {
-      for (int l = i; l < jb; l++) s = cadd(s, cmul(T[i + l * ldt], W[l + q * jb]));
+      for (int l = i; l < jb; l++) s = cadd(s, cmul(Ts[i + l * jb], W[l + q * jb]));
     }
-    W2[i + q * jb] = s;
+    W2[t] = s;
   }
-  __syncthreads();
-  // C -= V W2
-  for (int t = threadIdx.x; t < mp * cw; t += blockDim.x) {
-    int r = t % mp, q = t / mp;
-    cplx s = make_double2(0.0, 0.0);
-    int lmax = min(r, jb - 1);
-    for (int l = 0; l <= lmax; l++) {
-      cplx v = (r == l) ? make_double2(1.0, 0.0) : V[r + (long long)l * ldv];
-      s = cadd(s, cmul(v, W2[l + q * jb]));
+  // C -= V W2, chunk by chunk
+  for (int r0 = 0; r0 < mp; r0 += QR_CH) {
+    const int rows = min(QR_CH, mp - r0);
+    __syncthreads();
+    for (int t = tid; t < rows * jb; t += nt) {
+      const int r = t % rows, l = t / rows, gr = r0 + r;
+      cplx v = make_double2(0.0, 0.0);
+      if (gr > l) v = V[gr + (long long)l * ldv];
+      else if (gr == l) v = make_double2(1.0, 0.0);
+      Vs[r + l * QR_CH] = v;
     }
-    C[r + q * ldc] = csub(C[r + q * ldc], s);
+    __syncthreads();
+    for (int t = tid; t < rows * cw; t += nt) {
+      const int r = t % rows, q = t / rows;
+      cplx s = make_double2(0.0, 0.0);
+      for (int l = 0; l < jb; l++) s = cadd(s, cmul(Vs[r + l * QR_CH], W2[l + q * jb]));
+      C[r0 + r + q * ldc] = csub(C[r0 + r + q * ldc], s);
+    }
   }
   __syncthreads();
 }
@@ -154,161 +149,205 @@ struct QrParams {
   cplx* tau;    // K
 };
 
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ cplx warp_csum(cplx v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+// 2-norm of x[0..n) by one warp, with the largest component magnitude
+// factored out before squaring (the scaled sum of LAPACK's dznrm2):
+// rank-deficient sites produce trailing columns with entries far below
+// 1e-154, whose plain squares underflow to zero.  Every lane gets the result.
+__device__ double warp_scaled_norm(int n, const cplx* x) {
+  const int lane = threadIdx.x & 31;
+  double mx = 0.0;
+  for (int r = lane; r < n; r += 32) mx = fmax(mx, fmax(fabs(x[r].x), fabs(x[r].y)));
+  mx = warp_max(mx);
+  if (mx == 0.0) return 0.0;
+  const double inv = 1.0 / mx;
+  double part = 0.0;
+  for (int r = lane; r < n; r += 32) {
+    const double a = x[r].x * inv, b = x[r].y * inv;
+    part += a * a + b * b;
+  }
+  return mx * sqrt(warp_sum(part));
+}
+
+// Householder reflector of column c of the panel P (rows c..mp-1, ld mp),
+// computed by one warp (zlarfg): overwrites P[c, c] with beta and the rows
+// below with v (v_c = 1 implicit); returns tau.
+__device__ cplx warp_reflector(cplx* P, int mp, int c) {
+  const int lane = threadIdx.x & 31;
+  cplx* x = P + (c + 1) + (long long)c * mp;
+  const int nx = mp - c - 1;
+  double xnorm = warp_scaled_norm(nx, x);
+  cplx alpha = P[c + (long long)c * mp];
+  if (xnorm == 0.0 && alpha.y == 0.0) return make_double2(0.0, 0.0);  // H = I
+  double nrm = hypot3(alpha.x, alpha.y, xnorm);
+  double beta = alpha.x >= 0.0 ? -nrm : nrm;
+  // |beta| below kSafeMin: scale the column up (at most 20 times) so that
+  // 1 / (alpha - beta) stays finite; beta is scaled back at the end, tau and
+  // v are scale-invariant
+  int knt = 0;
+  while (fabs(beta) < kSafeMin && knt < 20) {
+    __syncwarp();
+    for (int r = lane; r < nx; r += 32) x[r] = cscale(x[r], 1.0 / kSafeMin);
+    beta /= kSafeMin;
+    alpha = cscale(alpha, 1.0 / kSafeMin);
+    knt++;
+  }
+  if (knt > 0) {
+    __syncwarp();
+    xnorm = warp_scaled_norm(nx, x);
+    nrm = hypot3(alpha.x, alpha.y, xnorm);
+    beta = alpha.x >= 0.0 ? -nrm : nrm;
+  }
+  const cplx tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+  const cplx scale = recip_smith(make_double2(alpha.x - beta, alpha.y));
+  for (int k = 0; k < knt; k++) beta *= kSafeMin;
+  __syncwarp();
+  for (int r = lane; r < nx; r += 32) x[r] = cmul(x[r], scale);
+  __syncwarp();
+  if (lane == 0) P[c + (long long)c * mp] = make_double2(beta, 0.0);
+  __syncwarp();
+  return tau;
+}
+
+// Factor the panel P (mp x jb, shared, ld mp) in place and build its block
+// factor T (jb x jb, forward columnwise, zlarft) into Tg; taus into taug.
+// Warp q owns panel column q: it applies the reflectors of the columns to
+// its left to its own column, then, on its turn, computes its reflector, so
+// one block barrier per column orders the reflectors.
+__device__ void factor_panel(cplx* P, int mp, int jb, cplx* Tg, int ldt, cplx* taug, cplx* Wsh, cplx* taus) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c = 0; c < jb; c++) {
+    if (warp == c) {
+      const cplx tau = warp_reflector(P, mp, c);
+      if (lane == 0) taus[c] = tau;
+    }
+    __syncthreads();
+    // warps to the right apply H_c^H = I - conj(tau_c) v v^H to their column
+    if (warp > c && warp < jb) {
+      const cplx tau = taus[c];
+      if (tau.x != 0.0 || tau.y != 0.0) {
+        cplx* a = P + (long long)warp * mp;
+        const cplx* v = P + (long long)c * mp;
+        cplx s = make_double2(0.0, 0.0);
+        for (int r = c + lane; r < mp; r += 32) s = cadd(s, ccmul(r == c ? make_double2(1.0, 0.0) : v[r], a[r]));
+        s = cmul(cconj(tau), warp_csum(s));
+        for (int r = c + lane; r < mp; r += 32) a[r] = csub(a[r], cmul(r == c ? make_double2(1.0, 0.0) : v[r], s));
+      }
+      __syncwarp();
+    }
+  }
+  // T: T[i, i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] (V[:, 0:i]^H v_i).
+  // First the Gram products G[l, i] = V[:, l]^H v_i (l < i), one warp each.
+  const int nw = blockDim.x >> 5;
+  for (int t = warp; t < jb * jb; t += nw) {
+    const int l = t % jb, i = t / jb;
+    if (l >= i) continue;
+    cplx s = make_double2(0.0, 0.0);
+    for (int r = i + lane; r < mp; r += 32) {
+      const cplx vl = P[r + (long long)l * mp];  // r > l
+      const cplx vi = (r == i) ? make_double2(1.0, 0.0) : P[r + (long long)i * mp];
+      s = cadd(s, ccmul(vl, vi));
+    }
+    s = warp_csum(s);
+    if (lane == 0) Wsh[l + i * jb] = s;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // column by column (one lane per row l < i), T kept in Wsh's upper part
+    // is read back from Tg; jb <= 32
+    for (int i = 0; i < jb; i++) {
+      const cplx ti = taus[i];
+      cplx v = make_double2(0.0, 0.0);
+      if (lane < i) {
+        cplx s = make_double2(0.0, 0.0);
+        for (int q = lane; q < i; q++) s = cadd(s, cmul(Tg[lane + q * ldt], Wsh[q + i * jb]));
+        v = cmul(make_double2(-ti.x, -ti.y), s);
+      } else if (lane == i) {
+        v = ti;
+      }
+      __syncwarp();
+      if (lane < jb) Tg[lane + i * ldt] = v;
+      if (lane == 0) taug[i] = ti;
+      __threadfence_block();
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(QR_THREADS) qr_factor_kernel(QrParams p) {
   cg::grid_group grid = cg::this_grid();
   extern __shared__ double smem_d[];
-  cplx* sm = reinterpret_cast<cplx*>(smem_d);
-  __shared__ double red[QR_THREADS / 32];
-  __shared__ cplx Wsh[16 * 16], W2sh[16 * 16];
-  __shared__ cplx coef;
   const int m = p.m, nb = p.nb;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-
+  cplx* C = reinterpret_cast<cplx*>(smem_d);       // m x nb
+  cplx* Vs = C + (size_t)m * nb;                    // QR_CH x nb
+  cplx* Ts = Vs + (size_t)QR_CH * nb;               // nb x nb
+  cplx* W = Ts + (size_t)nb * nb;
+  cplx* W2 = W + (size_t)nb * nb;
+  __shared__ cplx taus[32];
+  const int G = gridDim.x;
+  auto load_slice = [&](int r0, int c0, int rows, int cw) {
+    for (int t = threadIdx.x; t < rows * cw; t += blockDim.x) {
+      const int r = t % rows, c = t / rows;
+      C[t] = p.A[(r0 + r) + (long long)(c0 + c) * m];
+    }
+    __syncthreads();
+  };
+  auto store_slice = [&](int r0, int c0, int rows, int cw) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < rows * cw; t += blockDim.x) {
+      const int r = t % rows, c = t / rows;
+      p.A[(r0 + r) + (long long)(c0 + c) * m] = C[t];
+    }
+  };
   for (int pi = 0; pi < p.npanel; pi++) {
     const int j0 = pi * nb;
     const int jb = min(nb, p.K - j0);
     const int mp = m - j0;
     cplx* Tp = p.T + (long long)pi * nb * nb;
     if (blockIdx.x == 0) {
-      cplx* P = sm;  // mp x jb, ld = mp
-      for (int t = threadIdx.x; t < mp * jb; t += blockDim.x) {
-        int r = t % mp, c = t / mp;
-        P[t] = p.A[(j0 + r) + (long long)(j0 + c) * m];
-      }
-      __syncthreads();
-      for (int c = 0; c < jb; c++) {
-        // reflector of column c, rows c..mp-1 (block-uniform control flow:
-        // every thread holds the same norms, alpha and beta)
-        cplx* x = P + (c + 1) + c * mp;
-        const int nx = mp - c - 1;
-        double xnorm = block_scaled_norm(nx, x, red);
-        cplx alpha = P[c + c * mp];
-        cplx tau, scale;
-        bool ident = (xnorm == 0.0 && alpha.y == 0.0);
-        double beta = 0.0;
-        if (ident) {
-          tau = make_double2(0.0, 0.0);
-          scale = make_double2(0.0, 0.0);
-        } else {
-          double nrm = hypot3(alpha.x, alpha.y, xnorm);
-          beta = alpha.x >= 0.0 ? -nrm : nrm;
-          // |beta| below kSafeMin: scale the column up (at most 20 times)
-          // so that 1 / (alpha - beta) stays finite; beta is scaled back
-          // at the end, tau and v are scale-invariant
-          int knt = 0;
-          while (fabs(beta) < kSafeMin && knt < 20) {
-            __syncthreads();
-            for (int r = threadIdx.x; r < nx; r += blockDim.x) x[r] = cscale(x[r], 1.0 / kSafeMin);
-            beta /= kSafeMin;
-            alpha = cscale(alpha, 1.0 / kSafeMin);
-            knt++;
-          }
-          if (knt > 0) {
-            __syncthreads();
-            xnorm = block_scaled_norm(nx, x, red);
-            nrm = hypot3(alpha.x, alpha.y, xnorm);
-            beta = alpha.x >= 0.0 ? -nrm : nrm;
-          }
-          tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-          scale = recip_smith(make_double2(alpha.x - beta, alpha.y));
-          for (int k = 0; k < knt; k++) beta *= kSafeMin;
-        }
-        __syncthreads();
-        if (!ident) {
-          for (int r = threadIdx.x; r < nx; r += blockDim.x) x[r] = cmul(x[r], scale);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          if (!ident) P[c + c * mp] = make_double2(beta, 0.0);
-          p.tau[j0 + c] = tau;
-          coef = cconj(tau);
-        }
-        __syncthreads();
-        // apply H^H = I - conj(tau) v v^H to panel columns c+1..jb-1
-        if (!ident) {
-          for (int q = c + 1 + warp; q < jb; q += nw) {
-            cplx s = make_double2(0.0, 0.0);
-            for (int r = c + lane; r < mp; r += 32) {
-              cplx v = (r == c) ? make_double2(1.0, 0.0) : P[r + c * mp];
-              s = cadd(s, ccmul(v, P[r + q * mp]));
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-              s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-              s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-            }
-            s = cmul(coef, s);
-            for (int r = c + lane; r < mp; r += 32) {
-              cplx v = (r == c) ? make_double2(1.0, 0.0) : P[r + c * mp];
-              P[r + q * mp] = csub(P[r + q * mp], cmul(v, s));
-            }
-          }
-        }
-        __syncthreads();
-      }
-      // T factor (zlarft forward, columnwise)
-      for (int i = 0; i < jb; i++) {
-        cplx ti = p.tau[j0 + i];
-        // Wsh[l] = -tau_i * sum_r conj(V[r,l]) v_i[r], l < i
-        for (int l = warp; l < i; l += nw) {
-          cplx s = make_double2(0.0, 0.0);
-          for (int r = i + lane; r < mp; r += 32) {
-            cplx vl = P[r + l * mp];  // r > l always (r >= i > l)
-            cplx vi = (r == i) ? make_double2(1.0, 0.0) : P[r + i * mp];
-            s = cadd(s, ccmul(vl, vi));
-          }
-          for (int o = 16; o > 0; o >>= 1) {
-            s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-            s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-          }
-          if (lane == 0) Wsh[l] = cmul(make_double2(-ti.x, -ti.y), s);
-        }
-        __syncthreads();
-        // T[0:i, i] = T[0:i, 0:i] * Wsh
-        for (int l = threadIdx.x; l < i; l += blockDim.x) {
-          cplx s = make_double2(0.0, 0.0);
-          for (int q = l; q < i; q++) s = cadd(s, cmul(Tp[l + q * nb], Wsh[q]));
-          W2sh[l] = s;
-        }
-        __syncthreads();
-        for (int l = threadIdx.x; l < nb; l += blockDim.x) {
-          cplx v = make_double2(0.0, 0.0);
-          if (l < i) v = W2sh[l];
-          else if (l == i) v = ti;
-          Tp[l + i * nb] = v;
-        }
-        __threadfence_block();
-        __syncthreads();
-      }
-      // write the panel back
-      for (int t = threadIdx.x; t < mp * jb; t += blockDim.x) {
-        int r = t % mp, c = t / mp;
-        p.A[(j0 + r) + (long long)(j0 + c) * m] = P[t];
-      }
+      // the panel's columns were brought up to date by this CTA (look-ahead)
+      load_slice(j0, j0, mp, jb);
+      factor_panel(C, mp, jb, Tp, nb, p.tau + j0, W, taus);
+      store_slice(j0, j0, mp, jb);
       __threadfence();
     }
     grid.sync();
-    // trailing update of columns j0+jb .. n-1 in slices of nb columns
+    // trailing update of columns j0+jb .. n-1 in slices of nb columns: slice
+    // 0 (the next panel) by CTA 0, so that it can start on that panel while
+    // the other CTAs update the rest
     const int first = j0 + jb;
     const int nslices = (p.n - first + nb - 1) / nb;
     const cplx* V = p.A + j0 + (long long)j0 * m;  // mp x jb, ld = m
-    for (int sl = blockIdx.x; sl < nslices; sl += gridDim.x) {
-      int c0 = first + sl * nb;
-      int cw = min(nb, p.n - c0);
-      cplx* C = sm;  // mp x cw
-      for (int t = threadIdx.x; t < mp * cw; t += blockDim.x) {
-        int r = t % mp, c = t / mp;
-        C[t] = p.A[(j0 + r) + (long long)(c0 + c) * m];
-      }
-      __syncthreads();
-      apply_block_reflector(mp, jb, cw, V, m, Tp, nb, true, C, mp, Wsh, W2sh);
-      for (int t = threadIdx.x; t < mp * cw; t += blockDim.x) {
-        int r = t % mp, c = t / mp;
-        p.A[(j0 + r) + (long long)(c0 + c) * m] = C[t];
-      }
+    for (int sl = 0; sl < nslices; sl++) {
+      const int owner = (sl == 0 || G == 1) ? 0 : 1 + (sl - 1) % (G - 1);
+      if (owner != (int)blockIdx.x) continue;
+      const int c0 = first + sl * nb;
+      const int cw = min(nb, p.n - c0);
+      load_slice(j0, c0, mp, cw);
+      apply_block_reflector(mp, jb, cw, V, m, Tp, nb, true, C, mp, Vs, Ts, W, W2);
+      store_slice(j0, c0, mp, cw);
       __syncthreads();
     }
     __threadfence();
-    grid.sync();
+    // CTA 0 goes on with the next panel at once; the other CTAs must not
+    // start the next trailing update before that panel is factored, which
+    // the barrier at the top of the next iteration ensures
   }
 }
 
@@ -316,9 +355,12 @@ __global__ void __launch_bounds__(QR_THREADS) qr_factor_kernel(QrParams p) {
 __global__ void __launch_bounds__(QR_THREADS) qr_form_q_kernel(QrParams p, cplx* Q, long long ldq,
                                                                cplx* R, long long ldr) {
   extern __shared__ double smem_d[];
-  cplx* sm = reinterpret_cast<cplx*>(smem_d);
-  __shared__ cplx Wsh[16 * 16], W2sh[16 * 16];
   const int m = p.m, nb = p.nb;
+  cplx* C = reinterpret_cast<cplx*>(smem_d);
+  cplx* Vs = C + (size_t)m * nb;
+  cplx* Ts = Vs + (size_t)QR_CH * nb;
+  cplx* W = Ts + (size_t)nb * nb;
+  cplx* W2 = W + (size_t)nb * nb;
   const int nslices = (p.K + nb - 1) / nb;
   if (R) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)p.K * p.n;
@@ -331,18 +373,18 @@ __global__ void __launch_bounds__(QR_THREADS) qr_form_q_kernel(QrParams p, cplx*
   for (int sl = blockIdx.x; sl < nslices; sl += gridDim.x) {
     const int c0 = sl * nb;
     const int cw = min(nb, p.K - c0);
-    cplx* C = sm;  // m x cw : columns c0.. of the identity
     for (int t = threadIdx.x; t < m * cw; t += blockDim.x) {
       int r = t % m, c = t / m;
       C[t] = make_double2(r == c0 + c ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
-    for (int pi = p.npanel - 1; pi >= 0; pi--) {
+    // H_j only touch rows >= j0: panels that start below the slice's last
+    // column leave its unit columns unchanged
+    for (int pi = min(p.npanel - 1, (c0 + cw - 1) / nb); pi >= 0; pi--) {
       const int j0 = pi * nb;
       const int jb = min(nb, p.K - j0);
-      // H_j only touch rows >= j0; columns c < j0 of E stay unit vectors above
-      apply_block_reflector(m - j0, jb, cw, p.A + j0 + (long long)j0 * m, m,
-                            p.T + (long long)pi * nb * nb, nb, false, C + j0, m, Wsh, W2sh);
+      apply_block_reflector(m - j0, jb, cw, p.A + j0 + (long long)j0 * m, m, p.T + (long long)pi * nb * nb, nb,
+                            false, C + j0, m, Vs, Ts, W, W2);
     }
     for (int t = threadIdx.x; t < m * cw; t += blockDim.x) {
       int r = t % m, c = t / m;
@@ -368,11 +410,11 @@ void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, lo
   char* ws = (char*)scratch.get((size_t)p.npanel * nb * nb * sizeof(cplx) + (size_t)K * sizeof(cplx) + 256);
   p.T = (cplx*)ws;
   p.tau = p.T + (size_t)p.npanel * nb * nb;
-  size_t smem = (size_t)m * nb * sizeof(cplx);
+  const size_t smem = qr_smem_bytes(m, nb);
   static std::atomic<unsigned long long> attr_done{0};
   if (device_needs_setup(attr_done)) {
-    MPSGPU_CUDA(cudaFuncSetAttribute(qr_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    MPSGPU_CUDA(cudaFuncSetAttribute(qr_form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    MPSGPU_CUDA(cudaFuncSetAttribute(qr_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, QR_SMEM_ATTR));
+    MPSGPU_CUDA(cudaFuncSetAttribute(qr_form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, QR_SMEM_ATTR));
     mark_device_done(attr_done);
   }
   int dev = 0, nsm = 148, per_sm = 1;
@@ -402,8 +444,11 @@ void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, lo
 // allocation failure half way through a sweep.
 // For them this variant keeps every byte of its working memory in one
 // file-scope device array: the working copy of A (factored in place), the
-// block-reflector factors T and the scalars tau.  The array is reserved when
-// the library is loaded, on every GPU that loads it, and held until exit.
+// block-reflector factors T and the scalars tau.  CUDA loads a module's
+// device code (and places its __device__ arrays) lazily, on first use in a
+// context, so mpsgpu_create places the array on its device at once
+// (noalloc_qr_prepare below): after a context exists on a GPU, the entry
+// point needs no new device memory there.  The array is held until exit.
 // ---------------------------------------------------------------------------
 
 namespace mpsgpu {
@@ -438,9 +483,9 @@ mpsgpu_status noalloc_scratch_on(int dev, double2** out) {
     g_noalloc_ptr[dev] = static_cast<double2*>(p);
   }
   if (!g_noalloc_attr[dev]) {
-    if (cudaFuncSetAttribute(qr_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+    if (cudaFuncSetAttribute(qr_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, QR_SMEM_ATTR) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(qr_form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+        cudaFuncSetAttribute(qr_form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, QR_SMEM_ATTR) !=
             cudaSuccess)
       return MPSGPU_CUDA_ERROR;
     g_noalloc_attr[dev] = true;
@@ -450,6 +495,15 @@ mpsgpu_status noalloc_scratch_on(int dev, double2** out) {
 }
 
 }  // namespace
+
+// Called by mpsgpu_create with `dev` current: loads this file's module on the
+// device, which places the scratch array, and sets the kernel attributes.
+mpsgpu_status noalloc_qr_prepare(int dev) {
+  if (dev < 0 || dev >= MAX_DEVICES) return MPSGPU_CUDA_ERROR;
+  double2* p = nullptr;
+  return noalloc_scratch_on(dev, &p);
+}
+
 }  // namespace mpsgpu
 
 extern "C" mpsgpu_status mpsgpu_qr_device_noalloc(int m, int n, const double* A, double* Q, double* R,
@@ -479,7 +533,7 @@ extern "C" mpsgpu_status mpsgpu_qr_device_noalloc(int m, int n, const double* A,
   p.tau = p.T + NOALLOC_T_ELEMS;
   if (cudaMemcpyAsync(p.A, A, (size_t)m * n * sizeof(double2), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
     return MPSGPU_CUDA_ERROR;
-  const size_t smem = (size_t)m * NOALLOC_NB * sizeof(double2);
+  const size_t smem = qr_smem_bytes(m, NOALLOC_NB);
   int nsm = 148, per_sm = 1;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qr_factor_kernel, QR_THREADS, smem) != cudaSuccess ||
@@ -492,8 +546,15 @@ extern "C" mpsgpu_status mpsgpu_qr_device_noalloc(int m, int n, const double* A,
     return MPSGPU_CUDA_ERROR;
   int qgrid = std::max(1, std::min((K + NOALLOC_NB - 1) / NOALLOC_NB, nsm));
   if (R && !Q) qgrid = std::max(qgrid, 8);
-  qr_form_q_kernel<<<qgrid, QR_THREADS, smem, s>>>(p, reinterpret_cast<double2*>(Q), m,
-                                                   reinterpret_cast<double2*>(R), K);
-  if (cudaGetLastError() != cudaSuccess) return MPSGPU_CUDA_ERROR;
+  // launched through cudaLaunchKernel, whose return code is this launch's
+  // alone (cudaGetLastError would also report, and clear, an unrelated
+  // earlier error of the calling thread)
+  double2* Qd = reinterpret_cast<double2*>(Q);
+  double2* Rd = reinterpret_cast<double2*>(R);
+  long long ldq = m, ldr = K;
+  void* qargs[] = {&p, &Qd, &ldq, &Rd, &ldr};
+  if (cudaLaunchKernel((const void*)qr_form_q_kernel, dim3(qgrid), dim3(QR_THREADS), qargs, smem, s) !=
+      cudaSuccess)
+    return MPSGPU_CUDA_ERROR;
   return MPSGPU_OK;
 }

@@ -55,6 +55,48 @@ struct TridiagLowest {
     invit(a, b, k, theta - 1e-14 * std::max(normT, 1e-300), 1e-15 * std::max(normT, 1e-300), s);
   }
 
+  // As solve(), with the bracket started below an upper bound `ub` of the
+  // lowest eigenvalue (the lowest Ritz value of the previous step: by
+  // Cauchy interlacing the lowest eigenvalue of T_k is at most that of
+  // T_{k-1}) at a guessed distance `step`, widened until the Sturm count
+  // shows no eigenvalue below it; bisection then needs only the steps that
+  // the bracket's width calls for.  Falls back to the Gershgorin interval.
+  void solve_from(const std::vector<double>& a, const std::vector<double>& b, int k, double ub, double step,
+                  double& theta, std::vector<double>& s, double& normT) {
+    double lo = a[0], hi = a[0];
+    for (int i = 0; i < k; i++) {
+      const double r = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i < k - 1 ? std::fabs(b[i]) : 0.0);
+      lo = std::min(lo, a[i] - r);
+      hi = std::max(hi, a[i] + r);
+    }
+    normT = std::max(std::fabs(lo), std::fabs(hi));
+    double h = std::min(hi, ub + 8e-16 * normT);
+    if (!(std::isfinite(h) && count_below(a, b, k, h) >= 1)) h = hi;
+    double st = std::max(std::fabs(step), 1e-15 * normT);
+    double l = lo;
+    for (int it = 0; it < 64; it++) {
+      const double cand = h - st;
+      if (!(cand > lo)) break;
+      if (count_below(a, b, k, cand) == 0) {
+        l = cand;
+        break;
+      }
+      h = cand;  // still an upper bound
+      st *= 16.0;
+    }
+    for (int it = 0; it < 200; it++) {
+      if (!(h - l > 4e-16 * std::max(std::fabs(l), std::fabs(h)) + 1e-300)) break;
+      const double mid = 0.5 * (l + h);
+      if (mid == l || mid == h) break;
+      if (count_below(a, b, k, mid) >= 1) h = mid;
+      else l = mid;
+    }
+    theta = 0.5 * (l + h);
+    s.assign(k, 1.0);
+    if (k == 1) return;
+    invit(a, b, k, theta - 1e-14 * std::max(normT, 1e-300), 1e-15 * std::max(normT, 1e-300), s);
+  }
+
   // Three steps of inverse iteration on T - shift I from the start vector s
   // (overwritten by the normalised result).
   void invit(const std::vector<double>& a, const std::vector<double>& b, int k, double shift, double tiny,

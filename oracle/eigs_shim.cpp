@@ -40,6 +40,11 @@
 using namespace std;
 using namespace shrt;
 
+// Work counters read by the oracle driver (oracle/ref_driver.cpp): products
+// with the effective Hamiltonian and local eigensolves since program start.
+long long g_shim_products = 0;
+long long g_shim_solves = 0;
+
 namespace {
 
 typedef std::complex<double> cd;
@@ -129,6 +134,7 @@ void tridiag_lowest(const vector<double>& a, const vector<double>& b, int k,
 }
 
 void apply(Multiplier& multi, const vector<cd>& x, vector<cd>& y, int N) {
+  g_shim_products++;
   mwArray in(Indices(N, 1), (const complex_t*)x.data());
   mwArray out;
   multi.product(in, out);
@@ -233,6 +239,7 @@ int solve_into(Multiplier& multi, int nev, bool smallest,
   }
   double lambda;
   vector<cd> x;
+  g_shim_solves++;
   int ret = lanczos_lowest(multi, U, tol, lambda, x);
   int N = multi.getSize();
   Dval.clear();

@@ -729,8 +729,9 @@ def lowest_eigpair(matvec, n: int, x0: np.ndarray, dense=None, tol: float = 1e-1
     x = x / nx if nx > 0 else np.full(n, 1 / math.sqrt(n), dtype=np.complex128)
     m = min(n, max_krylov)
     theta = 0.0
+    V = np.empty((m, n), dtype=np.complex128)  # basis rows, filled in place
     for _ in range(max_restarts):
-        V = [x]
+        V[0] = x
         a, b = [], []
         conv = False
         for j in range(m):
@@ -739,7 +740,7 @@ def lowest_eigpair(matvec, n: int, x0: np.ndarray, dense=None, tol: float = 1e-1
             w = w - a[j] * V[j]
             if j > 0:
                 w = w - b[j - 1] * V[j - 1]
-            Vm = np.array(V)
+            Vm = V[: j + 1]
             for _p in range(2):
                 w = w - Vm.T @ (Vm.conj() @ w)
             beta = float(np.linalg.norm(w))
@@ -752,8 +753,8 @@ def lowest_eigpair(matvec, n: int, x0: np.ndarray, dense=None, tol: float = 1e-1
                 conv = True
                 break
             if j + 1 < m:
-                V.append(w / beta)
-        y = np.array(V[: len(a)]).T @ s
+                V[j + 1] = w / beta
+        y = V[: len(a)].T @ s
         x = y / np.linalg.norm(y)
         if conv:
             break

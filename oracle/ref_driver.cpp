@@ -42,6 +42,9 @@
  *   profile model D eigtol init n  timed sample: n site steps of the ground-state sweep
  *                                  around the chain centre (CPU baseline of the bench)
  *   gauge mps dir out              MPS::gaugeCond(dir, true)          (MPS.cpp:306-364)
+ *   savempo model file             MPO::saveMPO of the model's H     (MPO.cpp:214-231)
+ *   optsum D convtol init out ket re im [ket re im ...]
+ *                                  Contractor::optimizeSum            (Contractor.cpp:2332-2477)
  */
 #include "Contractor.h"
 #include "IsingHamiltonian.h"
@@ -70,7 +73,17 @@
 using namespace std;
 using namespace shrt;
 
+// Counters of the eigensolver shim (oracle/eigs_shim.cpp).
+extern long long g_shim_products;
+extern long long g_shim_solves;
+
 namespace {
+
+double now_s() {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return t.tv_sec + 1e-9 * t.tv_nsec;
+}
 
 mwArray load_array(const char* fn) {
   ifstream in(fn, ios::binary);
@@ -266,9 +279,12 @@ int main(int argc, const char* argv[]) {
     MPS gs;
     gs.importMPS(argv[6]);
     double E0 = 0;
+    double t0 = now_s();
     contractor.findGroundState(m.H(), D, &E0, gs);
+    double t1 = now_s();
     gs.exportMPS(argv[7]);
-    print_json({{"E0", E0}});
+    print_json({{"E0", E0}, {"seconds", t1 - t0}, {"products", (double)g_shim_products},
+                {"site_solves", (double)g_shim_solves}});
   } else if (cmd == "exc") {
     Model m = make_model(argv[2]);
     int D = atoi(argv[3]);
@@ -278,13 +294,21 @@ int main(int argc, const char* argv[]) {
     gs.importMPS(argv[6]);
     exc.importMPS(argv[7]);
     double E0 = 0, E1 = 0;
+    double t0 = now_s();
     contractor.findGroundState(m.H(), D, &E0, gs);
+    double t1 = now_s();
+    long long p0 = g_shim_products, s0 = g_shim_solves;
+    gs.exportMPS(argv[8]);
     vector<MPS*> levels(1, &gs);
     contractor.findNextExcitedState(m.H(), D, levels, &E1, exc);
-    gs.exportMPS(argv[8]);
+    double t2 = now_s();
     exc.exportMPS(argv[9]);
     complex_t ov = contractor.contract(exc, gs);
-    print_json({{"E0", E0}, {"E1", E1}, {"gap", E1 - E0}, {"overlap_abs", abs(ov)}});
+    print_json({{"E0", E0}, {"E1", E1}, {"gap", E1 - E0}, {"overlap_abs", abs(ov)},
+                {"gs_seconds", t1 - t0}, {"exc_seconds", t2 - t1},
+                {"gs_products", (double)p0}, {"gs_site_solves", (double)s0},
+                {"exc_products", (double)(g_shim_products - p0)},
+                {"exc_site_solves", (double)(g_shim_solves - s0)}});
   } else if (cmd == "imag") {
     Model m = make_model(argv[2]);
     int D = atoi(argv[3]);
@@ -367,6 +391,29 @@ int main(int argc, const char* argv[]) {
     else t.applyExactly(U, dagger, dir);
     t.exportMPS(argv[9]);
     print_json({{"bond", (double)t.getBond()}, {"normfact", t.getNormFact()}});
+  } else if (cmd == "savempo") {
+    Model m = make_model(argv[2]);
+    m.H().saveMPO(argv[3]);
+    print_json({{"L", (double)m.L}});
+  } else if (cmd == "optsum") {
+    int D = atoi(argv[2]);
+    contractor.setConvTol(atof(argv[3]));
+    MPS init;
+    init.importMPS(argv[4]);
+    vector<MPS*> own;
+    vector<const MPS*> kets;
+    vector<complex_t> beta;
+    for (int a = 6; a + 2 < argc; a += 3) {
+      MPS* k = new MPS();
+      k->importMPS(argv[a]);
+      own.push_back(k);
+      kets.push_back(k);
+      beta.push_back((complex_t){atof(argv[a + 1]), atof(argv[a + 2])});
+    }
+    contractor.optimizeSum(kets, beta, init, D);
+    init.exportMPS(argv[5]);
+    print_json({{"normfact", init.getNormFact()}, {"terms", (double)kets.size()}});
+    for (auto* k : own) delete k;
   } else if (cmd == "gauge") {
     MPS s;
     s.importMPS(argv[2]);

@@ -7,6 +7,7 @@ small .npz/.json files.  Needs the reference tree (only in the build
 container); the fixtures themselves travel with the repository.
 
     make -C oracle && python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --io-optsum   # only io_optsum.npz
 """
 from __future__ import annotations
 
@@ -39,7 +40,39 @@ def rand_c(rng, shape):
     return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
 
 
+def io_and_optsum(tmp: str) -> None:
+    """MPO files written by MPO::saveMPO (bytes, for byte-exact interop) and
+    Contractor::optimizeSum results (state vectors, normfact) into
+    io_optsum.npz; nothing else is touched."""
+    out = {}
+    for name, spec in [("ising6", "ising:6:1:1:0.3"), ("schwinger6", "schwinger:6:2.5:100:0:0")]:
+        fn = os.path.join(tmp, name + ".mpo")
+        run("savempo", spec, fn)
+        with open(fn, "rb") as f:
+            out[f"mpofile_{name}"] = np.frombuffer(f.read(), dtype=np.uint8)
+    # unit-norm kets: with norms ~1e4 the reference's distance (a difference
+    # of terms ~|M|^2) is rounding noise and its increase test exits 212
+    k1, k2 = os.path.join(tmp, "k1.mps"), os.path.join(tmp, "k2.mps")
+    for fn, seed in ((k1, 41), (k2, 42)):
+        m = mo.random_mps(8, 2, 6, seed)
+        m.sites[0] = m.sites[0] / np.linalg.norm(mo.mps_to_vector(m))
+        mo.write_mps(fn, m)
+    for tag, D, terms in [("sum2_D4", 4, [(k1, 0.7, 0.2), (k2, -0.3, 0.5)]), ("one_D3", 3, [(k1, 1.0, 0.0)])]:
+        fi, fo = os.path.join(tmp, "oi.mps"), os.path.join(tmp, "oo.mps")
+        mo.write_mps(fi, mo.random_mps(8, 2, D, 43))
+        args = [a for t in terms for a in t]
+        r = run("optsum", D, 1e-10, fi, fo, *args)
+        res = mo.read_mps(fo)
+        out[f"optsum_{tag}_vec"] = mo.mps_to_vector(res)
+        out[f"optsum_{tag}_normfact"] = np.array(r["normfact"])
+        out[f"optsum_{tag}_dims"] = np.array([a.shape for a in res.sites])
+    np.savez_compressed(os.path.join(HERE, "io_optsum.npz"), **out)
+
+
 def main() -> None:
+    if len(sys.argv) > 1 and sys.argv[1] == "--io-optsum":
+        io_and_optsum(tempfile.mkdtemp())
+        return
     tmp = tempfile.mkdtemp()
     golden = {}
 
@@ -165,6 +198,7 @@ def main() -> None:
     r = run("opterr", "ising:8:1:1.1:0.2", 0.05, 0, 6, fc)
     golden["opterr_ising_L8_D6_state9_ureal005"] = [r["errN"], r["errT"], r["normfact"]]
 
+    io_and_optsum(tmp)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print(json.dumps({k: (v if not isinstance(v, list) else v[:3]) for k, v in golden.items()}, indent=1))

@@ -78,3 +78,62 @@ def test_cancel_queued_and_running():
     assert res[queued_id]["status"] == CANCELLED
     assert res[long_id]["status"] == CANCELLED
     assert res[long_id]["t_end"] - res[long_id]["t_start"] < 30
+
+
+def test_first_fit_admission_passes_a_large_head():
+    """A request too large for the memory left waits while smaller ones that
+    fit start in the free slots (first fit, not head-of-line blocking)."""
+    from mpsdyn_b200 import capi
+    with capi.Server(0, slots=4, hbm_budget_bytes=1) as tmp:
+        big = tmp.footprint(ISING, 60, 128)
+        small = tmp.footprint(ISING, 16, 8)
+    with capi.Server(0, slots=4, hbm_budget_bytes=1) as tmp:
+        mid = tmp.footprint(ISING, 100, 64)
+    assert mid > 2 * small and big + small >= mid
+    budget = big + 2 * small  # room for the big one only when little else runs
+    with capi.Server(0, slots=4, hbm_budget_bytes=budget) as srv:
+        first = srv.submit(ISING, 100, 64, 1.0, 1.0, 0.0, 5)   # occupies memory for a while
+        big_id = srv.submit(ISING, 60, 128, 1.0, 1.0, 0.0, 6)  # cannot start next to it
+        small_ids = [srv.submit(ISING, 16, 8, 1.0, 0.9, 0.0, 20 + i) for i in range(2)]
+        res = {r["id"]: r for r in _wait(srv, 4, timeout=600)}
+    assert all(r["status"] == 0 for r in res.values())
+    # the small requests started before the large one that was queued ahead of them
+    assert all(res[i]["t_start"] < res[big_id]["t_start"] for i in small_ids)
+    assert res[first]["status"] == 0
+
+
+def test_time_evolution_request_alone_and_in_the_mix(tmp_path):
+    """A served quench gives the same observables alone and next to other
+    requests, equal to the library called directly, and writes its final
+    state to the requested file."""
+    from mpsdyn_b200 import capi
+    L, D, g, steps = 16, 16, 1.3, 6
+    with capi.Server(0, slots=1) as srv:
+        rid, sx_a, ent_a = srv.submit_evolution(L, D, 1.0, g, 0.1, steps, 0.05)
+        alone = _wait(srv, 1)[0]
+    out = tmp_path / "final.mps"
+    with capi.Server(0, slots=3) as srv:
+        ids = [srv.submit(ISING, 30, 24, 1.0, 0.8, 0.1, 50)]
+        rid2, sx_b, ent_b = srv.submit_evolution(L, D, 1.0, g, 0.1, steps, 0.05, result_file=out)
+        ids.append(srv.submit(ISING, 24, 16, 1.0, 1.1, 0.0, 51))
+        res = {r["id"]: r for r in _wait(srv, 3)}
+    assert alone["status"] == 0 and res[rid2]["status"] == 0
+    np.testing.assert_array_equal(sx_a, sx_b)
+    np.testing.assert_array_equal(ent_a, ent_b)
+    assert res[rid2]["energy"] == alone["energy"]
+    # against the library's own calls (the quench loop of the batched workload)
+    with capi.Context(0) as c:
+        U = c.mpo_ising_evolution(L, 1.0, g, 0.1, 0.05, False)
+        st = c.mps_product(L, 2, 1)
+        o = c.options(convtol=1e-10)
+        for k in range(steps):
+            aux = st.copy()
+            c.optimize(U, aux, st, D, o)
+            aux.free()
+            assert c.expectation_local(st, mo.SIGX)[L // 2] == sx_a[k]
+            st.gauge("L")
+            assert c.entropy(st, L // 2) == ent_a[k]
+        saved = c.mps_import(out)
+        H = c.mpo_ising(L, 1.0, g, 0.1)
+        e = c.contract(saved, H, saved).real / c.contract(saved, None, saved).real
+        assert abs(e - alone["energy"]) <= 1e-10 * abs(e)
