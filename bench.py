@@ -41,12 +41,6 @@ WORKLOAD = dict(workload="schwinger_N100_D128_gs+gap", N=100, x=100.0, mg=0.125,
 MU = 2 * WORKLOAD["mg"] * np.sqrt(WORKLOAD["x"])
 METRIC = "DMRG solves/s (Schwinger N=100 D=128, E0 + first gap, |dE/E|<=1e-10)"
 UNIT = "solves/s"
-# Algorithmic flops of one FP64 solve of this workload as counted by the
-# library (GS + excited state: 19 699 + 21 187 products with the
-# thick-restart Lanczos, the work a complete-precision solve does); both the
-# reference arm and the CPU baseline of the GPU arm turn a measured CPU flop
-# rate into solves/s with it.
-FLOPS_PER_SOLVE_FP64 = 2.14e13
 
 
 def parse():
@@ -55,14 +49,22 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="mpsgpu", choices=["mpsgpu", "reference"])
-    p.add_argument("--cpu-sample-sites", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ref-max-sites", type=int, default=0,
+                   help="reference arm / CPU baseline: site steps per process (0 = the whole block)")
+    p.add_argument("--ref-iter-cap", type=int, default=0,
+                   help="tests only: cap the reference eigensolver (the line is then not a measurement)")
     p.add_argument("--batch", type=int, default=8, help="concurrent solves per step")
     p.add_argument("--plain", type=int, default=1, help="also time one solve alone (the plain form)")
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="mixed: split-precision products until the energy settles, then FP64")
-    p.add_argument("--workload", default="schwinger", choices=["schwinger", "grouped", "serving", "quench"],
-                   help="schwinger: the headline line; the others time the secondary workloads")
+    p.add_argument("--workload", default="schwinger",
+                   choices=["schwinger", "grouped", "serving", "quench", "sample", "split_gemm"],
+                   help="schwinger: the headline line; grouped/serving/quench: the secondary workloads; "
+                        "sample/split_gemm: bounded cases for profilers")
+    p.add_argument("--sites", type=int, default=40, help="sample: chain length of the bounded sweep sample")
+    p.add_argument("--rounds", type=int, default=1, help="sample: half-sweeps of the bounded sweep sample")
+    p.add_argument("--mnk", default="4096,4096,2048", help="split_gemm: m,n,k")
     p.add_argument("--instances", type=int, default=512, help="grouped: matvec instances")
     p.add_argument("--requests", type=int, default=48, help="serving: requests in the stream")
     p.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate, req/s")
@@ -122,51 +124,110 @@ class ClockSampler:
 # CPU baseline: the reference compiled from source (oracle/_ref), bounded sample
 # ---------------------------------------------------------------------------
 
-def reference_sample(nsites: int, procs: int, iters: int = 80) -> dict:
-    """Run `procs` single-threaded reference processes, each timing `nsites`
-    site steps (eigensolve + QR gauge + environment update) of the ground-state
-    sweep at the chain centre; returns the aggregate flop rate.  Each local
-    eigensolve is capped at `iters` Lanczos iterations, the library's average
-    per site solve on this workload (47185 products over 596 site solves)."""
+def reference_counts() -> dict:
+    """Products and wall time of the reference's complete solve of this
+    workload (findGroundState + findNextExcitedState, one core), from the
+    pinned reference run (tests/golden/golden.json, written by
+    tests/golden/make_golden_large.py); None when not generated."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+            t = json.load(f).get("reference_timing", {})
+        return {"gs": t["schwinger_N100_D128_gs"], "exc": t["schwinger_N100_D128_exc"]}
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def reference_sample(procs: int, max_sites: int = 0, iter_cap: int = 0) -> dict:
+    """One half-sweep of the reference's ground-state sweep of this workload
+    (site steps 0..N-2: eigensolve with no iteration cap, QR gauge move,
+    environment update), cut into `procs` contiguous blocks of sites, each
+    timed by one single-threaded process of oracle/_ref (the reference
+    compiled from source; eigensolver shim above the dense branch); with
+    max_sites > 0 every block keeps only its first max_sites sites (a shorter
+    sample spread over the chain).  Returns the products, the core-seconds
+    and the wall time."""
     from oracle import mps_oracle as mo  # the checker/baseline only
     drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
     if not os.path.exists(drv):
         raise FileNotFoundError("oracle/_ref/ref_driver not built (make -C oracle)")
     tmp = tempfile.mkdtemp()
     fn = os.path.join(tmp, "init.mps")
-    mo.write_mps(fn, mo.random_mps(WORKLOAD["N"], 2, WORKLOAD["D"], WORKLOAD["seed_gs"]))
-    env = dict(os.environ, OPENBLAS_NUM_THREADS="1", ASAN_OPTIONS="detect_leaks=0",
-               MPSDYN_SHIM_MAX_ITERS=str(iters))
-    model = f"schwinger:{WORKLOAD['N']}:{MU}:{WORKLOAD['x']}:0:0"
+    N = WORKLOAD["N"]
+    mo.write_mps(fn, mo.random_mps(N, 2, WORKLOAD["D"], WORKLOAD["seed_gs"]))
+    env = dict(os.environ, OPENBLAS_NUM_THREADS="1", ASAN_OPTIONS="detect_leaks=0")
+    env.pop("MPSDYN_SHIM_MAX_ITERS", None)
+    if iter_cap > 0:  # tests of the arm's plumbing only: the measured sample is never capped
+        env["MPSDYN_SHIM_MAX_ITERS"] = str(iter_cap)
+    model = f"schwinger:{N}:{MU}:{WORKLOAD['x']}:0:0"
+    procs = max(1, min(procs, N - 1))
+    cuts = [round(i * (N - 1) / procs) for i in range(procs + 1)]
     t0 = time.time()
-    ps = [subprocess.Popen([drv, "profile", model, str(WORKLOAD["D"]), "0", fn, str(nsites)],
+    def nsites(i):
+        n = cuts[i + 1] - cuts[i]
+        return min(n, max_sites) if max_sites > 0 else n
+    ps = [subprocess.Popen([drv, "profile", model, str(WORKLOAD["D"]), "0", fn, str(nsites(i)), str(cuts[i])],
                            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, env=env)
-          for _ in range(procs)]
+          for i in range(procs) if cuts[i + 1] > cuts[i]]
     outs = [p.communicate()[0] for p in ps]
     wall = time.time() - t0
     res = [json.loads([l for l in o.splitlines() if l.startswith("{")][-1]) for o in outs]
-    rate = sum(r["flops"] / r["seconds"] for r in res)
-    return {"flop_rate": rate, "per_process_seconds": float(np.mean([r["seconds"] for r in res])),
-            "wall": wall, "procs": procs, "nsites": nsites, "iterations": res[0]["iterations"]}
+    return {"products": sum(r["iterations"] for r in res), "core_seconds": sum(r["seconds"] for r in res),
+            "wall": wall, "procs": len(res), "sites": sum(r["nsites"] for r in res),
+            "max_process_seconds": max(r["seconds"] for r in res)}
+
+
+def reference_rate(procs: int, max_sites: int = 0, iter_cap: int = 0) -> tuple:
+    """Solves/s of the reference on `procs` cores (independent solves, one
+    per core) and the description of how it was obtained."""
+    s = reference_sample(procs, max_sites, iter_cap)
+    per_core = s["products"] / s["core_seconds"]  # products per core-second, site-step overheads included
+    rc = reference_counts()
+    if rc:
+        # the excited-state products are Hermitian multipliers: two products each
+        products = rc["gs"]["products"] + 2 * rc["exc"]["products"]
+        src = (f"the reference's own counts of its complete solve (ground state {rc['gs']['products']} + "
+               f"2 x {rc['exc']['products']} Hermitian excited-state products, pinned run of "
+               f"{rc['gs']['seconds'] + rc['exc']['seconds']:.0f} s on one core of the build host)")
+    else:
+        products = 2 * 19699 + 2 * 21187  # fallback: the library's FP64 counts (Lanczos, same tolerance)
+        src = "the library's FP64 product counts (the reference's pinned counts were not available)"
+    t_core = products / per_core
+    value = s["procs"] / t_core
+    part = ("one uncapped half-sweep" if max_sites <= 0 else
+            f"the first {max_sites} site step(s) of each block of one uncapped half-sweep")
+    sample = (f"{part} (site steps 0..{WORKLOAD['N'] - 2}, edges included: eigensolve, QR "
+              f"gauge move, environment update) of the reference compiled from source (oracle/_ref), split "
+              f"into {s['procs']} contiguous blocks timed by {s['procs']} single-threaded processes "
+              f"({s['products']} products, {s['core_seconds']:.1f} core-s, {s['wall']:.1f} s wall); "
+              f"extrapolated to a complete solve (one per core) by {src}")
+    return value, sample, {"products_sample": s["products"], "core_seconds_sample": s["core_seconds"],
+                           "products_per_solve": products, "core_seconds_per_solve": t_core,
+                           "wall_s": s["wall"]}
 
 
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     procs = min(os.cpu_count() or 1, 64)
-    s = reference_sample(args.cpu_sample_sites, procs)
-    fps = FLOPS_PER_SOLVE_FP64
-    per_step = fps / s["flop_rate"]
-    value = 1.0 / per_step
-    sample = (f"{args.cpu_sample_sites} centre site step(s) of the ground-state sweep per process "
-              f"(reference eigensolver shim, QR gauge, environment update), {procs} single-threaded "
-              f"processes; solves/s = aggregate flop rate / {fps:.3g} flops per solve")
+    # every step is one sample; the whole run stays within a few minutes: a
+    # full half-sweep per step for up to 3 steps, shorter blocks beyond
+    full = -(-(WORKLOAD["N"] - 1) // procs)
+    max_sites = args.ref_max_sites or (0 if args.steps <= 3 else max(1, full * 3 // args.steps))
+    vals, last = [], None
+    for _ in range(max(1, args.steps)):  # no warm-up: nothing on the CPU path warms up
+        v, sample, detail = reference_rate(procs, max_sites, args.ref_iter_cap)
+        if args.ref_iter_cap > 0:
+            sample += f" [eigensolver capped at {args.ref_iter_cap} products: plumbing test, not a measurement]"
+        vals.append(v)
+        last = (sample, detail)
+    value = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
+            "steps": len(vals), "warmup": 0, "warmup_requested": args.warmup, "ms_per_step": 1e3 / value * procs,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic (seeded complex Gaussian initial MPS)",
             "config": {**WORKLOAD, "parallelism": f"replicas{world}", "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": last[0]},
+            "detail": last[1],
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -175,14 +236,32 @@ def run_reference(args, rank: int, world: int) -> None:
 # GPU arm
 # ---------------------------------------------------------------------------
 
-def bf16_peak() -> tuple:
-    """Dense BF16 tensor throughput measured on this pool (MEASURED_PEAKS.json,
-    burst figure), else the fallback measurement; returns (TFLOP/s, source)."""
+def measured_peaks() -> dict:
+    """HBM copy bandwidth and dense BF16 tensor throughput measured on this
+    pool (MEASURED_PEAKS.json, driver-written), else the earlier measurement
+    on this pool (fallback), with their sources."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return float(json.load(f)["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops (measured, burst)"
+            m = json.load(f)
+        return {"hbm_gbs": float(m["hbm_gbs"]), "hbm_src": "MEASURED_PEAKS.json hbm_gbs (measured)",
+                "bf16": float(m["bf16_tflops"]), "bf16_sustained": float(m.get("bf16_tflops_sustained",
+                                                                              m["bf16_tflops"])),
+                "bf16_src": "MEASURED_PEAKS.json bf16_tflops_sustained (measured)"}
     except Exception:
-        return 1590.0, "fallback 1.59 PFLOP/s (earlier measurement on this pool)"
+        return {"hbm_gbs": 6650.0, "hbm_src": "fallback 6.65 TB/s (earlier measurement on this pool)",
+                "bf16": 1590.0, "bf16_sustained": 1400.0,
+                "bf16_src": "fallback 1.4 PFLOP/s sustained (earlier measurement on this pool)"}
+
+
+def bf16_peak() -> tuple:
+    """Burst BF16 peak (for a kernel timed alone) and its source."""
+    p = measured_peaks()
+    return p["bf16"], p["bf16_src"].replace("_sustained", "").replace("sustained", "burst")
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum per launch from ncu captures of
+# the same shapes (profiles/), None until captured
+KERNEL_TRAFFIC = {"gemm_fp64_dmma": None, "gemm_split_tcgen05": None, "lanczos_step": None, "qr": None}
 
 
 def fp64_gemm_peak(torch) -> float:
@@ -337,38 +416,47 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     e2e_total = allreduce(float(sum(e2e_ms)), torch.distributed.ReduceOp.MAX if dist else None)
     e2e_value = solves / (e2e_total * 1e-3)
 
-    # ---- the same batch in FP64 throughout (the comparison of the mixed
-    # form): same seeds, so the energies compare instance by instance ----
-    fp64 = None
-    if mixed:
+    # ---- comparison arms, same seeds: the batch in FP64 throughout, and in
+    # FP64 with the mixed form's schedule of tolerances (precision 2), which
+    # splits mixed / FP64 into what the schedule saves and what the tensor
+    # cores save ----
+    def batch_arm(precision):
+        o = ctxs[0].options(convtol=W["convtol"], precision=precision)
         barrier()
-        spans64 = []
-        energies64 = []
+        spans_a, energies_a = [], []
         for _ in range(args.steps):
             flush_l2()
-            span, _ = run_batch(lambda i: solve_resident(i, opts64))
-            spans64.append(span)
-            energies64.append([(r["E0"], r["E1"]) for r in results])
-        t64 = allreduce(float(sum(spans64)), torch.distributed.ReduceOp.MAX if dist else None)
+            span, _ = run_batch(lambda i: solve_resident(i, o))
+            spans_a.append(span)
+            energies_a.append([(r["E0"], r["E1"]) for r in results])
+        t = allreduce(float(sum(spans_a)), torch.distributed.ReduceOp.MAX if dist else None)
         dE = max(max(abs(a[0] - b[0]) / abs(b[0]), abs(a[1] - b[1]) / abs(b[1]))
-                 for sa, sb in zip(energies, energies64) for a, b in zip(sa, sb))
-        fp64 = {"value": solves / (t64 * 1e-3), "ms_per_step": t64 / args.steps,
-                "max_rel_dE_mixed_vs_fp64": dE}
+                 for sa, sb in zip(energies, energies_a) for a, b in zip(sa, sb))
+        return {"value": solves / (t * 1e-3), "ms_per_step": t / args.steps, "max_rel_dE_vs_line": dE,
+                "products_per_solve": results[0]["gs"]["matvecs"] + results[0]["exc"]["matvecs"]}
 
-    # ---- the plain form: one FP64 solve alone on the GPU, with the library's
-    # GEMM profiler on (events around 1 in 32 GEMM launches of its stream):
-    # alone on the device, a launch's event time is its own duration ----
-    plain_ms, prof = None, None
-    if args.plain:
+    fp64 = fp64_sched = None
+    if mixed:
+        fp64 = batch_arm(0)
+        fp64_sched = batch_arm(2)
+
+    # ---- single solves alone on the GPU with the library's kernel profiler
+    # on (events around 1 in 32 launches of each kernel class): the plain
+    # FP64 form, and the mixed form of the line ----
+    def profiled_single(o):
         flush_l2()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ctxs[0].profile_begin()
         ev0.record(exts[0])
-        solve_resident(0, opts64)
+        solve_resident(0, o)
         ev1.record(exts[0])
         ev1.synchronize()
         prof = ctxs[0].profile_end()
-        plain_ms = ev0.elapsed_time(ev1)
+        r = results[0]
+        return ev0.elapsed_time(ev1), prof, r
+
+    plain_ms, prof64, r64 = profiled_single(opts64) if args.plain else (None, None, None)
+    mixed_ms, profmx, rmx = profiled_single(opts) if (args.plain and mixed) else (None, None, None)
 
     if rank != 0:
         for c in ctxs:
@@ -377,44 +465,58 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             dist.destroy_process_group()
         return
 
-    # ---- roofline of the dominant kernel (the DMMA complex GEMM) ----
-    peak = fp64_gemm_peak(torch)
-    gemm_ms = prof["gemm_ms"] if prof else 0.0
-    gemm_flops = prof["gemm_flops"] if prof else 0.0
-    gemm_tflops = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else 0.0
-    s_gs, s_ex = stats["gs"], stats["exc"]
-    flops_per_solve = s_gs["flops"] + s_ex["flops"]
-    roofline = {"bound": "tensor", "achieved": gemm_tflops, "peak": peak, "unit": "TFLOP/s",
-                "frac": gemm_tflops / peak if peak else None,
-                # dram__bytes_read.sum + dram__bytes_write.sum of the dominant
-                # launch shape (M=640 N=256 K=128), one ncu capture
-                # (profiles/zgemm_dmma_schwinger_N100_D128.md)
-                "traffic": 1.85e6, "traffic_unit": "bytes per launch",
-                "kernel": "zgemm_dmma_kernel (complex FP64, mma.sync m8n8k4 f64)",
-                "peak_source": "cuBLAS complex128 GEMM 4096^3 measured in this run (FP64 tensor pipe)",
-                "note": ("achieved = sampled GEMM flops / their summed event time, one solve alone "
-                         "(the plain form); the batch overlaps launches of 8 streams"),
-                # 1 in 32 GEMM launches is sampled: x32 estimates all GEMM time
-                "gemm_share_of_plain_solve": (32.0 * gemm_ms / plain_ms) if prof and plain_ms else None,
-                "all_kernels_tflops_batch": flops_per_solve * args.steps * B / (sum(spans) * 1e-3) / 1e12}
+    # ---- roofline of the dominant kernels, from the profiled single solves ----
+    peak64 = fp64_gemm_peak(torch)
+    peaks = measured_peaks()
+
+    def kernel_table(prof, total_ms):
+        out = {}
+        for name, k in (prof or {}).get("kernels", {}).items():
+            if not k["calls"] or k["ms"] <= 0:
+                continue
+            rate = k["work"] / (k["ms"] * 1e-3)
+            if name == "lanczos_step":
+                ach, pk, unit, bound, src = rate / 1e9, peaks["hbm_gbs"], "GB/s", "hbm", peaks["hbm_src"]
+            elif name == "gemm_split_tcgen05":
+                ach, pk, unit, bound, src = rate / 1e12, peaks["bf16_sustained"], "TFLOP/s", "tensor", peaks["bf16_src"]
+            else:
+                ach, pk, unit, bound = rate / 1e12, peak64, "TFLOP/s", "tensor"
+                src = "cuBLAS complex128 GEMM 4096^3 measured in this run (FP64 tensor pipe)"
+            out[name] = {"bound": bound, "achieved": ach, "peak": pk, "unit": unit, "frac": ach / pk,
+                         "peak_source": src, "sampled_launches": k["calls"],
+                         "share_of_solve": 32.0 * k["ms"] / total_ms if total_ms else None}
+        return out
+
+    table64 = kernel_table(prof64, plain_ms)
+    tablemx = kernel_table(profmx, mixed_ms)
+
+    def dominant(table, note):
+        if not table:
+            return None
+        name = max(table, key=lambda n: table[n]["share_of_solve"] or 0.0)
+        d = dict(table[name])
+        d.update(kernel=name, traffic=KERNEL_TRAFFIC.get(name), traffic_unit="bytes per launch", note=note)
+        return d
+
+    roofline = dominant(tablemx if mixed else table64,
+                        "achieved = sampled launches' algorithmic work / their summed CUDA-event time, one solve "
+                        "of the line's precision alone on the GPU; lanczos_step bytes: basis read twice + "
+                        "work vector traffic (the basis of one solve, 33 MB, is L2-resident)")
 
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
             procs = min(os.cpu_count() or 1, 64)
-            s = reference_sample(args.cpu_sample_sites, procs)
-            cv = s["flop_rate"] / FLOPS_PER_SOLVE_FP64
-            cpu = {"value": cv, "unit": UNIT, "cores": procs, "kind": "reference",
-                   "sample": (f"{args.cpu_sample_sites} centre site step(s) of the ground-state sweep per "
-                              f"process (oracle/_ref: reference compiled from source, eigensolver shim), "
-                              f"{procs} single-threaded processes, {s['per_process_seconds']:.1f} s each; "
-                              f"solves/s = aggregate flop rate / {FLOPS_PER_SOLVE_FP64:.3g} flops per FP64 solve")}
+            cv, sample, detail = reference_rate(procs, args.ref_max_sites)
+            cpu = {"value": cv, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample,
+                   "detail": detail}
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
     lat_s = np.array(lat) * 1e-3
     e0s = [e for step in energies for e in step]
     plain_rate = 1e3 / plain_ms if plain_ms else None
+    s_gs, s_ex = stats["gs"], stats["exc"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -431,8 +533,16 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         "plain_single_solve_ms": plain_ms,
         "plain_fp64_solves_per_s": plain_rate,
         "vs_plain_fp64": (value / plain_rate) if plain_rate else None,
+        "mixed_single_solve_ms": mixed_ms,
         "fp64_batched": fp64,
+        "fp64_batched_mixed_schedule": fp64_sched,
+        "attribution": ({"schedule": fp64_sched["value"] / fp64["value"],
+                         "tensor_cores": value / fp64_sched["value"],
+                         "concurrency": fp64["value"] / plain_rate if plain_rate else None}
+                        if fp64 and fp64_sched else None),
         "roofline": roofline,
+        "kernels_mixed_single": tablemx,
+        "kernels_fp64_single": table64,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
@@ -653,6 +763,57 @@ def run_quench(args) -> None:
         sys.exit(1)
 
 
+def run_sample(args) -> None:
+    """A bounded sample of the headline sweep for profilers: the ground-state
+    sweep of the Schwinger chain (x = 100, m/g = 0.125, seed-1 initial MPS,
+    convergence 1e-10) on --sites sites with D = 128, stopped after --rounds
+    half-sweeps (the library returns MPSGPU_NOT_CONVERGED at the round limit,
+    which ends the sample), in --precision.  With 40 sites, 26 bulk sites
+    have the (128, 5, 128) shapes of the 100-site chain, so the kernel mix per
+    site step is the headline's while the launch count stays small enough for
+    a profiler that slows every launch down."""
+    from mpsdyn_b200 import capi
+    with capi.Context(0) as ctx:
+        H = ctx.mpo_schwinger(args.sites, MU, WORKLOAD["x"])
+        psi = ctx.mps_random(args.sites, 2, WORKLOAD["D"], 1)
+        o = ctx.options(convtol=1e-10, max_rounds=args.rounds, precision=1 if args.precision == "mixed" else 0)
+        l0 = ctx.launches
+        t0 = time.perf_counter()
+        status = "converged"
+        try:
+            ctx.find_ground_state(H, WORKLOAD["D"], psi, 0.0, o)
+        except capi.MpsgpuError as e:
+            if e.status != 2:  # anything but the round limit is a failure
+                raise
+            status = "round limit"
+        ctx.synchronize()
+        print(json.dumps({"sample": f"schwinger N={args.sites} D={WORKLOAD['D']}, {args.rounds} half-sweep(s), "
+                                    f"{args.precision}", "status": status, "launches": ctx.launches - l0,
+                          "seconds": time.perf_counter() - t0}), flush=True)
+
+
+def run_split_gemm(args) -> None:
+    """One split-precision complex GEMM C = A B (seeded complex Gaussian A,
+    B) through mpsgpu_zgemm_split, timed over --steps runs with CUDA events,
+    with its largest entrywise error relative to |A||B| on a 64 x 64 corner."""
+    from mpsdyn_b200 import capi
+    m, n, k = (int(v) for v in args.mnk.split(","))
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
+    Bm = rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))
+    with capi.Context(0) as ctx:
+        Cm, t_all, t_mma = capi.zgemm_split(ctx, A, Bm, repeats=args.steps)
+    c = min(64, m, n)
+    ref = A[:c] @ Bm[:, :c]
+    rel = float(np.max(np.abs(Cm[:c, :c] - ref) / (np.abs(A[:c]) @ np.abs(Bm[:, :c]))))
+    fl = 8.0 * m * n * k
+    out = {"m": m, "n": n, "k": k, "max_rel_error_corner": rel}
+    if args.steps:
+        out.update(ms_total=t_all, ms_mma=t_mma, bf16_tflops_mma=6 * fl / (t_mma * 1e-3) / 1e12,
+                   fp64_equivalent_tflops_mma=fl / (t_mma * 1e-3) / 1e12)
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -667,6 +828,10 @@ def main():
         run_serving(args)
     elif args.workload == "quench":
         run_quench(args)
+    elif args.workload == "sample":
+        run_sample(args)
+    elif args.workload == "split_gemm":
+        run_split_gemm(args)
     else:
         run_gpu(args, rank, world, local_rank)
 

@@ -119,6 +119,13 @@ mpsgpu_status mpsgpu_get_stream(mpsgpu_context* ctx, void** stream);
 mpsgpu_status mpsgpu_profile_begin(mpsgpu_context* ctx);
 mpsgpu_status mpsgpu_profile_end(mpsgpu_context* ctx, double* gemm_ms, double* gemm_flops,
                                  long long* gemm_calls);
+/* After mpsgpu_profile_end: the same per kernel class (arrays of 4, each
+ * may be null): 0 complex FP64 GEMMs on the DMMA pipe, 1 split-precision
+ * GEMMs on tcgen05 (work = BF16 tensor flops), 2 the fused Lanczos step
+ * (work = algorithmic bytes), 3 Householder QR (flops).  Sampled launches:
+ * one in 32 of each class; ms their summed device time, work their summed
+ * algorithmic work. */
+mpsgpu_status mpsgpu_profile_kernels(mpsgpu_context* ctx, double* ms, double* work, long long* calls);
 
 /* ---- MPO (replaces MPO / Operator storage, src/core/headers/MPO.h:33-176) --
  * dims[4k..4k+3] = (du, Dl, dd, Dr) of operator k; data[k] its column-major

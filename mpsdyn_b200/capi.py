@@ -21,7 +21,7 @@ STATUS = {
 EXPORTS = [
     "mpsgpu_default_options", "mpsgpu_create", "mpsgpu_destroy", "mpsgpu_status_string",
     "mpsgpu_last_error", "mpsgpu_launch_count", "mpsgpu_synchronize", "mpsgpu_get_stream",
-    "mpsgpu_profile_begin", "mpsgpu_profile_end", "mpsgpu_mpo_upload",
+    "mpsgpu_profile_begin", "mpsgpu_profile_end", "mpsgpu_profile_kernels", "mpsgpu_mpo_upload",
     "mpsgpu_mpo_free", "mpsgpu_mpo_info", "mpsgpu_mpo_download", "mpsgpu_mpo_ising", "mpsgpu_mpo_ising_evolution", "mpsgpu_mpo_schwinger", "mpsgpu_mpo_heisenberg", "mpsgpu_mpo_bosehubbard",
     "mpsgpu_mps_upload", "mpsgpu_mps_random", "mpsgpu_mps_random_state", "mpsgpu_mps_product",
     "mpsgpu_mps_copy", "mpsgpu_mps_info", "mpsgpu_mps_download", "mpsgpu_mps_free",
@@ -35,6 +35,11 @@ EXPORTS = [
     "mpsgpu_server_create", "mpsgpu_server_submit", "mpsgpu_server_poll", "mpsgpu_server_cancel",
     "mpsgpu_server_drain", "mpsgpu_request_footprint", "mpsgpu_server_destroy",
 ]
+
+
+# kernel classes of mpsgpu_profile_kernels (work units: flops, BF16 tensor
+# flops, bytes, flops); one launch in 32 of each class is sampled
+PROFILE_CLASSES = ("gemm_fp64_dmma", "gemm_split_tcgen05", "lanczos_step", "qr")
 
 
 class Options(C.Structure):
@@ -173,7 +178,12 @@ class Context:
     def profile_end(self) -> dict:
         ms, fl, n = C.c_double(), C.c_double(), C.c_longlong()
         self._check(self.lib.mpsgpu_profile_end(self.h, C.byref(ms), C.byref(fl), C.byref(n)))
-        return {"gemm_ms": ms.value, "gemm_flops": fl.value, "gemm_calls": n.value}
+        out = {"gemm_ms": ms.value, "gemm_flops": fl.value, "gemm_calls": n.value}
+        kms, kwork, kcalls = (C.c_double * 4)(), (C.c_double * 4)(), (C.c_longlong * 4)()
+        self._check(self.lib.mpsgpu_profile_kernels(self.h, kms, kwork, kcalls))
+        out["kernels"] = {name: {"ms": kms[i], "work": kwork[i], "calls": kcalls[i]}
+                          for i, name in enumerate(PROFILE_CLASSES)}
+        return out
 
     # ---- objects ----
     def mpo(self, ops: list) -> "DeviceMPO":

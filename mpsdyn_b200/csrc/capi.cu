@@ -251,13 +251,24 @@ mpsgpu_status mpsgpu_profile_begin(mpsgpu_context* ctx) {
 mpsgpu_status mpsgpu_profile_end(mpsgpu_context* ctx, double* gemm_ms, double* gemm_flops, long long* gemm_calls) {
   if (!ctx) return MPSGPU_INVALID;
   return guarded(ctx, [&] {
-    ctx->c.prof.on = false;
-    const double ms = ctx->c.prof.resolve_ms();
-    if (gemm_ms) *gemm_ms = ms;
-    if (gemm_flops) *gemm_flops = ctx->c.prof.flops;
-    if (gemm_calls) *gemm_calls = ctx->c.prof.calls;
-    ctx->c.prof.reset();
+    auto& p = ctx->c.prof;
+    p.on = false;
+    p.resolve();
+    if (gemm_ms) *gemm_ms = p.ms[GemmProfiler::GEMM64];
+    if (gemm_flops) *gemm_flops = p.work[GemmProfiler::GEMM64];
+    if (gemm_calls) *gemm_calls = p.calls[GemmProfiler::GEMM64];
   });
+}
+
+mpsgpu_status mpsgpu_profile_kernels(mpsgpu_context* ctx, double* ms, double* work, long long* calls) {
+  if (!ctx) return MPSGPU_INVALID;
+  const auto& p = ctx->c.prof;
+  for (int c = 0; c < GemmProfiler::NCLS; c++) {
+    if (ms) ms[c] = p.ms[c];
+    if (work) work[c] = p.work[c];
+    if (calls) calls[c] = p.calls[c];
+  }
+  return MPSGPU_OK;
 }
 
 mpsgpu_status mpsgpu_mpo_upload(mpsgpu_context* ctx, int L, const int* dims, const double* const* data,

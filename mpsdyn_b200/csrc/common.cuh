@@ -56,18 +56,27 @@ struct Error : public std::runtime_error {
     if (!(cond)) throw ::mpsgpu::Error((status), (msg));   \
   } while (0)
 
-// Device-time accounting of the tensor-pipe GEMM launches: CUDA events are
-// recorded on the launching stream around every GEMM while active and
-// resolved once at the end (no synchronisation inside the sweep).
+// Device-time accounting of the hot kernels by class: while on, CUDA events
+// are recorded on the launching stream around one launch in `every` of each
+// class, with the launch's algorithmic work (flops, or bytes for the
+// bandwidth-bound Lanczos step); resolved once at the end (no
+// synchronisation inside the sweep).  Alone on the device, a sampled
+// launch's event time is its own duration.
 struct GemmProfiler {
+  // 0: complex FP64 GEMMs on the DMMA pipe (zgemm, the fused contractions);
+  // 1: split-precision GEMM on tcgen05 (work = BF16 tensor flops);
+  // 2: the fused Lanczos step (work = bytes); 3: Householder QR (flops)
+  enum { GEMM64 = 0, SPLIT = 1, LZSTEP = 2, QR = 3, NCLS = 4 };
   bool on = false;
-  int every = 32;       // sample one GEMM launch in `every` (keeps event traffic low)
-  long long seen = 0;   // GEMM launches since begin
+  int every = 32;
+  long long seen[NCLS] = {0, 0, 0, 0};
   std::vector<cudaEvent_t> pool;
+  std::vector<int> tags;  // class of each recorded pair
   size_t used = 0;
-  double flops = 0.0;   // algorithmic flops of the sampled launches
-  long long calls = 0;  // sampled launches
-  bool sample() { return on && (seen++ % every) == 0; }
+  double work[NCLS] = {0, 0, 0, 0};
+  long long calls[NCLS] = {0, 0, 0, 0};
+  double ms[NCLS] = {0, 0, 0, 0};  // filled by resolve()
+  bool sample(int cls) { return on && (seen[cls]++ % every) == 0; }
   cudaEvent_t next() {
     if (used == pool.size()) {
       cudaEvent_t e;
@@ -76,16 +85,20 @@ struct GemmProfiler {
     }
     return pool[used++];
   }
-  void reset() { used = 0; flops = 0.0; calls = 0; seen = 0; }
-  // Sum of (end - start) over the recorded pairs; synchronises on the last event.
-  double resolve_ms() {
-    double ms = 0.0;
+  void reset() {
+    used = 0;
+    tags.clear();
+    for (int c = 0; c < NCLS; c++) seen[c] = calls[c] = 0, work[c] = ms[c] = 0.0;
+  }
+  // Sums (end - start) per class over the recorded pairs; synchronises on
+  // the last event.
+  void resolve() {
+    for (int c = 0; c < NCLS; c++) ms[c] = 0.0;
     if (used >= 2) cudaEventSynchronize(pool[used - 1]);
     for (size_t i = 0; i + 1 < used; i += 2) {
       float t = 0.f;
-      if (cudaEventElapsedTime(&t, pool[i], pool[i + 1]) == cudaSuccess) ms += t;
+      if (cudaEventElapsedTime(&t, pool[i], pool[i + 1]) == cudaSuccess) ms[tags[i / 2]] += t;
     }
-    return ms;
   }
   ~GemmProfiler() {
     for (auto e : pool) cudaEventDestroy(e);
@@ -107,6 +120,31 @@ inline void after_launch(const Stream& st) {
 }
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Brackets one launch of class `cls` with profiler events when it is sampled.
+struct ProfScope {
+  GemmProfiler* p = nullptr;
+  cudaStream_t s = nullptr;
+  int cls = 0;
+  double work = 0.0;
+  ProfScope(const Stream& st, int cls_, double work_) : s(st.s), cls(cls_), work(work_) {
+    if (st.prof && st.prof->sample(cls)) {
+      cudaEvent_t e0 = st.prof->next();
+      if (e0 && cudaEventRecord(e0, s) == cudaSuccess) p = st.prof;
+    }
+  }
+  ~ProfScope() {
+    if (!p) return;
+    cudaEvent_t e1 = p->next();
+    if (e1 && cudaEventRecord(e1, s) == cudaSuccess) {
+      p->tags.push_back(cls);
+      p->work[cls] += work;
+      p->calls[cls]++;
+    } else if (p->used > 0) {
+      p->used -= e1 ? 2 : 1;  // drop the unmatched start event
+    }
+  }
+};
 
 // One-time set-up per device (kernel attributes live in each device's
 // context): true until mark_device_done has recorded the current device.

@@ -384,6 +384,13 @@ void heff_gemm1w(const Stream& st, Gemm1wBatch& b) {
     d.tile_begin = tiles;
     tiles += d.tiles_x * d.tiles_y;
   }
+  double work = 0.0;  // GEMM flops plus the MPO-leg epilogue
+  for (int q = 0; q < b.n; q++) {
+    const Gemm1wDesc& d = b.d[q];
+    const double nin = (double)d.n_i0 * d.n_i1, nout = (double)d.n_o0 * d.n_o1;
+    work += 8.0 * ((double)d.X * d.n_i0 * d.Y * d.n_i1 * d.K + (double)d.X * d.Y * nout * nin);
+  }
+  ProfScope ps(st, GemmProfiler::GEMM64, work);
   if (bm == 64)
     heff_gemm1w_kernel<64, 32><<<tiles, NT_, ring_bytes<64, 32>(), st.s>>>(b);
   else
@@ -422,6 +429,9 @@ void heff_gemm3(const Stream& st, Gemm3Batch& b) {
     tiles += d.tiles_m * d.tiles_n;
   }
   const dim3 grid(tiles * cs);
+  double work = 0.0;
+  for (int q = 0; q < b.n; q++) work += 8.0 * (double)b.d[q].M * b.d[q].N * (b.d[q].K1 + b.d[q].K2);
+  ProfScope ps(st, GemmProfiler::GEMM64, work);
 #define MPSGPU_G3(BMv, CSv)                                                                   \
   heff_gemm3_kernel<BMv, 32, CSv><<<grid, NT_, ring_bytes<BMv, 32>(), st.s>>>(b)
   if (bm == 64) {

@@ -441,6 +441,13 @@ void lanczos_step(const Stream& st, LzBatch& b) {
     mark_device_done(g_lz_setup);
   }
   const int grid = std::max(1, std::min(g_lz_grid[dev], b.nrb_total));
+  // algorithmic bytes: the basis read twice (projections, update), w read
+  // and written three times (three-term step, update, normalisation) and
+  // v_{j-1} once; the projector vectors twice
+  double bytes = 0.0;
+  for (int q = 0; q < b.ninst; q++)
+    bytes += 16.0 * (double)b.in[q].n * (2.0 * b.in[q].k + 6.0 + 2.0 * b.in[q].nu);
+  ProfScope ps(st, GemmProfiler::LZSTEP, bytes);
   void* args[] = {&b};
   MPSGPU_CUDA(cudaLaunchCooperativeKernel((void*)lanczos_step_kernel, dim3(grid), dim3(T), args, 0, st.s));
   after_launch(st);

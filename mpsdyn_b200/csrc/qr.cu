@@ -61,11 +61,17 @@ constexpr double kSafeMin = 2.2250738585072014e-308 / 1.1102230246251565e-16;
 // product W (nb x nb) and W2 (nb x nb, also the per-thread partial sums of
 // W: QR_THREADS entries).
 constexpr int QR_CH = 128;
-__host__ __device__ inline size_t qr_smem_bytes(int m, int nb) {
-  const size_t w2 = (size_t)nb * nb > (size_t)QR_THREADS ? (size_t)nb * nb : (size_t)QR_THREADS;
-  return ((size_t)m * nb + (size_t)QR_CH * nb + 2 * (size_t)nb * nb + w2) * sizeof(cplx);
+__host__ __device__ constexpr size_t qr_smem_bytes(int m, int nb) {
+  return ((size_t)m * nb + (size_t)QR_CH * nb + 2 * (size_t)nb * nb +
+          ((size_t)nb * nb > (size_t)QR_THREADS ? (size_t)nb * nb : (size_t)QR_THREADS)) *
+         sizeof(cplx);
 }
-constexpr int QR_SMEM_ATTR = 227 * 1024;
+// The largest plan the launchers use (m <= 640 with 16-column panels; above,
+// 8-column panels up to m = 1280 need less); the dynamic limit must leave
+// room for the kernels' static shared memory within the 227 KB per block.
+constexpr int QR_SMEM_ATTR = (int)(qr_smem_bytes(640, 16) > qr_smem_bytes(1280, 8) ? qr_smem_bytes(640, 16)
+                                                                                   : qr_smem_bytes(1280, 8));
+static_assert(QR_SMEM_ATTR + 4096 <= 227 * 1024, "QR shared-memory plan exceeds the per-block limit");
 
 // Apply (I - V T' V^H) to the mp x cw column slice C (shared, ld = ldc), where
 // V (mp x jb, unit lower trapezoidal: its upper triangle and diagonal are not
@@ -403,6 +409,9 @@ void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, lo
   MPSGPU_CHECK(m > 0 && n > 0, MPSGPU_BAD_SHAPE, "qr: empty matrix");
   const int K = std::min(m, n);
   const int nb = (m <= 640) ? 16 : 8;
+  // factorisation and explicit Q, complex flops (8 per complex MAC)
+  ProfScope ps(st, GemmProfiler::QR,
+               16.0 * (2.0 * m * n * K - (double)(m + n) * K * K + 2.0 * (double)K * K * K / 3.0));
   MPSGPU_CHECK(m <= 1280, MPSGPU_BAD_SHAPE, "qr: more than 1280 rows is not supported");
   QrParams p;
   p.m = m; p.n = n; p.K = K; p.nb = nb; p.npanel = (K + nb - 1) / nb;

@@ -512,6 +512,8 @@ void zgemm_split_prepared(const Stream& st, const SplitPlan& pl, const uint8_t* 
   MPSGPU_CHECK(((uintptr_t)Ap & 15) == 0 && ((uintptr_t)Bp & 15) == 0, MPSGPU_INVALID,
                "zgemm_split: operands not 16-byte aligned");
   MPSGPU_CHECK(pl.splits == 1 || part != nullptr, MPSGPU_INVALID, "zgemm_split: split K needs a partial buffer");
+  // 24 BF16 MMAs (M x N x 16) per complex k-step of 16: 48 M N K tensor flops
+  ProfScope ps(st, GemmProfiler::SPLIT, 48.0 * (double)pl.M * pl.N * pl.K);
   SplitGemmParams p;
   p.M = pl.M;
   p.N = pl.N;

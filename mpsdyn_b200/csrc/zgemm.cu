@@ -429,18 +429,8 @@ void zgemm(const Stream& st, const GemmArgs& g0, Scratch& scratch) {
     return;
   }
   const GemmCfg cfg = choose_cfg(st, g, scratch);
-  const bool prof = st.prof && st.prof->sample();
-  if (prof) {
-    cudaEvent_t e0 = st.prof->next();
-    if (e0) cudaEventRecord(e0, st.s);
-  }
+  ProfScope ps(st, GemmProfiler::GEMM64, 8.0 * (double)g.M * g.N * g.K * g.batch);
   run_cfg(st, g, cfg, scratch);
-  if (prof) {
-    cudaEvent_t e1 = st.prof->next();
-    if (e1) cudaEventRecord(e1, st.s);
-    st.prof->flops += 8.0 * (double)g.M * g.N * g.K * g.batch;
-    st.prof->calls++;
-  }
 }
 
 long long grouped_tiles(GroupedGemm* descs, int n) {

@@ -39,8 +39,10 @@
  *   applympo model delta imag D dagger dir mps out
  *                                  U-MPO of getUMPO applied to mps: MPS::applyExactly (D = 0) or
  *                                  MPS::approximate (D > 0), MPS.cpp:853-936
- *   profile model D eigtol init n  timed sample: n site steps of the ground-state sweep
- *                                  around the chain centre (CPU baseline of the bench)
+ *   profile model D eigtol init n [pos0]
+ *                                  timed sample: n site steps of the ground-state sweep
+ *                                  from site pos0 (default: around the chain centre),
+ *                                  the CPU baseline of the bench
  *   gauge mps dir out              MPS::gaugeCond(dir, true)          (MPS.cpp:306-364)
  *   savempo model file             MPO::saveMPO of the model's H     (MPO.cpp:214-231)
  *   optsum D convtol init out ket re im [ket re im ...]
@@ -439,7 +441,8 @@ int main(int argc, const char* argv[]) {
     auto mvflops = [&](int d, int w1, int w2, int dl, int dr) {
       return 8.0 * ((double)dl * w1 * dl * d * dr + (double)dl * d * d * w1 * w2 * dr + (double)dl * d * dr * w2 * dr);
     };
-    int pos0 = max(1, L / 2 - nsites / 2);
+    int pos0 = argc > 7 ? atoi(argv[7]) : max(1, L / 2 - nsites / 2);
+    pos0 = max(0, min(pos0, L - 2));
     vector<mwArray> Ls(L), Rs(L);
     Ls[0] = mwArray(ONE_c); Ls[0].reshape(Indices(1, 1, 1));
     Rs[L - 1] = mwArray(ONE_c); Rs[L - 1].reshape(Indices(1, 1, 1));
@@ -482,7 +485,7 @@ int main(int argc, const char* argv[]) {
     clock_gettime(CLOCK_MONOTONIC, &t1);
     double secs = (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
     print_json({{"seconds", secs}, {"flops", flops}, {"iterations", (double)iters},
-                {"pos0", (double)pos0}, {"nsites", (double)nsites}});
+                {"pos0", (double)pos0}, {"nsites", (double)min(nsites, L - 1 - pos0)}});
   } else {
     cerr << "unknown command " << cmd << endl;
     return 2;

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
                     reason="oracle/_ref not built")
 def test_reference_arm_prints_its_line():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                        "--cpu-sample-sites", "1", "--steps", "2", "--warmup", "3"],
+                        "--ref-max-sites", "1", "--ref-iter-cap", "10", "--steps", "2", "--warmup", "3"],
                        capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
@@ -24,7 +24,8 @@ def test_reference_arm_prints_its_line():
     sys.path.insert(0, ROOT)
     import bench
     assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
-    assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 2 and d["warmup"] == 3
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 2
+    assert d["warmup"] == 0 and d["warmup_requested"] == 3  # the CPU path has nothing to warm up
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
