@@ -55,6 +55,9 @@ def parse():
     p.add_argument("--ref-iter-cap", type=int, default=0,
                    help="tests only: cap the reference eigensolver (the line is then not a measurement)")
     p.add_argument("--batch", type=int, default=8, help="concurrent solves per step")
+    p.add_argument("--batch-form", default="lockstep", choices=["lockstep", "streams"],
+                   help="lockstep: one context sweeps the batch together (grouped launches); "
+                        "streams: one context, stream and host thread per solve")
     p.add_argument("--plain", type=int, default=1, help="also time one solve alone (the plain form)")
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="mixed: split-precision products until the energy settles, then FP64")
@@ -308,7 +311,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
 
     W = WORKLOAD
     B = args.batch
-    # one library context (own CUDA stream) and one host thread per concurrent solve
+    lockstep = args.batch_form == "lockstep"
+    # one library context (own CUDA stream) per concurrent solve; the
+    # lockstep form runs the whole batch on the first one
     ctxs = [capi.Context(local_rank) for _ in range(B)]
     exts = [torch.cuda.ExternalStream(c.stream) for c in ctxs]
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -317,8 +322,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     opts64 = ctxs[0].options(convtol=W["convtol"], precision=0)
     mpos = [c.mpo_schwinger(W["N"], MU, W["x"]) for c in ctxs]
     seeds = [(W["seed_gs"] + 1000 * (rank * B + i), W["seed_exc"] + 1000 * (rank * B + i)) for i in range(B)]
+    owner = [ctxs[0] if lockstep else c for c in ctxs]
     inits = [(c.mps_random(W["N"], 2, W["D"], sg), c.mps_random(W["N"], 2, W["D"], se))
-             for c, (sg, se) in zip(ctxs, seeds)]
+             for c, (sg, se) in zip(owner, seeds)]
     hosts = [(g.download()[0], x.download()[0]) for g, x in inits]
     h2d_mps = sum(a.nbytes for a in hosts[0][0]) + sum(a.nbytes for a in hosts[0][1])
     mpo_bytes = 16 * (2 * 1 * 2 * 5 + 2 * 5 * 2 * 1 + (W["N"] - 2) * 2 * 5 * 2 * 5)
@@ -347,7 +353,47 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         x.free()
         m.free()
 
-    def run_batch(fn, timed_events=True):
+    def lockstep_solves(o, e2e=False):
+        # all B solves swept in lockstep on one context: their local
+        # eigenproblems share the grouped launches of every Lanczos round
+        c = ctxs[0]
+        if e2e:
+            ms = [c.mpo_schwinger(W["N"], MU, W["x"]) for _ in range(B)]       # host build + upload
+            gs = [c.mps(hosts[i][0]) for i in range(B)]                          # host -> device
+            xs = [c.mps(hosts[i][1]) for i in range(B)]
+        else:
+            ms = [mpos[0]] * B
+            gs = [inits[i][0].copy() for i in range(B)]
+            xs = [inits[i][1].copy() for i in range(B)]
+        e0, st0, s0 = c.find_ground_state_batch(ms, W["D"], gs, 0.0, o)
+        if any(st0):
+            raise RuntimeError(f"ground-state batch: statuses {st0}")
+        e1, st1, s1 = c.find_next_excited_state_batch(ms, W["D"], [[g] for g in gs], xs, 0.0, o)
+        if any(st1):
+            raise RuntimeError(f"excited-state batch: statuses {st1}")
+        for i in range(B):
+            results[i] = {"E0": e0[i], "E1": e1[i], "gs": s0[i], "exc": s1[i]}
+            if e2e:
+                og, _ = gs[i].download()                                          # device -> host
+                ox, _ = xs[i].download()
+                results[i]["d2h"] = sum(a.nbytes for a in og) + sum(a.nbytes for a in ox) + 16
+        for v in gs + xs:
+            v.free()
+        if e2e:
+            for m in ms:
+                m.free()
+
+    def run_batch(fn, timed_events=True, o=None, e2e=False):
+        if lockstep:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(exts[0])
+            lockstep_solves(o or opts, e2e)
+            ev1.record(exts[0])
+            torch.cuda.synchronize()
+            if not timed_events:
+                return None, None
+            span = ev0.elapsed_time(ev1)
+            return span, [span] * B  # every solve completes with the batch
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(B)]
         go = threading.Barrier(B)
 
@@ -410,7 +456,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     for _ in range(args.steps):
         flush_l2()
         t0 = time.perf_counter()
-        run_batch(solve_e2e, timed_events=False)
+        run_batch(solve_e2e, timed_events=False, e2e=True)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     d2h = sum(r["d2h"] for r in results)
     e2e_total = allreduce(float(sum(e2e_ms)), torch.distributed.ReduceOp.MAX if dist else None)
@@ -426,7 +472,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         spans_a, energies_a = [], []
         for _ in range(args.steps):
             flush_l2()
-            span, _ = run_batch(lambda i: solve_resident(i, o))
+            span, _ = run_batch(lambda i: solve_resident(i, o), o=o)
             spans_a.append(span)
             energies_a.append([(r["E0"], r["E1"]) for r in results])
         t = allreduce(float(sum(spans_a)), torch.distributed.ReduceOp.MAX if dist else None)
@@ -525,7 +571,10 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         "config": {**WORKLOAD, "mu": MU, "parallelism": f"replicas{world}",
                    "precision": ("mixed: split-precision (BF16-limb tcgen05) products until the half-sweep "
                                  "energy changes < 1e-6, then FP64" if mixed else "fp64"),
-                   "batch": B, "batch_form": "concurrent independent solves, one stream each",
+                   "batch": B,
+                   "batch_form": ("lockstep: the B solves swept together on one stream, their local "
+                                  "eigenproblems in shared grouped launches" if lockstep else
+                                  "concurrent independent solves, one stream and host thread each"),
                    "l2": "flushed between steps (256 MB write)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": B * (h2d_mps + mpo_bytes),
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.steps},

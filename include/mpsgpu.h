@@ -98,6 +98,11 @@ typedef struct {
   double matvec_seconds;     /* device time spent in matvec kernels (events) */
   long long split_matvecs;   /* products run in split precision (precision = 1) */
   int split_rounds;          /* half-sweeps run in split precision */
+  /* host time of the local eigensolver's loop: launching the iterations,
+   * waiting for their results, solving the projected tridiagonal problem */
+  double host_launch_seconds;
+  double host_wait_seconds;
+  double host_tridiag_seconds;
 } mpsgpu_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -265,6 +270,24 @@ mpsgpu_status mpsgpu_find_next_excited_state(mpsgpu_context* ctx,
                                              const mpsgpu_options* opt,
                                              mpsgpu_mps* init, double* lambda,
                                              mpsgpu_stats* stats);
+/* Batches of independent solves on one context, swept in lockstep: the local
+ * eigenproblems of all solves at the same site share grouped launches of the
+ * two contractions and of the Lanczos step (the reference runs one
+ * findGroundState / findNextExcitedState after another; the result of each
+ * solve is the one it has alone).  ops[i], inits[i]: solve i (all with the
+ * same length; inits are overwritten by the results); lambdas[i] its energy;
+ * status[i] (may be null) its own status, stats[i] (may be null) its
+ * counters.  The call returns the first failing solve's status, MPSGPU_OK
+ * when all succeed.  Excited states: solve i projects out the nlevels[i]
+ * states that follow in `levels` (the lists of all solves concatenated). */
+mpsgpu_status mpsgpu_find_ground_state_batch(mpsgpu_context* ctx, int n, const mpsgpu_mpo* const* ops, int D,
+                                             double offset, const mpsgpu_options* opt, mpsgpu_mps* const* inits,
+                                             double* lambdas, int* status, mpsgpu_stats* stats);
+mpsgpu_status mpsgpu_find_next_excited_state_batch(mpsgpu_context* ctx, int n, const mpsgpu_mpo* const* ops, int D,
+                                                   const mpsgpu_mps* const* levels, const int* nlevels,
+                                                   double offset, const mpsgpu_options* opt,
+                                                   mpsgpu_mps* const* inits, double* lambdas, int* status,
+                                                   mpsgpu_stats* stats);
 /* optimize(ops, orig, init, D, errN, errT) (Contractor.cpp:77-278): the
  * variational MPO.MPS product used for time evolution.  errN (nullable)
  * receives <orig|ops^dag ops|orig> + <init|init> - 2 Re <init|ops|orig> and

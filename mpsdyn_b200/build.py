@@ -23,7 +23,7 @@ FACADE_DIR = os.path.join(HERE, "cpp")
 FACADE_INC = os.path.join(FACADE_DIR, "include")
 FACADE_LIB = os.path.join(HERE, "libmpsdyn_facade.so")
 
-SOURCES = ["zgemm.cu", "blas1.cu", "lanczos.cu", "lzstep.cu", "heff.cu", "qr.cu", "svd.cu", "grouped.cu", "umma.cu", "engine.cu", "capi.cu", "mpsio.cpp", "models.cpp", "server.cpp"]
+SOURCES = ["zgemm.cu", "blas1.cu", "lzstep.cu", "heff.cu", "qr.cu", "svd.cu", "grouped.cu", "umma.cu", "engine.cu", "capi.cu", "mpsio.cpp", "models.cpp", "server.cpp"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [
     "-std=c++17", "-O3",

@@ -28,6 +28,7 @@ EXPORTS = [
     "mpsgpu_mps_export", "mpsgpu_mps_import", "mpsgpu_mpo_save", "mpsgpu_mpo_load",
     "mpsgpu_optimize_sum", "mpsgpu_optimize_mps",
     "mpsgpu_mps_gauge", "mpsgpu_mps_gauge_cond", "mpsgpu_mps_increase_bond", "mpsgpu_mps_bond", "mpsgpu_mps_set_normfact", "mpsgpu_mps_approximate", "mpsgpu_mps_apply_mpo", "mpsgpu_find_ground_state", "mpsgpu_find_ground_state_two_site", "mpsgpu_find_next_excited_state",
+    "mpsgpu_find_ground_state_batch", "mpsgpu_find_next_excited_state_batch",
     "mpsgpu_optimize", "mpsgpu_contract", "mpsgpu_contract2", "mpsgpu_expectation_local", "mpsgpu_entropy",
     "mpsgpu_schmidt_values", "mpsgpu_heff_matvec", "mpsgpu_heff_matvec_grouped", "mpsgpu_heff_matvec_grouped_ex", "mpsgpu_zgemm_split", "mpsgpu_set_autotune", "mpsgpu_autotune_entries",
     "mpsgpu_env_left", "mpsgpu_env_right",
@@ -57,6 +58,8 @@ class Stats(C.Structure):
         ("env_updates", C.c_longlong), ("qr_calls", C.c_longlong), ("flops", C.c_double),
         ("seconds", C.c_double), ("matvec_seconds", C.c_double),
         ("split_matvecs", C.c_longlong), ("split_rounds", C.c_int),
+        ("host_launch_seconds", C.c_double), ("host_wait_seconds", C.c_double),
+        ("host_tridiag_seconds", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -304,6 +307,39 @@ class Context:
         self._check(self.lib.mpsgpu_find_next_excited_state(self.h, ops.h, D, arr, len(levels), offset,
                                                             C.byref(o), init.h, C.byref(e), C.byref(st)))
         return e.value, st.as_dict()
+
+    def find_ground_state_batch(self, ops: list, D: int, inits: list, offset: float = 0.0, opts=None):
+        """mpsgpu_find_ground_state_batch: solves swept in lockstep; returns
+        (energies, statuses, stats dicts); raises only on a call-level error."""
+        n = len(inits)
+        P = C.c_void_p
+        e = (C.c_double * n)()
+        stv = (C.c_int * n)()
+        sts = (Stats * n)()
+        o = opts or self.options()
+        r = self.lib.mpsgpu_find_ground_state_batch(self.h, n, (P * n)(*[m.h for m in ops]), D, C.c_double(offset),
+                                                    C.byref(o), (P * n)(*[s.h for s in inits]), e, stv, sts)
+        if r != 0 and all(v == 0 for v in stv):
+            self._check(r)
+        return list(e), list(stv), [x.as_dict() for x in sts]
+
+    def find_next_excited_state_batch(self, ops: list, D: int, levels: list, inits: list, offset: float = 0.0,
+                                      opts=None):
+        """levels[i]: the list of states solve i projects out."""
+        n = len(inits)
+        P = C.c_void_p
+        flat = [lv.h for group in levels for lv in group]
+        e = (C.c_double * n)()
+        stv = (C.c_int * n)()
+        sts = (Stats * n)()
+        o = opts or self.options()
+        r = self.lib.mpsgpu_find_next_excited_state_batch(
+            self.h, n, (P * n)(*[m.h for m in ops]), D, (P * len(flat))(*flat),
+            (C.c_int * n)(*[len(g) for g in levels]), C.c_double(offset), C.byref(o),
+            (P * n)(*[s.h for s in inits]), e, stv, sts)
+        if r != 0 and all(v == 0 for v in stv):
+            self._check(r)
+        return list(e), list(stv), [x.as_dict() for x in sts]
 
     def optimize(self, ops, orig, init, D=0, opts=None, want_err=False):
         st = Stats()

@@ -74,6 +74,9 @@ void fill_stats(mpsgpu_stats* st, const Counters& c, double secs) {
   st->matvec_seconds = c.mv_ms * 1e-3;
   st->split_matvecs = c.split_matvecs;
   st->split_rounds = c.split_rounds;
+  st->host_launch_seconds = c.host_launch_s;
+  st->host_wait_seconds = c.host_wait_s;
+  st->host_tridiag_seconds = c.host_tridiag_s;
 }
 
 double now_s() {
@@ -164,18 +167,11 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
     MPSGPU_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
     MPSGPU_CUDA(cudaMalloc((void**)&c.dscal, 1024 * sizeof(double)));
     MPSGPU_CUDA(cudaMalloc((void**)&c.dcplx, 1024 * sizeof(cplx)));
-    MPSGPU_CUDA(cudaMalloc((void**)&c.dS, 1024 * sizeof(double)));
     MPSGPU_CUDA(cudaMallocHost((void**)&c.hscal, 1024 * sizeof(double)));
     MPSGPU_CUDA(cudaMallocHost((void**)&c.hcplx, 1024 * sizeof(cplx)));
     MPSGPU_CUDA(cudaEventCreate(&c.ev));
     MPSGPU_CUDA(cudaEventCreate(&c.mv0));
     MPSGPU_CUDA(cudaEventCreate(&c.mv1));
-    MPSGPU_CUDA(cudaMalloc((void**)&c.dsc, sizeof(LanczosScalars)));
-    // pinned and mapped: the fused Lanczos kernels write alpha_j, beta_j
-    // straight into it (no copy per iteration); the host reads them after
-    // the iteration's event
-    MPSGPU_CUDA(cudaHostAlloc((void**)&c.hsc, sizeof(LanczosScalars), cudaHostAllocMapped));
-    MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.hsc_dev, c.hsc, 0));
     MPSGPU_CUDA(cudaHostAlloc((void**)&c.hsplit_err, sizeof(int), cudaHostAllocMapped));
     MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dsplit_err, c.hsplit_err, 0));
     *c.hsplit_err = 0;
@@ -184,7 +180,6 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
     *c.hlz_err = 0;
     MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 128 * sizeof(unsigned)));
     MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 128 * sizeof(unsigned)));
-    MPSGPU_CUDA(cudaMemset(c.dsc, 0, sizeof(LanczosScalars)));
     c.iter_ev.resize(257);
     for (auto& e : c.iter_ev) MPSGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   });
@@ -200,7 +195,7 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   if (!ctx) return MPSGPU_INVALID;
   Context& c = ctx->c;
   cudaSetDevice(c.device);
-  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lanV, &c.lanW, &c.lanT, &c.lanQ,
+  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR,
                   &c.lzws, &c.spX, &c.spT, &c.spPart})
     dbuf_free(c, *b);
   c.scratch.release();
@@ -208,7 +203,6 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   if (c.stream) cudaStreamSynchronize(c.stream);
   cudaFree(c.dscal);
   cudaFree(c.dcplx);
-  cudaFree(c.dS);
   cudaFreeHost(c.hscal);
   cudaFreeHost(c.hcplx);
   if (c.ev) cudaEventDestroy(c.ev);
@@ -216,8 +210,7 @@ mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   if (c.mv1) cudaEventDestroy(c.mv1);
   for (auto e : c.iter_ev)
     if (e) cudaEventDestroy(e);
-  cudaFree(c.dsc);
-  cudaFreeHost(c.hsc);
+  c.lzone.release(c);
   if (c.hsplit_err) cudaFreeHost(c.hsplit_err);
   if (c.hlz_err) cudaFreeHost(c.hlz_err);
   cudaFree(c.dcounter);
@@ -579,6 +572,89 @@ mpsgpu_status mpsgpu_find_next_excited_state(mpsgpu_context* ctx, const mpsgpu_m
   });
   fill_stats(stats, cnt, now_s() - t0);
   return st;
+}
+
+mpsgpu_status mpsgpu_find_ground_state_batch(mpsgpu_context* ctx, int n, const mpsgpu_mpo* const* ops, int D,
+                                             double offset, const mpsgpu_options* opt, mpsgpu_mps* const* inits,
+                                             double* lambdas, int* status, mpsgpu_stats* stats) {
+  if (!ctx || n < 1 || !ops || !inits || !lambdas) return MPSGPU_INVALID;
+  for (int i = 0; i < n; i++)
+    if (!ops[i] || !inits[i]) return MPSGPU_INVALID;
+  std::vector<Counters> cnt;
+  std::vector<int> st;
+  std::vector<std::string> err;
+  double t0 = now_s();
+  mpsgpu_status r = guarded(ctx, [&] {
+    mpsgpu_options dflt;
+    mpsgpu_default_options(&dflt);
+    std::vector<const MpoDev*> o(n);
+    std::vector<MpsDev*> in(n);
+    for (int i = 0; i < n; i++) {
+      o[i] = &ops[i]->m;
+      in[i] = &inits[i]->s;
+    }
+    std::vector<double> e;
+    find_ground_state_batch(ctx->c, o, D, in, offset, to_opts(opt ? opt : &dflt), e, cnt, st, err);
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    for (int i = 0; i < n; i++) lambdas[i] = e[i];
+  });
+  const double secs = now_s() - t0;
+  for (int i = 0; i < n; i++) {
+    if (status) status[i] = i < (int)st.size() ? st[i] : r;
+    if (stats && i < (int)cnt.size()) fill_stats(&stats[i], cnt[i], secs);
+  }
+  if (r != MPSGPU_OK) return r;
+  for (int i = 0; i < n; i++)
+    if (st[i] != MPSGPU_OK) {
+      ctx->c.last_error = "solve " + std::to_string(i) + ": " + err[i];
+      return (mpsgpu_status)st[i];
+    }
+  return MPSGPU_OK;
+}
+
+mpsgpu_status mpsgpu_find_next_excited_state_batch(mpsgpu_context* ctx, int n, const mpsgpu_mpo* const* ops, int D,
+                                                   const mpsgpu_mps* const* levels, const int* nlevels,
+                                                   double offset, const mpsgpu_options* opt,
+                                                   mpsgpu_mps* const* inits, double* lambdas, int* status,
+                                                   mpsgpu_stats* stats) {
+  if (!ctx || n < 1 || !ops || !inits || !lambdas || !levels || !nlevels) return MPSGPU_INVALID;
+  std::vector<Counters> cnt;
+  std::vector<int> st;
+  std::vector<std::string> err;
+  double t0 = now_s();
+  mpsgpu_status r = guarded(ctx, [&] {
+    mpsgpu_options dflt;
+    mpsgpu_default_options(&dflt);
+    std::vector<const MpoDev*> o(n);
+    std::vector<MpsDev*> in(n);
+    std::vector<std::vector<const MpsDev*>> lv(n);
+    int off = 0;
+    for (int i = 0; i < n; i++) {
+      MPSGPU_CHECK(ops[i] && inits[i] && nlevels[i] >= 1, MPSGPU_INVALID, "null handle or no level");
+      o[i] = &ops[i]->m;
+      in[i] = &inits[i]->s;
+      for (int k = 0; k < nlevels[i]; k++, off++) {
+        MPSGPU_CHECK(levels[off] != nullptr, MPSGPU_INVALID, "null level");
+        lv[i].push_back(&levels[off]->s);
+      }
+    }
+    std::vector<double> e;
+    find_next_excited_state_batch(ctx->c, o, D, lv, in, offset, to_opts(opt ? opt : &dflt), e, cnt, st, err);
+    MPSGPU_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    for (int i = 0; i < n; i++) lambdas[i] = e[i];
+  });
+  const double secs = now_s() - t0;
+  for (int i = 0; i < n; i++) {
+    if (status) status[i] = i < (int)st.size() ? st[i] : r;
+    if (stats && i < (int)cnt.size()) fill_stats(&stats[i], cnt[i], secs);
+  }
+  if (r != MPSGPU_OK) return r;
+  for (int i = 0; i < n; i++)
+    if (st[i] != MPSGPU_OK) {
+      ctx->c.last_error = "solve " + std::to_string(i) + ": " + err[i];
+      return (mpsgpu_status)st[i];
+    }
+  return MPSGPU_OK;
 }
 
 mpsgpu_status mpsgpu_optimize(mpsgpu_context* ctx, const mpsgpu_mpo* ops, const mpsgpu_mps* orig,

@@ -11,6 +11,7 @@
 // is one GEMM or one MPO-leg contraction; none of the explicit permutes of
 // TensorMultiplier::product (TensorMultiplier.cpp:61-93) remain.
 #include <algorithm>
+#include <memory>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -884,181 +885,358 @@ cplx contract2(Context& c, const MpoDev& ops, const MpsDev& ket, const MpsDev& b
 
 // ---------------------------------------------------------------------------
 // Lanczos for the lowest eigenpair (replaces the PRIMME call of
-// Contractor::solveEigs, Contractor.cpp:3067-3138; and its dense branch).
+// Contractor::solveEigs, Contractor.cpp:3067-3138; and its dense branch),
+// for a batch of independent local problems advanced in lockstep.
 // Thick-restarted Lanczos with full reorthogonalisation, FP64; convergence
-// ||r|| <= tol * max|Ritz|.  apply(x, y, sigma) must compute y = (H - sigma) x
-// (the products of the excited-state multiplier without its projector);
-// sigma follows the latest Ritz value (shift0 before the first one is
-// known), which keeps the Gram-Schmidt passes well conditioned.  With nu > 0,
-// U (N x nu) holds the projector vectors with the square roots of the
-// penalties folded in, and the step adds U (U^H v_j) to every product
-// (TensorMultiplierProjMulti.cpp:81-90).  Each iteration is the product (two
-// launches in FP64) and one cooperative launch of the Lanczos step
-// (lzstep.cu), which writes alpha_j, beta_j into mapped host memory.
+// ||r|| <= tol * max|Ritz|.  Every task's product computes y = (H - sigma) x
+// (the excited-state multiplier without its projector); sigma follows the
+// task's latest Ritz value (shift0 before the first one is known), which
+// keeps the Gram-Schmidt passes well conditioned.  With nu > 0, U (N x nu)
+// holds the projector vectors with the square roots of the penalties folded
+// in, and the step adds U (U^H v_j) to every product
+// (TensorMultiplierProjMulti.cpp:81-90).
+//
+// One round = one iteration of every active task: FP64 products are
+// appended to grouped launches of the two contractions (heff.cu), a task in
+// its split-precision phase launches its own product chain, then one
+// cooperative launch of the Lanczos step (lzstep.cu) serves all tasks and
+// writes each task's alpha_j, beta_j into its mapped host mirror.  The host
+// enqueues round r+1 before it waits for round r, so the convergence tests
+// (tridiagonal eigenpairs on the host) overlap the device work; a
+// speculative iteration after convergence is discarded (it only writes the
+// task's V[:, j+2], w and the coefficients of step j+1).  Tasks converge,
+// restart and leave the batch independently; the arithmetic of a task is
+// the same whatever else runs in its rounds.
 // ---------------------------------------------------------------------------
 
-template <class Op>
-static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, int max_krylov, int* iters,
-                             double shift0, const cplx* U = nullptr, int nu = 0) {
-  const int m = std::min(N, std::max(2, std::min(max_krylov, 200)));
-  dbuf_reserve(c, c.lanV, (long long)N * (m + 1));
-  dbuf_reserve(c, c.lanW, N);
-  cplx* V = c.lanV.p;
-  cplx* w = c.lanW.p;
-  const Stream st = c.st();
-  double* d_tmp = c.dscal + 512;
-  // workspace of the step: partial dots (nrb x 256), two partial-norm
-  // arrays (nrb), the coefficients h, h2 (256 each)
-  const long long nrb = ceil_div(N, lanczos_step_rows_per_block());
-  dbuf_reserve(c, c.lzws, nrb * 256 + 512 + nrb + 8);
-  LzBatch b;
-  b.ninst = 1;
-  b.part = c.lzws.p;
-  b.h = c.lzws.p + nrb * 256;
-  b.h2 = b.h + 256;
-  b.pn1 = reinterpret_cast<double*>(b.h2 + 256);
-  b.pn2 = b.pn1 + nrb;
-  b.bar = c.dcounter + 96;
-  b.err = c.dlz_err;
-  LzInst& in = b.in[0];
-  in.n = N;
-  in.V = V;
-  in.ldv = N;
-  in.w = w;
-  in.U = U;
-  in.nu = nu;
-  in.sc = c.dsc;
-  in.mirror = c.hsc_dev;
-  // v0 = x / ||x||
-  dznrm2(st, N, x, d_tmp, c.scratch);
-  MPSGPU_CUDA(cudaMemcpyAsync(c.hscal, d_tmp, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-  MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
-  if (!(c.hscal[0] > 0.0) || !std::isfinite(c.hscal[0])) {
-    zfill(st, N, make_double2(1.0 / std::sqrt((double)N), 0.0), x);
-    dznrm2(st, N, x, d_tmp, c.scratch);
+void LzWork::init(Context& c) {
+  if (dsc) return;
+  MPSGPU_CUDA(cudaMalloc((void**)&dsc, sizeof(LanczosScalars)));
+  MPSGPU_CUDA(cudaMemsetAsync(dsc, 0, sizeof(LanczosScalars), c.stream));
+  MPSGPU_CUDA(cudaHostAlloc((void**)&hsc, sizeof(LanczosScalars), cudaHostAllocMapped));
+  MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&hsc_dev, hsc, 0));
+  MPSGPU_CUDA(cudaMalloc((void**)&dS, 256 * sizeof(double)));
+}
+
+void LzWork::release(Context& c) {
+  for (DBuf* b : {&V, &w, &t2, &t3, &T, &Q}) dbuf_free(c, *b);
+  if (dsc) {
+    cudaStreamSynchronize(c.stream);
+    cudaFree(dsc);
+    cudaFreeHost(hsc);
+    cudaFree(dS);
   }
-  zscal_inv(st, N, x, d_tmp, V);
-  std::vector<double> a, b2v, s;
-  double theta = 0.0, step_hint = 0.0;
+  dsc = nullptr;
+  hsc = hsc_dev = nullptr;
+  dS = nullptr;
+}
+
+namespace {
+
+struct LzState {
+  LzTask* t = nullptr;
+  int m = 0, keep = 0, max_restarts = 0, restart = 0;
+  int j0 = 0;        // first iteration of the current cycle
+  int jq = -1;       // last iteration enqueued
+  int jr = -1;       // last iteration whose result was read
+  bool done = false;
+  bool pending_restart = false;  // next round starts a new cycle at j0
+  std::vector<double> a, b, s, gq;
+  std::vector<cplx> gqc;
+  double theta = 0.0, step_hint = 0.0, sigma = 0.0;
   bool have_theta = false;
-  double sigma = std::isfinite(shift0) ? shift0 : 0.0;
-  int total = 0;
   TridiagLowest tri;
-  // Iteration j: product, Lanczos step, event.  The host enqueues iteration
-  // j+1 before it waits for j, so the convergence test (tridiagonal
-  // eigenpair on the host) overlaps the device work; a speculative
-  // iteration after convergence is discarded (it only writes V[:, j+2], w
-  // and the coefficients of step j+1).
-  auto enqueue = [&](int j) {
-    apply(V + (long long)j * N, w, sigma);
-    in.j = j;
-    in.k = j + 1;
-    in.sigma = sigma;
-    in.write_next = j + 1 < m ? 1 : 0;
-    lanczos_step(st, b);
-    MPSGPU_CUDA(cudaEventRecord(c.iter_ev[j], c.stream));
-    total++;
-  };
+  ThickRestart thick;
+};
+
+}  // namespace
+
+void lanczos_batch(Context& c, std::vector<LzTask*>& tasks) {
+  using clk = std::chrono::steady_clock;
+  auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+  const Stream st = c.st();
+  const int nt = (int)tasks.size();
+  if (nt == 0) return;
+  std::vector<LzState> S(nt);
+  long long nrb_total = 0;
+  double* d_tmp = c.dscal + 512;
+  for (int q = 0; q < nt; q++) {
+    LzTask& t = *tasks[q];
+    LzState& z = S[q];
+    z.t = &t;
+    MPSGPU_CHECK(t.ws != nullptr && t.N > 0, MPSGPU_INVALID, "lanczos: task without workspace");
+    MPSGPU_CHECK(t.nu <= LZ_MAXU, MPSGPU_BAD_SHAPE, "lanczos: at most 8 projector vectors");
+    LzWork& ws = *t.ws;
+    ws.init(c);
+    const int N = t.N;
+    z.m = std::min(N, std::max(2, std::min(t.max_krylov, 200)));
+    z.keep = std::max(1, z.m / 2);
+    // budget of about 3840 products (60 cycles of a 64-vector space), whatever m
+    z.max_restarts = std::max(60, 3840 / std::max(1, z.m - z.keep));
+    z.sigma = std::isfinite(t.shift0) ? t.shift0 : 0.0;
+    dbuf_reserve(c, ws.V, (long long)N * (z.m + 1));
+    dbuf_reserve(c, ws.w, N);
+    nrb_total += ceil_div(N, lanczos_step_rows_per_block());
+    // v0 = x / ||x|| (a zero or non-finite start becomes the flat vector)
+    dznrm2(st, N, t.x, d_tmp, c.scratch);
+    MPSGPU_CUDA(cudaMemcpyAsync(c.hscal, d_tmp, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    if (!(c.hscal[0] > 0.0) || !std::isfinite(c.hscal[0])) {
+      zfill(st, N, make_double2(1.0 / std::sqrt((double)N), 0.0), t.x);
+      dznrm2(st, N, t.x, d_tmp, c.scratch);
+    }
+    zscal_inv(st, N, t.x, d_tmp, ws.V.p);
+    t.iters = 0;
+  }
+  // workspace of the step, shared by the instances of a launch: partial dots
+  // (row blocks x 256), two partial-norm arrays, the coefficients h, h2
+  const long long hcap = 256LL * LZ_MAXI;
+  dbuf_reserve(c, c.lzws, nrb_total * 256 + 2 * hcap + nrb_total + 8);
+  cplx* part = c.lzws.p;
+  cplx* hbuf = part + nrb_total * 256;
+  cplx* h2buf = hbuf + hcap;
+  double* pn1 = reinterpret_cast<double*>(h2buf + hcap);
+  double* pn2 = pn1 + nrb_total;
+
   auto check_step = [&]() {
     if (*c.hlz_err) {
       MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
-      MPSGPU_CUDA(cudaMemsetAsync(b.bar, 0, 2 * sizeof(unsigned), c.stream));
+      MPSGPU_CUDA(cudaMemsetAsync(c.dcounter + 96, 0, 2 * sizeof(unsigned), c.stream));
       MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
       *c.hlz_err = 0;
       throw Error(MPSGPU_TIMEOUT, "lanczos: a bounded grid barrier of the Lanczos step ran out");
     }
   };
-  // Ritz vector of the current tridiagonal (k x k) into x, normalised
-  auto ritz_vector = [&](int k) {
-    MPSGPU_CUDA(cudaMemcpyAsync(c.dS, s.data(), k * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    combine_real(st, N, k, V, N, c.dS, x);
-    dznrm2(st, N, x, d_tmp, c.scratch);
-    zscal_inv(st, N, x, d_tmp, x);
-    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
-    check_step();
-    if (iters) *iters = total;
-  };
-  // Thick-restarted Lanczos: after m steps the factorisation is compressed
-  // to about m/2 vectors spanning the lowest Ritz vectors, in tridiagonal
-  // form (ThickRestart), so the reorthogonalised recurrence continues
-  // unchanged from index r.  Keeping many Ritz vectors preserves the
-  // convergence of the lowest pair when it is nearly degenerate, where a
-  // one-vector restart stalls.
-  const int keep = std::max(1, m / 2);
-  // budget of about 3840 matvecs (60 cycles of a 64-vector space), whatever m
-  const int max_restarts = std::max(60, 3840 / std::max(1, m - keep));
-  ThickRestart thick;
-  std::vector<double> gq;
-  std::vector<cplx> gqc;
-  int j0 = 0;
-  for (int restart = 0; restart < max_restarts; restart++) {
-    enqueue(j0);
-    for (int j = j0; j < m; j++) {
-      if (j + 1 < m) enqueue(j + 1);
-      MPSGPU_CUDA(cudaEventSynchronize(c.iter_ev[j]));
-      check_step();
-      const double alpha = c.hsc->alpha[j];
-      const double beta = c.hsc->beta[j];
-      MPSGPU_CHECK(std::isfinite(alpha) && std::isfinite(beta), MPSGPU_NAN, "lanczos: non-finite value");
-      a.push_back(alpha);
-      b2v.push_back(beta);
-      double normT = 0.0;
-      const double th_old = theta;
-      if (have_theta)
-        tri.solve_from(a, b2v, (int)a.size(), th_old, 4.0 * step_hint, theta, s, normT);
-      else
-        tri.solve(a, b2v, (int)a.size(), theta, s, normT);
-      step_hint = have_theta ? std::fabs(th_old - theta) : 0.0;
-      have_theta = true;
-      sigma = theta;
-      const double res = beta * std::fabs(s[j]);
-      const double scale = std::max(normT, std::fabs(theta));
-      if (res <= tol * scale || beta <= 1e-14 * scale || j + 1 == N) {
-        ritz_vector(j + 1);
-        return theta;
+
+  // Enqueue one round: iteration it[q] of every listed task.
+  std::vector<std::pair<int, int>> round;  // (task, iteration)
+  auto launch_round = [&](const std::vector<std::pair<int, int>>& items, cudaEvent_t ev) {
+    const auto t0 = clk::now();
+    Gemm1wBatch g1;
+    Gemm3Batch g3;
+    auto flush = [&]() {
+      if (g1.n) heff_gemm1w(st, g1);
+      if (g3.n) heff_gemm3(st, g3);
+      g1.n = g3.n = 0;
+    };
+    for (auto& it : items) {
+      LzState& z = S[it.first];
+      LzTask& t = *z.t;
+      if (g1.n + 2 > GEMM_MAXP || g3.n + 1 > GEMM_MAXP) flush();
+      t.product(t.ws->V.p + (long long)it.second * t.N, t.ws->w.p, z.sigma, g1, g3);
+    }
+    flush();
+    for (size_t i0 = 0; i0 < items.size(); i0 += LZ_MAXI) {
+      LzBatch b;
+      b.ninst = (int)std::min<size_t>(LZ_MAXI, items.size() - i0);
+      b.part = part;
+      b.h = hbuf;
+      b.h2 = h2buf;
+      b.pn1 = pn1;
+      b.pn2 = pn2;
+      b.bar = c.dcounter + 96;
+      b.err = c.dlz_err;
+      for (int i = 0; i < b.ninst; i++) {
+        LzState& z = S[items[i0 + i].first];
+        LzTask& t = *z.t;
+        const int j = items[i0 + i].second;
+        LzInst& in = b.in[i];
+        in.n = t.N;
+        in.j = j;
+        in.k = j + 1;
+        in.nu = t.nu;
+        in.U = t.U;
+        in.write_next = j + 1 < z.m ? 1 : 0;
+        in.sigma = z.sigma;
+        in.V = t.ws->V.p;
+        in.ldv = t.N;
+        in.w = t.ws->w.p;
+        in.sc = t.ws->dsc;
+        in.mirror = t.ws->hsc_dev;
       }
+      lanczos_step(st, b);
     }
-    if (keep >= m) {
+    MPSGPU_CUDA(cudaEventRecord(ev, c.stream));
+    for (auto& it : items) {
+      S[it.first].jq = it.second;
+      S[it.first].t->iters++;
+    }
+    const double dt = secs(t0, clk::now()) / items.size();
+    for (auto& it : items)
+      if (S[it.first].t->cnt) S[it.first].t->cnt->host_launch_s += dt;
+  };
+
+  // Ritz vector of a task's tridiagonal (k x k) into its x, normalised (enqueued)
+  auto ritz_vector = [&](LzState& z, int k) {
+    LzTask& t = *z.t;
+    MPSGPU_CUDA(cudaMemcpyAsync(t.ws->dS, z.s.data(), k * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    combine_real(st, t.N, k, t.ws->V.p, t.N, t.ws->dS, t.x);
+    dznrm2(st, t.N, t.x, d_tmp, c.scratch);
+    zscal_inv(st, t.N, t.x, d_tmp, t.x);
+    t.theta = z.theta;
+    z.done = true;
+  };
+
+  // compress after a cycle without convergence (ThickRestart); true when
+  // the kept space already holds the converged pair
+  auto compress = [&](LzState& z) -> bool {
+    LzTask& t = *z.t;
+    const int m = z.m, N = t.N;
+    if (z.keep >= m) {
       // no room to keep more than one vector: restart from the Ritz vector
-      ritz_vector(m);
-      zcopy(st, N, x, V);
-      a.clear();
-      b2v.clear();
-      j0 = 0;
-      continue;
+      ritz_vector(z, m);
+      z.done = false;
+      zcopy(st, N, t.x, t.ws->V.p);
+      z.a.clear();
+      z.b.clear();
+      z.j0 = 0;
+      return false;
     }
-    // compress: V[:, 0..r) <- V G; V[:, r] = f / |f| with f = w, the
-    // orthogonalised (not normalised) residual of step m-1
-    const double fnorm = b2v[m - 1];
-    const int r = thick.compress(a, b2v, m, keep, fnorm, gq);
-    gqc.resize(gq.size());
-    for (size_t i = 0; i < gq.size(); i++) gqc[i] = make_double2(gq[i], 0.0);
-    dbuf_reserve(c, c.lanQ, (long long)gqc.size());
-    dbuf_reserve(c, c.lanT, (long long)N * r);
-    MPSGPU_CUDA(cudaMemcpyAsync(c.lanQ.p, gqc.data(), gqc.size() * sizeof(cplx), cudaMemcpyHostToDevice,
+    // V[:, 0..r) <- V G; V[:, r] = f / |f| with f = w, the orthogonalised
+    // (not normalised) residual of step m-1
+    const double fnorm = z.b[m - 1];
+    const int r = z.thick.compress(z.a, z.b, m, z.keep, fnorm, z.gq);
+    z.gqc.resize(z.gq.size());
+    for (size_t i = 0; i < z.gq.size(); i++) z.gqc[i] = make_double2(z.gq[i], 0.0);
+    dbuf_reserve(c, t.ws->Q, (long long)z.gqc.size());
+    dbuf_reserve(c, t.ws->T, (long long)N * r);
+    MPSGPU_CUDA(cudaMemcpyAsync(t.ws->Q.p, z.gqc.data(), z.gqc.size() * sizeof(cplx), cudaMemcpyHostToDevice,
                                 c.stream));
     GemmArgs g;
     g.M = N; g.N = r; g.K = m;
-    g.A = V; g.lda = N;
-    g.B = c.lanQ.p; g.ldb = m;
-    g.C = c.lanT.p; g.ldc = N;
+    g.A = t.ws->V.p; g.lda = N;
+    g.B = t.ws->Q.p; g.ldb = m;
+    g.C = t.ws->T.p; g.ldc = N;
     zgemm(st, g, c.scratch);
-    MPSGPU_CUDA(cudaMemcpyAsync(V, c.lanT.p, (size_t)N * r * sizeof(cplx), cudaMemcpyDeviceToDevice, c.stream));
+    MPSGPU_CUDA(cudaMemcpyAsync(t.ws->V.p, t.ws->T.p, (size_t)N * r * sizeof(cplx), cudaMemcpyDeviceToDevice,
+                                c.stream));
     double normT = 0.0;
-    tri.solve(a, b2v, r, theta, s, normT);
-    const double scale = std::max(normT, std::fabs(theta));
-    if (b2v[r - 1] * std::fabs(s[r - 1]) <= tol * scale || b2v[r - 1] <= 1e-14 * scale) {
-      ritz_vector(r);  // converged within the kept space
-      return theta;
+    z.tri.solve(z.a, z.b, r, z.theta, z.s, normT);
+    const double scale = std::max(normT, std::fabs(z.theta));
+    if (z.b[r - 1] * std::fabs(z.s[r - 1]) <= t.tol * scale || z.b[r - 1] <= 1e-14 * scale) {
+      ritz_vector(z, r);  // converged within the kept space
+      return true;
     }
-    zscal_inv(st, N, w, &c.dsc->beta[m - 1], V + (long long)r * N);  // beta[m-1] = |f| on the device
+    zscal_inv(st, N, t.ws->w.p, &t.ws->dsc->beta[m - 1], t.ws->V.p + (long long)r * N);  // beta[m-1] = |f|
     // the coupling of V[:, r-1] to the new V[:, r], used by the next step
-    MPSGPU_CUDA(cudaMemcpyAsync(&c.dsc->beta[r - 1], &b2v[r - 1], sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    sigma = theta;
-    j0 = r;
+    MPSGPU_CUDA(cudaMemcpyAsync(&t.ws->dsc->beta[r - 1], &z.b[r - 1], sizeof(double), cudaMemcpyHostToDevice,
+                                c.stream));
+    z.sigma = z.theta;
+    z.j0 = r;
+    return false;
+  };
+
+  int rid = 0;
+  auto next_event = [&]() { return c.iter_ev[(rid++) % c.iter_ev.size()]; };
+  // round 0: the first iteration of every task
+  std::vector<std::pair<int, int>> cur;
+  for (int q = 0; q < nt; q++) cur.push_back({q, 0});
+  cudaEvent_t cur_ev = next_event();
+  launch_round(cur, cur_ev);
+  while (!cur.empty()) {
+    // speculative next round: every task of this round that continues its cycle,
+    // plus tasks restarting a cycle
+    std::vector<std::pair<int, int>> nxt;
+    for (int q = 0; q < nt; q++) {
+      LzState& z = S[q];
+      if (z.done) continue;
+      if (z.pending_restart) {
+        nxt.push_back({q, z.j0});
+        z.pending_restart = false;
+      } else if (z.jq >= 0 && z.jq + 1 < z.m && z.jq == z.jr + 1) {
+        nxt.push_back({q, z.jq + 1});
+      }
+    }
+    cudaEvent_t nxt_ev = nullptr;
+    if (!nxt.empty()) {
+      nxt_ev = next_event();
+      launch_round(nxt, nxt_ev);
+    }
+    const auto tw = clk::now();
+    MPSGPU_CUDA(cudaEventSynchronize(cur_ev));
+    check_step();
+    const auto tt = clk::now();
+    for (auto& it : cur) {
+      LzState& z = S[it.first];
+      LzTask& t = *z.t;
+      if (t.cnt) t.cnt->host_wait_s += secs(tw, tt) / cur.size();
+      if (z.done) continue;  // a speculative iteration after convergence
+      const int j = it.second;
+      z.jr = j;
+      const auto t0 = clk::now();
+      const double alpha = t.ws->hsc->alpha[j];
+      const double beta = t.ws->hsc->beta[j];
+      MPSGPU_CHECK(std::isfinite(alpha) && std::isfinite(beta), MPSGPU_NAN, "lanczos: non-finite value");
+      z.a.push_back(alpha);
+      z.b.push_back(beta);
+      double normT = 0.0;
+      const double th_old = z.theta;
+      if (z.have_theta)
+        z.tri.solve_from(z.a, z.b, (int)z.a.size(), th_old, 4.0 * z.step_hint, z.theta, z.s, normT);
+      else
+        z.tri.solve(z.a, z.b, (int)z.a.size(), z.theta, z.s, normT);
+      z.step_hint = z.have_theta ? std::fabs(th_old - z.theta) : 0.0;
+      z.have_theta = true;
+      z.sigma = z.theta;
+      const double res = beta * std::fabs(z.s[j]);
+      const double scale = std::max(normT, std::fabs(z.theta));
+      if (res <= t.tol * scale || beta <= 1e-14 * scale || j + 1 == t.N) {
+        ritz_vector(z, j + 1);
+      } else if (j + 1 == z.m) {
+        if (++z.restart >= z.max_restarts) throw Error(MPSGPU_NOT_CONVERGED, "lanczos: no convergence");
+        if (!compress(z)) {
+          z.pending_restart = true;
+          z.jq = z.jr = z.j0 - 1;
+        }
+      }
+      if (t.cnt) t.cnt->host_tridiag_s += secs(t0, clk::now());
+    }
+    cur = std::move(nxt);
+    cur_ev = nxt_ev;
+    // tasks that restarted (or stopped speculating) and are not in the round
+    // just launched start their next round after it
+    if (cur.empty()) {
+      for (int q = 0; q < nt; q++) {
+        LzState& z = S[q];
+        if (z.done) continue;
+        std::vector<std::pair<int, int>> one;
+        if (z.pending_restart) {
+          cur.push_back({q, z.j0});
+          z.pending_restart = false;
+        } else if (z.jq + 1 < z.m && z.jq == z.jr) {
+          cur.push_back({q, z.jq + 1});
+        }
+      }
+      if (!cur.empty()) {
+        cur_ev = next_event();
+        launch_round(cur, cur_ev);
+      }
+    }
   }
-  if (iters) *iters = total;
-  throw Error(MPSGPU_NOT_CONVERGED, "lanczos: no convergence");
+  for (auto& z : S) MPSGPU_CHECK(z.done, MPSGPU_NOT_CONVERGED, "lanczos: a task left the batch unfinished");
+  MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+  check_step();
+}
+
+// One local problem with a product that launches its own kernels (the
+// two-site sweep), as a batch of one.
+template <class Op>
+static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, int max_krylov, int* iters,
+                             double shift0, Counters* cnt = nullptr) {
+  LzWork& ws = c.lzone;
+  LzTask t;
+  t.N = N;
+  t.x = x;
+  t.tol = tol;
+  t.shift0 = shift0;
+  t.max_krylov = max_krylov;
+  t.ws = &ws;
+  t.cnt = cnt;
+  t.product = [&](const cplx* xin, cplx* yout, double sigma, Gemm1wBatch&, Gemm3Batch&) { apply(xin, yout, sigma); };
+  std::vector<LzTask*> v{&t};
+  lanczos_batch(c, v);
+  if (iters) *iters = t.iters;
+  return t.theta;
 }
 
 // ---------------------------------------------------------------------------
@@ -1252,113 +1430,252 @@ static void prepare_init(Context& c, MpsDev& init, int D) {
   mps_gauge_all(c, init, 'L', true);
 }
 
-double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
-                         const SolveOptions& opt, Counters& cnt) {
-  const int L = ops.L;
-  MPSGPU_CHECK(init.L == L, MPSGPU_BAD_SHAPE, "findGroundState: lengths differ");
-  for (int k = 0; k < L; k++)
-    MPSGPU_CHECK(init.dims[k][0] == ops.dims[k][2] && ops.dims[k][0] == ops.dims[k][2],
-                 MPSGPU_BAD_SHAPE, "findGroundState: physical dimensions differ");
-  prepare_init(c, init, D);
+namespace {
+
+// The single-site ground-state sweep of Contractor::findGroundState
+// (Contractor.cpp:1352-1533) as a state machine: prepare() builds the local
+// eigenproblem of the current site (environments, and the product that
+// effective Hamiltonian applies), finish() takes its lowest eigenvalue and
+// moves on (energy-increase guard, gauge move, convergence at the chain
+// ends), so that the sweeps of several chains at the same site can share
+// the launches of their local eigensolvers (lanczos_batch).
+//
+// Mixed precision (opt.precision == 1): split-precision products while the
+// sweep is far from convergence, FP64 from the half-sweep after the energy
+// change first falls below kSplitSwitchTol; the FP64 phase ends by the
+// reference's test, after at least one full FP64 round.  Energies in the
+// split phase carry the products' error (about 1e-7 relative), so its
+// eigensolver tolerance and energy-increase margin are set at that level,
+// and the first FP64 round is not tested for an increase.  precision 2:
+// the same schedule of tolerances with FP64 products (to separate what the
+// schedule saves from what the tensor cores save).
+struct GsSweep {
+  Context& c;
+  const MpoDev& ops;
+  MpsDev& init;
+  const SolveOptions& opt;
+  Counters& cnt;
+  LzWork& ws;
+  int D = 0, L = 0;
+  double offset = 0.0, tol = 1e-12;
   EnvCache E;
-  E.init(c, L);
-  double energy = contract(c, init, &ops, init).x;
-  double val = energy;
+  double energy = 0.0, val = 0.0;
   bool right = true, done = false;
   int pos = 0, round = 0;
-  const double tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
-  const cplx off = make_double2(offset, 0.0);
-  // Mixed precision (opt.precision == 1): split-precision products while the
-  // sweep is far from convergence, FP64 from the half-sweep after the energy
-  // change first falls below kSplitSwitchTol; the FP64 phase ends by the
-  // reference's test, after at least one full FP64 round.  Energies in the
-  // split phase carry the products' error (about 1e-7 relative), so its
-  // eigensolver tolerance and energy-increase margin are set at that level,
-  // and the first FP64 round is not tested for an increase.
-  // precision 2: the same schedule of tolerances with FP64 products (to
-  // separate what the schedule saves from what the tensor cores save)
-  bool split_phase = (opt.precision == 1 || opt.precision == 2);
-  const bool split_products = (opt.precision == 1);
-  bool first64 = false;
+  bool split_phase = false, split_products = false, first64 = false;
   SplitMatvec smv;
-  if (split_phase) *c.hsplit_err = 0;
-  try {
-    while (!done) {
-      opt.check_cancel();
-      calc_left(c, E, pos, &ops, init, init, &cnt);
-      calc_right(c, E, pos, &ops, init, init, &cnt);
-      const auto dims = init.dims[pos];
-      const int N = (int)nel(dims);
-      const cplx* Le = E.Le[pos].p;
-      const cplx* Rt = E.Re[pos].p;
-      auto ld = E.ldims[pos];
-      auto rd = E.rdims[pos];
-      smv.ready = false;
-      if (split_phase && split_products) split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
-      auto apply = [&](const cplx* xin, cplx* yout, double sg) {
-        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, make_double2(off.x - sg, off.y), &cnt,
-                   split_phase && split_products ? &smv : nullptr);
-      };
-      int its = 0;
-      const double etol = split_phase ? std::max(tol, kSplitEigTol) : first64 ? std::max(tol, kFirst64EigTol) : tol;
-      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, etol, opt.max_krylov, &its, val + offset);
-      cnt.site_solves++;
-      if (split_phase && *c.hsplit_err)
-        throw Error(MPSGPU_TIMEOUT, "findGroundState: a bounded wait in the tensor-core kernel ran out");
-      val = theta - offset;
-      if (!first64 && (val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
-        const double margin = split_phase ? std::max(opt.convtol, kSplitIncreaseTol) : opt.convtol;
-        if (val - energy > std::fabs(energy + offset) * margin)
-          throw Error(MPSGPU_ENERGY_INCREASE, "findGroundState: energy increasing");
+  // the current site
+  const cplx* Le = nullptr;
+  const cplx* Rt = nullptr;
+  std::array<int, 3> ld{}, rd{};
+
+  GsSweep(Context& c_, const MpoDev& ops_, int D_, MpsDev& init_, double offset_, const SolveOptions& opt_,
+          Counters& cnt_, LzWork& ws_)
+      : c(c_), ops(ops_), init(init_), opt(opt_), cnt(cnt_), ws(ws_), D(D_), L(ops_.L), offset(offset_) {}
+
+  void begin() {
+    MPSGPU_CHECK(init.L == L, MPSGPU_BAD_SHAPE, "findGroundState: lengths differ");
+    for (int k = 0; k < L; k++)
+      MPSGPU_CHECK(init.dims[k][0] == ops.dims[k][2] && ops.dims[k][0] == ops.dims[k][2], MPSGPU_BAD_SHAPE,
+                   "findGroundState: physical dimensions differ");
+    prepare_init(c, init, D);
+    E.init(c, L);
+    energy = contract(c, init, &ops, init).x;
+    val = energy;
+    tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
+    split_phase = (opt.precision == 1 || opt.precision == 2);
+    split_products = (opt.precision == 1);
+    if (split_phase) *c.hsplit_err = 0;
+  }
+
+  void prepare(LzTask& t) {
+    opt.check_cancel();
+    calc_left(c, E, pos, &ops, init, init, &cnt);
+    calc_right(c, E, pos, &ops, init, init, &cnt);
+    Le = E.Le[pos].p;
+    Rt = E.Re[pos].p;
+    ld = E.ldims[pos];
+    rd = E.rdims[pos];
+    smv.ready = false;
+    if (split_phase && split_products) split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
+    t = LzTask();
+    t.N = (int)nel(init.dims[pos]);
+    t.x = init.A[pos].p;
+    t.tol = split_phase ? std::max(tol, kSplitEigTol) : first64 ? std::max(tol, kFirst64EigTol) : tol;
+    t.shift0 = val + offset;
+    t.max_krylov = opt.max_krylov;
+    t.ws = &ws;
+    t.cnt = &cnt;
+    t.product = [this](const cplx* xin, cplx* yout, double sg, Gemm1wBatch& g1, Gemm3Batch& g3) {
+      const cplx o = make_double2(offset - sg, 0.0);
+      if (split_phase && split_products) {
+        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, o, &cnt, &smv);
+        return;
       }
-      mps_gauge_site(c, init, pos, right ? 'R' : 'L', true, &cnt);
-      for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
-      for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
-      const bool at_end = right ? (pos == L - 1) : (pos == 0);
-      if (at_end) {
-        const double change = std::fabs(energy - val);
-        const bool was_split = split_phase;
-        done = change < opt.convtol * std::fabs(energy + offset);
-        if (!done && std::fabs(val) < 1e-13) done = true;
-        if (split_phase) {
-          cnt.split_rounds++;
-          if (change < std::max(opt.convtol, kSplitSwitchTol) * std::fabs(energy + offset)) {
-            split_phase = false;
-            first64 = true;
-          }
-          done = false;
-        } else if (first64) {
-          // the first FP64 half-sweep was compared with a split-phase energy
-          first64 = false;
-          done = false;
-        }
-        energy = val;
-        if (opt.verbose)
-          printf("mpsgpu: round %d energy %.15g%s\n", round, val, was_split ? " (split)" : "");
-        if (!done) {
-          mps_gauge_site(c, init, pos, right ? 'L' : 'R', true, &cnt);
-          pos += right ? -1 : 1;
-        }
-        right = !right;
-        round++;
-        // intermediate result every checkpoint_every half-sweeps (Contractor.cpp:1526-1530)
-        if (!done && !opt.checkpoint.empty() && round % std::max(1, opt.checkpoint_every) == 0)
-          mps_export_file(c, init, opt.checkpoint);
-      } else {
-        pos += right ? 1 : -1;
-      }
-      if (!done && round >= opt.max_rounds)
-        throw Error(MPSGPU_NOT_CONVERGED, "findGroundState: round limit reached");
+      const auto& wd = ops.dims[pos];
+      const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
+      const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
+      MPSGPU_CHECK(ld[1] == wl && rd[1] == wr, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
+      dbuf_reserve(c, ws.t2, (long long)Dlb * du * Drk * wr);
+      g1.d[g1.n++] = heff_first_desc(Le, Dlb, Dlk, wl, xin, dd, Drk, ops.Wlr[pos].p, du, wr, ws.t2.p);
+      g3.d[g3.n++] = heff_last_desc(ws.t2.p, Dlb * du, Rt, Drk * wr, Drb, yout, xin, o);
+      cnt.matvecs++;
+      cnt.flops += mv_flops(dd, wl, wr, Dlb, Drb);
+    };
+  }
+
+  void finish(double theta) {
+    cnt.site_solves++;
+    if (split_phase && *c.hsplit_err)
+      throw Error(MPSGPU_TIMEOUT, "findGroundState: a bounded wait in the tensor-core kernel ran out");
+    val = theta - offset;
+    if (!first64 && (val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
+      const double margin = split_phase ? std::max(opt.convtol, kSplitIncreaseTol) : opt.convtol;
+      if (val - energy > std::fabs(energy + offset) * margin)
+        throw Error(MPSGPU_ENERGY_INCREASE, "findGroundState: energy increasing");
     }
-  } catch (...) {
+    mps_gauge_site(c, init, pos, right ? 'R' : 'L', true, &cnt);
+    for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
+    for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
+    const bool at_end = right ? (pos == L - 1) : (pos == 0);
+    if (at_end) {
+      const double change = std::fabs(energy - val);
+      const bool was_split = split_phase;
+      done = change < opt.convtol * std::fabs(energy + offset);
+      if (!done && std::fabs(val) < 1e-13) done = true;
+      if (split_phase) {
+        cnt.split_rounds++;
+        if (change < std::max(opt.convtol, kSplitSwitchTol) * std::fabs(energy + offset)) {
+          split_phase = false;
+          first64 = true;
+        }
+        done = false;
+      } else if (first64) {
+        // the first FP64 half-sweep was compared with a split-phase energy
+        first64 = false;
+        done = false;
+      }
+      energy = val;
+      if (opt.verbose) printf("mpsgpu: round %d energy %.15g%s\n", round, val, was_split ? " (split)" : "");
+      if (!done) {
+        mps_gauge_site(c, init, pos, right ? 'L' : 'R', true, &cnt);
+        pos += right ? -1 : 1;
+      }
+      right = !right;
+      round++;
+      // intermediate result every checkpoint_every half-sweeps (Contractor.cpp:1526-1530)
+      if (!done && !opt.checkpoint.empty() && round % std::max(1, opt.checkpoint_every) == 0)
+        mps_export_file(c, init, opt.checkpoint);
+    } else {
+      pos += right ? 1 : -1;
+    }
+    if (!done && round >= opt.max_rounds) throw Error(MPSGPU_NOT_CONVERGED, "findGroundState: round limit reached");
+  }
+
+  void release() {
     E.release(c);
     split_matvec_release(c, smv);
+    cnt.rounds += round;
+  }
+};
+
+// Drives sweeps that share the same site positions: each round of site
+// steps prepares every live sweep, solves all their local problems in one
+// lanczos_batch and lets each sweep finish its step.  A sweep that fails
+// stops with its own status; the others go on.
+template <class Sweep>
+void run_sweeps(Context& c, std::vector<Sweep*>& sw, std::vector<int>& status, std::vector<std::string>& err) {
+  const int n = (int)sw.size();
+  status.assign(n, MPSGPU_OK);
+  err.assign(n, std::string());
+  auto fail = [&](int i, const Error& e) {
+    status[i] = e.status;
+    err[i] = e.what();
+  };
+  std::vector<char> live(n, 1);
+  for (int i = 0; i < n; i++) {
+    try {
+      sw[i]->begin();
+    } catch (const Error& e) {
+      fail(i, e);
+      live[i] = 0;
+    }
+  }
+  std::vector<LzTask> tasks(n);
+  for (;;) {
+    std::vector<LzTask*> tp;
+    std::vector<int> idx;
+    for (int i = 0; i < n; i++) {
+      if (!live[i] || sw[i]->done) continue;
+      try {
+        sw[i]->prepare(tasks[i]);
+        tp.push_back(&tasks[i]);
+        idx.push_back(i);
+      } catch (const Error& e) {
+        fail(i, e);
+        live[i] = 0;
+      }
+    }
+    if (tp.empty()) break;
+    try {
+      lanczos_batch(c, tp);
+    } catch (const Error& e) {
+      // the round's local problems are lost: every sweep in it stops
+      for (int i : idx) {
+        fail(i, e);
+        live[i] = 0;
+      }
+      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+      continue;
+    }
+    for (size_t q = 0; q < idx.size(); q++) {
+      const int i = idx[q];
+      try {
+        sw[i]->finish(tasks[i].theta);
+      } catch (const Error& e) {
+        fail(i, e);
+        live[i] = 0;
+      }
+    }
+  }
+  for (int i = 0; i < n; i++) sw[i]->release();
+}
+
+}  // namespace
+
+double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
+                         const SolveOptions& opt, Counters& cnt) {
+  GsSweep s(c, ops, D, init, offset, opt, cnt, c.lzone);
+  std::vector<GsSweep*> sw{&s};
+  std::vector<int> status;
+  std::vector<std::string> err;
+  run_sweeps(c, sw, status, err);
+  if (status[0] != MPSGPU_OK) throw Error((mpsgpu_status)status[0], err[0]);
+  return s.energy;
+}
+
+void find_ground_state_batch(Context& c, const std::vector<const MpoDev*>& ops, int D, std::vector<MpsDev*>& inits,
+                             double offset, const SolveOptions& opt, std::vector<double>& energies,
+                             std::vector<Counters>& cnts, std::vector<int>& status, std::vector<std::string>& err) {
+  const int n = (int)inits.size();
+  MPSGPU_CHECK(n >= 1 && (int)ops.size() == n, MPSGPU_INVALID, "findGroundState batch: sizes");
+  cnts.assign(n, Counters());
+  std::vector<LzWork> ws(n);
+  std::vector<std::unique_ptr<GsSweep>> own;
+  std::vector<GsSweep*> sw;
+  for (int i = 0; i < n; i++) {
+    own.emplace_back(new GsSweep(c, *ops[i], D, *inits[i], offset, opt, cnts[i], ws[i]));
+    sw.push_back(own.back().get());
+  }
+  try {
+    run_sweeps(c, sw, status, err);
+  } catch (...) {
+    for (auto& w : ws) w.release(c);
     throw;
   }
-  E.release(c);
-  split_matvec_release(c, smv);
-  cnt.rounds += round;
-  return energy;
+  energies.assign(n, 0.0);
+  for (int i = 0; i < n; i++) energies[i] = sw[i]->energy;
+  for (auto& w : ws) w.release(c);
 }
 
 // ---------------------------------------------------------------------------
@@ -1473,7 +1790,7 @@ double find_ground_state_two_site(Context& c, const MpoDev& ops, int D, MpsDev& 
         heff2_apply(c, Le, ld, ops, pos, Rt, rd, xin, yout, make_double2(off.x - sg, off.y), &cnt);
       };
       int its = 0;
-      const double theta = lanczos_lowest(c, (int)N, apply, th.p, tol, opt.max_krylov, &its, val + offset);
+      const double theta = lanczos_lowest(c, (int)N, apply, th.p, tol, opt.max_krylov, &its, val + offset, &cnt);
       cnt.site_solves++;
       val = theta - offset;
       // split Theta (Dl d1 x d2 Dr) = U S V^H, cut to D; the singular values
@@ -1551,189 +1868,245 @@ struct LevelCache {
 
 }  // namespace
 
-static double gs_with_projector_penalty(Context& c, const MpoDev& ops, int D, const std::vector<double>& pens,
-                                        const std::vector<const MpsDev*>& levels, MpsDev& init, double offset,
-                                        const SolveOptions& opt, Counters& cnt) {
-  const int L = ops.L;
-  const int nk = (int)levels.size();
-  MPSGPU_CHECK(nk <= LZ_MAXU, MPSGPU_BAD_SHAPE, "findNextExcitedState: at most 8 computed levels");
-  prepare_init(c, init, D);
-  double energy = contract(c, init, &ops, init).x + offset;
-  for (int k = 0; k < nk; k++) {
-    cplx ov = contract(c, init, nullptr, *levels[k]);
-    energy += pens[k] * cabs2(ov);
-  }
-  energy -= offset;
+namespace {
+
+// findGroundStateWithProjectorPenalty (Contractor.cpp:2739-2956) as a state
+// machine (see GsSweep), with the Hermitian, projected multiplier
+// TensorMultiplierProjMulti(hermitian=true) (TensorMultiplierProjMulti.cpp:
+// 81-90).  Mixed precision as in GsSweep: split-precision products of both
+// halves of the Hermitian multiplier until the half-sweep energy settles,
+// then FP64 (at least one full round).
+struct ExcSweep {
+  Context& c;
+  const MpoDev& ops;
+  MpsDev& init;
+  const SolveOptions& opt;
+  Counters& cnt;
+  LzWork& ws;
+  std::vector<double> pens;
+  std::vector<const MpsDev*> levels;
+  int D = 0, L = 0, nk = 0;
+  double offset = 0.0, tol = 1e-12;
   EnvCache E;
-  E.init(c, L);
-  std::vector<EnvCache> NC(nk);
-  for (auto& n : NC) n.init(c, L);
-  DBuf Lh, Rth, U, y2, sq;
-  double val = energy;
+  std::vector<EnvCache> NC;
+  DBuf Lh, Rth, U;
+  double energy = 0.0, val = 0.0;
   bool right = true, done = false;
   int pos = 0, round = 0;
-  const double tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
-  // mixed precision as in find_ground_state: split-precision products of
-  // both halves of the Hermitian multiplier until the half-sweep energy
-  // settles, then FP64 (at least one full round)
-  bool split_phase = (opt.precision == 1 || opt.precision == 2);
-  const bool split_products = (opt.precision == 1);
-  bool first64 = false;
+  bool split_phase = false, split_products = false, first64 = false;
   SplitMatvec smv, smvh;
-  if (split_phase) *c.hsplit_err = 0;
-  auto last_saved = std::chrono::steady_clock::now();
-  auto cleanup = [&]() {
-    E.release(c);
-    for (auto& n : NC) n.release(c);
-    for (DBuf* b : {&Lh, &Rth, &U, &y2, &sq}) dbuf_free(c, *b);
-    split_matvec_release(c, smv);
-    split_matvec_release(c, smvh);
-  };
-  try {
-    while (!done) {
-      // calculateLexck / calculateRexck (Contractor.cpp:2958-2988): one set of flags
-      {
-        std::vector<int> needL, needR;
-        int p = pos;
-        while (!E.okL[p]) needL.push_back(p--);
-        for (int q = (int)needL.size() - 1; q >= 0; q--) {
-          const int pp = needL[q];
-          env_left_update(c, E.Le[pp - 1].p, E.ldims[pp - 1], init, &ops, pp - 1, init, E.Le[pp], E.ldims[pp], &cnt);
-          for (int k = 0; k < nk; k++)
-            env_left_update(c, NC[k].Le[pp - 1].p, NC[k].ldims[pp - 1], init, nullptr, pp - 1, *levels[k],
-                            NC[k].Le[pp], NC[k].ldims[pp], &cnt);
-          E.okL[pp] = 1;
-        }
-        p = pos;
-        while (!E.okR[p]) needR.push_back(p++);
-        for (int q = (int)needR.size() - 1; q >= 0; q--) {
-          const int pp = needR[q];
-          env_right_update(c, E.Re[pp + 1].p, E.rdims[pp + 1], init, &ops, pp + 1, init, E.Re[pp], E.rdims[pp], &cnt);
-          for (int k = 0; k < nk; k++)
-            env_right_update(c, NC[k].Re[pp + 1].p, NC[k].rdims[pp + 1], init, nullptr, pp + 1, *levels[k],
-                             NC[k].Re[pp], NC[k].rdims[pp], &cnt);
-          E.okR[pp] = 1;
-        }
+  std::chrono::steady_clock::time_point last_saved;
+  const cplx* Le = nullptr;
+  const cplx* Rt = nullptr;
+  std::array<int, 3> ld{}, rd{};
+
+  ExcSweep(Context& c_, const MpoDev& ops_, int D_, const std::vector<double>& pens_,
+           const std::vector<const MpsDev*>& levels_, MpsDev& init_, double offset_, const SolveOptions& opt_,
+           Counters& cnt_, LzWork& ws_)
+      : c(c_), ops(ops_), init(init_), opt(opt_), cnt(cnt_), ws(ws_), pens(pens_), levels(levels_), D(D_),
+        L(ops_.L), nk((int)levels_.size()), offset(offset_) {}
+
+  void begin() {
+    MPSGPU_CHECK(nk <= LZ_MAXU, MPSGPU_BAD_SHAPE, "findNextExcitedState: at most 8 computed levels");
+    prepare_init(c, init, D);
+    energy = contract(c, init, &ops, init).x + offset;
+    for (int k = 0; k < nk; k++) {
+      cplx ov = contract(c, init, nullptr, *levels[k]);
+      energy += pens[k] * cabs2(ov);
+    }
+    energy -= offset;
+    E.init(c, L);
+    NC.resize(nk);
+    for (auto& n : NC) n.init(c, L);
+    val = energy;
+    tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
+    split_phase = (opt.precision == 1 || opt.precision == 2);
+    split_products = (opt.precision == 1);
+    if (split_phase) *c.hsplit_err = 0;
+    last_saved = std::chrono::steady_clock::now();
+  }
+
+  void prepare(LzTask& t) {
+    opt.check_cancel();
+    // calculateLexck / calculateRexck (Contractor.cpp:2958-2988): one set of flags
+    {
+      std::vector<int> needL, needR;
+      int p = pos;
+      while (!E.okL[p]) needL.push_back(p--);
+      for (int q = (int)needL.size() - 1; q >= 0; q--) {
+        const int pp = needL[q];
+        env_left_update(c, E.Le[pp - 1].p, E.ldims[pp - 1], init, &ops, pp - 1, init, E.Le[pp], E.ldims[pp], &cnt);
+        for (int k = 0; k < nk; k++)
+          env_left_update(c, NC[k].Le[pp - 1].p, NC[k].ldims[pp - 1], init, nullptr, pp - 1, *levels[k],
+                          NC[k].Le[pp], NC[k].ldims[pp], &cnt);
+        E.okL[pp] = 1;
       }
-      const auto dims = init.dims[pos];
-      const int N = (int)nel(dims);
-      const int Dlk = dims[1], d = dims[0], Drk = dims[2];
-      const auto ld = E.ldims[pos];
-      const auto rd = E.rdims[pos];
-      // adjoint environments: L^dag(bra,w,ket) = conj(L(ket,w,bra)), Rt^dag likewise
-      dbuf_reserve(c, Lh, nel(ld));
-      dbuf_reserve(c, Rth, nel(rd));
-      transpose_pqr_to_rqp(c.st(), ld[0], ld[1], ld[2], E.Le[pos].p, Lh.p, true);
-      transpose_pqr_to_rqp(c.st(), rd[0], rd[1], rd[2], E.Re[pos].p, Rth.p, true);
-      // projector vectors u_k (sqrt(pen_k) folded in), columns of U (N x nk)
-      dbuf_reserve(c, U, (long long)N * nk);
-      for (int k = 0; k < nk; k++) {
-        const MpsDev& lv = *levels[k];
-        const auto bd = lv.dims[pos];
-        const auto nl = NC[k].ldims[pos];  // (Dlb, 1, Dlk)
-        const auto nr = NC[k].rdims[pos];  // (Drk, 1, Drb)
-        dbuf_reserve(c, c.t3, (long long)Dlk * d * bd[2]);
-        GemmArgs g1;
-        g1.M = Dlk; g1.N = d * bd[2]; g1.K = nl[0];
-        g1.A = NC[k].Le[pos].p; g1.lda = nl[0]; g1.opA = OP_C;
-        g1.B = lv.A[pos].p; g1.ldb = bd[1];
-        g1.C = c.t3.p; g1.ldc = Dlk;
-        zgemm(c.st(), g1, c.scratch);
-        GemmArgs g2;
-        g2.M = Dlk * d; g2.N = Drk; g2.K = bd[2];
-        g2.A = c.t3.p; g2.lda = (long long)Dlk * d;
-        g2.B = NC[k].Re[pos].p; g2.ldb = nr[0]; g2.opB = OP_C;
-        g2.C = U.p + (long long)k * N; g2.ldc = (long long)Dlk * d;
-        g2.alpha = make_double2(std::sqrt(pens[k]), 0.0);
-        zgemm(c.st(), g2, c.scratch);
-      }
-      const cplx* Le = E.Le[pos].p;
-      const cplx* Rt = E.Re[pos].p;
-      smv.ready = smvh.ready = false;
-      if (split_phase && split_products) {
-        split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
-        split_matvec_prepare(c, smvh, Lh.p, ld, ops, pos, Rth.p, rd);
-      }
-      // 1/2 (H + H^dag) x + (offset - sigma) x; the projector term
-      // sum_k pen_k u_k (u_k^H x) is added by the Lanczos step
-      auto apply = [&](const cplx* xin, cplx* yout, double sg) {
-        heff_apply_hermitian(c, Le, Lh.p, ld, ops, pos, Rt, Rth.p, rd, xin, yout, make_double2(offset - sg, 0.0),
-                             &cnt, split_phase && split_products ? &smv : nullptr,
-                             split_phase && split_products ? &smvh : nullptr);
-      };
-      int its = 0;
-      const double etol = split_phase ? std::max(tol, kSplitEigTol) : first64 ? std::max(tol, kFirst64EigTol) : tol;
-      double theta = lanczos_lowest(c, N, apply, init.A[pos].p, etol, opt.max_krylov, &its, val + offset, U.p, nk);
-      cnt.site_solves++;
-      if (split_phase && *c.hsplit_err)
-        throw Error(MPSGPU_TIMEOUT, "findNextExcitedState: a bounded wait in the tensor-core kernel ran out");
-      val = theta - offset;
-      if (!first64 && (val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
-        const double margin = split_phase ? kSplitIncreaseTol : 1e-6;
-        if (val - energy > std::fabs(energy + offset) * margin)
-          throw Error(MPSGPU_ENERGY_INCREASE, "findNextExcitedState: energy increasing");
-      }
-      mps_gauge_site(c, init, pos, right ? 'R' : 'L', true, &cnt);
-      for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
-      for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
-      const bool at_end = (right && pos == L - 1) || (!right && pos == 0);
-      if (at_end && !opt.checkpoint.empty()) {
-        // save at the end of every half-sweep, or every checkpoint_seconds
-        // (Contractor.cpp:2868-2883)
-        const auto now = std::chrono::steady_clock::now();
-        if (opt.checkpoint_seconds <= 0.0 ||
-            std::chrono::duration<double>(now - last_saved).count() >= opt.checkpoint_seconds) {
-          mps_export_file(c, init, opt.checkpoint);
-          last_saved = now;
-        }
-      }
-      if (at_end) {
-        const double change = std::fabs(energy - val);
-        const bool was_split = split_phase;
-        done = change < opt.convtol * std::fabs(energy + offset);
-        if (!done && (change < 1e-12 || round > MAX_ROUND_EXCTD)) done = true;
-        if (split_phase) {
-          cnt.split_rounds++;
-          if (change < std::max(opt.convtol, kSplitSwitchTol) * std::fabs(energy + offset) ||
-              round > MAX_ROUND_EXCTD) {
-            split_phase = false;
-            first64 = true;
-          }
-          done = false;
-        } else if (first64) {
-          first64 = false;
-          done = false;
-        }
-        energy = val;
-        if (opt.verbose)
-          printf("mpsgpu: excited round %d energy %.15g%s\n", round, val, was_split ? " (split)" : "");
-        if (!done) {
-          if (right) { mps_gauge_site(c, init, pos, 'L', true, &cnt); pos--; }
-          else { mps_gauge_site(c, init, pos, 'R', true, &cnt); pos++; }
-        }
-        right = !right;
-        round++;
-        if (!done && round >= opt.max_rounds)
-          throw Error(MPSGPU_NOT_CONVERGED, "findNextExcitedState: round limit reached");
-      } else {
-        pos += right ? 1 : -1;
+      p = pos;
+      while (!E.okR[p]) needR.push_back(p++);
+      for (int q = (int)needR.size() - 1; q >= 0; q--) {
+        const int pp = needR[q];
+        env_right_update(c, E.Re[pp + 1].p, E.rdims[pp + 1], init, &ops, pp + 1, init, E.Re[pp], E.rdims[pp], &cnt);
+        for (int k = 0; k < nk; k++)
+          env_right_update(c, NC[k].Re[pp + 1].p, NC[k].rdims[pp + 1], init, nullptr, pp + 1, *levels[k],
+                           NC[k].Re[pp], NC[k].rdims[pp], &cnt);
+        E.okR[pp] = 1;
       }
     }
-  } catch (...) {
-    cleanup();
-    throw;
+    const auto dims = init.dims[pos];
+    const int N = (int)nel(dims);
+    const int Dlk = dims[1], d = dims[0], Drk = dims[2];
+    ld = E.ldims[pos];
+    rd = E.rdims[pos];
+    // adjoint environments: L^dag(bra,w,ket) = conj(L(ket,w,bra)), Rt^dag likewise
+    dbuf_reserve(c, Lh, nel(ld));
+    dbuf_reserve(c, Rth, nel(rd));
+    transpose_pqr_to_rqp(c.st(), ld[0], ld[1], ld[2], E.Le[pos].p, Lh.p, true);
+    transpose_pqr_to_rqp(c.st(), rd[0], rd[1], rd[2], E.Re[pos].p, Rth.p, true);
+    // projector vectors u_k (sqrt(pen_k) folded in), columns of U (N x nk)
+    // (Contractor::contractMbraId, Contractor.cpp:880-903)
+    dbuf_reserve(c, U, (long long)N * nk);
+    for (int k = 0; k < nk; k++) {
+      const MpsDev& lv = *levels[k];
+      const auto bd = lv.dims[pos];
+      const auto nl = NC[k].ldims[pos];  // (Dlb, 1, Dlk)
+      const auto nr = NC[k].rdims[pos];  // (Drk, 1, Drb)
+      dbuf_reserve(c, c.t3, (long long)Dlk * d * bd[2]);
+      GemmArgs g1;
+      g1.M = Dlk; g1.N = d * bd[2]; g1.K = nl[0];
+      g1.A = NC[k].Le[pos].p; g1.lda = nl[0]; g1.opA = OP_C;
+      g1.B = lv.A[pos].p; g1.ldb = bd[1];
+      g1.C = c.t3.p; g1.ldc = Dlk;
+      zgemm(c.st(), g1, c.scratch);
+      GemmArgs g2;
+      g2.M = Dlk * d; g2.N = Drk; g2.K = bd[2];
+      g2.A = c.t3.p; g2.lda = (long long)Dlk * d;
+      g2.B = NC[k].Re[pos].p; g2.ldb = nr[0]; g2.opB = OP_C;
+      g2.C = U.p + (long long)k * N; g2.ldc = (long long)Dlk * d;
+      g2.alpha = make_double2(std::sqrt(pens[k]), 0.0);
+      zgemm(c.st(), g2, c.scratch);
+    }
+    Le = E.Le[pos].p;
+    Rt = E.Re[pos].p;
+    smv.ready = smvh.ready = false;
+    if (split_phase && split_products) {
+      split_matvec_prepare(c, smv, Le, ld, ops, pos, Rt, rd);
+      split_matvec_prepare(c, smvh, Lh.p, ld, ops, pos, Rth.p, rd);
+    }
+    t = LzTask();
+    t.N = N;
+    t.x = init.A[pos].p;
+    t.tol = split_phase ? std::max(tol, kSplitEigTol) : first64 ? std::max(tol, kFirst64EigTol) : tol;
+    t.shift0 = val + offset;
+    t.max_krylov = opt.max_krylov;
+    t.U = U.p;
+    t.nu = nk;
+    t.ws = &ws;
+    t.cnt = &cnt;
+    // 1/2 (H + H^dag) x + (offset - sigma) x; the projector term
+    // sum_k pen_k u_k (u_k^H x) is added by the Lanczos step
+    t.product = [this](const cplx* xin, cplx* yout, double sg, Gemm1wBatch& g1, Gemm3Batch& g3) {
+      const cplx o = make_double2(offset - sg, 0.0);
+      if (split_phase && split_products) {
+        heff_apply_hermitian(c, Le, Lh.p, ld, ops, pos, Rt, Rth.p, rd, xin, yout, o, &cnt, &smv, &smvh);
+        return;
+      }
+      const auto& wd = ops.dims[pos];
+      const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
+      const int Dlb = ld[0], Dlk_ = ld[2], Drk_ = rd[0], Drb = rd[2];
+      MPSGPU_CHECK(ld[1] == wl && rd[1] == wr && ops.Wlr_h[pos].p, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
+      const long long n2 = (long long)Dlb * du * Drk_ * wr;
+      dbuf_reserve(c, ws.t2, n2);
+      dbuf_reserve(c, ws.t3, n2);
+      g1.d[g1.n++] = heff_first_desc(Le, Dlb, Dlk_, wl, xin, dd, Drk_, ops.Wlr[pos].p, du, wr, ws.t2.p);
+      g1.d[g1.n++] = heff_first_desc(Lh.p, Dlb, Dlk_, wl, xin, dd, Drk_, ops.Wlr_h[pos].p, du, wr, ws.t3.p);
+      Gemm3Desc h = heff_last_desc(ws.t2.p, Dlb * du, Rt, Drk_ * wr, Drb, yout, xin, o);
+      h.K2 = Drk_ * wr;
+      h.A2 = ws.t3.p;
+      h.lda2 = (long long)Dlb * du;
+      h.B2 = Rth.p;
+      h.ldb2 = (long long)Drk_ * wr;
+      h.alpha = make_double2(0.5, 0.0);
+      g3.d[g3.n++] = h;
+      cnt.matvecs++;
+      cnt.flops += 2.0 * mv_flops(dd, wl, wr, Dlb, Drb);
+    };
   }
-  cleanup();
-  cnt.rounds += round;
-  return energy;
-}
 
-double find_next_excited_state(Context& c, const MpoDev& ops, int D, const std::vector<const MpsDev*>& levels,
-                               MpsDev& init, double offset, const SolveOptions& opt, Counters& cnt) {
+  void finish(double theta) {
+    cnt.site_solves++;
+    if (split_phase && *c.hsplit_err)
+      throw Error(MPSGPU_TIMEOUT, "findNextExcitedState: a bounded wait in the tensor-core kernel ran out");
+    val = theta - offset;
+    if (!first64 && (val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
+      const double margin = split_phase ? kSplitIncreaseTol : 1e-6;
+      if (val - energy > std::fabs(energy + offset) * margin)
+        throw Error(MPSGPU_ENERGY_INCREASE, "findNextExcitedState: energy increasing");
+    }
+    mps_gauge_site(c, init, pos, right ? 'R' : 'L', true, &cnt);
+    for (int l = pos + 1; l < L; l++) E.outofdate_l(l);
+    for (int l = pos - 1; l >= 0; l--) E.outofdate_r(l);
+    const bool at_end = (right && pos == L - 1) || (!right && pos == 0);
+    if (at_end && !opt.checkpoint.empty()) {
+      // save at the end of every half-sweep, or every checkpoint_seconds
+      // (Contractor.cpp:2868-2883)
+      const auto now = std::chrono::steady_clock::now();
+      if (opt.checkpoint_seconds <= 0.0 ||
+          std::chrono::duration<double>(now - last_saved).count() >= opt.checkpoint_seconds) {
+        mps_export_file(c, init, opt.checkpoint);
+        last_saved = now;
+      }
+    }
+    if (at_end) {
+      const double change = std::fabs(energy - val);
+      const bool was_split = split_phase;
+      done = change < opt.convtol * std::fabs(energy + offset);
+      if (!done && (change < 1e-12 || round > MAX_ROUND_EXCTD)) done = true;
+      if (split_phase) {
+        cnt.split_rounds++;
+        if (change < std::max(opt.convtol, kSplitSwitchTol) * std::fabs(energy + offset) || round > MAX_ROUND_EXCTD) {
+          split_phase = false;
+          first64 = true;
+        }
+        done = false;
+      } else if (first64) {
+        first64 = false;
+        done = false;
+      }
+      energy = val;
+      if (opt.verbose) printf("mpsgpu: excited round %d energy %.15g%s\n", round, val, was_split ? " (split)" : "");
+      if (!done) {
+        if (right) {
+          mps_gauge_site(c, init, pos, 'L', true, &cnt);
+          pos--;
+        } else {
+          mps_gauge_site(c, init, pos, 'R', true, &cnt);
+          pos++;
+        }
+      }
+      right = !right;
+      round++;
+      if (!done && round >= opt.max_rounds)
+        throw Error(MPSGPU_NOT_CONVERGED, "findNextExcitedState: round limit reached");
+    } else {
+      pos += right ? 1 : -1;
+    }
+  }
+
+  void release() {
+    E.release(c);
+    for (auto& n : NC) n.release(c);
+    for (DBuf* b : {&Lh, &Rth, &U}) dbuf_free(c, *b);
+    split_matvec_release(c, smv);
+    split_matvec_release(c, smvh);
+    cnt.rounds += round;
+  }
+};
+
+// The penalties of findNextExcitedState (Contractor.cpp:2676-2727): 20 times
+// the spread of the levels' energies, or L/2 for a single level.
+std::vector<double> excited_penalties(Context& c, const MpoDev& ops, const std::vector<const MpsDev*>& levels,
+                                      double offset) {
   const int nk = (int)levels.size();
-  MPSGPU_CHECK(nk >= 1, MPSGPU_INVALID, "findNextExcitedState: no levels");
-  for (auto* lv : levels) MPSGPU_CHECK(lv->L == ops.L, MPSGPU_BAD_SHAPE, "findNextExcitedState: level length");
-  MPSGPU_CHECK(init.L == ops.L, MPSGPU_BAD_SHAPE, "findNextExcitedState: init length");
   double minE = 0, maxE = 0;
   for (int k = 0; k < nk; k++) {
     double e = contract(c, *levels[k], &ops, *levels[k]).x + offset;
@@ -1742,20 +2115,99 @@ double find_next_excited_state(Context& c, const MpoDev& ops, int D, const std::
   }
   double newOffset = std::max(20 * (maxE - minE), std::fabs(offset));
   if (nk == 1 || newOffset < 1e-6) newOffset = levels[0]->L * 0.5;
-  std::vector<double> pens(nk, newOffset);
-  for (;;) {
-    double e = gs_with_projector_penalty(c, ops, D, pens, levels, init, offset, opt, cnt);
-    if (opt.excorthtol <= 0) return e;
-    bool again = false;
-    for (int k = 0; k < nk; k++) {
-      cplx ov = contract(c, init, nullptr, *levels[k]);
-      if (std::sqrt(cabs2(ov)) > opt.excorthtol) {
-        pens[k] *= 2;
-        again = true;
-      }
+  return std::vector<double>(nk, newOffset);
+}
+
+void check_levels(const MpoDev& ops, const std::vector<const MpsDev*>& levels, const MpsDev& init) {
+  MPSGPU_CHECK(!levels.empty(), MPSGPU_INVALID, "findNextExcitedState: no levels");
+  for (auto* lv : levels) MPSGPU_CHECK(lv->L == ops.L, MPSGPU_BAD_SHAPE, "findNextExcitedState: level length");
+  MPSGPU_CHECK(init.L == ops.L, MPSGPU_BAD_SHAPE, "findNextExcitedState: init length");
+}
+
+// excorthtol > 0: the levels the state still overlaps by more than
+// excorthtol get their penalty doubled (true: run again)
+bool raise_penalties(Context& c, const std::vector<const MpsDev*>& levels, const MpsDev& init, double excorthtol,
+                     std::vector<double>& pens) {
+  bool again = false;
+  for (size_t k = 0; k < levels.size(); k++) {
+    cplx ov = contract(c, init, nullptr, *levels[k]);
+    if (std::sqrt(cabs2(ov)) > excorthtol) {
+      pens[k] *= 2;
+      again = true;
     }
-    if (!again) return e;
   }
+  return again;
+}
+
+}  // namespace
+
+double find_next_excited_state(Context& c, const MpoDev& ops, int D, const std::vector<const MpsDev*>& levels,
+                               MpsDev& init, double offset, const SolveOptions& opt, Counters& cnt) {
+  check_levels(ops, levels, init);
+  std::vector<double> pens = excited_penalties(c, ops, levels, offset);
+  for (;;) {
+    ExcSweep s(c, ops, D, pens, levels, init, offset, opt, cnt, c.lzone);
+    std::vector<ExcSweep*> sw{&s};
+    std::vector<int> status;
+    std::vector<std::string> err;
+    run_sweeps(c, sw, status, err);
+    if (status[0] != MPSGPU_OK) throw Error((mpsgpu_status)status[0], err[0]);
+    if (opt.excorthtol <= 0 || !raise_penalties(c, levels, init, opt.excorthtol, pens)) return s.energy;
+  }
+}
+
+void find_next_excited_state_batch(Context& c, const std::vector<const MpoDev*>& ops, int D,
+                                   const std::vector<std::vector<const MpsDev*>>& levels, std::vector<MpsDev*>& inits,
+                                   double offset, const SolveOptions& opt, std::vector<double>& energies,
+                                   std::vector<Counters>& cnts, std::vector<int>& status,
+                                   std::vector<std::string>& err) {
+  const int n = (int)inits.size();
+  MPSGPU_CHECK(n >= 1 && (int)ops.size() == n && (int)levels.size() == n, MPSGPU_INVALID,
+               "findNextExcitedState batch: sizes");
+  cnts.assign(n, Counters());
+  energies.assign(n, 0.0);
+  status.assign(n, MPSGPU_OK);
+  err.assign(n, std::string());
+  std::vector<std::vector<double>> pens(n);
+  std::vector<int> todo;
+  for (int i = 0; i < n; i++) {
+    try {
+      check_levels(*ops[i], levels[i], *inits[i]);
+      pens[i] = excited_penalties(c, *ops[i], levels[i], offset);
+      todo.push_back(i);
+    } catch (const Error& e) {
+      status[i] = e.status;
+      err[i] = e.what();
+    }
+  }
+  std::vector<LzWork> ws(n);
+  try {
+    while (!todo.empty()) {
+      std::vector<std::unique_ptr<ExcSweep>> own;
+      std::vector<ExcSweep*> sw;
+      for (int i : todo) {
+        own.emplace_back(new ExcSweep(c, *ops[i], D, pens[i], levels[i], *inits[i], offset, opt, cnts[i], ws[i]));
+        sw.push_back(own.back().get());
+      }
+      std::vector<int> st;
+      std::vector<std::string> er;
+      run_sweeps(c, sw, st, er);
+      std::vector<int> again;
+      for (size_t q = 0; q < todo.size(); q++) {
+        const int i = todo[q];
+        status[i] = st[q];
+        err[i] = er[q];
+        energies[i] = sw[q]->energy;
+        if (st[q] == MPSGPU_OK && opt.excorthtol > 0 && raise_penalties(c, levels[i], *inits[i], opt.excorthtol, pens[i]))
+          again.push_back(i);
+      }
+      todo = again;
+    }
+  } catch (...) {
+    for (auto& w : ws) w.release(c);
+    throw;
+  }
+  for (auto& w : ws) w.release(c);
 }
 
 // ---------------------------------------------------------------------------

@@ -5,6 +5,7 @@
 
 #include <array>
 #include <atomic>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -23,6 +24,20 @@ struct Context;
 
 void dbuf_reserve(Context& c, DBuf& b, long long n);
 void dbuf_free(Context& c, DBuf& b);
+
+// Workspace of one local eigenproblem (one per concurrent sweep): Krylov
+// basis V (N x (m+1)), the product w, the product's temporaries, the thick
+// restart's V G and G, and the Lanczos coefficients (device, and a pinned
+// host mirror the step writes through its mapping).
+struct LzWork {
+  DBuf V, w, t2, t3, T, Q;
+  LanczosScalars* dsc = nullptr;
+  LanczosScalars* hsc = nullptr;
+  LanczosScalars* hsc_dev = nullptr;
+  double* dS = nullptr;
+  void init(Context& c);
+  void release(Context& c);
+};
 
 struct MpoDev {
   int L = 0;
@@ -53,9 +68,8 @@ struct Context {
   std::string last_error;
   // reusable workspaces (complex elements)
   DBuf t1, t2, t3, t4, matA, matQ, matR;
-  DBuf lanV, lanW;     // Lanczos basis and work vector
-  DBuf lanT, lanQ;     // thick restart: V G product and the restart matrix G
   DBuf lzws;           // workspace of the fused Lanczos step (partial dots and norms)
+  LzWork lzone;        // eigensolver workspace of single solves
   int* hlz_err = nullptr;  // pinned, mapped: set when a grid barrier of the Lanczos step ran out
   int* dlz_err = nullptr;  // its device address
   // split-precision matvec: prepared x and T2 (BF16 limb planes) and split-K partials
@@ -66,10 +80,6 @@ struct Context {
   cplx* dcplx = nullptr;       // device complex scalars (dots)
   double* hscal = nullptr;     // pinned host mirror
   cplx* hcplx = nullptr;
-  double* dS = nullptr;        // Ritz coefficients on device
-  LanczosScalars* dsc = nullptr;  // alpha/beta written by the fused kernels
-  LanczosScalars* hsc = nullptr;  // pinned, mapped host mirror
-  LanczosScalars* hsc_dev = nullptr;  // its device address
   unsigned* dcounter = nullptr;   // last-block ticket of the fused reductions
   std::vector<cudaEvent_t> iter_ev;  // one per Lanczos iteration in flight
   cudaEvent_t ev = nullptr;
@@ -109,6 +119,7 @@ struct Counters {
   int rounds = 0;
   long long split_matvecs = 0;  // products in split precision
   int split_rounds = 0;         // half-sweeps in split precision
+  double host_launch_s = 0.0, host_wait_s = 0.0, host_tridiag_s = 0.0;  // eigensolver loop, host side
 };
 
 struct SolveOptions {
@@ -187,6 +198,28 @@ void mps_import_file(Context& c, const std::string& fn, MpsDev& s);
 void mpo_save_file(Context& c, const MpoDev& m, const std::string& fn);
 void mpo_load_file(Context& c, const std::string& fn, MpoDev& m);
 
+// ---- local eigensolver (batched thick-restart Lanczos) ----
+// One local problem: product(x, y, sigma, g1, g3) must make y = (H - sigma) x
+// appear on the context's stream, either by appending FP64 descriptors to
+// the grouped launches g1/g3 (launched by the caller in the same round) or by
+// launching its own kernels.
+struct LzTask {
+  int N = 0;
+  cplx* x = nullptr;  // start vector in, normalised eigenvector out
+  double tol = 1e-12, shift0 = 0.0;
+  const cplx* U = nullptr;  // projector vectors (N x nu), sqrt(penalty) folded in
+  int nu = 0;
+  int max_krylov = 64;
+  std::function<void(const cplx*, cplx*, double, Gemm1wBatch&, Gemm3Batch&)> product;
+  LzWork* ws = nullptr;
+  Counters* cnt = nullptr;
+  double theta = 0.0;  // out: lowest Ritz value
+  int iters = 0;       // out: products
+};
+// Lowest eigenpairs of every task, advanced in lockstep rounds of grouped
+// launches; returns when all have converged (their x written).
+void lanczos_batch(Context& c, std::vector<LzTask*>& tasks);
+
 // ---- algorithms (Contractor) ----
 double find_ground_state(Context& c, const MpoDev& ops, int D, MpsDev& init, double offset,
                          const SolveOptions& opt, Counters& cnt);
@@ -195,6 +228,17 @@ double find_ground_state_two_site(Context& c, const MpoDev& ops, int D, MpsDev& 
 double find_next_excited_state(Context& c, const MpoDev& ops, int D,
                                const std::vector<const MpsDev*>& levels, MpsDev& init,
                                double offset, const SolveOptions& opt, Counters& cnt);
+// Several independent solves swept in lockstep on the context's stream: the
+// local eigenproblems of all chains at the same site share grouped launches
+// (lanczos_batch).  Per-solve results, counters, status and message.
+void find_ground_state_batch(Context& c, const std::vector<const MpoDev*>& ops, int D, std::vector<MpsDev*>& inits,
+                             double offset, const SolveOptions& opt, std::vector<double>& energies,
+                             std::vector<Counters>& cnts, std::vector<int>& status, std::vector<std::string>& err);
+void find_next_excited_state_batch(Context& c, const std::vector<const MpoDev*>& ops, int D,
+                                   const std::vector<std::vector<const MpsDev*>>& levels, std::vector<MpsDev*>& inits,
+                                   double offset, const SolveOptions& opt, std::vector<double>& energies,
+                                   std::vector<Counters>& cnts, std::vector<int>& status,
+                                   std::vector<std::string>& err);
 void optimize(Context& c, const MpoDev& ops, const MpsDev& orig, MpsDev& init, int D,
               const SolveOptions& opt, double* errN, double* errT, Counters& cnt);
 // optimizeSum: init ~ sum_k beta_k kets[k] at bond D (Contractor.cpp:2332-2477).

@@ -242,22 +242,10 @@ struct LanczosScalars {
   double ap;   // first-pass Re h_j, while a second pass is pending
   int flag;    // second pass needed
 };
-// One reorthogonalised Lanczos step after the matvec (lanczos.cu): with
-// k = j+1 basis vectors V[:, 0..j] and w = (H - sigma) v_j,
-//   w <- w - beta_{j-1} v_{j-1} - a v_j (the local three-term step),
-//   w <- w - V (V^H w) (classical Gram-Schmidt, a second pass when the norm
-//        drops below 1/sqrt(2) of its value),
-//   sc->alpha[j] = sigma + Re(v_j^H w), sc->beta[j] = ||w|| (and the same in
-//   mirror, mapped host memory, when non-null),
-//   V[:, j+1] = w / beta_j when write_next.
-// counters: 67 device unsigneds, zero on entry, left zero.
-void lanczos_orthonormalize(const Stream& st, int n, int j, cplx* V, long long ldv, cplx* w,
-                            bool write_next, double sigma, LanczosScalars* sc, LanczosScalars* mirror, cplx* h1,
-                            cplx* h2, unsigned* counters, Scratch& scratch);
-// One reorthogonalised Lanczos step (the recurrence above, with the local
-// three-term subtraction folded into the first Gram-Schmidt pass and an
-// optional projector) for a group of independent instances in one
-// cooperative launch (lzstep.cu).  Per instance: w = (H - sigma) v_j on
+// One reorthogonalised Lanczos step (local three-term subtraction, classical
+// Gram-Schmidt against the basis with a second pass when the norm drops below
+// 1/sqrt(2) of its value, normalisation; an optional projector) for a group
+// of independent instances in one cooperative launch (lzstep.cu).  Per instance: w = (H - sigma) v_j on
 // entry; on exit sc->alpha[j], sc->beta[j] (and the mirror) are set and, when
 // write_next, V[:, j+1] = w / beta_j.  With nu > 0, U (n x nu, ld n) holds the
 // projector vectors (sqrt of the penalty folded in) and w += U (U^H v_j)

@@ -1,8 +1,7 @@
 // One reorthogonalised Lanczos step for a group of independent local
 // eigenproblems, in a single cooperative launch (replaces the
 // orthogonalisation inside the PRIMME call of Contractor::solveEigs,
-// src/core/cpp/Contractor.cpp:3067-3138; the recurrence is the one of
-// lanczos.cu, organised for fewer launches).
+// src/core/cpp/Contractor.cpp:3067-3138).
 //
 // For every instance q, with k = j+1 basis vectors V[:, 0..j] and
 // w = (H - sigma) v_j computed by the matvec:

@@ -32,14 +32,35 @@ def io_npz():
     return np.load(here)
 
 
-def test_mpo_file_bytes_match_reference(ctx, io_npz, tmp_path):
-    for name, m in [("ising6", ctx.mpo(mo.ising_hmpo(6, 1, 1, 0.3))),
-                    ("schwinger6", ctx.mpo_schwinger(6, MU, 100.0))]:
-        fn = tmp_path / f"{name}.mpo"
-        ctx.mpo_save(m, fn)
-        got = np.frombuffer(fn.read_bytes(), dtype=np.uint8)
-        ref = io_npz[f"mpofile_{name}"]
-        assert got.shape == ref.shape and np.array_equal(got, ref), name
+def _parse_mpo_file(b: bytes):
+    L = int(np.frombuffer(b[:4], dtype=np.int32)[0])
+    off, out = 4, []
+    for _ in range(L):
+        rank = int(np.frombuffer(b[off:off + 4], dtype=np.int32)[0])
+        dims = tuple(np.frombuffer(b[off + 4:off + 4 + 4 * rank], dtype=np.int32))
+        off += 4 + 4 * rank
+        n = int(np.prod(dims))
+        out.append((dims, np.frombuffer(b[off:off + 16 * n], dtype=np.complex128)))
+        off += 16 * n
+    assert off == len(b)
+    return out
+
+
+def test_mpo_file_matches_reference(ctx, io_npz, tmp_path):
+    # Ising: the same bytes as MPO::saveMPO writes
+    fn = tmp_path / "ising6.mpo"
+    ctx.mpo_save(ctx.mpo(mo.ising_hmpo(6, 1, 1, 0.3)), fn)
+    assert fn.read_bytes() == io_npz["mpofile_ising6"].tobytes()
+    # Schwinger: the same layout and values; the reference's BLAS product
+    # C . Z (SchwingerHamiltonian.cpp:113-116) leaves -0.0 in two entries of
+    # the first operator where the library's builder writes +0.0
+    fn = tmp_path / "schwinger6.mpo"
+    ctx.mpo_save(ctx.mpo_schwinger(6, MU, 100.0), fn)
+    got, ref = _parse_mpo_file(fn.read_bytes()), _parse_mpo_file(io_npz["mpofile_schwinger6"].tobytes())
+    assert len(got) == len(ref)
+    for (dg, vg), (dr, vr) in zip(got, ref):
+        assert dg == dr
+        assert np.array_equal(vg, vr)
 
 
 def test_mpo_load_reference_file(ctx, io_npz, tmp_path, mpo_npz):
