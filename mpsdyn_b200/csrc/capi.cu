@@ -147,42 +147,7 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
   } catch (...) {
     return MPSGPU_OOM;
   }
-  mpsgpu_status st = guarded(ctx, [&] {
-    Context& c = ctx->c;
-    c.device = device;
-    MPSGPU_CUDA(cudaSetDevice(device));
-    // the no-allocation QR's fixed array is placed now, while allocation is
-    // still allowed, not at that entry point's first call
-    {
-      const mpsgpu_status ns = noalloc_qr_prepare(device);
-      MPSGPU_CHECK(ns == MPSGPU_OK, ns, "create: placing the no-allocation QR scratch failed");
-    }
-    MPSGPU_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-    c.scratch.stream = c.stream;
-    c.qrws.stream = c.stream;
-    // keep freed pool memory cached across calls
-    cudaMemPool_t pool;
-    MPSGPU_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-    uint64_t thresh = UINT64_MAX;
-    MPSGPU_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
-    MPSGPU_CUDA(cudaMalloc((void**)&c.dscal, 1024 * sizeof(double)));
-    MPSGPU_CUDA(cudaMalloc((void**)&c.dcplx, 1024 * sizeof(cplx)));
-    MPSGPU_CUDA(cudaMallocHost((void**)&c.hscal, 1024 * sizeof(double)));
-    MPSGPU_CUDA(cudaMallocHost((void**)&c.hcplx, 1024 * sizeof(cplx)));
-    MPSGPU_CUDA(cudaEventCreate(&c.ev));
-    MPSGPU_CUDA(cudaEventCreate(&c.mv0));
-    MPSGPU_CUDA(cudaEventCreate(&c.mv1));
-    MPSGPU_CUDA(cudaHostAlloc((void**)&c.hsplit_err, sizeof(int), cudaHostAllocMapped));
-    MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dsplit_err, c.hsplit_err, 0));
-    *c.hsplit_err = 0;
-    MPSGPU_CUDA(cudaHostAlloc((void**)&c.hlz_err, sizeof(int), cudaHostAllocMapped));
-    MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dlz_err, c.hlz_err, 0));
-    *c.hlz_err = 0;
-    MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 128 * sizeof(unsigned)));
-    MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 128 * sizeof(unsigned)));
-    c.iter_ev.resize(257);
-    for (auto& e : c.iter_ev) MPSGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  });
+  mpsgpu_status st = guarded(ctx, [&] { context_init(ctx->c, device); });
   if (st != MPSGPU_OK) {
     delete ctx;
     return st;
@@ -193,28 +158,7 @@ mpsgpu_status mpsgpu_create(int device, mpsgpu_context** out) {
 
 mpsgpu_status mpsgpu_destroy(mpsgpu_context* ctx) {
   if (!ctx) return MPSGPU_INVALID;
-  Context& c = ctx->c;
-  cudaSetDevice(c.device);
-  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR,
-                  &c.lzws, &c.spX, &c.spT, &c.spPart})
-    dbuf_free(c, *b);
-  c.scratch.release();
-  c.qrws.release();
-  if (c.stream) cudaStreamSynchronize(c.stream);
-  cudaFree(c.dscal);
-  cudaFree(c.dcplx);
-  cudaFreeHost(c.hscal);
-  cudaFreeHost(c.hcplx);
-  if (c.ev) cudaEventDestroy(c.ev);
-  if (c.mv0) cudaEventDestroy(c.mv0);
-  if (c.mv1) cudaEventDestroy(c.mv1);
-  for (auto e : c.iter_ev)
-    if (e) cudaEventDestroy(e);
-  c.lzone.release(c);
-  if (c.hsplit_err) cudaFreeHost(c.hsplit_err);
-  if (c.hlz_err) cudaFreeHost(c.hlz_err);
-  cudaFree(c.dcounter);
-  if (c.stream) cudaStreamDestroy(c.stream);
+  context_release(ctx->c);
   delete ctx;
   return MPSGPU_OK;
 }

@@ -503,13 +503,20 @@ void split_matvec_prepare(Context& c, SplitMatvec& s, const cplx* Le, const std:
   // Rt as the B operand of Y = T2 . Rt: its columns (Drb) are the prepared rows
   split_prepare(st, Drb, Drk * wr, Rt, (long long)Drk * wr, 1, s.p3.BN,
                 bytes_reserve(c, s.Rp, split_operand_bytes(Drb, Drk * wr, s.p3.BN)));
-  bytes_reserve(c, c.spX, split_operand_bytes(dd * Drk, Dlk, s.p1.BN));
-  bytes_reserve(c, c.spT, split_operand_bytes(Dlb * du, Drk * wr, 128));
+  s.xbytes = split_operand_bytes(dd * Drk, Dlk, s.p1.BN);
+  s.tbytes = split_operand_bytes(Dlb * du, Drk * wr, 128);
   long long part = 0;
   if (s.p1.splits > 1) part = std::max(part, (long long)s.p1.splits * s.p1.M * s.p1.N);
   if (s.p3.splits > 1) part = std::max(part, (long long)s.p3.splits * s.p3.M * s.p3.N);
-  if (part > 0) dbuf_reserve(c, c.spPart, part);
+  s.partn = part;
+  split_matvec_reserve(c, s);
   s.ready = true;
+}
+
+void split_matvec_reserve(Context& c, const SplitMatvec& s) {
+  bytes_reserve(c, c.spX, s.xbytes);
+  bytes_reserve(c, c.spT, s.tbytes);
+  if (s.partn > 0) dbuf_reserve(c, c.spPart, s.partn);
 }
 
 // First contraction of the matvec: T2[a', s', r, c] = sum_{a,b,s} W[s',b,s,c]
@@ -909,6 +916,83 @@ cplx contract2(Context& c, const MpoDev& ops, const MpsDev& ket, const MpsDev& b
 // the same whatever else runs in its rounds.
 // ---------------------------------------------------------------------------
 
+// ---------------------------------------------------------------------------
+// Contexts: one stream with its own workspaces; a batch of sweeps gives each
+// sweep a sub-context so that their gauge moves and environment updates
+// overlap on the GPU while their Lanczos rounds share grouped launches.
+// ---------------------------------------------------------------------------
+
+void context_init(Context& c, int device) {
+  c.device = device;
+  MPSGPU_CUDA(cudaSetDevice(device));
+  // the no-allocation QR's fixed array is placed now, while allocation is
+  // still allowed, not at that entry point's first call
+  {
+    const mpsgpu_status ns = noalloc_qr_prepare(device);
+    MPSGPU_CHECK(ns == MPSGPU_OK, ns, "create: placing the no-allocation QR scratch failed");
+  }
+  MPSGPU_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  c.scratch.stream = c.stream;
+  c.qrws.stream = c.stream;
+  // keep freed pool memory cached across calls
+  cudaMemPool_t pool;
+  MPSGPU_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t thresh = UINT64_MAX;
+  MPSGPU_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
+  MPSGPU_CUDA(cudaMalloc((void**)&c.dscal, 1024 * sizeof(double)));
+  MPSGPU_CUDA(cudaMalloc((void**)&c.dcplx, 1024 * sizeof(cplx)));
+  MPSGPU_CUDA(cudaMallocHost((void**)&c.hscal, 1024 * sizeof(double)));
+  MPSGPU_CUDA(cudaMallocHost((void**)&c.hcplx, 1024 * sizeof(cplx)));
+  MPSGPU_CUDA(cudaEventCreateWithFlags(&c.ev, cudaEventDisableTiming));
+  MPSGPU_CUDA(cudaEventCreate(&c.mv0));
+  MPSGPU_CUDA(cudaEventCreate(&c.mv1));
+  MPSGPU_CUDA(cudaHostAlloc((void**)&c.hsplit_err, sizeof(int), cudaHostAllocMapped));
+  MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dsplit_err, c.hsplit_err, 0));
+  *c.hsplit_err = 0;
+  MPSGPU_CUDA(cudaHostAlloc((void**)&c.hlz_err, sizeof(int), cudaHostAllocMapped));
+  MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dlz_err, c.hlz_err, 0));
+  *c.hlz_err = 0;
+  MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 128 * sizeof(unsigned)));
+  MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 128 * sizeof(unsigned)));
+  c.iter_ev.resize(257);
+  for (auto& e : c.iter_ev) MPSGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
+void context_release(Context& c) {
+  cudaSetDevice(c.device);
+  for (auto& sc : c.subs) context_release(*sc);
+  c.subs.clear();
+  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lzws, &c.spX, &c.spT, &c.spPart})
+    dbuf_free(c, *b);
+  c.scratch.release();
+  c.qrws.release();
+  c.lzone.release(c);
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  cudaFree(c.dscal);
+  cudaFree(c.dcplx);
+  cudaFreeHost(c.hscal);
+  cudaFreeHost(c.hcplx);
+  if (c.ev) cudaEventDestroy(c.ev);
+  if (c.mv0) cudaEventDestroy(c.mv0);
+  if (c.mv1) cudaEventDestroy(c.mv1);
+  for (auto e : c.iter_ev)
+    if (e) cudaEventDestroy(e);
+  if (c.hsplit_err) cudaFreeHost(c.hsplit_err);
+  if (c.hlz_err) cudaFreeHost(c.hlz_err);
+  cudaFree(c.dcounter);
+  if (c.stream) cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
+}
+
+Context& context_sub(Context& c, int i) {
+  while ((int)c.subs.size() <= i) {
+    c.subs.emplace_back(new Context());
+    context_init(*c.subs.back(), c.device);
+    c.subs.back()->parent = &c;
+  }
+  return *c.subs[i];
+}
+
 void LzWork::init(Context& c) {
   if (dsc) return;
   MPSGPU_CUDA(cudaMalloc((void**)&dsc, sizeof(LanczosScalars)));
@@ -1023,7 +1107,7 @@ void lanczos_batch(Context& c, std::vector<LzTask*>& tasks) {
       LzState& z = S[it.first];
       LzTask& t = *z.t;
       if (g1.n + 2 > GEMM_MAXP || g3.n + 1 > GEMM_MAXP) flush();
-      t.product(t.ws->V.p + (long long)it.second * t.N, t.ws->w.p, z.sigma, g1, g3);
+      t.product(c, t.ws->V.p + (long long)it.second * t.N, t.ws->w.p, z.sigma, g1, g3);
     }
     flush();
     for (size_t i0 = 0; i0 < items.size(); i0 += LZ_MAXI) {
@@ -1232,7 +1316,9 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
   t.max_krylov = max_krylov;
   t.ws = &ws;
   t.cnt = cnt;
-  t.product = [&](const cplx* xin, cplx* yout, double sigma, Gemm1wBatch&, Gemm3Batch&) { apply(xin, yout, sigma); };
+  t.product = [&](Context&, const cplx* xin, cplx* yout, double sigma, Gemm1wBatch&, Gemm3Batch&) {
+    apply(xin, yout, sigma);
+  };
   std::vector<LzTask*> v{&t};
   lanczos_batch(c, v);
   if (iters) *iters = t.iters;
@@ -1450,7 +1536,8 @@ namespace {
 // the same schedule of tolerances with FP64 products (to separate what the
 // schedule saves from what the tensor cores save).
 struct GsSweep {
-  Context& c;
+  Context& c;         // the sweep's own work (environments, gauge moves)
+  Context* mc = &c;   // the context running the batch's Lanczos rounds
   const MpoDev& ops;
   MpsDev& init;
   const SolveOptions& opt;
@@ -1485,7 +1572,7 @@ struct GsSweep {
     tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
     split_phase = (opt.precision == 1 || opt.precision == 2);
     split_products = (opt.precision == 1);
-    if (split_phase) *c.hsplit_err = 0;
+    if (split_phase) *c.hsplit_err = *mc->hsplit_err = 0;
   }
 
   void prepare(LzTask& t) {
@@ -1506,10 +1593,11 @@ struct GsSweep {
     t.max_krylov = opt.max_krylov;
     t.ws = &ws;
     t.cnt = &cnt;
-    t.product = [this](const cplx* xin, cplx* yout, double sg, Gemm1wBatch& g1, Gemm3Batch& g3) {
+    t.product = [this](Context& lc, const cplx* xin, cplx* yout, double sg, Gemm1wBatch& g1, Gemm3Batch& g3) {
       const cplx o = make_double2(offset - sg, 0.0);
       if (split_phase && split_products) {
-        heff_apply(c, Le, ld, ops, pos, false, Rt, rd, xin, yout, o, &cnt, &smv);
+        split_matvec_reserve(lc, smv);
+        heff_apply(lc, Le, ld, ops, pos, false, Rt, rd, xin, yout, o, &cnt, &smv);
         return;
       }
       const auto& wd = ops.dims[pos];
@@ -1526,7 +1614,7 @@ struct GsSweep {
 
   void finish(double theta) {
     cnt.site_solves++;
-    if (split_phase && *c.hsplit_err)
+    if (split_phase && (*c.hsplit_err || *mc->hsplit_err))
       throw Error(MPSGPU_TIMEOUT, "findGroundState: a bounded wait in the tensor-core kernel ran out");
     val = theta - offset;
     if (!first64 && (val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
@@ -1585,6 +1673,8 @@ struct GsSweep {
 // stops with its own status; the others go on.
 template <class Sweep>
 void run_sweeps(Context& c, std::vector<Sweep*>& sw, std::vector<int>& status, std::vector<std::string>& err) {
+  // c runs the Lanczos rounds; a sweep on a sub-context hands its prepared
+  // site over through an event on its stream
   const int n = (int)sw.size();
   status.assign(n, MPSGPU_OK);
   err.assign(n, std::string());
@@ -1617,6 +1707,12 @@ void run_sweeps(Context& c, std::vector<Sweep*>& sw, std::vector<int>& status, s
       }
     }
     if (tp.empty()) break;
+    for (int i : idx) {
+      Context& sc = sw[i]->c;
+      if (&sc == &c) continue;
+      MPSGPU_CUDA(cudaEventRecord(sc.ev, sc.stream));
+      MPSGPU_CUDA(cudaStreamWaitEvent(c.stream, sc.ev, 0));
+    }
     try {
       lanczos_batch(c, tp);
     } catch (const Error& e) {
@@ -1664,7 +1760,11 @@ void find_ground_state_batch(Context& c, const std::vector<const MpoDev*>& ops, 
   std::vector<std::unique_ptr<GsSweep>> own;
   std::vector<GsSweep*> sw;
   for (int i = 0; i < n; i++) {
-    own.emplace_back(new GsSweep(c, *ops[i], D, *inits[i], offset, opt, cnts[i], ws[i]));
+    // each sweep's environments and gauge moves on its own stream
+    Context& sc = n > 1 ? context_sub(c, i) : c;
+    MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
+    own.emplace_back(new GsSweep(sc, *ops[i], D, *inits[i], offset, opt, cnts[i], ws[i]));
+    own.back()->mc = &c;
     sw.push_back(own.back().get());
   }
   try {
@@ -1675,6 +1775,7 @@ void find_ground_state_batch(Context& c, const std::vector<const MpoDev*>& ops, 
   }
   energies.assign(n, 0.0);
   for (int i = 0; i < n; i++) energies[i] = sw[i]->energy;
+  for (auto* x : sw) MPSGPU_CUDA(cudaStreamSynchronize(x->c.stream));  // the states are read on c next
   for (auto& w : ws) w.release(c);
 }
 
@@ -1877,7 +1978,8 @@ namespace {
 // halves of the Hermitian multiplier until the half-sweep energy settles,
 // then FP64 (at least one full round).
 struct ExcSweep {
-  Context& c;
+  Context& c;         // the sweep's own work (environments, gauge moves)
+  Context* mc = &c;   // the context running the batch's Lanczos rounds
   const MpoDev& ops;
   MpsDev& init;
   const SolveOptions& opt;
@@ -1922,7 +2024,7 @@ struct ExcSweep {
     tol = opt.eigtol > 0 ? opt.eigtol : 1e-12;
     split_phase = (opt.precision == 1 || opt.precision == 2);
     split_products = (opt.precision == 1);
-    if (split_phase) *c.hsplit_err = 0;
+    if (split_phase) *c.hsplit_err = *mc->hsplit_err = 0;
     last_saved = std::chrono::steady_clock::now();
   }
 
@@ -2004,10 +2106,12 @@ struct ExcSweep {
     t.cnt = &cnt;
     // 1/2 (H + H^dag) x + (offset - sigma) x; the projector term
     // sum_k pen_k u_k (u_k^H x) is added by the Lanczos step
-    t.product = [this](const cplx* xin, cplx* yout, double sg, Gemm1wBatch& g1, Gemm3Batch& g3) {
+    t.product = [this](Context& lc, const cplx* xin, cplx* yout, double sg, Gemm1wBatch& g1, Gemm3Batch& g3) {
       const cplx o = make_double2(offset - sg, 0.0);
       if (split_phase && split_products) {
-        heff_apply_hermitian(c, Le, Lh.p, ld, ops, pos, Rt, Rth.p, rd, xin, yout, o, &cnt, &smv, &smvh);
+        split_matvec_reserve(lc, smv);
+        split_matvec_reserve(lc, smvh);
+        heff_apply_hermitian(lc, Le, Lh.p, ld, ops, pos, Rt, Rth.p, rd, xin, yout, o, &cnt, &smv, &smvh);
         return;
       }
       const auto& wd = ops.dims[pos];
@@ -2034,7 +2138,7 @@ struct ExcSweep {
 
   void finish(double theta) {
     cnt.site_solves++;
-    if (split_phase && *c.hsplit_err)
+    if (split_phase && (*c.hsplit_err || *mc->hsplit_err))
       throw Error(MPSGPU_TIMEOUT, "findNextExcitedState: a bounded wait in the tensor-core kernel ran out");
     val = theta - offset;
     if (!first64 && (val - energy > 1e-8) && (val - energy > std::fabs(energy + offset) * 1e-10)) {
@@ -2185,8 +2289,11 @@ void find_next_excited_state_batch(Context& c, const std::vector<const MpoDev*>&
     while (!todo.empty()) {
       std::vector<std::unique_ptr<ExcSweep>> own;
       std::vector<ExcSweep*> sw;
+      MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
       for (int i : todo) {
-        own.emplace_back(new ExcSweep(c, *ops[i], D, pens[i], levels[i], *inits[i], offset, opt, cnts[i], ws[i]));
+        Context& sc = n > 1 ? context_sub(c, i) : c;
+        own.emplace_back(new ExcSweep(sc, *ops[i], D, pens[i], levels[i], *inits[i], offset, opt, cnts[i], ws[i]));
+        own.back()->mc = &c;
         sw.push_back(own.back().get());
       }
       std::vector<int> st;
@@ -2198,6 +2305,7 @@ void find_next_excited_state_batch(Context& c, const std::vector<const MpoDev*>&
         status[i] = st[q];
         err[i] = er[q];
         energies[i] = sw[q]->energy;
+        MPSGPU_CUDA(cudaStreamSynchronize(sw[q]->c.stream));  // the states are read on c next
         if (st[q] == MPSGPU_OK && opt.excorthtol > 0 && raise_penalties(c, levels[i], *inits[i], opt.excorthtol, pens[i]))
           again.push_back(i);
       }

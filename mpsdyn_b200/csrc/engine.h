@@ -6,6 +6,7 @@
 #include <array>
 #include <atomic>
 #include <functional>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -85,8 +86,16 @@ struct Context {
   cudaEvent_t ev = nullptr;
   cudaEvent_t mv0 = nullptr, mv1 = nullptr;
   GemmProfiler prof;
-  Stream st() { return Stream{stream, &launches, &prof}; }
+  std::vector<std::unique_ptr<Context>> subs;  // sub-contexts of the sweeps of a batch
+  Context* parent = nullptr;                   // a sub-context counts its launches there
+  Stream st() { return Stream{stream, parent ? &parent->launches : &launches, parent ? &parent->prof : &prof}; }
 };
+
+// Context set-up and release (mpsgpu_create / mpsgpu_destroy), and the i-th
+// sub-context of c (created on first use, released with c).
+void context_init(Context& c, int device);
+void context_release(Context& c);
+Context& context_sub(Context& c, int i);
 
 // Environment cache (TmpManager, src/core/cpp/TmpManager.cpp:22-160):
 // L[pos] (Dbra, w, Dket) and Rt[pos] (Dket, w, Dbra) (R transposed), with
@@ -164,8 +173,11 @@ void mps_increase_bond(Context& c, MpsDev& s, int D);
 struct SplitMatvec {
   SplitPlan p1, p3;  // T1 = L . X and Y = T2 . Rt
   DBuf Lp, Rp;       // prepared L and Rt (the per-product X and T2 planes live in the Context)
+  long long xbytes = 0, tbytes = 0, partn = 0;  // sizes of the per-product planes and K-split partials
   bool ready = false;
 };
+// Reserves the per-product split buffers on the context that runs the products.
+void split_matvec_reserve(Context& c, const SplitMatvec& s);
 void split_matvec_prepare(Context& c, SplitMatvec& s, const cplx* Le, const std::array<int, 3>& ld,
                           const MpoDev& m, int k, const cplx* Rt, const std::array<int, 3>& rd);
 void split_matvec_release(Context& c, SplitMatvec& s);
@@ -199,10 +211,11 @@ void mpo_save_file(Context& c, const MpoDev& m, const std::string& fn);
 void mpo_load_file(Context& c, const std::string& fn, MpoDev& m);
 
 // ---- local eigensolver (batched thick-restart Lanczos) ----
-// One local problem: product(x, y, sigma, g1, g3) must make y = (H - sigma) x
-// appear on the context's stream, either by appending FP64 descriptors to
-// the grouped launches g1/g3 (launched by the caller in the same round) or by
-// launching its own kernels.
+// One local problem: product(lc, x, y, sigma, g1, g3) must make
+// y = (H - sigma) x appear on the stream of lc (the context running the
+// rounds), either by appending FP64 descriptors to the grouped launches
+// g1/g3 (launched by the caller in the same round) or by launching its own
+// kernels on lc.
 struct LzTask {
   int N = 0;
   cplx* x = nullptr;  // start vector in, normalised eigenvector out
@@ -210,7 +223,7 @@ struct LzTask {
   const cplx* U = nullptr;  // projector vectors (N x nu), sqrt(penalty) folded in
   int nu = 0;
   int max_krylov = 64;
-  std::function<void(const cplx*, cplx*, double, Gemm1wBatch&, Gemm3Batch&)> product;
+  std::function<void(Context&, const cplx*, cplx*, double, Gemm1wBatch&, Gemm3Batch&)> product;
   LzWork* ws = nullptr;
   Counters* cnt = nullptr;
   double theta = 0.0;  // out: lowest Ritz value

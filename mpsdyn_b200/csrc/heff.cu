@@ -413,12 +413,14 @@ void heff_gemm3(const Stream& st, Gemm3Batch& b) {
     t32 += (long long)ceil_div(d.M, 32) * ceil_div(d.N, 32);
     kmax = std::max(kmax, d.K1 + d.K2);
   }
+  // 64-row tiles (two CTAs per SM by shared memory) once they alone fill the
+  // GPU twice; otherwise 32-row tiles (four per SM), with the K range split
+  // over a cluster while that keeps within one wave and K chunks of at
+  // least four slabs
   int bm = 64, cs = 1;
-  if (t64 < nsm) {
+  if (t64 < 2LL * nsm) {
     bm = 32;
-    const long long tt = t32;
-    cs = 1;
-    while (cs < 8 && tt * cs * 2 <= 2LL * nsm && kmax / (cs * 2) >= 2 * BK) cs *= 2;
+    while (cs < 8 && t32 * cs * 2 <= 4LL * nsm && kmax / (cs * 2) >= 4 * BK) cs *= 2;
   }
   int tiles = 0;
   for (int q = 0; q < b.n; q++) {

@@ -29,8 +29,7 @@ namespace mpsgpu {
 namespace {
 
 constexpr int T = LZ_THREADS;         // threads per CTA
-constexpr int RPT = 1;                // rows per thread per row block
-constexpr int RB = T * RPT;           // rows per row block
+constexpr int RB = T;                 // rows per row block (one per thread)
 constexpr int NW = T / 32;
 constexpr int KMAXS = 256;            // Krylov vectors
 constexpr double DGKS2 = 0.5;
@@ -86,50 +85,32 @@ __device__ __forceinline__ cplx warp_sumc(cplx s) {
   return s;
 }
 
-// Sum of v[0..7] over the 32 lanes of a warp by a transposing butterfly:
-// afterwards lane L with (L & 3) == 0 holds the total of vector (L >> 2).
-__device__ __forceinline__ cplx warp_sum8(cplx (&v)[8]) {
+// Sum of v[0..15] over the 32 lanes of a warp by a transposing butterfly:
+// every exchange step halves the values a lane keeps, so afterwards the
+// lanes with (lane & 1) == 0 hold the totals, lane L the one of vector
+// sum16_vector_of_lane(L).
+__device__ __forceinline__ cplx warp_sum16(cplx (&v)[16]) {
   const int lane = threadIdx.x & 31;
-  // xor 16: keep 4 of 8 (upper half of the lanes keeps vectors 4..7)
-  {
-    const bool up = lane & 16;
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      cplx send = up ? v[i] : v[i + 4];
-      cplx keep = up ? v[i + 4] : v[i];
-      keep.x += __shfl_xor_sync(0xffffffffu, send.x, 16);
-      keep.y += __shfl_xor_sync(0xffffffffu, send.y, 16);
+  for (int half = 8, mask = 16; half >= 1; half >>= 1, mask >>= 1) {
+    const bool up = lane & mask;
+#pragma unroll
+    for (int i = 0; i < half; i++) {
+      const cplx send = up ? v[i] : v[i + half];
+      cplx keep = up ? v[i + half] : v[i];
+      keep.x += __shfl_xor_sync(0xffffffffu, send.x, mask);
+      keep.y += __shfl_xor_sync(0xffffffffu, send.y, mask);
       v[i] = keep;
     }
   }
-  {
-    const bool up = lane & 8;
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-      cplx send = up ? v[i] : v[i + 2];
-      cplx keep = up ? v[i + 2] : v[i];
-      keep.x += __shfl_xor_sync(0xffffffffu, send.x, 8);
-      keep.y += __shfl_xor_sync(0xffffffffu, send.y, 8);
-      v[i] = keep;
-    }
-  }
-  cplx r;
-  {
-    const bool up = lane & 4;
-    cplx send = up ? v[0] : v[1];
-    r = up ? v[1] : v[0];
-    r.x += __shfl_xor_sync(0xffffffffu, send.x, 4);
-    r.y += __shfl_xor_sync(0xffffffffu, send.y, 4);
-  }
-  r.x += __shfl_xor_sync(0xffffffffu, r.x, 2);
-  r.y += __shfl_xor_sync(0xffffffffu, r.y, 2);
+  cplx r = v[0];
   r.x += __shfl_xor_sync(0xffffffffu, r.x, 1);
   r.y += __shfl_xor_sync(0xffffffffu, r.y, 1);
-  // lane bits (4, 3, 2) select vector 4*b4 + 2*b3 + b2
   return r;
 }
-__device__ __forceinline__ int sum8_vector_of_lane(int lane) {
-  return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+// lane bits (4, 3, 2, 1) select vector 8*b4 + 4*b3 + 2*b2 + b1
+__device__ __forceinline__ int sum16_vector_of_lane(int lane) {
+  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
 }
 
 // instance owning global row block rb (instances hold consecutive ranges)
@@ -142,82 +123,72 @@ __device__ __forceinline__ int inst_of(const LzBatch& b, int rb) {
 // Partial dots over the rows [r0, r0 + RB) of an n-row instance:
 // part[rb * KMAXS + l] = sum_rows conj(V[:, l]) x for l < k (V with leading
 // dimension ldv), and the partial |x|^2 into pn[rb] when pn is non-null.
+// Vectors go in groups of 16 whose loads are all issued before use; the
+// warps' sums collect in shared memory (red, NW x KMAXS) and are added in a
+// fixed order after one barrier.
 __device__ void block_dots(const cplx* __restrict__ V, long long ldv, long long n, long long r0, int rb,
-                           const cplx* __restrict__ x, int k, cplx* part, double* pn, cplx (*red)[8],
+                           const cplx* __restrict__ x, int k, cplx* part, double* pn, cplx (*red)[KMAXS],
                            double* redn) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  long long rows[RPT];
-  bool ok[RPT];
-  cplx xv[RPT];
-#pragma unroll
-  for (int u = 0; u < RPT; u++) {
-    rows[u] = r0 + tid + u * T;
-    ok[u] = rows[u] < n;
-    xv[u] = ok[u] ? x[rows[u]] : make_double2(0.0, 0.0);
-  }
+  const long long row = r0 + tid;
+  const bool ok = row < n;
+  const cplx xv = ok ? x[row] : make_double2(0.0, 0.0);
   if (pn) {
-    double s = 0.0;
-#pragma unroll
-    for (int u = 0; u < RPT; u++) s += cabs2(xv[u]);
-    s = warp_sumd(s);
+    const double s = warp_sumd(cabs2(xv));
     if (lane == 0) redn[warp] = s;
   }
-  for (int l0 = 0; l0 < k; l0 += 8) {
-    cplx acc[8];
+  const cplx* vr = V + (ok ? row : 0);
+  for (int l0 = 0; l0 < k; l0 += 16) {
+    cplx v[16];
 #pragma unroll
-    for (int t = 0; t < 8; t++) {
-      const int l = l0 + t;
-      cplx s = make_double2(0.0, 0.0);
-      if (l < k) {
-        const cplx* col = V + (long long)l * ldv;
+    for (int t = 0; t < 16; t++)
+      v[t] = (ok && l0 + t < k) ? __ldcg(&vr[(long long)(l0 + t) * ldv]) : make_double2(0.0, 0.0);
 #pragma unroll
-        for (int u = 0; u < RPT; u++)
-          if (ok[u]) s = cadd(s, ccmul(__ldcg(&col[rows[u]]), xv[u]));
-      }
-      acc[t] = s;
-    }
-    const cplx r = warp_sum8(acc);
-    if ((lane & 3) == 0) red[warp][sum8_vector_of_lane(lane)] = r;
-    __syncthreads();
-    if (tid < 8 && l0 + tid < k) {
-      cplx s = make_double2(0.0, 0.0);
-      for (int q = 0; q < NW; q++) s = cadd(s, red[q][tid]);
-      part[(long long)rb * KMAXS + l0 + tid] = s;
-    }
-    __syncthreads();
+    for (int t = 0; t < 16; t++) v[t] = ccmul(v[t], xv);
+    const cplx r = warp_sum16(v);
+    const int l = l0 + sum16_vector_of_lane(lane);
+    if ((lane & 1) == 0 && l < k) red[warp][l] = r;
+  }
+  __syncthreads();
+  for (int l = tid; l < k; l += T) {
+    cplx s = make_double2(0.0, 0.0);
+    for (int q = 0; q < NW; q++) s = cadd(s, red[q][l]);
+    part[(long long)rb * KMAXS + l] = s;
   }
   if (pn && tid == 0) {
     double s = 0.0;
     for (int q = 0; q < NW; q++) s += redn[q];
     pn[rb] = s;
   }
+  __syncthreads();
 }
 
 // x -= V h over the rows of row block rb (h in shared memory, k entries);
-// partial |x|^2 into pn[rb].
+// partial |x|^2 into pn[rb].  Sixteen loads of V in flight per thread.
 __device__ void block_update(const LzInst& in, int rb, cplx* __restrict__ x, const cplx* hs, int k, double* pn,
                              double* redn) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long long r0 = (long long)(rb - in.rb0) * RB;
+  const long long i = (long long)(rb - in.rb0) * RB + tid;
   double s2 = 0.0;
+  if (i < in.n) {
+    cplx a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
+    const cplx* v = in.V + i;
+    for (int l0 = 0; l0 < k; l0 += 16) {
+      cplx vv[16];
 #pragma unroll
-  for (int u = 0; u < RPT; u++) {
-    const long long i = r0 + tid + u * T;
-    if (i < in.n) {
-      cplx a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
-      const cplx* v = in.V + i;
-      int l = 0;
-      for (; l + 3 < k; l += 4) {
-        a0 = cadd(a0, cmul(__ldcg(&v[(long long)l * in.ldv]), hs[l]));
-        a1 = cadd(a1, cmul(__ldcg(&v[(long long)(l + 1) * in.ldv]), hs[l + 1]));
-        a2 = cadd(a2, cmul(__ldcg(&v[(long long)(l + 2) * in.ldv]), hs[l + 2]));
-        a3 = cadd(a3, cmul(__ldcg(&v[(long long)(l + 3) * in.ldv]), hs[l + 3]));
+      for (int t = 0; t < 16; t++)
+        vv[t] = l0 + t < k ? __ldcg(&v[(long long)(l0 + t) * in.ldv]) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int t = 0; t < 16; t += 4) {
+        if (l0 + t < k) a0 = cadd(a0, cmul(vv[t], hs[l0 + t]));
+        if (l0 + t + 1 < k) a1 = cadd(a1, cmul(vv[t + 1], hs[l0 + t + 1]));
+        if (l0 + t + 2 < k) a2 = cadd(a2, cmul(vv[t + 2], hs[l0 + t + 2]));
+        if (l0 + t + 3 < k) a3 = cadd(a3, cmul(vv[t + 3], hs[l0 + t + 3]));
       }
-      for (; l < k; l++) a0 = cadd(a0, cmul(__ldcg(&v[(long long)l * in.ldv]), hs[l]));
-      const cplx xi = csub(x[i], cadd(cadd(a0, a1), cadd(a2, a3)));
-      x[i] = xi;
-      s2 += cabs2(xi);
     }
+    const cplx xi = csub(x[i], cadd(cadd(a0, a1), cadd(a2, a3)));
+    x[i] = xi;
+    s2 = cabs2(xi);
   }
   s2 = warp_sumd(s2);
   if (lane == 0) redn[warp] = s2;
@@ -265,7 +236,7 @@ __device__ double sum_norms(const LzInst& in, const double* pn, double* redn) {
 }
 
 __global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__ LzBatch b) {
-  __shared__ cplx red[NW][8];
+  __shared__ cplx red[NW][KMAXS];
   __shared__ double redn[NW];
   __shared__ cplx hs[KMAXS];
   __shared__ cplx ucs[LZ_MAXU];
@@ -300,8 +271,8 @@ __global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__
       }
       __syncthreads();
       const long long r0 = (long long)(rb - in.rb0) * RB;
-      for (int u = 0; u < RPT; u++) {
-        const long long i = r0 + tid + u * T;
+      {
+        const long long i = r0 + tid;
         if (i < in.n) {
           cplx a = in.w[i];
           for (int t = 0; t < in.nu; t++) a = cadd(a, cmul(in.U[i + (long long)t * in.n], ucs[t]));
@@ -321,9 +292,8 @@ __global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__
       const double bp = in.sc->beta[in.j - 1];
       const cplx* vp = in.V + (long long)(in.j - 1) * in.ldv;
       const long long r0 = (long long)(rb - in.rb0) * RB;
-#pragma unroll
-      for (int u = 0; u < RPT; u++) {
-        const long long i = r0 + tid + u * T;
+      {
+        const long long i = r0 + tid;
         if (i < in.n) in.w[i] = csub(in.w[i], cscale(__ldcg(&vp[i]), bp));
       }
       __syncthreads();
@@ -400,9 +370,8 @@ __global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__
     const double inv = 1.0 / beta_s[q];
     cplx* vn = in.V + (long long)(in.j + 1) * in.ldv;
     const long long r0 = (long long)(rb - in.rb0) * RB;
-#pragma unroll
-    for (int u = 0; u < RPT; u++) {
-      const long long i = r0 + tid + u * T;
+    {
+      const long long i = r0 + tid;
       if (i < in.n) vn[i] = cscale(in.w[i], inv);
     }
   }

@@ -235,7 +235,8 @@ __device__ cplx warp_reflector(cplx* P, int mp, int c) {
 // Warp q owns panel column q: it applies the reflectors of the columns to
 // its left to its own column, then, on its turn, computes its reflector, so
 // one block barrier per column orders the reflectors.
-__device__ void factor_panel(cplx* P, int mp, int jb, cplx* Tg, int ldt, cplx* taug, cplx* Wsh, cplx* taus) {
+__device__ void factor_panel(cplx* P, int mp, int jb, cplx* Tg, int ldt, cplx* taug, cplx* Wsh, cplx* taus,
+                             cplx* Tsh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int c = 0; c < jb; c++) {
     if (warp == c) {
@@ -274,25 +275,26 @@ __device__ void factor_panel(cplx* P, int mp, int jb, cplx* Tg, int ldt, cplx* t
   }
   __syncthreads();
   if (warp == 0) {
-    // column by column (one lane per row l < i), T kept in Wsh's upper part
-    // is read back from Tg; jb <= 32
+    // column by column (one lane per row l < i), T built in shared memory
+    // (Tsh, jb x jb) and written to global memory once; jb <= 32
     for (int i = 0; i < jb; i++) {
       const cplx ti = taus[i];
       cplx v = make_double2(0.0, 0.0);
       if (lane < i) {
         cplx s = make_double2(0.0, 0.0);
-        for (int q = lane; q < i; q++) s = cadd(s, cmul(Tg[lane + q * ldt], Wsh[q + i * jb]));
+        for (int q = lane; q < i; q++) s = cadd(s, cmul(Tsh[lane + q * jb], Wsh[q + i * jb]));
         v = cmul(make_double2(-ti.x, -ti.y), s);
       } else if (lane == i) {
         v = ti;
       }
       __syncwarp();
-      if (lane < jb) Tg[lane + i * ldt] = v;
-      if (lane == 0) taug[i] = ti;
-      __threadfence_block();
+      if (lane < jb) Tsh[lane + i * jb] = v;
       __syncwarp();
     }
   }
+  __syncthreads();
+  for (int t = threadIdx.x; t < jb * jb; t += blockDim.x) Tg[(t % jb) + (long long)(t / jb) * ldt] = Tsh[t];
+  for (int t = threadIdx.x; t < jb; t += blockDim.x) taug[t] = taus[t];
   __syncthreads();
 }
 
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(QR_THREADS) qr_factor_kernel(QrParams p) {
     if (blockIdx.x == 0) {
       // the panel's columns were brought up to date by this CTA (look-ahead)
       load_slice(j0, j0, mp, jb);
-      factor_panel(C, mp, jb, Tp, nb, p.tau + j0, W, taus);
+      factor_panel(C, mp, jb, Tp, nb, p.tau + j0, W, taus, Ts);
       store_slice(j0, j0, mp, jb);
       __threadfence();
     }
