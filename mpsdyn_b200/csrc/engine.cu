@@ -1075,12 +1075,13 @@ void lanczos_batch(Context& c, std::vector<LzTask*>& tasks) {
   // workspace of the step, shared by the instances of a launch: partial dots
   // (row blocks x 256), two partial-norm arrays, the coefficients h, h2
   const long long hcap = 256LL * LZ_MAXI;
-  dbuf_reserve(c, c.lzws, nrb_total * 256 + 2 * hcap + nrb_total + 8);
+  dbuf_reserve(c, c.lzws, nrb_total * 256 + 2 * hcap + nrb_total + LZ_MAXI + 8);
   cplx* part = c.lzws.p;
   cplx* hbuf = part + nrb_total * 256;
   cplx* h2buf = hbuf + hcap;
   double* pn1 = reinterpret_cast<double*>(h2buf + hcap);
   double* pn2 = pn1 + nrb_total;
+  double* nwbuf = pn2 + nrb_total;  // 2 * LZ_MAXI doubles
 
   auto check_step = [&]() {
     if (*c.hlz_err) {
@@ -1118,6 +1119,7 @@ void lanczos_batch(Context& c, std::vector<LzTask*>& tasks) {
       b.h2 = h2buf;
       b.pn1 = pn1;
       b.pn2 = pn2;
+      b.nw = nwbuf;
       b.bar = c.dcounter + 96;
       b.err = c.dlz_err;
       for (int i = 0; i < b.ninst; i++) {

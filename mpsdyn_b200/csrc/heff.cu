@@ -39,7 +39,14 @@ namespace {
 constexpr int BK = 16;
 constexpr int PADC = 2;      // complex padding of a shared row: conflict-free 16-byte fragment loads
 constexpr int STAGES = 3;
-constexpr int NT_ = 128;     // 4 warps, 2 x 2
+// Warp groups splitting the k steps of every slab: two for 32-row tiles
+// (twice the warps per SM for the small sweep shapes), one for 64-row
+// tiles (whose accumulators already fill the registers); each group is 4
+// warps, 2 x 2 over the tile.
+template <int BM>
+__host__ __device__ constexpr int kgroups() { return BM <= 32 ? 2 : 1; }
+template <int BM>
+__host__ __device__ constexpr int nthreads() { return 128 * kgroups<BM>(); }
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -81,7 +88,7 @@ template <int BM, int BN, class LA, class LB>
 __device__ __forceinline__ void mainloop(Ring<BM, BN>& r, Acc<BM, BN>& acc, int kbeg, int kend, LA loadA, LB loadB) {
   using AC = Acc<BM, BN>;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wm0 = (warp & 1) * AC::WM, wn0 = (warp >> 1) * AC::WN;
+  const int wm0 = (warp & 1) * AC::WM, wn0 = ((warp >> 1) & 1) * AC::WN, kg = warp >> 2;
   const int fr = lane >> 2, fc = lane & 3;
 #pragma unroll
   for (int i = 0; i < AC::MT; i++)
@@ -109,7 +116,8 @@ __device__ __forceinline__ void mainloop(Ring<BM, BN>& r, Acc<BM, BN>& acc, int 
     cp_async_commit();
     const int st = it % STAGES;
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
+    for (int kk0 = 0; kk0 < BK; kk0 += 4 * kgroups<BM>()) {
+      const int kk = kk0 + 4 * kg;  // this group's k step of the slab
       double are[AC::MT], aim[AC::MT], naim[AC::MT], bre[AC::NT], bim[AC::NT];
 #pragma unroll
       for (int i = 0; i < AC::MT; i++) {
@@ -139,23 +147,32 @@ __device__ __forceinline__ void mainloop(Ring<BM, BN>& r, Acc<BM, BN>& acc, int 
   __syncthreads();
 }
 
-// Accumulators -> shared tile Cs[m][n] (ld BN + PADC).
+// Accumulators -> shared tile Cs[m][n] (ld BN + PADC): the warp groups'
+// partial sums added in group order.  Every thread of the block calls it.
 template <int BM, int BN>
 __device__ __forceinline__ void acc_to_smem(const Acc<BM, BN>& acc, cplx* Cs) {
   using AC = Acc<BM, BN>;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wm0 = (warp & 1) * AC::WM, wn0 = (warp >> 1) * AC::WN;
+  const int wm0 = (warp & 1) * AC::WM, wn0 = ((warp >> 1) & 1) * AC::WN, kg = warp >> 2;
   const int fr = lane >> 2, fc = lane & 3;
 #pragma unroll
-  for (int i = 0; i < AC::MT; i++)
+  for (int g = 0; g < kgroups<BM>(); g++) {
+    if (kg == g) {
 #pragma unroll
-    for (int j = 0; j < AC::NT; j++)
+      for (int i = 0; i < AC::MT; i++)
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int m = wm0 + i * 8 + fr, n = wn0 + j * 8 + 2 * fc + h;
-        Cs[m * (BN + PADC) + n] =
-            make_double2(acc.v[i][j][0][h] + acc.v[i][j][1][h], acc.v[i][j][2][h] + acc.v[i][j][3][h]);
-      }
+        for (int j = 0; j < AC::NT; j++)
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int m = wm0 + i * 8 + fr, n = wn0 + j * 8 + 2 * fc + h;
+            const cplx v =
+                make_double2(acc.v[i][j][0][h] + acc.v[i][j][1][h], acc.v[i][j][2][h] + acc.v[i][j][3][h]);
+            cplx& c = Cs[m * (BN + PADC) + n];
+            c = g == 0 ? v : cadd(c, v);
+          }
+    }
+    __syncthreads();
+  }
 }
 
 // tile t -> problem index (descriptors hold consecutive tile ranges)
@@ -170,8 +187,9 @@ __device__ __forceinline__ int problem_of(const D* d, int n, int t) {
 // heff_gemm1w
 // ---------------------------------------------------------------------------
 template <int BM, int BN>
-__global__ void __launch_bounds__(NT_) heff_gemm1w_kernel(const __grid_constant__ Gemm1wBatch b) {
+__global__ void __launch_bounds__(nthreads<BM>()) heff_gemm1w_kernel(const __grid_constant__ Gemm1wBatch b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NT_ = nthreads<BM>();
   Ring<BM, BN>& ring = *reinterpret_cast<Ring<BM, BN>*>(smem_raw);
   const int q = problem_of(b.d, b.n, blockIdx.x);
   const Gemm1wDesc& d = b.d[q];
@@ -247,9 +265,10 @@ __global__ void __launch_bounds__(NT_) heff_gemm1w_kernel(const __grid_constant_
 // heff_gemm3 (cluster split-K)
 // ---------------------------------------------------------------------------
 template <int BM, int BN, int CS>
-__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT_)
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(nthreads<BM>())
     heff_gemm3_kernel(const __grid_constant__ Gemm3Batch b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NT_ = nthreads<BM>();
   Ring<BM, BN>& ring = *reinterpret_cast<Ring<BM, BN>*>(smem_raw);
   const int tile = blockIdx.x / CS, rank = blockIdx.x % CS;
   const int q = problem_of(b.d, b.n, tile);
@@ -392,9 +411,9 @@ void heff_gemm1w(const Stream& st, Gemm1wBatch& b) {
   }
   ProfScope ps(st, GemmProfiler::GEMM64, work);
   if (bm == 64)
-    heff_gemm1w_kernel<64, 32><<<tiles, NT_, ring_bytes<64, 32>(), st.s>>>(b);
+    heff_gemm1w_kernel<64, 32><<<tiles, nthreads<64>(), ring_bytes<64, 32>(), st.s>>>(b);
   else
-    heff_gemm1w_kernel<32, 32><<<tiles, NT_, ring_bytes<32, 32>(), st.s>>>(b);
+    heff_gemm1w_kernel<32, 32><<<tiles, nthreads<32>(), ring_bytes<32, 32>(), st.s>>>(b);
   after_launch(st);
 }
 
@@ -435,7 +454,7 @@ void heff_gemm3(const Stream& st, Gemm3Batch& b) {
   for (int q = 0; q < b.n; q++) work += 8.0 * (double)b.d[q].M * b.d[q].N * (b.d[q].K1 + b.d[q].K2);
   ProfScope ps(st, GemmProfiler::GEMM64, work);
 #define MPSGPU_G3(BMv, CSv)                                                                   \
-  heff_gemm3_kernel<BMv, 32, CSv><<<grid, NT_, ring_bytes<BMv, 32>(), st.s>>>(b)
+  heff_gemm3_kernel<BMv, 32, CSv><<<grid, nthreads<BMv>(), ring_bytes<BMv, 32>(), st.s>>>(b)
   if (bm == 64) {
     MPSGPU_G3(64, 1);
   } else if (cs == 1) {

@@ -273,6 +273,7 @@ struct LzBatch {
   double* pn2 = nullptr;
   cplx* h = nullptr;
   cplx* h2 = nullptr;
+  double* nw = nullptr;  // 2 x LZ_MAXI: summed partial norms of the two passes
   unsigned* bar = nullptr;
   int* err = nullptr;  // set when a bounded grid barrier ran out
 };

@@ -6,10 +6,14 @@
 // For every instance q, with k = j+1 basis vectors V[:, 0..j] and
 // w = (H - sigma) v_j computed by the matvec:
 //   projector  w += U (U^H v_j)        (excited states: U holds sqrt(pen) u_t)
-//   pass 1     w' = w - beta_{j-1} v_{j-1};  h = V^H w';  w'' = w' - V h
+//   pass 1     w' = w - beta_{j-1} v_{j-1};  h = V^H w', |w'|^2;  w'' = w' - V h
 //   pass 2     only when |w''|^2 < |w'|^2 / 2 (Daniel, Gragg, Kaufman,
 //              Stewart 1976): h2 = V^H w''; w''' = w'' - V h2
 //   alpha_j = sigma + Re(h_j + h2_j), beta_j = |w|, V[:, j+1] = w / beta_j.
+// Without a second pass |w''|^2 = |w'|^2 - |h|^2 (V orthonormal; the test
+// bounds the cancellation to a factor 2), so beta_j is known before the
+// update and the update writes v_{j+1} directly: two grid barriers per
+// step.  After a second pass the norm is summed explicitly.
 //
 // Rows of all instances are cut into row blocks of 256 (one per thread);
 // blocks are taken in grid-stride order by a grid that is resident all at
@@ -202,12 +206,25 @@ __device__ void block_update(const LzInst& in, int rb, cplx* __restrict__ x, con
 }
 
 // h[q][l] = sum over the row blocks of q of part[rb][l], one warp per (q, l),
-// for the instances selected by `sel` (bit q).
-__device__ void reduce_pairs(const LzBatch& b, const cplx* part, cplx* h, unsigned sel) {
+// for the instances selected by `sel` (bit q); further warps sum the
+// partial norms pn over the row blocks of every selected instance into
+// nw[q].  Fixed order throughout.
+__device__ void reduce_pairs(const LzBatch& b, const cplx* part, cplx* h, unsigned sel, const double* pn,
+                             double* nw) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int npairs = 0;
   for (int q = 0; q < b.ninst; q++) npairs += b.in[q].k;
-  for (int p = blockIdx.x * NW + warp; p < npairs; p += gridDim.x * NW) {
+  for (int p = blockIdx.x * NW + warp; p < npairs + b.ninst; p += gridDim.x * NW) {
+    if (p >= npairs) {
+      const int q = p - npairs;
+      if (!((sel >> q) & 1u)) continue;
+      const LzInst& in = b.in[q];
+      double s = 0.0;
+      for (int r = lane; r < in.nrb; r += 32) s += __ldcg(&pn[in.rb0 + r]);
+      s = warp_sumd(s);
+      if (lane == 0) nw[q] = s;
+      continue;
+    }
     int q = 0, rem = p;
     while (rem >= b.in[q].k) rem -= b.in[q].k, q++;
     if (!((sel >> q) & 1u)) continue;
@@ -216,6 +233,47 @@ __device__ void reduce_pairs(const LzBatch& b, const cplx* part, cplx* h, unsign
     for (int r = lane; r < in.nrb; r += 32) s = cadd(s, __ldcg(&part[(long long)(in.rb0 + r) * KMAXS + rem]));
     s = warp_sumc(s);
     if (lane == 0) h[q * KMAXS + rem] = s;
+  }
+}
+
+// |h[q]|^2 for every instance, one warp per instance, into hh (shared);
+// every CTA gets the same values.
+__device__ void coefficient_norms(const LzBatch& b, const cplx* h, double* hh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = warp; q < b.ninst; q += NW) {
+    double s = 0.0;
+    for (int l = lane; l < b.in[q].k; l += 32) s += cabs2(__ldcg(&h[q * KMAXS + l]));
+    s = warp_sumd(s);
+    if (lane == 0) hh[q] = s;
+  }
+  __syncthreads();
+}
+
+// x -= V h over the rows of row block rb, then V[:, j+1] = x / beta (or x
+// itself stored back into w when the basis is full: the residual the
+// restart needs).  No reduction.
+__device__ void block_update_final(const LzInst& in, int rb, const cplx* hs, int k, double inv_beta) {
+  const int tid = threadIdx.x;
+  const long long i = (long long)(rb - in.rb0) * RB + tid;
+  if (i < in.n) {
+    cplx a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
+    const cplx* v = in.V + i;
+    for (int l0 = 0; l0 < k; l0 += 16) {
+      cplx vv[16];
+#pragma unroll
+      for (int t = 0; t < 16; t++)
+        vv[t] = l0 + t < k ? __ldcg(&v[(long long)(l0 + t) * in.ldv]) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int t = 0; t < 16; t += 4) {
+        if (l0 + t < k) a0 = cadd(a0, cmul(vv[t], hs[l0 + t]));
+        if (l0 + t + 1 < k) a1 = cadd(a1, cmul(vv[t + 1], hs[l0 + t + 1]));
+        if (l0 + t + 2 < k) a2 = cadd(a2, cmul(vv[t + 2], hs[l0 + t + 2]));
+        if (l0 + t + 3 < k) a3 = cadd(a3, cmul(vv[t + 3], hs[l0 + t + 3]));
+      }
+    }
+    const cplx xi = csub(in.w[i], cadd(cadd(a0, a1), cadd(a2, a3)));
+    if (in.write_next) in.V[(long long)(in.j + 1) * in.ldv + i] = cscale(xi, inv_beta);
+    else in.w[i] = xi;
   }
 }
 
@@ -301,36 +359,47 @@ __global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__
     block_dots(in.V, in.ldv, in.n, (long long)(rb - in.rb0) * RB, rb, in.w, in.k, b.part, b.pn1, red, redn);
   }
   if (!grid_barrier(b.bar, b.err)) return;
-  reduce_pairs(b, b.part, b.h, 0xffffffffu);
+  reduce_pairs(b, b.part, b.h, 0xffffffffu, b.pn1, b.nw);
   if (!grid_barrier(b.bar, b.err)) return;
+
+  // ---- DGKS test (every CTA decides the same): after the first pass
+  // |w''|^2 = |w'|^2 - |h|^2 (the basis is orthonormal); a second pass when
+  // that drops below half of |w'|^2, else beta_j = |w''| at once ----
+  __shared__ double hh[LZ_MAXI];
+  __shared__ double beta_s[LZ_MAXI];
+  coefficient_norms(b, b.h, hh);
+  if (tid == 0) {
+    unsigned f = 0u;
+    for (int q = 0; q < b.ninst; q++) {
+      const double nw = __ldcg(&b.nw[q]);
+      const double b2 = nw - hh[q];
+      if (b2 < DGKS2 * nw) f |= 1u << q;
+      beta_s[q] = sqrt(fmax(b2, 0.0));
+    }
+    flagged = f;
+  }
+  __syncthreads();
+  const unsigned fl = flagged;
+
+  // ---- update: unflagged instances finish here (w'' / beta_j into the
+  // basis); flagged ones keep w'' and take its second-pass dots ----
   for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
     const int q = inst_of(b, rb);
     const LzInst& in = b.in[q];
     for (int l = tid; l < in.k; l += T) hs[l] = __ldcg(&b.h[q * KMAXS + l]);
     __syncthreads();
-    block_update(in, rb, in.w, hs, in.k, b.pn2, redn);
-  }
-  if (!grid_barrier(b.bar, b.err)) return;
-
-  // ---- DGKS test (every CTA decides the same) ----
-  if (tid == 0) flagged = 0u;
-  __syncthreads();
-  for (int q = 0; q < b.ninst; q++) {
-    const double nb2 = sum_norms(b.in[q], b.pn1, redn);
-    const double b2 = sum_norms(b.in[q], b.pn2, redn);
-    if (tid == 0 && b2 < DGKS2 * nb2) flagged |= 1u << q;
-  }
-  __syncthreads();
-  const unsigned fl = flagged;
-  if (fl) {
-    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
-      const int q = inst_of(b, rb);
-      if (!((fl >> q) & 1u)) continue;
-      const LzInst& in = b.in[q];
+    if (!((fl >> q) & 1u)) {
+      block_update_final(in, rb, hs, in.k, beta_s[q] > 0.0 ? 1.0 / beta_s[q] : 0.0);
+      __syncthreads();
+    } else {
+      block_update(in, rb, in.w, hs, in.k, b.pn2, redn);
       block_dots(in.V, in.ldv, in.n, (long long)(rb - in.rb0) * RB, rb, in.w, in.k, b.part, nullptr, red, redn);
     }
+  }
+
+  if (fl) {
     if (!grid_barrier(b.bar, b.err)) return;
-    reduce_pairs(b, b.part, b.h2, fl);
+    reduce_pairs(b, b.part, b.h2, fl, b.pn2, b.nw + LZ_MAXI);
     if (!grid_barrier(b.bar, b.err)) return;
     for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
       const int q = inst_of(b, rb);
@@ -338,18 +407,29 @@ __global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__
       const LzInst& in = b.in[q];
       for (int l = tid; l < in.k; l += T) hs[l] = __ldcg(&b.h2[q * KMAXS + l]);
       __syncthreads();
-      block_update(in, rb, in.w, hs, in.k, b.pn2, redn);
+      block_update(in, rb, in.w, hs, in.k, b.pn1, redn);
     }
+    // the norm after the second pass is summed explicitly (no cancellation
+    // argument holds for it)
     if (!grid_barrier(b.bar, b.err)) return;
+    for (int q = 0; q < b.ninst; q++) {
+      if (!((fl >> q) & 1u)) continue;
+      const double b2 = sum_norms(b.in[q], b.pn1, redn);
+      if (tid == 0) beta_s[q] = sqrt(b2);
+    }
+    __syncthreads();
+    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
+      const int q = inst_of(b, rb);
+      const LzInst& in = b.in[q];
+      if (!((fl >> q) & 1u) || !in.write_next) continue;
+      const double inv = beta_s[q] > 0.0 ? 1.0 / beta_s[q] : 0.0;
+      cplx* vn = in.V + (long long)(in.j + 1) * in.ldv;
+      const long long i = (long long)(rb - in.rb0) * RB + tid;
+      if (i < in.n) vn[i] = cscale(in.w[i], inv);
+    }
   }
 
-  // ---- alpha_j, beta_j; V[:, j+1] = w / beta_j ----
-  __shared__ double beta_s[LZ_MAXI];
-  for (int q = 0; q < b.ninst; q++) {
-    const double b2 = sum_norms(b.in[q], b.pn2, redn);
-    if (tid == 0) beta_s[q] = sqrt(b2);
-  }
-  __syncthreads();
+  // ---- alpha_j, beta_j ----
   if (blockIdx.x == 0 && tid < b.ninst) {
     const LzInst& in = b.in[tid];
     double alpha = in.sigma + __ldcg(&b.h[tid * KMAXS + in.j].x);
@@ -361,18 +441,6 @@ __global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__
     if (in.mirror) {  // mapped host memory, read by the host after the launch's event
       in.mirror->alpha[in.j] = alpha;
       in.mirror->beta[in.j] = beta;
-    }
-  }
-  for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
-    const int q = inst_of(b, rb);
-    const LzInst& in = b.in[q];
-    if (!in.write_next) continue;
-    const double inv = 1.0 / beta_s[q];
-    cplx* vn = in.V + (long long)(in.j + 1) * in.ldv;
-    const long long r0 = (long long)(rb - in.rb0) * RB;
-    {
-      const long long i = r0 + tid;
-      if (i < in.n) vn[i] = cscale(in.w[i], inv);
     }
   }
 }
@@ -403,9 +471,9 @@ void lanczos_step(const Stream& st, LzBatch& b) {
     MPSGPU_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     MPSGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lanczos_step_kernel, T, 0));
     MPSGPU_CHECK(per >= 1, MPSGPU_BAD_SHAPE, "lanczos step: kernel does not fit on an SM");
-    // one CTA per SM: room stays for the kernels of other streams (and for
-    // other cooperative launches) next to the step
-    g_lz_grid[dev] = nsm;
+    // at most two CTAs per SM: a group of several instances has row blocks
+    // enough for both, and room stays for the kernels of other streams
+    g_lz_grid[dev] = nsm * std::min(per, 2);
     mark_device_done(g_lz_setup);
   }
   const int grid = std::max(1, std::min(g_lz_grid[dev], b.nrb_total));

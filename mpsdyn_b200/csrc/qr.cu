@@ -201,7 +201,7 @@ __device__ cplx warp_reflector(cplx* P, int mp, int c) {
   cplx alpha = P[c + (long long)c * mp];
   if (xnorm == 0.0 && alpha.y == 0.0) return make_double2(0.0, 0.0);  // H = I
   double nrm = hypot3(alpha.x, alpha.y, xnorm);
-  double beta = alpha.x >= 0.0 ? -nrm : nrm;
+  double beta = -copysign(nrm, alpha.x);  // -sign(Re alpha) nrm, signed zero as LAPACK
   // |beta| below kSafeMin: scale the column up (at most 20 times) so that
   // 1 / (alpha - beta) stays finite; beta is scaled back at the end, tau and
   // v are scale-invariant
@@ -217,7 +217,7 @@ __device__ cplx warp_reflector(cplx* P, int mp, int c) {
     __syncwarp();
     xnorm = warp_scaled_norm(nx, x);
     nrm = hypot3(alpha.x, alpha.y, xnorm);
-    beta = alpha.x >= 0.0 ? -nrm : nrm;
+    beta = -copysign(nrm, alpha.x);
   }
   const cplx tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
   const cplx scale = recip_smith(make_double2(alpha.x - beta, alpha.y));
@@ -402,6 +402,465 @@ __global__ void __launch_bounds__(QR_THREADS) qr_form_q_kernel(QrParams p, cplx*
   }
 }
 
+// ---------------------------------------------------------------------------
+// Cluster QR: the whole matrix in the shared memory of one thread-block
+// cluster of S <= 8 CTAs (m <= 256 rows).  Column slice q (16 columns) lives
+// in CTA q % S; panel q is the first min(16, K - 16q) columns of slice q, so
+// its owner factors it where it lies and the other CTAs read its reflectors
+// V and block factor T through distributed shared memory after one cluster
+// barrier.  Q is formed slice by slice in the same launch (slice q by the
+// owner of panel q, applying H_q, H_{q-1}, ..., H_0 to unit columns), so
+// neither the factored matrix nor T ever goes to global memory.
+//
+// Inside a panel, thread i holds row i of the panel (16 columns) in
+// registers.  For column c one block reduction of 16 slots gives at once
+// the squared norm of x = A[c+1:, c] (slot c; its imaginary part carries
+// sum_r max(|Re x_r|, |Im x_r|), a scale and zero test), the products
+// x^H A[c+1:, q] with the panel's later columns (slots q > c), and the
+// products V[c+1:, l]^H x with the earlier reflectors (slots l < c), from
+// which the column of T follows (zlarft's V^H v), since v = x / (alpha -
+// beta) below its unit entry.  When the scale test finds x tiny or huge
+// (entries of rank-deficient sites below 1e-154 square to zero), the slots
+// are summed again with x / scale, as zlarfg rescales.
+// ---------------------------------------------------------------------------
+
+constexpr int CQ_NB = 16;    // slice and panel width
+constexpr int CQ_T = 256;    // threads per CTA: one panel row each
+constexpr int CQ_MAXM = CQ_T;
+constexpr int CQ_MAXS = 8;   // CTAs per cluster (portable limit)
+
+struct CqParams {
+  int m, n, K;
+  int npa, np;     // column slices of A (ceil(n/16)); panels = slices of Q (ceil(K/16))
+  int S, nA, nQ;   // cluster size; slices of A and of Q per CTA (most)
+  const cplx* A;   // m x n, ld m (read only)
+  cplx* Q; long long ldq;
+  cplx* R; long long ldr;
+};
+
+// Shared memory of the cluster kernel in complex entries: A slices, Q
+// slices, the staging copy of a panel's V (m x 16), the T factors of the
+// panels owned, and 16 x 16 scratch: T staging, W, W2, the Gram columns G,
+// the warps' slot sums (8 x 16), the slot totals, two row buffers, tau.
+__host__ __device__ constexpr size_t cq_smem_elems(int m, int nA, int nQ) {
+  return (size_t)(nA + nQ + 1) * m * CQ_NB + (size_t)nQ * 256 + 4 * 256 + (CQ_T / 32) * 16 + 16 + 32 + 16;
+}
+
+// Sum of v[0..31] over the lanes of a warp by a transposing butterfly: after
+// the five exchange steps lane L holds the total of v[L].
+__device__ __forceinline__ cplx warp_sum32(cplx (&v)[32]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int half = 16; half >= 1; half >>= 1) {
+    const bool up = lane & half;
+#pragma unroll
+    for (int i = 0; i < half; i++) {
+      const cplx send = up ? v[i] : v[i + half];
+      cplx keep = up ? v[i + half] : v[i];
+      keep.x += __shfl_xor_sync(0xffffffffu, send.x, half);
+      keep.y += __shfl_xor_sync(0xffffffffu, send.y, half);
+      v[i] = keep;
+    }
+  }
+  return v[0];
+}
+
+// The same for 16 values: afterwards lanes L and L ^ 1 hold the total of
+// v[L >> 1].
+__device__ __forceinline__ cplx warp_sum16x(cplx (&v)[16]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int half = 8, mask = 16; half >= 1; half >>= 1, mask >>= 1) {
+    const bool up = lane & mask;
+#pragma unroll
+    for (int i = 0; i < half; i++) {
+      const cplx send = up ? v[i] : v[i + half];
+      cplx keep = up ? v[i + half] : v[i];
+      keep.x += __shfl_xor_sync(0xffffffffu, send.x, mask);
+      keep.y += __shfl_xor_sync(0xffffffffu, send.y, mask);
+      v[i] = keep;
+    }
+  }
+  cplx r = v[0];
+  r.x += __shfl_xor_sync(0xffffffffu, r.x, 1);
+  r.y += __shfl_xor_sync(0xffffffffu, r.y, 1);
+  return r;
+}
+
+// Copy panel (V, T) of slice Vr (possibly another CTA's shared memory, ld
+// m) into Vs (rows j0.. as rows 0.., ld mp, unit lower trapezoidal in its
+// first jb columns, zero elsewhere) and Ts (16 x 16, zero outside jb x jb).
+__device__ void cq_stage(const cplx* Vr, const cplx* Tr, int m, int j0, int jb, cplx* Vs, cplx* Ts) {
+  const int mp = m - j0;
+  for (int t = threadIdx.x; t < mp * CQ_NB; t += CQ_T) {
+    const int r = t % mp, l = t / mp;
+    cplx v = make_double2(0.0, 0.0);
+    if (l < jb) {
+      if (r > l) v = Vr[j0 + r + (long long)l * m];
+      else if (r == l) v = make_double2(1.0, 0.0);
+    }
+    Vs[t] = v;
+  }
+  for (int t = threadIdx.x; t < 256; t += CQ_T) {
+    const int i = t % 16, l = t / 16;
+    Ts[t] = (i < jb && l < jb) ? Tr[t] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+}
+
+// C[j0:, 0:16] <- (I - V T' V^H) C[j0:, 0:16] for the staged panel (Vs, Ts);
+// T' = T^H (conjT: the factorisation's H^H) or T (forming Q).  C is a slice
+// in this CTA's shared memory (ld m).  W = V^H C by warps owning 4 x 8
+// blocks (lanes take rows), W2 = T' W, then C -= V W2 by rows.
+__device__ void cq_apply(cplx* C, int m, int j0, const cplx* Vs, const cplx* Ts, bool conjT, cplx* W, cplx* W2) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int mp = m - j0;
+  {
+    const int l0 = (warp >> 1) * 4, q0 = (warp & 1) * 8;
+    cplx acc[32];
+#pragma unroll
+    for (int e = 0; e < 32; e++) acc[e] = make_double2(0.0, 0.0);
+    for (int r = lane; r < mp; r += 32) {
+      cplx v[4], c[8];
+#pragma unroll
+      for (int i = 0; i < 4; i++) v[i] = Vs[r + (l0 + i) * mp];
+#pragma unroll
+      for (int k = 0; k < 8; k++) c[k] = C[j0 + r + (long long)(q0 + k) * m];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[i * 8 + k] = cadd(acc[i * 8 + k], ccmul(v[i], c[k]));
+    }
+    const cplx s = warp_sum32(acc);
+    W[(l0 + (lane >> 3)) + 16 * (q0 + (lane & 7))] = s;
+  }
+  __syncthreads();
+  {
+    const int i = tid & 15, q = tid >> 4;  // 256 threads: one entry of W2 each
+    cplx s = make_double2(0.0, 0.0);
+    if (conjT) {
+      for (int l = 0; l <= i; l++) s = cadd(s, ccmul(Ts[l + 16 * i], W[l + 16 * q]));
+    } else {
+      for (int l = i; l < 16; l++) s = cadd(s, cmul(Ts[i + 16 * l], W[l + 16 * q]));
+    }
+    W2[i + 16 * q] = s;
+  }
+  __syncthreads();
+  for (int it = tid; it < mp * 4; it += CQ_T) {
+    const int r = it % mp, q0 = (it / mp) * 4;
+    cplx a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
+#pragma unroll
+    for (int l = 0; l < 16; l++) {
+      const cplx v = Vs[r + l * mp];
+      a0 = cadd(a0, cmul(v, W2[l + 16 * (q0 + 0)]));
+      a1 = cadd(a1, cmul(v, W2[l + 16 * (q0 + 1)]));
+      a2 = cadd(a2, cmul(v, W2[l + 16 * (q0 + 2)]));
+      a3 = cadd(a3, cmul(v, W2[l + 16 * (q0 + 3)]));
+    }
+    cplx* c = C + j0 + r + (long long)q0 * m;
+    c[0] = csub(c[0], a0);
+    c[m] = csub(c[m], a1);
+    c[2LL * m] = csub(c[2LL * m], a2);
+    c[3LL * m] = csub(c[3LL * m], a3);
+  }
+  __syncthreads();
+}
+
+// Block sum of the 16 slots of every thread: warp sums, then threads 0..15
+// add the warps' values in a fixed order into tot[0..15].
+__device__ __forceinline__ void cq_reduce16(cplx (&s)[16], cplx* red, cplx* tot) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const cplx r = warp_sum16x(s);
+  if ((lane & 1) == 0) red[warp * 16 + (lane >> 1)] = r;
+  __syncthreads();
+  if (tid < 16) {
+    cplx a = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int w = 0; w < CQ_T / 32; w++) a = cadd(a, red[w * 16 + tid]);
+    tot[tid] = a;
+  }
+  __syncthreads();
+}
+
+// The 16 slots of one row for column c: conj(V[i, l]) x (l < c), conj(x)
+// A[i, q] (q > c) and (|x|^2, max(|Re x|, |Im x|)) in slot c.  Register
+// indices are compile-time; c only enters through predicates, so one copy
+// of the code serves every column.
+__device__ __forceinline__ void cq_slots(const cplx (&a)[16], int c, cplx x, bool with_max, cplx (&s)[16]) {
+#pragma unroll
+  for (int l = 0; l < 16; l++) {
+    if (l < c) s[l] = ccmul(a[l], x);
+    else if (l > c) s[l] = ccmul(x, a[l]);
+    else s[l] = make_double2(cabs2(x), with_max ? fmax(fabs(x.x), fabs(x.y)) : 0.0);
+  }
+}
+
+// One column of the panel factorisation (zlarfg for column c, then H_c^H on
+// the panel's later columns), for the panel row held in a (this thread's
+// row i of the panel; i < 0: no row).
+__device__ __forceinline__ void cq_column(cplx (&a)[16], int c, int i, cplx* red, cplx* tot, cplx* rowbuf, cplx* G,
+                                       cplx* taus) {
+  const int tid = threadIdx.x;
+  cplx* rb = rowbuf + (c & 1) * 16;
+  if (i == c) {
+#pragma unroll
+    for (int l = 0; l < 16; l++) rb[l] = a[l];
+  }
+  const bool below = i > c;
+  cplx ac = make_double2(0.0, 0.0);  // a[c] without a runtime register index
+#pragma unroll
+  for (int l = 0; l < 16; l++)
+    if (l == c) ac = a[l];
+  cplx s[16];
+  cq_slots(a, c, below ? ac : make_double2(0.0, 0.0), true, s);
+  cq_reduce16(s, red, tot);
+  const cplx alpha = rb[c];
+  const double x1 = tot[c].y;
+  // scale test: x exactly zero, or every square and product representable
+  const bool slow = x1 != 0.0 && (x1 < 1e-140 || x1 > 1e140 || fabs(alpha.x) > 1e140 || fabs(alpha.y) > 1e140);
+  double sig = 1.0;
+  if (slow) {  // uniform over the block: every thread read the same total
+    sig = x1;
+    // x / sig by division (1 / sig may overflow)
+    cq_slots(a, c, below ? make_double2(ac.x / sig, ac.y / sig) : make_double2(0.0, 0.0), false, s);
+    cq_reduce16(s, red, tot);
+  }
+  const double n2 = tot[c].x;
+  const cplx al = slow ? make_double2(alpha.x / sig, alpha.y / sig) : alpha;
+  cplx tau = make_double2(0.0, 0.0), sv = make_double2(0.0, 0.0);
+  double beta = alpha.x;
+  const bool identity = (n2 == 0.0 && al.y == 0.0);
+  if (!identity) {
+    // |alpha|^2 + |x|^2 directly while it is representable (alpha alone can
+    // be tiny when x is exactly zero), else with the largest part factored out
+    const double nrm2 = al.x * al.x + al.y * al.y + n2;
+    const double nrm = (!slow && nrm2 > 1e-280 && nrm2 < 1e280) ? sqrt(nrm2) : hypot3(al.x, al.y, sqrt(n2));
+    const double bp = -copysign(nrm, al.x);  // -sign(Re alpha) nrm, signed zero as LAPACK
+    tau = make_double2((bp - al.x) / bp, -al.y / bp);
+    sv = recip_smith(make_double2(al.x - bp, al.y));
+    beta = bp * sig;
+  }
+  // Gram column c of T: V[:, l]^H v_c = conj(V[c, l]) + sv * (V[c+1:, l]^H x')
+  if (tid < c) G[tid + 16 * c] = cadd(cconj(rb[tid]), cmul(sv, tot[tid]));
+  if (tid == 0) taus[c] = tau;
+  if (i >= c) {
+    cplx v;
+    if (i == c) v = make_double2(1.0, 0.0);
+    else v = cmul(slow ? make_double2(ac.x / sig, ac.y / sig) : ac, sv);
+    const cplx diag = i == c ? make_double2(beta, 0.0) : v;
+    const cplx ct = cconj(tau);
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      if (q == c) {
+        if (!identity || i == c) a[q] = diag;
+      } else if (q > c && !identity) {
+        // s_q = v^H A[:, q] = A[c, q] + conj(sv) (x'^H A[c+1:, q]);  A[:, q] -= conj(tau) s_q v
+        const cplx sq = cadd(rb[q], ccmul(sv, tot[q]));
+        a[q] = csub(a[q], cmul(cmul(ct, sq), v));
+      }
+    }
+  }
+}
+
+// Factor panel rows j0.. of slice As (this CTA, ld m), jb columns, in place
+// (R on and above the diagonal, V below), and build its block factor T
+// (16 x 16, zero outside jb x jb, ld 16) into Tout.
+__device__ void cq_factor_panel(cplx* As, int m, int j0, int jb, cplx* Tout, cplx* red, cplx* tot, cplx* rowbuf,
+                                cplx* G, cplx* taus) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int mp = m - j0;
+  const int i = tid < mp ? tid : -1;
+  cplx a[16];
+#pragma unroll
+  for (int l = 0; l < 16; l++) a[l] = i >= 0 ? As[j0 + i + (long long)l * m] : make_double2(0.0, 0.0);
+#pragma unroll 1
+  for (int c = 0; c < jb; c++) cq_column(a, c, i, red, tot, rowbuf, G, taus);
+  if (i >= 0) {
+#pragma unroll
+    for (int l = 0; l < 16; l++) As[j0 + i + (long long)l * m] = a[l];
+  }
+  __syncthreads();
+  // T column by column (zlarft, forward, columnwise): T[c, c] = tau_c,
+  // T[0:c, c] = -tau_c T[0:c, 0:c] G[0:c, c]
+  if (warp == 0) {
+    for (int c = 0; c < 16; c++) {
+      cplx v = make_double2(0.0, 0.0);
+      if (c < jb) {
+        const cplx tc = taus[c];
+        if (lane < c) {
+          cplx s = make_double2(0.0, 0.0);
+          for (int q = lane; q < c; q++) s = cadd(s, cmul(Tout[lane + 16 * q], G[q + 16 * c]));
+          v = cmul(make_double2(-tc.x, -tc.y), s);
+        } else if (lane == c) {
+          v = tc;
+        }
+      }
+      __syncwarp();
+      if (lane < 16) Tout[lane + 16 * c] = v;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(CQ_T, 1) qr_cluster_kernel(const __grid_constant__ CqParams p) {
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ double smem_d[];
+  const int m = p.m, S = p.S;
+  const int rank = (int)cl.block_rank();
+  const long long sl = (long long)m * CQ_NB;
+  cplx* As = reinterpret_cast<cplx*>(smem_d);
+  cplx* Qs = As + p.nA * sl;
+  cplx* Vs = Qs + p.nQ * sl;
+  cplx* Tl = Vs + sl;
+  cplx* Ts = Tl + p.nQ * 256;
+  cplx* W = Ts + 256;
+  cplx* W2 = W + 256;
+  cplx* G = W2 + 256;
+  cplx* red = G + 256;
+  cplx* tot = red + (CQ_T / 32) * 16;
+  cplx* rowbuf = tot + 16;
+  cplx* taus = rowbuf + 32;
+  const int tid = threadIdx.x;
+
+  // this CTA's slices q = rank + i S of A (columns past n are zero)
+  for (int i = 0; i < p.nA; i++) {
+    const int q = rank + i * S;
+    if (q >= p.npa) break;
+    for (int t = tid; t < m * CQ_NB; t += CQ_T) {
+      const int r = t % m, j = q * CQ_NB + t / m;
+      As[i * sl + t] = j < p.n ? p.A[r + (long long)j * m] : make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+
+  for (int pn = 0; pn < p.np; pn++) {
+    const int owner = pn % S, li = pn / S;
+    const int j0 = pn * CQ_NB, jb = min(CQ_NB, p.K - j0);
+    if (rank == owner) cq_factor_panel(As + li * sl, m, j0, jb, Tl + li * 256, red, tot, rowbuf, G, taus);
+    cl.sync();  // panel pn published to the cluster
+    bool staged = false;
+    for (int i = 0; i < p.nA; i++) {
+      const int q = rank + i * S;
+      if (q >= p.npa) break;
+      if (q <= pn) continue;
+      if (!staged) {
+        cq_stage(cl.map_shared_rank(As + li * sl, owner), cl.map_shared_rank(Tl + li * 256, owner), m, j0, jb, Vs,
+                 Ts);
+        staged = true;
+      }
+      cq_apply(As + i * sl, m, j0, Vs, Ts, true, W, W2);
+    }
+  }
+
+  // Q slice q = H_0 H_1 ... H_q applied to unit columns q*16.. (H_p leaves
+  // rows above 16p and the unit columns left of 16p alone)
+  for (int i = 0; i < p.nQ; i++) {
+    const int q = rank + i * S;
+    if (q >= p.np) break;
+    cplx* C = Qs + i * sl;
+    for (int t = tid; t < m * CQ_NB; t += CQ_T) {
+      const int r = t % m, j = q * CQ_NB + t / m;
+      C[t] = make_double2((r == j && j < p.K) ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int pn = q; pn >= 0; pn--) {
+      const int owner = pn % S, li = pn / S;
+      const int j0 = pn * CQ_NB, jb = min(CQ_NB, p.K - j0);
+      cq_stage(cl.map_shared_rank(As + li * sl, owner), cl.map_shared_rank(Tl + li * 256, owner), m, j0, jb, Vs, Ts);
+      cq_apply(C, m, j0, Vs, Ts, false, W, W2);
+    }
+  }
+
+  // R (K x n): the upper trapezoid of the factored slices; Q (m x K)
+  if (p.R) {
+    for (int i = 0; i < p.nA; i++) {
+      const int q = rank + i * S;
+      if (q >= p.npa) break;
+      for (int t = tid; t < p.K * CQ_NB; t += CQ_T) {
+        const int r = t % p.K, j = q * CQ_NB + t / p.K;
+        if (j < p.n) p.R[r + (long long)j * p.ldr] = r <= j ? As[i * sl + r + (long long)(j - q * CQ_NB) * m]
+                                                            : make_double2(0.0, 0.0);
+      }
+    }
+  }
+  if (p.Q) {
+    for (int i = 0; i < p.nQ; i++) {
+      const int q = rank + i * S;
+      if (q >= p.np) break;
+      for (int t = tid; t < m * CQ_NB; t += CQ_T) {
+        const int r = t % m, j = q * CQ_NB + t / m;
+        if (j < p.K) p.Q[r + (long long)j * p.ldq] = Qs[i * sl + t];
+      }
+    }
+  }
+  cl.sync();  // the panels stay in shared memory until every CTA has read them
+}
+
+// Dynamic shared memory limit of the cluster kernel (the largest plan, m =
+// 256 with one slice of A and one of Q per CTA, takes 215 KB).
+constexpr size_t CQ_SMEM_ATTR = 225 * 1024;
+static_assert(cq_smem_elems(CQ_MAXM, 1, 1) * sizeof(cplx) <= CQ_SMEM_ATTR, "cluster QR plan exceeds its limit");
+
+std::atomic<unsigned long long> g_cq_setup{0};
+bool g_cq_ok[64] = {false};
+
+// The cluster QR when the matrix fits (m <= 256 and its slices within the
+// shared-memory limit) and the device can place a cluster of 8 such CTAs;
+// false otherwise (the caller then runs the global-memory kernels).
+bool cluster_qr(const Stream& st, int m, int n, const cplx* A, cplx* Q, long long ldq, cplx* R, long long ldr) {
+  if (m > CQ_MAXM) return false;
+  CqParams p;
+  p.m = m; p.n = n; p.K = std::min(m, n);
+  p.npa = ceil_div(n, CQ_NB);
+  p.np = ceil_div(p.K, CQ_NB);
+  p.S = std::min(CQ_MAXS, p.npa);
+  p.nA = ceil_div(p.npa, p.S);
+  p.nQ = ceil_div(p.np, p.S);
+  const size_t smem = cq_smem_elems(m, p.nA, p.nQ) * sizeof(cplx);
+  if (smem > CQ_SMEM_ATTR) return false;
+  int dev = 0;
+  MPSGPU_CUDA(cudaGetDevice(&dev));
+  if (dev >= 64) return false;
+  if (device_needs_setup(g_cq_setup)) {
+    MPSGPU_CUDA(cudaFuncSetAttribute(qr_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)CQ_SMEM_ATTR));
+    // can a cluster of the largest size and plan be placed at all?
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CQ_MAXS);
+    cfg.blockDim = dim3(CQ_T);
+    cfg.dynamicSmemBytes = cq_smem_elems(CQ_MAXM, 1, 1) * sizeof(cplx);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CQ_MAXS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    g_cq_ok[dev] = cudaOccupancyMaxActiveClusters(&clusters, qr_cluster_kernel, &cfg) == cudaSuccess && clusters > 0;
+    (void)cudaGetLastError();
+    mark_device_done(g_cq_setup);
+  }
+  if (!g_cq_ok[dev]) return false;
+  p.A = A; p.Q = Q; p.ldq = ldq; p.R = R; p.ldr = ldr;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(p.S);
+  cfg.blockDim = dim3(CQ_T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st.s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = p.S;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  MPSGPU_CUDA(cudaLaunchKernelEx(&cfg, qr_cluster_kernel, p));
+  after_launch(st);
+  return true;
+}
+
 }  // namespace
 
 // Factor the m x n column-major matrix A (ld = m, overwritten).  Q (m x K,
@@ -415,6 +874,7 @@ void householder_qr_inplace(const Stream& st, int m, int n, cplx* A, cplx* Q, lo
   ProfScope ps(st, GemmProfiler::QR,
                16.0 * (2.0 * m * n * K - (double)(m + n) * K * K + 2.0 * (double)K * K * K / 3.0));
   MPSGPU_CHECK(m <= 1280, MPSGPU_BAD_SHAPE, "qr: more than 1280 rows is not supported");
+  if (cluster_qr(st, m, n, A, Q, ldq, R, ldr)) return;
   QrParams p;
   p.m = m; p.n = n; p.K = K; p.nb = nb; p.npanel = (K + nb - 1) / nb;
   p.A = A;

@@ -83,6 +83,47 @@ def test_qr_zero_padded_matches_lapack(ctx):
     assert rel(Q, Qn) < 1e-14 and rel(R, Rn) < 1e-14
 
 
+@pytest.mark.parametrize("scale", [1e-160, 1e150])
+def test_qr_tiny_and_huge_columns_match_lapack(ctx, scale):
+    # trailing columns far below (or above) the range whose squares are
+    # representable: the reflectors are computed from rescaled columns, as
+    # zlarfg does, so the factors still equal LAPACK's
+    rng = np.random.default_rng(3)
+    A = rand_c(rng, (64, 32))
+    A[:, 20:] *= scale
+    Q, R = ctx.qr(A)
+    Qn, Rn = np.linalg.qr(A, mode="reduced")
+    assert rel(Q, Qn) < 1e-11 and rel(R, Rn) < 1e-11
+    assert np.abs(Q.conj().T @ Q - np.eye(32)).max() < 1e-13
+
+
+def test_qr_tiny_pivots_and_signed_zero_match_lapack(ctx):
+    # a column that is exactly zero below a tiny complex diagonal entry (its
+    # squared modulus underflows), and a diagonal entry with real part -0.0
+    # (LAPACK's sign(., -0.0) is negative)
+    A = np.zeros((6, 3), dtype=complex)
+    A[0, 0] = 1.0
+    A[1, 1] = 1e-170 + 2e-170j
+    A[2, 2] = complex(-0.0, -3e-200)
+    A[4, 2] = 1e-201
+    Q, R = ctx.qr(A)
+    Qn, Rn = np.linalg.qr(A, mode="reduced")
+    assert np.all(np.isfinite(Q)) and np.all(np.isfinite(R))
+    assert rel(Q, Qn) < 1e-12
+    for i in range(3):
+        assert abs(R[i, i] - Rn[i, i]) <= 1e-12 * abs(Rn[i, i])
+
+
+def test_qr_padded_site_256x128_matches_lapack(ctx):
+    # a D = 128 site grown from bond dimension 40: the other columns are zero
+    rng = np.random.default_rng(8)
+    A = np.zeros((256, 128), dtype=complex)
+    A[:80, :40] = rand_c(rng, (80, 40))
+    Q, R = ctx.qr(A)
+    Qn, Rn = np.linalg.qr(A, mode="reduced")
+    assert rel(Q, Qn) < 1e-11 and rel(R, Rn) < 1e-11
+
+
 @pytest.mark.parametrize("m,n", [(6, 20), (20, 6), (128, 256)])
 def test_lq_matches_lapack(ctx, m, n):
     rng = np.random.default_rng(m * n)
