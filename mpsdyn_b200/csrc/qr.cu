@@ -428,6 +428,7 @@ constexpr int CQ_NB = 16;    // slice and panel width
 constexpr int CQ_T = 256;    // threads per CTA: one panel row each
 constexpr int CQ_MAXM = CQ_T;
 constexpr int CQ_MAXS = 8;   // CTAs per cluster (portable limit)
+static_assert(CQ_T == 256, "the 16 x 16 scratch is staged one entry per thread");
 
 struct CqParams {
   int m, n, K;
@@ -441,9 +442,10 @@ struct CqParams {
 // Shared memory of the cluster kernel in complex entries: A slices, Q
 // slices, the staging copy of a panel's V (m x 16), the T factors of the
 // panels owned, and 16 x 16 scratch: T staging, W, W2, the Gram columns G,
-// the warps' slot sums (8 x 16), the slot totals, two row buffers, tau.
+// the warps' slot sums (8 x 16), the slot totals, two row buffers, tau and
+// the column's update coefficients.
 __host__ __device__ constexpr size_t cq_smem_elems(int m, int nA, int nQ) {
-  return (size_t)(nA + nQ + 1) * m * CQ_NB + (size_t)nQ * 256 + 4 * 256 + (CQ_T / 32) * 16 + 16 + 32 + 16;
+  return (size_t)(nA + nQ + 1) * m * CQ_NB + (size_t)nQ * 256 + 4 * 256 + (CQ_T / 32) * 16 + 16 + 32 + 16 + 16;
 }
 
 // Sum of v[0..31] over the lanes of a warp by a transposing butterfly: after
@@ -492,19 +494,28 @@ __device__ __forceinline__ cplx warp_sum16x(cplx (&v)[16]) {
 // first jb columns, zero elsewhere) and Ts (16 x 16, zero outside jb x jb).
 __device__ void cq_stage(const cplx* Vr, const cplx* Tr, int m, int j0, int jb, cplx* Vs, cplx* Ts) {
   const int mp = m - j0;
-  for (int t = threadIdx.x; t < mp * CQ_NB; t += CQ_T) {
+  // every load issued before the first store: a load from another CTA's
+  // shared memory takes several hundred cycles
+  constexpr int PER = CQ_MAXM * CQ_NB / CQ_T;
+  cplx v[PER];
+#pragma unroll
+  for (int u = 0; u < PER; u++) {
+    const int t = threadIdx.x + u * CQ_T;
     const int r = t % mp, l = t / mp;
-    cplx v = make_double2(0.0, 0.0);
-    if (l < jb) {
-      if (r > l) v = Vr[j0 + r + (long long)l * m];
-      else if (r == l) v = make_double2(1.0, 0.0);
+    v[u] = make_double2(0.0, 0.0);
+    if (t < mp * CQ_NB && l < jb) {
+      if (r > l) v[u] = Vr[j0 + r + (long long)l * m];
+      else if (r == l) v[u] = make_double2(1.0, 0.0);
     }
-    Vs[t] = v;
   }
-  for (int t = threadIdx.x; t < 256; t += CQ_T) {
-    const int i = t % 16, l = t / 16;
-    Ts[t] = (i < jb && l < jb) ? Tr[t] : make_double2(0.0, 0.0);
+  const cplx tv = threadIdx.x < 256 && (threadIdx.x % 16) < jb && (threadIdx.x / 16) < jb ? Tr[threadIdx.x]
+                                                                                        : make_double2(0.0, 0.0);
+#pragma unroll
+  for (int u = 0; u < PER; u++) {
+    const int t = threadIdx.x + u * CQ_T;
+    if (t < mp * CQ_NB) Vs[t] = v[u];
   }
+  if (threadIdx.x < 256) Ts[threadIdx.x] = tv;
   __syncthreads();
 }
 
@@ -583,23 +594,29 @@ __device__ __forceinline__ void cq_reduce16(cplx (&s)[16], cplx* red, cplx* tot)
 }
 
 // The 16 slots of one row for column c: conj(V[i, l]) x (l < c), conj(x)
-// A[i, q] (q > c) and (|x|^2, max(|Re x|, |Im x|)) in slot c.  Register
-// indices are compile-time; c only enters through predicates, so one copy
-// of the code serves every column.
+// A[i, q] (q > c) and (|x|^2, max(|Re x|, |Im x|)) in slot c.  Both kinds
+// are p_l = conj(a_l) x, conjugated for l > c; register indices are
+// compile-time and c only enters through predicates, so one copy of the
+// code serves every column.
 __device__ __forceinline__ void cq_slots(const cplx (&a)[16], int c, cplx x, bool with_max, cplx (&s)[16]) {
 #pragma unroll
   for (int l = 0; l < 16; l++) {
-    if (l < c) s[l] = ccmul(a[l], x);
-    else if (l > c) s[l] = ccmul(x, a[l]);
-    else s[l] = make_double2(cabs2(x), with_max ? fmax(fabs(x.x), fabs(x.y)) : 0.0);
+    const cplx p = ccmul(a[l], x);
+    s[l] = make_double2(p.x, l > c ? -p.y : p.y);
   }
+  const double mx = with_max ? fmax(fabs(x.x), fabs(x.y)) : 0.0;
+  const double n2 = cabs2(x);
+#pragma unroll
+  for (int l = 0; l < 16; l++)
+    if (l == c) s[l] = make_double2(n2, mx);
 }
 
 // One column of the panel factorisation (zlarfg for column c, then H_c^H on
 // the panel's later columns), for the panel row held in a (this thread's
-// row i of the panel; i < 0: no row).
+// row i of the panel; i < 0: no row).  tq (16, shared) carries the update
+// coefficients conj(tau) s_q, computed once per column.
 __device__ __forceinline__ void cq_column(cplx (&a)[16], int c, int i, cplx* red, cplx* tot, cplx* rowbuf, cplx* G,
-                                       cplx* taus) {
+                                          cplx* taus, cplx* tq) {
   const int tid = threadIdx.x;
   cplx* rb = rowbuf + (c & 1) * 16;
   if (i == c) {
@@ -640,24 +657,24 @@ __device__ __forceinline__ void cq_column(cplx (&a)[16], int c, int i, cplx* red
     sv = recip_smith(make_double2(al.x - bp, al.y));
     beta = bp * sig;
   }
-  // Gram column c of T: V[:, l]^H v_c = conj(V[c, l]) + sv * (V[c+1:, l]^H x')
-  if (tid < c) G[tid + 16 * c] = cadd(cconj(rb[tid]), cmul(sv, tot[tid]));
-  if (tid == 0) taus[c] = tau;
+  if (tid < 16) {
+    // Gram column c of T: V[:, l]^H v_c = conj(V[c, l]) + sv * (V[c+1:, l]^H x');
+    // update coefficients: s_q = v^H A[:, q] = A[c, q] + conj(sv) (x'^H A[c+1:, q])
+    if (tid < c) G[tid + 16 * c] = cadd(cconj(rb[tid]), cmul(sv, tot[tid]));
+    tq[tid] = (tid > c && !identity) ? cmul(cconj(tau), cadd(rb[tid], ccmul(sv, tot[tid]))) : make_double2(0.0, 0.0);
+    if (tid == 0) taus[c] = tau;
+  }
+  __syncthreads();
   if (i >= c) {
-    cplx v;
-    if (i == c) v = make_double2(1.0, 0.0);
-    else v = cmul(slow ? make_double2(ac.x / sig, ac.y / sig) : ac, sv);
-    const cplx diag = i == c ? make_double2(beta, 0.0) : v;
-    const cplx ct = cconj(tau);
+    // A[:, q] -= conj(tau) s_q v for q > c (tq is zero elsewhere)
+    const cplx v = i == c ? make_double2(1.0, 0.0) : cmul(slow ? make_double2(ac.x / sig, ac.y / sig) : ac, sv);
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-      if (q == c) {
-        if (!identity || i == c) a[q] = diag;
-      } else if (q > c && !identity) {
-        // s_q = v^H A[:, q] = A[c, q] + conj(sv) (x'^H A[c+1:, q]);  A[:, q] -= conj(tau) s_q v
-        const cplx sq = cadd(rb[q], ccmul(sv, tot[q]));
-        a[q] = csub(a[q], cmul(cmul(ct, sq), v));
-      }
+    for (int q = 0; q < 16; q++) a[q] = csub(a[q], cmul(tq[q], v));
+    const cplx diag = i == c ? make_double2(beta, 0.0) : v;
+    if (!identity || i == c) {
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (q == c) a[q] = diag;
     }
   }
 }
@@ -666,7 +683,7 @@ __device__ __forceinline__ void cq_column(cplx (&a)[16], int c, int i, cplx* red
 // (R on and above the diagonal, V below), and build its block factor T
 // (16 x 16, zero outside jb x jb, ld 16) into Tout.
 __device__ void cq_factor_panel(cplx* As, int m, int j0, int jb, cplx* Tout, cplx* red, cplx* tot, cplx* rowbuf,
-                                cplx* G, cplx* taus) {
+                                cplx* G, cplx* taus, cplx* tq) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int mp = m - j0;
   const int i = tid < mp ? tid : -1;
@@ -674,30 +691,33 @@ __device__ void cq_factor_panel(cplx* As, int m, int j0, int jb, cplx* Tout, cpl
 #pragma unroll
   for (int l = 0; l < 16; l++) a[l] = i >= 0 ? As[j0 + i + (long long)l * m] : make_double2(0.0, 0.0);
 #pragma unroll 1
-  for (int c = 0; c < jb; c++) cq_column(a, c, i, red, tot, rowbuf, G, taus);
+  for (int c = 0; c < jb; c++) cq_column(a, c, i, red, tot, rowbuf, G, taus, tq);
   if (i >= 0) {
 #pragma unroll
     for (int l = 0; l < 16; l++) As[j0 + i + (long long)l * m] = a[l];
   }
   __syncthreads();
   // T column by column (zlarft, forward, columnwise): T[c, c] = tau_c,
-  // T[0:c, c] = -tau_c T[0:c, 0:c] G[0:c, c]
+  // T[0:c, c] = -tau_c T[0:c, 0:c] G[0:c, c]; lane l keeps row l of T in
+  // registers
   if (warp == 0) {
-    for (int c = 0; c < 16; c++) {
-      cplx v = make_double2(0.0, 0.0);
-      if (c < jb) {
-        const cplx tc = taus[c];
-        if (lane < c) {
-          cplx s = make_double2(0.0, 0.0);
-          for (int q = lane; q < c; q++) s = cadd(s, cmul(Tout[lane + 16 * q], G[q + 16 * c]));
-          v = cmul(make_double2(-tc.x, -tc.y), s);
-        } else if (lane == c) {
-          v = tc;
-        }
-      }
-      __syncwarp();
-      if (lane < 16) Tout[lane + 16 * c] = v;
-      __syncwarp();
+    cplx trow[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) trow[q] = make_double2(0.0, 0.0);
+    for (int c = 0; c < jb; c++) {
+      const cplx tc = taus[c];
+      cplx acc = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (q >= lane && q < c) acc = cadd(acc, cmul(trow[q], G[q + 16 * c]));
+      const cplx v = lane < c ? cmul(make_double2(-tc.x, -tc.y), acc) : (lane == c ? tc : make_double2(0.0, 0.0));
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (q == c) trow[q] = v;
+    }
+    if (lane < 16) {
+#pragma unroll
+      for (int q = 0; q < 16; q++) Tout[lane + 16 * q] = trow[q];
     }
   }
   __syncthreads();
@@ -721,6 +741,7 @@ __global__ void __launch_bounds__(CQ_T, 1) qr_cluster_kernel(const __grid_consta
   cplx* tot = red + (CQ_T / 32) * 16;
   cplx* rowbuf = tot + 16;
   cplx* taus = rowbuf + 32;
+  cplx* tq = taus + 16;
   const int tid = threadIdx.x;
 
   // this CTA's slices q = rank + i S of A (columns past n are zero)
@@ -737,7 +758,7 @@ __global__ void __launch_bounds__(CQ_T, 1) qr_cluster_kernel(const __grid_consta
   for (int pn = 0; pn < p.np; pn++) {
     const int owner = pn % S, li = pn / S;
     const int j0 = pn * CQ_NB, jb = min(CQ_NB, p.K - j0);
-    if (rank == owner) cq_factor_panel(As + li * sl, m, j0, jb, Tl + li * 256, red, tot, rowbuf, G, taus);
+    if (rank == owner) cq_factor_panel(As + li * sl, m, j0, jb, Tl + li * 256, red, tot, rowbuf, G, taus, tq);
     cl.sync();  // panel pn published to the cluster
     bool staged = false;
     for (int i = 0; i < p.nA; i++) {
