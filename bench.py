@@ -58,7 +58,12 @@ def parse():
     p.add_argument("--batch-form", default="lockstep", choices=["lockstep", "streams"],
                    help="lockstep: one context sweeps the batch together (grouped launches); "
                         "streams: one context, stream and host thread per solve")
+    p.add_argument("--groups", type=int, default=1,
+                   help="lockstep: the batch as this many lockstep groups, each on its own context and host "
+                        "thread, so that one group's host work and site steps overlap another's rounds")
     p.add_argument("--plain", type=int, default=1, help="also time one solve alone (the plain form)")
+    p.add_argument("--arm-steps", type=int, default=1,
+                   help="steps of each comparison arm (FP64 batch, FP64 batch with the mixed schedule)")
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="mixed: split-precision products until the energy settles, then FP64")
     p.add_argument("--workload", default="schwinger",
@@ -67,6 +72,8 @@ def parse():
                         "sample/split_gemm: bounded cases for profilers")
     p.add_argument("--sites", type=int, default=40, help="sample: chain length of the bounded sweep sample")
     p.add_argument("--rounds", type=int, default=1, help="sample: half-sweeps of the bounded sweep sample")
+    p.add_argument("--sample-batch", type=int, default=1,
+                   help="sample: chains swept in lockstep (seeds 1, 1001, ...), one batch of grouped launches")
     p.add_argument("--mnk", default="4096,4096,2048", help="split_gemm: m,n,k")
     p.add_argument("--instances", type=int, default=512, help="grouped: matvec instances")
     p.add_argument("--requests", type=int, default=48, help="serving: requests in the stream")
@@ -286,6 +293,17 @@ def fp64_gemm_peak(torch) -> float:
     return best
 
 
+def reduce_over_ranks(dist, x: float, op, device: str) -> float:
+    """x combined over the ranks of the process group (MAX for times, SUM for
+    work), or x itself without a group.  The only exchange the replicas make."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
 def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     import torch
     from mpsdyn_b200 import capi
@@ -303,11 +321,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             dist.barrier()
 
     def allreduce(x: float, op) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=op)
-        return float(t.item())
+        return reduce_over_ranks(dist, x, op, "cuda")
 
     W = WORKLOAD
     B = args.batch
@@ -322,7 +336,10 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     opts64 = ctxs[0].options(convtol=W["convtol"], precision=0)
     mpos = [c.mpo_schwinger(W["N"], MU, W["x"]) for c in ctxs]
     seeds = [(W["seed_gs"] + 1000 * (rank * B + i), W["seed_exc"] + 1000 * (rank * B + i)) for i in range(B)]
-    owner = [ctxs[0] if lockstep else c for c in ctxs]
+    G = max(1, min(args.groups, B)) if lockstep else 1
+    members = [list(range(g * B // G, (g + 1) * B // G)) for g in range(G)]  # solves of each lockstep group
+    lead = {i: mem[0] for mem in members for i in mem}                      # a group's context: its first solve's
+    owner = [ctxs[lead[i]] if lockstep else ctxs[i] for i in range(B)]
     inits = [(c.mps_random(W["N"], 2, W["D"], sg), c.mps_random(W["N"], 2, W["D"], se))
              for c, (sg, se) in zip(owner, seeds)]
     hosts = [(g.download()[0], x.download()[0]) for g, x in inits]
@@ -353,29 +370,31 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         x.free()
         m.free()
 
-    def lockstep_solves(o, e2e=False):
-        # all B solves swept in lockstep on one context: their local
-        # eigenproblems share the grouped launches of every Lanczos round
-        c = ctxs[0]
+    def lockstep_solves(o, e2e=False, g=0):
+        # the solves of group g swept in lockstep on the group's context:
+        # their local eigenproblems share the grouped launches of every
+        # Lanczos round
+        mem = members[g]
+        c = ctxs[mem[0]]
         if e2e:
-            ms = [c.mpo_schwinger(W["N"], MU, W["x"]) for _ in range(B)]       # host build + upload
-            gs = [c.mps(hosts[i][0]) for i in range(B)]                          # host -> device
-            xs = [c.mps(hosts[i][1]) for i in range(B)]
+            ms = [c.mpo_schwinger(W["N"], MU, W["x"]) for _ in mem]            # host build + upload
+            gs = [c.mps(hosts[i][0]) for i in mem]                               # host -> device
+            xs = [c.mps(hosts[i][1]) for i in mem]
         else:
-            ms = [mpos[0]] * B
-            gs = [inits[i][0].copy() for i in range(B)]
-            xs = [inits[i][1].copy() for i in range(B)]
+            ms = [mpos[mem[0]]] * len(mem)
+            gs = [inits[i][0].copy() for i in mem]
+            xs = [inits[i][1].copy() for i in mem]
         e0, st0, s0 = c.find_ground_state_batch(ms, W["D"], gs, 0.0, o)
         if any(st0):
             raise RuntimeError(f"ground-state batch: statuses {st0}")
-        e1, st1, s1 = c.find_next_excited_state_batch(ms, W["D"], [[g] for g in gs], xs, 0.0, o)
+        e1, st1, s1 = c.find_next_excited_state_batch(ms, W["D"], [[x] for x in gs], xs, 0.0, o)
         if any(st1):
             raise RuntimeError(f"excited-state batch: statuses {st1}")
-        for i in range(B):
-            results[i] = {"E0": e0[i], "E1": e1[i], "gs": s0[i], "exc": s1[i]}
+        for q, i in enumerate(mem):
+            results[i] = {"E0": e0[q], "E1": e1[q], "gs": s0[q], "exc": s1[q]}
             if e2e:
-                og, _ = gs[i].download()                                          # device -> host
-                ox, _ = xs[i].download()
+                og, _ = gs[q].download()                                          # device -> host
+                ox, _ = xs[q].download()
                 results[i]["d2h"] = sum(a.nbytes for a in og) + sum(a.nbytes for a in ox) + 16
         for v in gs + xs:
             v.free()
@@ -385,15 +404,35 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
 
     def run_batch(fn, timed_events=True, o=None, e2e=False):
         if lockstep:
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record(exts[0])
-            lockstep_solves(o or opts, e2e)
-            ev1.record(exts[0])
+            # one host thread per group; the span runs from the earliest start
+            # event to the latest end event on the groups' streams
+            gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(G)]
+            errs = []
+
+            def group(g):
+                try:
+                    gev[g][0].record(exts[members[g][0]])
+                    lockstep_solves(o or opts, e2e, g)
+                    gev[g][1].record(exts[members[g][0]])
+                except Exception as ex:  # reported after the join
+                    errs.append(ex)
+
+            ths = [threading.Thread(target=group, args=(g,)) for g in range(G)]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
             torch.cuda.synchronize()
+            if errs:
+                raise errs[0]
             if not timed_events:
                 return None, None
-            span = ev0.elapsed_time(ev1)
-            return span, [span] * B  # every solve completes with the batch
+            t0 = min(range(G), key=lambda g: 0.0 if g == 0 else gev[0][0].elapsed_time(gev[g][0]))
+            span = max(gev[t0][0].elapsed_time(gev[g][1]) for g in range(G))
+            per = []
+            for g in range(G):
+                per += [gev[g][0].elapsed_time(gev[g][1])] * len(members[g])  # a solve completes with its group
+            return span, per
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(B)]
         go = threading.Barrier(B)
 
@@ -470,7 +509,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         o = ctxs[0].options(convtol=W["convtol"], precision=precision)
         barrier()
         spans_a, energies_a = [], []
-        for _ in range(args.steps):
+        arm_steps = max(1, args.arm_steps)
+        for _ in range(arm_steps):
             flush_l2()
             span, _ = run_batch(lambda i: solve_resident(i, o), o=o)
             spans_a.append(span)
@@ -478,7 +518,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         t = allreduce(float(sum(spans_a)), torch.distributed.ReduceOp.MAX if dist else None)
         dE = max(max(abs(a[0] - b[0]) / abs(b[0]), abs(a[1] - b[1]) / abs(b[1]))
                  for sa, sb in zip(energies, energies_a) for a, b in zip(sa, sb))
-        return {"value": solves / (t * 1e-3), "ms_per_step": t / args.steps, "max_rel_dE_vs_line": dE,
+        arm_solves = allreduce(float(arm_steps * B), torch.distributed.ReduceOp.SUM if dist else None)
+        return {"value": arm_solves / (t * 1e-3), "ms_per_step": t / arm_steps, "steps": arm_steps,
+                "max_rel_dE_vs_line": dE,
                 "products_per_solve": results[0]["gs"]["matvecs"] + results[0]["exc"]["matvecs"]}
 
     fp64 = fp64_sched = None
@@ -572,6 +614,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                    "precision": ("mixed: split-precision (BF16-limb tcgen05) products until the half-sweep "
                                  "energy changes < 1e-6, then FP64" if mixed else "fp64"),
                    "batch": B,
+                   "groups": G,
                    "batch_form": ("lockstep: the B solves swept together on one stream, their local "
                                   "eigenproblems in shared grouped launches" if lockstep else
                                   "concurrent independent solves, one stream and host thread each"),
@@ -820,25 +863,34 @@ def run_sample(args) -> None:
     which ends the sample), in --precision.  With 40 sites, 26 bulk sites
     have the (128, 5, 128) shapes of the 100-site chain, so the kernel mix per
     site step is the headline's while the launch count stays small enough for
-    a profiler that slows every launch down."""
+    a profiler that slows every launch down.  With --sample-batch B > 1, B
+    chains (seeds 1, 1001, ...) are swept in lockstep, as the bench line's
+    batches are."""
     from mpsdyn_b200 import capi
+    B = max(1, args.sample_batch)
     with capi.Context(0) as ctx:
         H = ctx.mpo_schwinger(args.sites, MU, WORKLOAD["x"])
-        psi = ctx.mps_random(args.sites, 2, WORKLOAD["D"], 1)
+        psis = [ctx.mps_random(args.sites, 2, WORKLOAD["D"], 1 + 1000 * i) for i in range(B)]
         o = ctx.options(convtol=1e-10, max_rounds=args.rounds, precision=1 if args.precision == "mixed" else 0)
         l0 = ctx.launches
         t0 = time.perf_counter()
         status = "converged"
-        try:
-            ctx.find_ground_state(H, WORKLOAD["D"], psi, 0.0, o)
-        except capi.MpsgpuError as e:
-            if e.status != 2:  # anything but the round limit is a failure
-                raise
-            status = "round limit"
+        if B == 1:
+            try:
+                ctx.find_ground_state(H, WORKLOAD["D"], psis[0], 0.0, o)
+            except capi.MpsgpuError as e:
+                if e.status != 2:  # anything but the round limit is a failure
+                    raise
+                status = "round limit"
+        else:
+            _, sts, _ = ctx.find_ground_state_batch([H] * B, WORKLOAD["D"], psis, 0.0, o)
+            if any(st not in (0, 2) for st in sts):
+                raise RuntimeError(f"sample batch: statuses {sts}")
+            status = "round limit" if any(st == 2 for st in sts) else "converged"
         ctx.synchronize()
         print(json.dumps({"sample": f"schwinger N={args.sites} D={WORKLOAD['D']}, {args.rounds} half-sweep(s), "
-                                    f"{args.precision}", "status": status, "launches": ctx.launches - l0,
-                          "seconds": time.perf_counter() - t0}), flush=True)
+                                    f"{args.precision}, {B} chain(s)", "status": status,
+                          "launches": ctx.launches - l0, "seconds": time.perf_counter() - t0}), flush=True)
 
 
 def run_split_gemm(args) -> None:
