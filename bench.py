@@ -27,7 +27,6 @@ import json
 import os
 import subprocess
 import sys
-import tempfile
 import threading
 import time
 
@@ -39,6 +38,13 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(workload="schwinger_N100_D128_gs+gap", N=100, x=100.0, mg=0.125, D=128,
                 seed_gs=1, seed_exc=11, convtol=1e-10, d=2, mpo_bond=5)
 MU = 2 * WORKLOAD["mg"] * np.sqrt(WORKLOAD["x"])
+PRECISION = {"schedule": 2, "mixed": 1, "fp64": 0}  # options.precision of each form
+PRECISION_TEXT = {
+    "schedule": "FP64 products; eigensolver residual 1e-6 until the half-sweep energy change first falls below "
+                "1e-6, then 1e-9 for one half-sweep, then the reference's 1e-12 to convergence",
+    "mixed": "split-precision (BF16-limb tcgen05) products and residual 1e-6 until the half-sweep energy change "
+             "first falls below 1e-6, then FP64 (1e-9 for one half-sweep, then 1e-12)",
+    "fp64": "FP64 products, eigensolver residual 1e-12 throughout (the reference's tolerance)"}
 METRIC = "DMRG solves/s (Schwinger N=100 D=128, E0 + first gap, |dE/E|<=1e-10)"
 UNIT = "solves/s"
 
@@ -50,22 +56,23 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="mpsgpu", choices=["mpsgpu", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--ref-max-sites", type=int, default=0,
-                   help="reference arm / CPU baseline: site steps per process (0 = the whole block)")
     p.add_argument("--ref-iter-cap", type=int, default=0,
-                   help="tests only: cap the reference eigensolver (the line is then not a measurement)")
-    p.add_argument("--batch", type=int, default=8, help="concurrent solves per step")
+                   help="tests only: stop the sampled eigensolves after this many products instead of the "
+                        "calibrated 60 (the line is then not a measurement)")
+    p.add_argument("--batch", type=int, default=16, help="concurrent solves per step")
     p.add_argument("--batch-form", default="lockstep", choices=["lockstep", "streams"],
                    help="lockstep: one context sweeps the batch together (grouped launches); "
                         "streams: one context, stream and host thread per solve")
-    p.add_argument("--groups", type=int, default=1,
+    p.add_argument("--groups", type=int, default=2,
                    help="lockstep: the batch as this many lockstep groups, each on its own context and host "
                         "thread, so that one group's host work and site steps overlap another's rounds")
     p.add_argument("--plain", type=int, default=1, help="also time one solve alone (the plain form)")
     p.add_argument("--arm-steps", type=int, default=1,
                    help="steps of each comparison arm (FP64 batch, FP64 batch with the mixed schedule)")
-    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
-                   help="mixed: split-precision products until the energy settles, then FP64")
+    p.add_argument("--precision", default="schedule", choices=["schedule", "mixed", "fp64"],
+                   help="schedule: FP64 products with the mixed schedule of eigensolver tolerances; mixed: the "
+                        "same schedule with split-precision (tcgen05) products until the energy settles; fp64: "
+                        "FP64 with the reference's tolerance throughout")
     p.add_argument("--workload", default="schwinger",
                    choices=["schwinger", "grouped", "serving", "quench", "sample", "split_gemm"],
                    help="schwinger: the headline line; grouped/serving/quench: the secondary workloads; "
@@ -134,105 +141,46 @@ class ClockSampler:
 # CPU baseline: the reference compiled from source (oracle/_ref), bounded sample
 # ---------------------------------------------------------------------------
 
-def reference_counts() -> dict:
-    """Products and wall time of the reference's complete solve of this
-    workload (findGroundState + findNextExcitedState, one core), from the
-    pinned reference run (tests/golden/golden.json, written by
-    tests/golden/make_golden_large.py); None when not generated."""
-    try:
-        with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
-            t = json.load(f).get("reference_timing", {})
-        return {"gs": t["schwinger_N100_D128_gs"], "exc": t["schwinger_N100_D128_exc"]}
-    except (OSError, KeyError, ValueError):
-        return None
-
-
-def reference_sample(procs: int, max_sites: int = 0, iter_cap: int = 0) -> dict:
-    """One half-sweep of the reference's ground-state sweep of this workload
-    (site steps 0..N-2: eigensolve with no iteration cap, QR gauge move,
-    environment update), cut into `procs` contiguous blocks of sites, each
-    timed by one single-threaded process of oracle/_ref (the reference
-    compiled from source; eigensolver shim above the dense branch); with
-    max_sites > 0 every block keeps only its first max_sites sites (a shorter
-    sample spread over the chain).  Returns the products, the core-seconds
-    and the wall time."""
-    from oracle import mps_oracle as mo  # the checker/baseline only
-    drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
-    if not os.path.exists(drv):
-        raise FileNotFoundError("oracle/_ref/ref_driver not built (make -C oracle)")
-    tmp = tempfile.mkdtemp()
-    fn = os.path.join(tmp, "init.mps")
-    N = WORKLOAD["N"]
-    mo.write_mps(fn, mo.random_mps(N, 2, WORKLOAD["D"], WORKLOAD["seed_gs"]))
-    env = dict(os.environ, OPENBLAS_NUM_THREADS="1", ASAN_OPTIONS="detect_leaks=0")
-    env.pop("MPSDYN_SHIM_MAX_ITERS", None)
-    if iter_cap > 0:  # tests of the arm's plumbing only: the measured sample is never capped
-        env["MPSDYN_SHIM_MAX_ITERS"] = str(iter_cap)
-    model = f"schwinger:{N}:{MU}:{WORKLOAD['x']}:0:0"
-    procs = max(1, min(procs, N - 1))
-    cuts = [round(i * (N - 1) / procs) for i in range(procs + 1)]
-    t0 = time.time()
-    def nsites(i):
-        n = cuts[i + 1] - cuts[i]
-        return min(n, max_sites) if max_sites > 0 else n
-    ps = [subprocess.Popen([drv, "profile", model, str(WORKLOAD["D"]), "0", fn, str(nsites(i)), str(cuts[i])],
-                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, env=env)
-          for i in range(procs) if cuts[i + 1] > cuts[i]]
-    outs = [p.communicate()[0] for p in ps]
-    wall = time.time() - t0
-    res = [json.loads([l for l in o.splitlines() if l.startswith("{")][-1]) for o in outs]
-    return {"products": sum(r["iterations"] for r in res), "core_seconds": sum(r["seconds"] for r in res),
-            "wall": wall, "procs": len(res), "sites": sum(r["nsites"] for r in res),
-            "max_process_seconds": max(r["seconds"] for r in res)}
-
-
-def reference_rate(procs: int, max_sites: int = 0, iter_cap: int = 0) -> tuple:
-    """Solves/s of the reference on `procs` cores (independent solves, one
-    per core) and the description of how it was obtained."""
-    s = reference_sample(procs, max_sites, iter_cap)
-    per_core = s["products"] / s["core_seconds"]  # products per core-second, site-step overheads included
-    rc = reference_counts()
-    if rc:
-        # the excited-state products are Hermitian multipliers: two products each
-        products = rc["gs"]["products"] + 2 * rc["exc"]["products"]
-        src = (f"the reference's own counts of its complete solve (ground state {rc['gs']['products']} + "
-               f"2 x {rc['exc']['products']} Hermitian excited-state products, pinned run of "
-               f"{rc['gs']['seconds'] + rc['exc']['seconds']:.0f} s on one core of the build host)")
-    else:
-        products = 2 * 19699 + 2 * 21187  # fallback: the library's FP64 counts (Lanczos, same tolerance)
-        src = "the library's FP64 product counts (the reference's pinned counts were not available)"
-    t_core = products / per_core
-    value = s["procs"] / t_core
-    part = ("one uncapped half-sweep" if max_sites <= 0 else
-            f"the first {max_sites} site step(s) of each block of one uncapped half-sweep")
-    sample = (f"{part} (site steps 0..{WORKLOAD['N'] - 2}, edges included: eigensolve, QR "
-              f"gauge move, environment update) of the reference compiled from source (oracle/_ref), split "
-              f"into {s['procs']} contiguous blocks timed by {s['procs']} single-threaded processes "
-              f"({s['products']} products, {s['core_seconds']:.1f} core-s, {s['wall']:.1f} s wall); "
-              f"extrapolated to a complete solve (one per core) by {src}")
-    return value, sample, {"products_sample": s["products"], "core_seconds_sample": s["core_seconds"],
-                           "products_per_solve": products, "core_seconds_per_solve": t_core,
-                           "wall_s": s["wall"]}
+def reference_rate(procs: int, cap: int = 0) -> tuple:
+    """Solves/s of the reference on `procs` cores of this host (independent
+    solves, one per core), from its pinned complete solve scaled by this
+    host's speed on a bounded sample (oracle/ref_timing.py); with the
+    products per core-second of the sample and how the value was obtained."""
+    from oracle import ref_timing  # the checker/baseline only
+    s = ref_timing.speed_sample(procs, cap or ref_timing.CAP)
+    secs, why = ref_timing.solve_seconds_here(s, strict=not cap or cap == ref_timing.CAP)
+    sample = (f"one bulk site step per process of the reference's ground-state sweep of this workload "
+              f"(oracle/_ref: the reference compiled from source; environments set up untimed; eigensolve stopped "
+              f"after {s['cap']} products, then its QR gauge move and environment update), sites "
+              f"{s['positions'][0]}..{s['positions'][-1]}, {s['procs']} single-threaded processes at once "
+              f"({s['products']} products, {s['core_seconds']:.1f} core-s, {s['wall']:.1f} s wall)")
+    detail = {"products_sample": s["products"], "core_seconds_sample": s["core_seconds"],
+              "products_per_core_second": s["rate"], "wall_s": s["wall"]}
+    if secs is None:
+        return None, sample + f"; no value: {why}", detail
+    detail["core_seconds_per_solve"] = secs
+    return s["procs"] / secs, sample + f"; scaled to the complete solve: {why}", detail
 
 
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     procs = min(os.cpu_count() or 1, 64)
-    # every step is one sample; the whole run stays within a few minutes: a
-    # full half-sweep per step for up to 3 steps, shorter blocks beyond
-    full = -(-(WORKLOAD["N"] - 1) // procs)
-    max_sites = args.ref_max_sites or (0 if args.steps <= 3 else max(1, full * 3 // args.steps))
-    vals, last = [], None
+    vals, walls, last = [], [], None
     for _ in range(max(1, args.steps)):  # no warm-up: nothing on the CPU path warms up
-        v, sample, detail = reference_rate(procs, max_sites, args.ref_iter_cap)
+        v, sample, detail = reference_rate(procs, args.ref_iter_cap)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": sample}), flush=True)
+            return
         if args.ref_iter_cap > 0:
-            sample += f" [eigensolver capped at {args.ref_iter_cap} products: plumbing test, not a measurement]"
+            sample += f" [eigensolves stopped after {args.ref_iter_cap} products: plumbing test, not a measurement]"
         vals.append(v)
+        walls.append(detail["wall_s"])
         last = (sample, detail)
     value = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": len(vals), "warmup": 0, "warmup_requested": args.warmup, "ms_per_step": 1e3 / value * procs,
+            "steps": len(vals), "warmup": 0, "warmup_requested": args.warmup,
+            "ms_per_step": 1e3 * float(np.mean(walls)),  # the sample's wall time; the solve's is in detail
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic (seeded complex Gaussian initial MPS)",
             "config": {**WORKLOAD, "parallelism": f"replicas{world}", "l2": "n/a (CPU)"},
@@ -293,6 +241,19 @@ def fp64_gemm_peak(torch) -> float:
     return best
 
 
+def attribution(form: str, value: float, arms: dict, plain_rate) -> dict:
+    """Batched solves/s of the three forms, split into factors: the tolerance
+    schedule (schedule / fp64), the tensor cores (mixed / schedule, the same
+    schedule with split-precision products) and the batching (fp64 batched /
+    one plain FP64 solve alone)."""
+    v = {k: a["value"] for k, a in arms.items()}
+    v[form] = value
+    if not all(k in v for k in ("fp64", "schedule", "mixed")):
+        return None
+    return {"schedule": v["schedule"] / v["fp64"], "tensor_cores": v["mixed"] / v["schedule"],
+            "concurrency": v["fp64"] / plain_rate if plain_rate else None}
+
+
 def reduce_over_ranks(dist, x: float, op, device: str) -> float:
     """x combined over the ranks of the process group (MAX for times, SUM for
     work), or x itself without a group.  The only exchange the replicas make."""
@@ -332,7 +293,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     exts = [torch.cuda.ExternalStream(c.stream) for c in ctxs]
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     mixed = args.precision == "mixed"
-    opts = ctxs[0].options(convtol=W["convtol"], precision=1 if mixed else 0)
+    prec = PRECISION[args.precision]
+    opts = ctxs[0].options(convtol=W["convtol"], precision=prec)
     opts64 = ctxs[0].options(convtol=W["convtol"], precision=0)
     mpos = [c.mpo_schwinger(W["N"], MU, W["x"]) for c in ctxs]
     seeds = [(W["seed_gs"] + 1000 * (rank * B + i), W["seed_exc"] + 1000 * (rank * B + i)) for i in range(B)]
@@ -523,10 +485,14 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                 "max_rel_dE_vs_line": dE,
                 "products_per_solve": results[0]["gs"]["matvecs"] + results[0]["exc"]["matvecs"]}
 
-    fp64 = fp64_sched = None
-    if mixed:
-        fp64 = batch_arm(0)
-        fp64_sched = batch_arm(2)
+    # the other two forms, same seeds (the line's own form is the line)
+    arms = {}
+    if prec != 0:
+        arms["fp64"] = batch_arm(0)
+        if prec == 2:
+            arms["mixed"] = batch_arm(1)
+        else:
+            arms["schedule"] = batch_arm(2)
 
     # ---- single solves alone on the GPU with the library's kernel profiler
     # on (events around 1 in 32 launches of each kernel class): the plain
@@ -544,7 +510,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         return ev0.elapsed_time(ev1), prof, r
 
     plain_ms, prof64, r64 = profiled_single(opts64) if args.plain else (None, None, None)
-    mixed_ms, profmx, rmx = profiled_single(opts) if (args.plain and mixed) else (None, None, None)
+    line_ms, profln, rln = profiled_single(opts) if (args.plain and prec != 0) else (None, None, None)
 
     if rank != 0:
         for c in ctxs:
@@ -576,7 +542,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         return out
 
     table64 = kernel_table(prof64, plain_ms)
-    tablemx = kernel_table(profmx, mixed_ms)
+    tableln = kernel_table(profln, line_ms)
 
     def dominant(table, note):
         if not table:
@@ -586,7 +552,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         d.update(kernel=name, traffic=KERNEL_TRAFFIC.get(name), traffic_unit="bytes per launch", note=note)
         return d
 
-    roofline = dominant(tablemx if mixed else table64,
+    roofline = dominant(tableln if prec != 0 else table64,
                         "achieved = sampled launches' algorithmic work / their summed CUDA-event time, one solve "
                         "of the line's precision alone on the GPU; lanczos_step bytes: basis read twice + "
                         "work vector traffic (the basis of one solve, 33 MB, is L2-resident)")
@@ -595,7 +561,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     if not args.no_cpu_baseline and world == 1:
         try:
             procs = min(os.cpu_count() or 1, 64)
-            cv, sample, detail = reference_rate(procs, args.ref_max_sites)
+            cv, sample, detail = reference_rate(procs)
             cpu = {"value": cv, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample,
                    "detail": detail}
         except Exception as e:  # the baseline is reported, not required
@@ -611,8 +577,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "c128/bf16x3" if mixed else "c128",
         "data": "synthetic (seeded complex Gaussian initial MPS, model MPO built in-library)",
         "config": {**WORKLOAD, "mu": MU, "parallelism": f"replicas{world}",
-                   "precision": ("mixed: split-precision (BF16-limb tcgen05) products until the half-sweep "
-                                 "energy changes < 1e-6, then FP64" if mixed else "fp64"),
+                   "precision": f"{args.precision}: {PRECISION_TEXT[args.precision]}",
                    "batch": B,
                    "groups": G,
                    "batch_form": ("lockstep: the B solves swept together on one stream, their local "
@@ -625,15 +590,11 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         "plain_single_solve_ms": plain_ms,
         "plain_fp64_solves_per_s": plain_rate,
         "vs_plain_fp64": (value / plain_rate) if plain_rate else None,
-        "mixed_single_solve_ms": mixed_ms,
-        "fp64_batched": fp64,
-        "fp64_batched_mixed_schedule": fp64_sched,
-        "attribution": ({"schedule": fp64_sched["value"] / fp64["value"],
-                         "tensor_cores": value / fp64_sched["value"],
-                         "concurrency": fp64["value"] / plain_rate if plain_rate else None}
-                        if fp64 and fp64_sched else None),
+        "line_form_single_solve_ms": line_ms,
+        "arms": arms,
+        "attribution": attribution(args.precision, value, arms, plain_rate),
         "roofline": roofline,
-        "kernels_mixed_single": tablemx,
+        "kernels_line_form_single": tableln,
         "kernels_fp64_single": table64,
         "cpu_baseline": cpu,
         "clocks": clk,
@@ -701,7 +662,7 @@ def run_grouped(args) -> None:
     roof64 = {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
               "peak_source": "cuBLAS complex128 GEMM 4096^3 measured in this run"}
     split = None
-    if args.precision == "mixed":
+    if args.precision != "fp64":
         # the same products in split precision (tcgen05, BF16 limbs); the
         # environments' limb planes are made once (ms_prepare), x and the
         # intermediate in every product
@@ -776,23 +737,24 @@ def run_serving(args) -> None:
                 "energies": {int(r["id"]): r["energy"] for r in ok}}
 
     mixed = args.precision == "mixed"
-    main = stream(1 if mixed else 0)
-    fp64 = stream(0) if mixed else None
+    prec = PRECISION[args.precision]
+    main = stream(prec)
+    fp64 = stream(0) if prec != 0 else None
     cmp = None
     if fp64:
         common = set(main["energies"]) & set(fp64["energies"])
         cmp = {"value": fp64["value"], "latency_s": fp64["latency_s"], "completed": fp64["completed"],
                "failed": fp64["failed"],
-               "max_rel_dE_mixed_vs_fp64": max((abs(main["energies"][k] - fp64["energies"][k]) /
-                                                abs(fp64["energies"][k]) for k in common), default=None),
-               "mixed_over_fp64": main["value"] / fp64["value"] if fp64["value"] else None}
+               "max_rel_dE_vs_fp64": max((abs(main["energies"][k] - fp64["energies"][k]) /
+                                          abs(fp64["energies"][k]) for k in common), default=None),
+               "line_over_fp64": main["value"] / fp64["value"] if fp64["value"] else None}
     line = {"metric": "served DMRG solves/s (Ising mix)", "value": main["value"], "unit": "solves/s",
             "n_gpus": 1, "steps": n, "warmup": 0, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128/bf16x3" if mixed else "c128",
             "data": "synthetic request stream (numpy seed 4)",
             "config": {"workload": "serving_ising_poisson", "requests": n, "rate_req_s": args.rate,
                        "slots": args.batch, "hbm_budget_bytes": budget, "L": "U[16,256]", "D": "U{32,64,128,256}",
-                       "precision": "mixed" if mixed else "fp64"},
+                       "precision": f"{args.precision}: {PRECISION_TEXT[args.precision]}"},
             "latency_s": main["latency_s"], "completed": main["completed"], "failed": main["failed"],
             "wall_s": main["wall_s"], "flops_total": main["flops_total"], "fp64_stream": cmp}
     print(json.dumps(line), flush=True)
@@ -871,7 +833,7 @@ def run_sample(args) -> None:
     with capi.Context(0) as ctx:
         H = ctx.mpo_schwinger(args.sites, MU, WORKLOAD["x"])
         psis = [ctx.mps_random(args.sites, 2, WORKLOAD["D"], 1 + 1000 * i) for i in range(B)]
-        o = ctx.options(convtol=1e-10, max_rounds=args.rounds, precision=1 if args.precision == "mixed" else 0)
+        o = ctx.options(convtol=1e-10, max_rounds=args.rounds, precision=PRECISION[args.precision])
         l0 = ctx.launches
         t0 = time.perf_counter()
         status = "converged"

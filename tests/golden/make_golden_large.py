@@ -74,7 +74,24 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--from-logs", default=None, help="parse <name>.log files of an earlier run")
     ap.add_argument("--logs", default=None, help="directory for the logs and inputs (default: a temp dir)")
+    ap.add_argument("--calibrate", action="store_true",
+                    help="only time the bounded speed sample of oracle/ref_timing.py on this host (all cores) and "
+                         "store it next to the full run it calibrates")
     a = ap.parse_args()
+    if a.calibrate:
+        from oracle import ref_timing
+        s = ref_timing.speed_sample(os.cpu_count() or 1)
+        gfile = os.path.join(HERE, "golden.json")
+        with open(gfile) as f:
+            golden = json.load(f)
+        golden.setdefault("reference_timing", {})["schwinger_N100_D128_calibration"] = {
+            "products_per_core_second": s["rate"], "cap": s["cap"], "procs": s["procs"],
+            "products": s["products"], "core_seconds": s["core_seconds"], "positions": s["positions"],
+            "note": "oracle/ref_timing.speed_sample on the host of the full run, all its cores"}
+        with open(gfile, "w") as f:
+            json.dump(golden, f, indent=1)
+        print(json.dumps(golden["reference_timing"]["schwinger_N100_D128_calibration"]))
+        return
     if a.from_logs:
         d = a.from_logs
     else:

@@ -55,7 +55,7 @@ def test_reference_arm_under_torchrun_two_ranks():
     r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
                         "--master-addr", "127.0.0.1", "--master-port", str(port),
                         os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
-                        "--ref-max-sites", "1", "--ref-iter-cap", "10", "--steps", "1", "--warmup", "1"],
+                        "--ref-iter-cap", "10", "--steps", "1", "--warmup", "1"],
                        capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
                     reason="oracle/_ref not built")
 def test_reference_arm_prints_its_line():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                        "--ref-max-sites", "1", "--ref-iter-cap", "10", "--steps", "2", "--warmup", "3"],
+                        "--ref-iter-cap", "10", "--steps", "2", "--warmup", "3"],
                        capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
