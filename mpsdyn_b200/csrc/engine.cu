@@ -491,32 +491,16 @@ static uint8_t* bytes_reserve(Context& c, DBuf& b, long long bytes) {
 void split_matvec_prepare(Context& c, SplitMatvec& s, const cplx* Le, const std::array<int, 3>& ld,
                           const MpoDev& m, int k, const cplx* Rt, const std::array<int, 3>& rd) {
   const auto& wd = m.dims[k];
-  const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
+  const int wl = wd[1], wr = wd[3];
   const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
-  const int nsm = device_sms(c);
-  s.p1 = split_plan(Dlb * wl, dd * Drk, Dlk, nsm);
-  s.p3 = split_plan(Dlb * du, Drb, Drk * wr, nsm);
   const Stream st = c.st();
   // L as the A operand of T1 = L . X: rows Dlb*wl, inner Dlk, column-major
   split_prepare(st, Dlb * wl, Dlk, Le, 1, (long long)Dlb * wl, 128,
                 bytes_reserve(c, s.Lp, split_operand_bytes(Dlb * wl, Dlk, 128)));
   // Rt as the B operand of Y = T2 . Rt: its columns (Drb) are the prepared rows
-  split_prepare(st, Drb, Drk * wr, Rt, (long long)Drk * wr, 1, s.p3.BN,
-                bytes_reserve(c, s.Rp, split_operand_bytes(Drb, Drk * wr, s.p3.BN)));
-  s.xbytes = split_operand_bytes(dd * Drk, Dlk, s.p1.BN);
-  s.tbytes = split_operand_bytes(Dlb * du, Drk * wr, 128);
-  long long part = 0;
-  if (s.p1.splits > 1) part = std::max(part, (long long)s.p1.splits * s.p1.M * s.p1.N);
-  if (s.p3.splits > 1) part = std::max(part, (long long)s.p3.splits * s.p3.M * s.p3.N);
-  s.partn = part;
-  split_matvec_reserve(c, s);
+  split_prepare(st, Drb, Drk * wr, Rt, (long long)Drk * wr, 1, 128,
+                bytes_reserve(c, s.Rp, split_operand_bytes(Drb, Drk * wr, 128)));
   s.ready = true;
-}
-
-void split_matvec_reserve(Context& c, const SplitMatvec& s) {
-  bytes_reserve(c, c.spX, s.xbytes);
-  bytes_reserve(c, c.spT, s.tbytes);
-  if (s.partn > 0) dbuf_reserve(c, c.spPart, s.partn);
 }
 
 // First contraction of the matvec: T2[a', s', r, c] = sum_{a,b,s} W[s',b,s,c]
@@ -556,108 +540,42 @@ void split_matvec_release(Context& c, SplitMatvec& s) {
 
 void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpoDev& m, int k,
                 bool adjoint, const cplx* Rt, const std::array<int, 3>& rd, const cplx* x, cplx* y,
-                cplx offset, Counters* cnt, const SplitMatvec* sp) {
+                cplx offset, Counters* cnt) {
   const auto& wd = m.dims[k];
   const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
   const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
   MPSGPU_CHECK(ld[1] == wl && rd[1] == wr, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
-  const bool split = sp && sp->ready;
-  if (!split) {
-    // FP64: steps 1 and 2 in one kernel (the MPO legs applied in the epilogue
-    // of L . X), step 3 with the offset in the epilogue
-    const cplx* Wm = adjoint ? m.Wlr_h[k].p : m.Wlr[k].p;
-    MPSGPU_CHECK(Wm != nullptr, MPSGPU_BAD_SHAPE, "heff: adjoint needs du == dd");
-    dbuf_reserve(c, c.t2, (long long)Dlb * du * Drk * wr);
-    Gemm1wBatch g1;
-    g1.n = 1;
-    g1.d[0] = heff_first_desc(Le, Dlb, Dlk, wl, x, dd, Drk, Wm, du, wr, c.t2.p);
-    heff_gemm1w(c.st(), g1);
-    Gemm3Batch g3;
-    g3.n = 1;
-    g3.d[0] = heff_last_desc(c.t2.p, Dlb * du, Rt, Drk * wr, Drb, y, x, offset);
-    heff_gemm3(c.st(), g3);
-    if (cnt) {
-      cnt->matvecs++;
-      cnt->flops += mv_flops(dd, wl, wr, Dlb, Drb);
-    }
-    return;
-  }
-  // split precision: step 1: T1[(a',b),(s,r)] = L((Dlb*wl) x Dlk) . X(Dlk x dd*Drk)
-  const long long n1 = (long long)Dlb * wl * dd * Drk;
-  dbuf_reserve(c, c.t1, n1);
-  GemmArgs g;
-  g.M = Dlb * wl; g.N = dd * Drk; g.K = Dlk;
-  g.A = Le; g.lda = (long long)Dlb * wl;
-  g.B = x; g.ldb = Dlk;
-  g.C = c.t1.p; g.ldc = (long long)Dlb * wl;
-  // the caller prepared sp from the same Le and Rt (the adjoint ones for adjoint)
-  {
-    // X as the B operand: its columns (dd*Drk) are the prepared rows
-    uint8_t* xp = reinterpret_cast<uint8_t*>(c.spX.p);
-    split_prepare(c.st(), dd * Drk, Dlk, x, Dlk, 1, sp->p1.BN, xp);
-    zgemm_split_prepared(c.st(), sp->p1, reinterpret_cast<const uint8_t*>(sp->Lp.p), xp, c.t1.p, g.ldc,
-                         make_double2(1.0, 0.0), nullptr, 0, make_double2(0.0, 0.0), c.spPart.p, c.dsplit_err);
-  }
-  // step 2: T2[a', s', r, c] = sum_{b,s} W[s',b,s,c] T1[a',b,s,r]
-  const long long n2 = (long long)Dlb * du * Drk * wr;
-  dbuf_reserve(c, c.t2, n2);
-  WContractArgs wa;
-  wa.nx = Dlb; wa.ny = Drk;
-  wa.in = c.t1.p; wa.ix = 1; wa.iy = (long long)Dlb * wl * dd; wa.si0 = Dlb; wa.si1 = (long long)Dlb * wl;
-  wa.n_i0 = wl; wa.n_i1 = dd;
-  wa.out = c.t2.p; wa.ox = 1; wa.oy = (long long)Dlb * du; wa.so0 = Dlb; wa.so1 = (long long)Dlb * du * Drk;
-  wa.n_o0 = du; wa.n_o1 = wr;
-  wa.Wm = adjoint ? m.Wlr_h[k].p : m.Wlr[k].p;
-  MPSGPU_CHECK(wa.Wm != nullptr, MPSGPU_BAD_SHAPE, "heff: adjoint needs du == dd");
-  wcontract(c.st(), wa);
-  // step 3: Y[(a',s'), r'] = T2((Dlb*du) x (Drk*wr)) . Rt((Drk*wr) x Drb) + offset X
-  GemmArgs h;
-  h.M = Dlb * du; h.N = Drb; h.K = Drk * wr;
-  h.A = c.t2.p; h.lda = (long long)Dlb * du;
-  h.B = Rt; h.ldb = (long long)Drk * wr;
-  h.C = y; h.ldc = (long long)Dlb * du;
-  if (offset.x != 0.0 || offset.y != 0.0) {
-    h.Cin = x; h.ldcin = (long long)Dlb * du; h.beta = offset;
-  }
-  {
-    uint8_t* tp = reinterpret_cast<uint8_t*>(c.spT.p);
-    split_prepare(c.st(), h.M, h.K, c.t2.p, 1, h.lda, 128, tp);
-    zgemm_split_prepared(c.st(), sp->p3, tp, reinterpret_cast<const uint8_t*>(sp->Rp.p), y, h.ldc,
-                         make_double2(1.0, 0.0), h.Cin, h.ldcin, h.beta, c.spPart.p, c.dsplit_err);
-  }
+  // steps 1 and 2 in one kernel (the MPO legs applied in the epilogue of
+  // L . X), step 3 with the offset in the epilogue
+  const cplx* Wm = adjoint ? m.Wlr_h[k].p : m.Wlr[k].p;
+  MPSGPU_CHECK(Wm != nullptr, MPSGPU_BAD_SHAPE, "heff: adjoint needs du == dd");
+  dbuf_reserve(c, c.t2, (long long)Dlb * du * Drk * wr);
+  Gemm1wBatch g1;
+  g1.n = 1;
+  g1.d[0] = heff_first_desc(Le, Dlb, Dlk, wl, x, dd, Drk, Wm, du, wr, c.t2.p);
+  heff_gemm1w(c.st(), g1);
+  Gemm3Batch g3;
+  g3.n = 1;
+  g3.d[0] = heff_last_desc(c.t2.p, Dlb * du, Rt, Drk * wr, Drb, y, x, offset);
+  heff_gemm3(c.st(), g3);
   if (cnt) {
     cnt->matvecs++;
-    cnt->split_matvecs++;
     cnt->flops += mv_flops(dd, wl, wr, Dlb, Drb);
   }
 }
 
 // Hermitian part of the effective Hamiltonian, TensorMultiplierHermitian
 // (TensorMultiplierHermitian.cpp:37-70): y = 1/2 (H x + H^dag x) + offset x,
-// with H^dag from the adjoint environments (Lh, Rth) and MPO legs.  FP64:
-// both first contractions in one grouped launch, the two last ones as one
-// product with the two sources concatenated along K.
+// with H^dag from the adjoint environments (Lh, Rth) and MPO legs: both
+// first contractions in one grouped launch, the two last ones as one product
+// with the two sources concatenated along K.
 void heff_apply_hermitian(Context& c, const cplx* Le, const cplx* Lh, const std::array<int, 3>& ld,
                           const MpoDev& m, int k, const cplx* Rt, const cplx* Rth, const std::array<int, 3>& rd,
-                          const cplx* x, cplx* y, cplx offset, Counters* cnt, const SplitMatvec* sp,
-                          const SplitMatvec* sph) {
+                          const cplx* x, cplx* y, cplx offset, Counters* cnt) {
   const auto& wd = m.dims[k];
   const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
   const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
   MPSGPU_CHECK(m.Wlr_h[k].p != nullptr, MPSGPU_BAD_SHAPE, "heff: adjoint needs du == dd");
-  if (sp && sp->ready) {
-    const long long N = (long long)Dlb * du * Drb;
-    dbuf_reserve(c, c.t4, N);
-    heff_apply(c, Le, ld, m, k, false, Rt, rd, x, y, make_double2(0.0, 0.0), cnt, sp);
-    heff_apply(c, Lh, ld, m, k, true, Rth, rd, x, c.t4.p, make_double2(0.0, 0.0), cnt, sph);
-    if (cnt) {
-      cnt->matvecs--;  // the pair counts as one product of the Hermitian multiplier
-      cnt->split_matvecs--;
-    }
-    zaxpby(c.st(), (int)N, make_double2(0.5, 0.0), c.t4.p, make_double2(0.5, 0.0), y);
-    if (offset.x != 0.0 || offset.y != 0.0) zaxpby(c.st(), (int)N, offset, x, make_double2(1.0, 0.0), y);
-    return;
-  }
   MPSGPU_CHECK(ld[1] == wl && rd[1] == wr, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
   const long long n2 = (long long)Dlb * du * Drk * wr;
   dbuf_reserve(c, c.t2, n2);
@@ -681,6 +599,133 @@ void heff_apply_hermitian(Context& c, const cplx* Le, const cplx* Lh, const std:
     cnt->matvecs++;
     cnt->flops += 2.0 * mv_flops(dd, wl, wr, Dlb, Drb);
   }
+}
+
+// Copies a descriptor blob into the next slot of the context's ring and
+// returns the slot's device address (the copy is ordered on c's stream before
+// the launches that read it).
+static uint8_t* desc_upload(Context& c, const std::vector<uint8_t>& blob) {
+  MPSGPU_CHECK(blob.size() <= kDescSlotBytes, MPSGPU_BAD_SHAPE, "grouped launch: descriptor tables too large");
+  const int s = c.desc_next;
+  c.desc_next = (s + 1) % kDescSlots;
+  MPSGPU_CUDA(cudaEventSynchronize(c.desc_ev[s]));  // the slot's previous copy has completed
+  uint8_t* h = c.hdesc + (size_t)s * kDescSlotBytes;
+  uint8_t* d = c.ddesc + (size_t)s * kDescSlotBytes;
+  std::memcpy(h, blob.data(), blob.size());
+  MPSGPU_CUDA(cudaMemcpyAsync(d, h, blob.size(), cudaMemcpyHostToDevice, c.stream));
+  MPSGPU_CUDA(cudaEventRecord(c.desc_ev[s], c.stream));
+  return d;
+}
+
+template <class T>
+static size_t blob_put(std::vector<uint8_t>& blob, const std::vector<T>& v) {
+  const size_t off = (blob.size() + 15) & ~size_t(15);
+  blob.resize(off + v.size() * sizeof(T));
+  if (!v.empty()) std::memcpy(blob.data() + off, v.data(), v.size() * sizeof(T));
+  return off;
+}
+
+void split_round_run(Context& c, SplitRound& r) {
+  const int n = (int)r.p.size();
+  if (n == 0) return;
+  const Stream st = c.st();
+  const int nsm = device_sms(c);
+  // K of the last products split into chunks of at least four k-steps, so
+  // that the round's tiles give about one CTA per SM (at most 8 chunks)
+  long long tiles3 = 0;
+  int ks3 = 1;
+  for (const SplitProduct& q : r.p) {
+    tiles3 += (long long)q.nh * ceil_div(q.Dlb * q.du, 128) * ceil_div(q.Drb, 128);
+    ks3 = std::max(ks3, ceil_div(q.Drk * q.wr, 16));
+  }
+  int S = (int)std::min<long long>(8, std::max<long long>(1, (nsm + tiles3 - 1) / std::max<long long>(1, tiles3)));
+  S = std::max(1, std::min(S, ks3 / 4));
+  std::vector<SplitPrepJob> jx, jt;
+  std::vector<SplitProblem> g1, g3;
+  std::vector<WGroup> wg;
+  std::vector<SplitReduceJob> red;
+  long long pix = 0;
+  int maxnin = 1;
+  double work = 0.0;
+  for (const SplitProduct& q : r.p) {
+    const int M1 = q.Dlb * q.wl, N1 = q.dd * q.Drk, K1 = q.Dlk;
+    const int M3 = q.Dlb * q.du, N3 = q.Drb, K3 = q.Drk * q.wr;
+    const long long n1 = (long long)M1 * N1, n2 = (long long)M3 * K3, n3 = (long long)M3 * N3;
+    const int KS3 = ceil_div(K3, 16), kps = ceil_div(KS3, S), nch = ceil_div(KS3, kps);
+    LzWork& w = *q.ws;
+    dbuf_reserve(c, w.s1, q.nh * n1);
+    dbuf_reserve(c, w.s2, q.nh * n2);
+    dbuf_reserve(c, w.spart, (long long)q.nh * nch * n3);
+    const long long xb = split_operand_bytes(N1, K1, 128), tb = split_operand_bytes(M3, K3, 128);
+    uint8_t* xp = bytes_reserve(c, w.sx, xb);
+    uint8_t* tp = bytes_reserve(c, w.st, q.nh * tb);
+    // x as the B operand of T1 = L . X: its columns (dd*Drk) are the prepared rows
+    jx.push_back(SplitPrepJob{N1, K1, 0, q.x, K1, 1, xp, 0});
+    for (int h = 0; h < q.nh; h++) {
+      MPSGPU_CHECK(q.sp[h] && q.sp[h]->ready && q.Wm[h], MPSGPU_INVALID, "split round: operands not prepared");
+      cplx* T1 = w.s1.p + h * n1;
+      cplx* T2 = w.s2.p + h * n2;
+      uint8_t* th = tp + h * tb;
+      SplitProblem a;
+      a.M = M1; a.N = N1; a.K = K1;
+      a.Ap = reinterpret_cast<const uint8_t*>(q.sp[h]->Lp.p);
+      a.Bp = xp;
+      a.C = T1; a.ldc = M1;
+      g1.push_back(a);
+      // T2[a', s', r, c] = sum_{b,s} W[s',b,s,c] T1[a',b,s,r]
+      WGroup W;
+      WContractArgs& wa = W.a;
+      wa.nx = q.Dlb; wa.ny = q.Drk;
+      wa.in = T1; wa.ix = 1; wa.iy = (long long)q.Dlb * q.wl * q.dd; wa.si0 = q.Dlb; wa.si1 = (long long)q.Dlb * q.wl;
+      wa.n_i0 = q.wl; wa.n_i1 = q.dd;
+      wa.out = T2; wa.ox = 1; wa.oy = (long long)q.Dlb * q.du; wa.so0 = q.Dlb; wa.so1 = (long long)q.Dlb * q.du * q.Drk;
+      wa.n_o0 = q.du; wa.n_o1 = q.wr;
+      wa.Wm = q.Wm[h];
+      W.pix_begin = pix;
+      pix += (long long)q.Dlb * q.Drk;
+      wg.push_back(W);
+      maxnin = std::max(maxnin, q.wl * q.dd);
+      // T2 ((Dlb du) x (Drk wr), column-major) as the A operand
+      jt.push_back(SplitPrepJob{M3, K3, 0, T2, 1, M3, th, 0});
+      for (int s = 0; s < nch; s++) {
+        SplitProblem b;
+        b.M = M3; b.N = N3; b.K = K3;
+        b.Ap = th;
+        b.Bp = reinterpret_cast<const uint8_t*>(q.sp[h]->Rp.p);
+        b.C = w.spart.p + (h * nch + s) * n3; b.ldc = M3;
+        b.k0 = s * kps;
+        b.nk = std::min(kps, KS3 - s * kps);
+        g3.push_back(b);
+      }
+      work += 48.0 * ((double)M1 * N1 * K1 + (double)M3 * N3 * K3);
+    }
+    SplitReduceJob rj;
+    rj.M = M3; rj.N = N3; rj.nparts = q.nh * nch;
+    rj.part = w.spart.p;
+    rj.C = q.y; rj.ldc = M3;
+    rj.alpha = q.alpha;
+    if (q.offset.x != 0.0 || q.offset.y != 0.0) {
+      rj.Cin = q.x; rj.ldcin = M3; rj.beta = q.offset;
+    }
+    red.push_back(rj);
+  }
+  const long long thr_x = split_prepare_jobs(jx.data(), (int)jx.size());
+  const long long t1 = split_group_tiles(g1.data(), (int)g1.size());
+  const long long thr_t = split_prepare_jobs(jt.data(), (int)jt.size());
+  const long long t3 = split_group_tiles(g3.data(), (int)g3.size());
+  const long long rtot = split_reduce_jobs(red.data(), (int)red.size());
+  std::vector<uint8_t> blob;
+  const size_t ox = blob_put(blob, jx), o1 = blob_put(blob, g1), ow = blob_put(blob, wg), ot = blob_put(blob, jt),
+               o3 = blob_put(blob, g3), orr = blob_put(blob, red);
+  uint8_t* d = desc_upload(c, blob);
+  ProfScope ps(st, GemmProfiler::SPLIT, work);
+  split_prepare_grouped(st, reinterpret_cast<const SplitPrepJob*>(d + ox), (int)jx.size(), thr_x);
+  zgemm_split_grouped(st, reinterpret_cast<const SplitProblem*>(d + o1), (int)g1.size(), t1, c.dsplit_err);
+  wcontract_grouped(st, reinterpret_cast<const WGroup*>(d + ow), (int)wg.size(), pix, maxnin);
+  split_prepare_grouped(st, reinterpret_cast<const SplitPrepJob*>(d + ot), (int)jt.size(), thr_t);
+  zgemm_split_grouped(st, reinterpret_cast<const SplitProblem*>(d + o3), (int)g3.size(), t3, c.dsplit_err);
+  split_reduce_grouped(st, reinterpret_cast<const SplitReduceJob*>(d + orr), (int)red.size(), rtot);
+  r.p.clear();
 }
 
 void env_left_update(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpsDev& ket,
@@ -952,18 +997,20 @@ void context_init(Context& c, int device) {
   MPSGPU_CUDA(cudaHostAlloc((void**)&c.hlz_err, sizeof(int), cudaHostAllocMapped));
   MPSGPU_CUDA(cudaHostGetDevicePointer((void**)&c.dlz_err, c.hlz_err, 0));
   *c.hlz_err = 0;
-  MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, 128 * sizeof(unsigned)));
-  MPSGPU_CUDA(cudaMemset(c.dcounter, 0, 128 * sizeof(unsigned)));
+  MPSGPU_CUDA(cudaMalloc((void**)&c.dcounter, kCounterWords * sizeof(unsigned)));
+  MPSGPU_CUDA(cudaMemset(c.dcounter, 0, kCounterWords * sizeof(unsigned)));
   c.iter_ev.resize(257);
   for (auto& e : c.iter_ev) MPSGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  MPSGPU_CUDA(cudaMallocHost((void**)&c.hdesc, kDescSlots * kDescSlotBytes));
+  MPSGPU_CUDA(cudaMalloc((void**)&c.ddesc, kDescSlots * kDescSlotBytes));
+  for (auto& e : c.desc_ev) MPSGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 }
 
 void context_release(Context& c) {
   cudaSetDevice(c.device);
   for (auto& sc : c.subs) context_release(*sc);
   c.subs.clear();
-  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lzws, &c.spX, &c.spT, &c.spPart})
-    dbuf_free(c, *b);
+  for (DBuf* b : {&c.t1, &c.t2, &c.t3, &c.t4, &c.matA, &c.matQ, &c.matR, &c.lzws}) dbuf_free(c, *b);
   c.scratch.release();
   c.qrws.release();
   c.lzone.release(c);
@@ -980,6 +1027,12 @@ void context_release(Context& c) {
   if (c.hsplit_err) cudaFreeHost(c.hsplit_err);
   if (c.hlz_err) cudaFreeHost(c.hlz_err);
   cudaFree(c.dcounter);
+  for (auto e : c.desc_ev)
+    if (e) cudaEventDestroy(e);
+  if (c.hdesc) cudaFreeHost(c.hdesc);
+  cudaFree(c.ddesc);
+  c.hdesc = nullptr;
+  c.ddesc = nullptr;
   if (c.stream) cudaStreamDestroy(c.stream);
   c.stream = nullptr;
 }
@@ -1003,7 +1056,7 @@ void LzWork::init(Context& c) {
 }
 
 void LzWork::release(Context& c) {
-  for (DBuf* b : {&V, &w, &t2, &t3, &T, &Q}) dbuf_free(c, *b);
+  for (DBuf* b : {&V, &w, &t2, &t3, &T, &Q, &s1, &s2, &spart, &sx, &st}) dbuf_free(c, *b);
   if (dsc) {
     cudaStreamSynchronize(c.stream);
     cudaFree(dsc);
@@ -1074,19 +1127,16 @@ void lanczos_batch(Context& c, std::vector<LzTask*>& tasks) {
   }
   // workspace of the step, shared by the instances of a launch: partial dots
   // (row blocks x 256), two partial-norm arrays, the coefficients h, h2
-  const long long hcap = 256LL * LZ_MAXI;
-  dbuf_reserve(c, c.lzws, nrb_total * 256 + 2 * hcap + nrb_total + LZ_MAXI + 8);
+  dbuf_reserve(c, c.lzws, 2 * nrb_total * 256 + nrb_total + 8);
   cplx* part = c.lzws.p;
-  cplx* hbuf = part + nrb_total * 256;
-  cplx* h2buf = hbuf + hcap;
-  double* pn1 = reinterpret_cast<double*>(h2buf + hcap);
+  cplx* part2 = part + nrb_total * 256;
+  double* pn1 = reinterpret_cast<double*>(part2 + nrb_total * 256);
   double* pn2 = pn1 + nrb_total;
-  double* nwbuf = pn2 + nrb_total;  // 2 * LZ_MAXI doubles
 
   auto check_step = [&]() {
     if (*c.hlz_err) {
       MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
-      MPSGPU_CUDA(cudaMemsetAsync(c.dcounter + 96, 0, 2 * sizeof(unsigned), c.stream));
+      MPSGPU_CUDA(cudaMemsetAsync(c.dcounter + kLzBarrierOffset, 0, 2 * LZ_MAXI * sizeof(unsigned), c.stream));
       MPSGPU_CUDA(cudaStreamSynchronize(c.stream));
       *c.hlz_err = 0;
       throw Error(MPSGPU_TIMEOUT, "lanczos: a bounded grid barrier of the Lanczos step ran out");
@@ -1097,30 +1147,28 @@ void lanczos_batch(Context& c, std::vector<LzTask*>& tasks) {
   std::vector<std::pair<int, int>> round;  // (task, iteration)
   auto launch_round = [&](const std::vector<std::pair<int, int>>& items, cudaEvent_t ev) {
     const auto t0 = clk::now();
-    Gemm1wBatch g1;
-    Gemm3Batch g3;
+    RoundBatch rb;
     auto flush = [&]() {
-      if (g1.n) heff_gemm1w(st, g1);
-      if (g3.n) heff_gemm3(st, g3);
-      g1.n = g3.n = 0;
+      if (rb.g1.n) heff_gemm1w(st, rb.g1);
+      if (rb.g3.n) heff_gemm3(st, rb.g3);
+      rb.g1.n = rb.g3.n = 0;
     };
     for (auto& it : items) {
       LzState& z = S[it.first];
       LzTask& t = *z.t;
-      if (g1.n + 2 > GEMM_MAXP || g3.n + 1 > GEMM_MAXP) flush();
-      t.product(c, t.ws->V.p + (long long)it.second * t.N, t.ws->w.p, z.sigma, g1, g3);
+      if (rb.g1.n + 2 > GEMM_MAXP || rb.g3.n + 1 > GEMM_MAXP) flush();
+      t.product(c, t.ws->V.p + (long long)it.second * t.N, t.ws->w.p, z.sigma, rb);
     }
     flush();
+    split_round_run(c, rb.sr);
     for (size_t i0 = 0; i0 < items.size(); i0 += LZ_MAXI) {
       LzBatch b;
       b.ninst = (int)std::min<size_t>(LZ_MAXI, items.size() - i0);
       b.part = part;
-      b.h = hbuf;
-      b.h2 = h2buf;
+      b.part2 = part2;
       b.pn1 = pn1;
       b.pn2 = pn2;
-      b.nw = nwbuf;
-      b.bar = c.dcounter + 96;
+      b.bar = c.dcounter + kLzBarrierOffset;
       b.err = c.dlz_err;
       for (int i = 0; i < b.ninst; i++) {
         LzState& z = S[items[i0 + i].first];
@@ -1318,9 +1366,7 @@ static double lanczos_lowest(Context& c, int N, Op apply, cplx* x, double tol, i
   t.max_krylov = max_krylov;
   t.ws = &ws;
   t.cnt = cnt;
-  t.product = [&](Context&, const cplx* xin, cplx* yout, double sigma, Gemm1wBatch&, Gemm3Batch&) {
-    apply(xin, yout, sigma);
-  };
+  t.product = [&](Context&, const cplx* xin, cplx* yout, double sigma, RoundBatch&) { apply(xin, yout, sigma); };
   std::vector<LzTask*> v{&t};
   lanczos_batch(c, v);
   if (iters) *iters = t.iters;
@@ -1595,22 +1641,31 @@ struct GsSweep {
     t.max_krylov = opt.max_krylov;
     t.ws = &ws;
     t.cnt = &cnt;
-    t.product = [this](Context& lc, const cplx* xin, cplx* yout, double sg, Gemm1wBatch& g1, Gemm3Batch& g3) {
+    t.product = [this](Context& lc, const cplx* xin, cplx* yout, double sg, RoundBatch& rb) {
       const cplx o = make_double2(offset - sg, 0.0);
-      if (split_phase && split_products) {
-        split_matvec_reserve(lc, smv);
-        heff_apply(lc, Le, ld, ops, pos, false, Rt, rd, xin, yout, o, &cnt, &smv);
-        return;
-      }
       const auto& wd = ops.dims[pos];
       const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
       const int Dlb = ld[0], Dlk = ld[2], Drk = rd[0], Drb = rd[2];
       MPSGPU_CHECK(ld[1] == wl && rd[1] == wr, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
-      dbuf_reserve(c, ws.t2, (long long)Dlb * du * Drk * wr);
-      g1.d[g1.n++] = heff_first_desc(Le, Dlb, Dlk, wl, xin, dd, Drk, ops.Wlr[pos].p, du, wr, ws.t2.p);
-      g3.d[g3.n++] = heff_last_desc(ws.t2.p, Dlb * du, Rt, Drk * wr, Drb, yout, xin, o);
       cnt.matvecs++;
       cnt.flops += mv_flops(dd, wl, wr, Dlb, Drb);
+      if (split_phase && split_products) {
+        SplitProduct p;
+        p.nh = 1;
+        p.sp[0] = &smv;
+        p.Wm[0] = ops.Wlr[pos].p;
+        p.Dlb = Dlb; p.Dlk = Dlk; p.wl = wl; p.dd = dd; p.Drk = Drk; p.du = du; p.wr = wr; p.Drb = Drb;
+        p.x = xin;
+        p.y = yout;
+        p.offset = o;
+        p.ws = &ws;
+        rb.sr.p.push_back(p);
+        cnt.split_matvecs++;
+        return;
+      }
+      dbuf_reserve(lc, ws.t2, (long long)Dlb * du * Drk * wr);
+      rb.g1.d[rb.g1.n++] = heff_first_desc(Le, Dlb, Dlk, wl, xin, dd, Drk, ops.Wlr[pos].p, du, wr, ws.t2.p);
+      rb.g3.d[rb.g3.n++] = heff_last_desc(ws.t2.p, Dlb * du, Rt, Drk * wr, Drb, yout, xin, o);
     };
   }
 
@@ -2108,23 +2163,36 @@ struct ExcSweep {
     t.cnt = &cnt;
     // 1/2 (H + H^dag) x + (offset - sigma) x; the projector term
     // sum_k pen_k u_k (u_k^H x) is added by the Lanczos step
-    t.product = [this](Context& lc, const cplx* xin, cplx* yout, double sg, Gemm1wBatch& g1, Gemm3Batch& g3) {
+    t.product = [this](Context& lc, const cplx* xin, cplx* yout, double sg, RoundBatch& rb) {
       const cplx o = make_double2(offset - sg, 0.0);
-      if (split_phase && split_products) {
-        split_matvec_reserve(lc, smv);
-        split_matvec_reserve(lc, smvh);
-        heff_apply_hermitian(lc, Le, Lh.p, ld, ops, pos, Rt, Rth.p, rd, xin, yout, o, &cnt, &smv, &smvh);
-        return;
-      }
       const auto& wd = ops.dims[pos];
       const int du = wd[0], wl = wd[1], dd = wd[2], wr = wd[3];
       const int Dlb = ld[0], Dlk_ = ld[2], Drk_ = rd[0], Drb = rd[2];
       MPSGPU_CHECK(ld[1] == wl && rd[1] == wr && ops.Wlr_h[pos].p, MPSGPU_BAD_SHAPE, "heff: MPO bond mismatch");
+      cnt.matvecs++;
+      cnt.flops += 2.0 * mv_flops(dd, wl, wr, Dlb, Drb);
+      if (split_phase && split_products) {
+        SplitProduct p;
+        p.nh = 2;
+        p.sp[0] = &smv;
+        p.sp[1] = &smvh;
+        p.Wm[0] = ops.Wlr[pos].p;
+        p.Wm[1] = ops.Wlr_h[pos].p;
+        p.Dlb = Dlb; p.Dlk = Dlk_; p.wl = wl; p.dd = dd; p.Drk = Drk_; p.du = du; p.wr = wr; p.Drb = Drb;
+        p.x = xin;
+        p.y = yout;
+        p.alpha = make_double2(0.5, 0.0);
+        p.offset = o;
+        p.ws = &ws;
+        rb.sr.p.push_back(p);
+        cnt.split_matvecs++;
+        return;
+      }
       const long long n2 = (long long)Dlb * du * Drk_ * wr;
-      dbuf_reserve(c, ws.t2, n2);
-      dbuf_reserve(c, ws.t3, n2);
-      g1.d[g1.n++] = heff_first_desc(Le, Dlb, Dlk_, wl, xin, dd, Drk_, ops.Wlr[pos].p, du, wr, ws.t2.p);
-      g1.d[g1.n++] = heff_first_desc(Lh.p, Dlb, Dlk_, wl, xin, dd, Drk_, ops.Wlr_h[pos].p, du, wr, ws.t3.p);
+      dbuf_reserve(lc, ws.t2, n2);
+      dbuf_reserve(lc, ws.t3, n2);
+      rb.g1.d[rb.g1.n++] = heff_first_desc(Le, Dlb, Dlk_, wl, xin, dd, Drk_, ops.Wlr[pos].p, du, wr, ws.t2.p);
+      rb.g1.d[rb.g1.n++] = heff_first_desc(Lh.p, Dlb, Dlk_, wl, xin, dd, Drk_, ops.Wlr_h[pos].p, du, wr, ws.t3.p);
       Gemm3Desc h = heff_last_desc(ws.t2.p, Dlb * du, Rt, Drk_ * wr, Drb, yout, xin, o);
       h.K2 = Drk_ * wr;
       h.A2 = ws.t3.p;
@@ -2132,9 +2200,7 @@ struct ExcSweep {
       h.B2 = Rth.p;
       h.ldb2 = (long long)Drk_ * wr;
       h.alpha = make_double2(0.5, 0.0);
-      g3.d[g3.n++] = h;
-      cnt.matvecs++;
-      cnt.flops += 2.0 * mv_flops(dd, wl, wr, Dlb, Drb);
+      rb.g3.d[rb.g3.n++] = h;
     };
   }
 

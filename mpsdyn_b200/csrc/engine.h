@@ -21,6 +21,14 @@ struct DBuf {
   long long cap = 0;  // complex elements
 };
 
+// Device words of a context (zero at rest): one barrier pair per instance of
+// a Lanczos-step launch, from kLzBarrierOffset.
+constexpr int kLzBarrierOffset = 0;
+constexpr int kCounterWords = 2 * LZ_MAXI;
+// Descriptor ring of a context: slots of kDescSlotBytes.
+constexpr int kDescSlots = 8;
+constexpr size_t kDescSlotBytes = 64 * 1024;
+
 struct Context;
 
 void dbuf_reserve(Context& c, DBuf& b, long long n);
@@ -32,6 +40,7 @@ void dbuf_free(Context& c, DBuf& b);
 // host mirror the step writes through its mapping).
 struct LzWork {
   DBuf V, w, t2, t3, T, Q;
+  DBuf s1, s2, spart, sx, st;  // split-precision products: T1, T2, partials (FP64); x, T2 planes (bytes)
   LanczosScalars* dsc = nullptr;
   LanczosScalars* hsc = nullptr;
   LanczosScalars* hsc_dev = nullptr;
@@ -73,15 +82,20 @@ struct Context {
   LzWork lzone;        // eigensolver workspace of single solves
   int* hlz_err = nullptr;  // pinned, mapped: set when a grid barrier of the Lanczos step ran out
   int* dlz_err = nullptr;  // its device address
-  // split-precision matvec: prepared x and T2 (BF16 limb planes) and split-K partials
-  DBuf spX, spT, spPart;
+  // descriptor tables of grouped launches: a ring of pinned host slots copied
+  // to device slots in stream order (a slot is rewritten only after its copy
+  // has completed, and on the device only by a later copy on the same stream)
+  uint8_t* hdesc = nullptr;
+  uint8_t* ddesc = nullptr;
+  cudaEvent_t desc_ev[kDescSlots] = {};
+  int desc_next = 0;
   int* hsplit_err = nullptr;   // pinned, mapped: set by a tensor-core kernel whose bounded wait ran out
   int* dsplit_err = nullptr;   // its device address
   double* dscal = nullptr;     // device scalars (alpha, beta, norms)
   cplx* dcplx = nullptr;       // device complex scalars (dots)
   double* hscal = nullptr;     // pinned host mirror
   cplx* hcplx = nullptr;
-  unsigned* dcounter = nullptr;   // last-block ticket of the fused reductions
+  unsigned* dcounter = nullptr;   // kCounterWords device words: the Lanczos step's barrier pairs
   std::vector<cudaEvent_t> iter_ev;  // one per Lanczos iteration in flight
   cudaEvent_t ev = nullptr;
   cudaEvent_t mv0 = nullptr, mv1 = nullptr;
@@ -169,28 +183,51 @@ void mps_increase_bond(Context& c, MpsDev& s, int D);
 
 // y = Heff x (+ offset x); environments in device layout.
 // Operands of one site's effective Hamiltonian prepared for the split-precision
-// products (BF16 limb planes of L and Rt, made once per site solve).
+// products: BF16 limb planes of L (rows Dlb*wl, inner Dlk) and Rt (rows Drb,
+// inner Drk*wr), both with 128-row tiles, made once per site solve.
 struct SplitMatvec {
-  SplitPlan p1, p3;  // T1 = L . X and Y = T2 . Rt
-  DBuf Lp, Rp;       // prepared L and Rt (the per-product X and T2 planes live in the Context)
-  long long xbytes = 0, tbytes = 0, partn = 0;  // sizes of the per-product planes and K-split partials
+  DBuf Lp, Rp;
   bool ready = false;
 };
-// Reserves the per-product split buffers on the context that runs the products.
-void split_matvec_reserve(Context& c, const SplitMatvec& s);
 void split_matvec_prepare(Context& c, SplitMatvec& s, const cplx* Le, const std::array<int, 3>& ld,
                           const MpoDev& m, int k, const cplx* Rt, const std::array<int, 3>& rd);
 void split_matvec_release(Context& c, SplitMatvec& s);
-// y = Heff x + offset x; in split precision when sp is non-null and ready.
+// y = Heff x + offset x in FP64.
 void heff_apply(Context& c, const cplx* Le, const std::array<int, 3>& ld, const MpoDev& m, int k,
                 bool adjoint, const cplx* Rt, const std::array<int, 3>& rd, const cplx* x,
-                cplx* y, cplx offset, Counters* cnt, const SplitMatvec* sp = nullptr);
-// y = 1/2 (H x + H^dag x) + offset x (TensorMultiplierHermitian); Lh, Rth the
-// adjoint environments; sp/sph the split operands of both halves, or null.
+                cplx* y, cplx offset, Counters* cnt);
+// y = 1/2 (H x + H^dag x) + offset x (TensorMultiplierHermitian) in FP64; Lh,
+// Rth the adjoint environments.
 void heff_apply_hermitian(Context& c, const cplx* Le, const cplx* Lh, const std::array<int, 3>& ld,
                           const MpoDev& m, int k, const cplx* Rt, const cplx* Rth, const std::array<int, 3>& rd,
-                          const cplx* x, cplx* y, cplx offset, Counters* cnt, const SplitMatvec* sp = nullptr,
-                          const SplitMatvec* sph = nullptr);
+                          const cplx* x, cplx* y, cplx offset, Counters* cnt);
+// Split-precision products of one lockstep round, run together: for every
+// product y = alpha sum_h L_h W_h R_h x + offset x over its one half (the
+// plain multiplier, alpha = 1) or two (H and H^dag, alpha = 1/2), as six
+// grouped launches for all of them (x planes, T1 = L X on tcgen05, MPO legs,
+// T2 planes, T2 Rt on tcgen05 with K split into partial products, and the
+// sum of the partials with the offset term).
+struct SplitProduct {
+  int nh = 1;
+  const SplitMatvec* sp[2] = {nullptr, nullptr};
+  const cplx* Wm[2] = {nullptr, nullptr};  // MPO leg matrices (du*wr) x (wl*dd)
+  int Dlb = 0, Dlk = 0, wl = 0, dd = 0, Drk = 0, du = 0, wr = 0, Drb = 0;
+  const cplx* x = nullptr;
+  cplx* y = nullptr;
+  cplx alpha = {1.0, 0.0}, offset = {0.0, 0.0};
+  LzWork* ws = nullptr;  // the product's intermediates
+};
+struct SplitRound {
+  std::vector<SplitProduct> p;
+};
+// Enqueues the round's products on c's stream and empties the round.
+void split_round_run(Context& c, SplitRound& r);
+// The grouped launches of one Lanczos round that products append to.
+struct RoundBatch {
+  Gemm1wBatch g1;
+  Gemm3Batch g3;
+  SplitRound sr;
+};
 // Descriptors of the two FP64 contractions of one product (heff.cu).
 Gemm1wDesc heff_first_desc(const cplx* Le, int Dlb, int Dlk, int wl, const cplx* x, int dd, int Drk, const cplx* Wm,
                            int du, int wr, cplx* t2);
@@ -211,11 +248,11 @@ void mpo_save_file(Context& c, const MpoDev& m, const std::string& fn);
 void mpo_load_file(Context& c, const std::string& fn, MpoDev& m);
 
 // ---- local eigensolver (batched thick-restart Lanczos) ----
-// One local problem: product(lc, x, y, sigma, g1, g3) must make
-// y = (H - sigma) x appear on the stream of lc (the context running the
-// rounds), either by appending FP64 descriptors to the grouped launches
-// g1/g3 (launched by the caller in the same round) or by launching its own
-// kernels on lc.
+// One local problem: product(lc, x, y, sigma, rb) must make y = (H - sigma) x
+// appear on the stream of lc (the context running the rounds), either by
+// appending to the round's grouped launches rb (FP64 descriptors of the two
+// contractions, or a split-precision product; the caller launches them in
+// the same round) or by launching its own kernels on lc.
 struct LzTask {
   int N = 0;
   cplx* x = nullptr;  // start vector in, normalised eigenvector out
@@ -223,7 +260,7 @@ struct LzTask {
   const cplx* U = nullptr;  // projector vectors (N x nu), sqrt(penalty) folded in
   int nu = 0;
   int max_krylov = 64;
-  std::function<void(Context&, const cplx*, cplx*, double, Gemm1wBatch&, Gemm3Batch&)> product;
+  std::function<void(Context&, const cplx*, cplx*, double, RoundBatch&)> product;
   LzWork* ws = nullptr;
   Counters* cnt = nullptr;
   double theta = 0.0;  // out: lowest Ritz value

@@ -16,11 +16,6 @@ namespace mpsgpu {
 
 namespace {
 
-struct WGroup {
-  WContractArgs a;
-  long long pix_begin;
-};
-
 // Wm[(s' + du*c) + (du*wr)*(b + wl*s)] = W[s' + du*(b + wl*(s + dd*c))] for every instance
 struct WPerm {
   const cplx* W;
@@ -81,6 +76,16 @@ __global__ void wcontract_grouped_kernel(const WGroup* __restrict__ g, int n, lo
 }
 
 }  // namespace
+
+void wcontract_grouped(const Stream& st, const WGroup* d_wg, int n, long long pixels, int maxnin) {
+  MPSGPU_CHECK(maxnin >= 1 && maxnin <= 32, MPSGPU_BAD_SHAPE, "wcontract_grouped: MPO legs too wide");
+  if (pixels <= 0) return;
+  const int g = (int)std::min<long long>((pixels + 127) / 128, 148LL * 16);
+  if (maxnin <= 8) wcontract_grouped_kernel<8><<<g, 128, 0, st.s>>>(d_wg, n, pixels);
+  else if (maxnin <= 16) wcontract_grouped_kernel<16><<<g, 128, 0, st.s>>>(d_wg, n, pixels);
+  else wcontract_grouped_kernel<32><<<g, 128, 0, st.s>>>(d_wg, n, pixels);
+  after_launch(st);
+}
 
 GroupedMatvecPlan::~GroupedMatvecPlan() {}
 
@@ -240,11 +245,7 @@ void grouped_matvec_run(const Stream& st, GroupedMatvecPlan& plan) {
   } else {
     zgemm_grouped(st, plan.d_g1, plan.n, plan.tiles1, plan.ctas);
   }
-  const int g = (int)std::min<long long>(ceil_div(plan.pixels, 128), 148LL * 16);
-  if (plan.maxnin <= 8) wcontract_grouped_kernel<8><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
-  else if (plan.maxnin <= 16) wcontract_grouped_kernel<16><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
-  else wcontract_grouped_kernel<32><<<g, 128, 0, st.s>>>((const WGroup*)plan.d_wg, plan.n, plan.pixels);
-  after_launch(st);
+  wcontract_grouped(st, (const WGroup*)plan.d_wg, plan.n, plan.pixels, plan.maxnin);
   if (plan.split) {
     split_prepare_grouped(st, plan.d_jt, plan.n, plan.thr_t);
     zgemm_split_grouped(st, plan.d_s3, plan.n, plan.stiles3, plan.err);

@@ -385,7 +385,10 @@ int sm_count() {
 void heff_gemm1w(const Stream& st, Gemm1wBatch& b) {
   MPSGPU_CHECK(b.n >= 1 && b.n <= GEMM_MAXP, MPSGPU_BAD_SHAPE, "gemm1w: group size");
   heff_setup();
-  // tile rows: 64 when the group already fills the GPU, else 32 (twice the CTAs)
+  // tile rows: 32 (two warp groups splitting the k steps, twice the warps per
+  // SM), measured faster for the grouped products of lockstep batches of 8
+  // chains at D = 128 as well as for one chain; 64 only for groups that fill
+  // the GPU many times over
   long long t64 = 0;
   for (int q = 0; q < b.n; q++) {
     const Gemm1wDesc& d = b.d[q];
@@ -393,7 +396,7 @@ void heff_gemm1w(const Stream& st, Gemm1wBatch& b) {
                  MPSGPU_BAD_SHAPE, "gemm1w: leg dimensions");
     t64 += (long long)ceil_div(d.X, 64 / d.n_i0) * ceil_div(d.Y, 32 / d.n_i1);
   }
-  const int bm = t64 >= sm_count() ? 64 : 32;
+  const int bm = t64 >= 16LL * sm_count() ? 64 : 32;
   int tiles = 0;
   for (int q = 0; q < b.n; q++) {
     Gemm1wDesc& d = b.d[q];

@@ -89,7 +89,9 @@ void zgemm_split_prepared(const Stream& st, const SplitPlan& pl, const uint8_t* 
                           int* err);
 // Grouped form: every operand prepared with 128-row tiles (split_prepare
 // with RT = 128, or the grouped preparation below); one launch computes all
-// C_q = A_q B_q (M_q x N_q, inner K_q), one CTA per 128 x 128 tile.
+// C_q = A_q B_q (M_q x N_q, inner K_q), one CTA per 128 x 128 tile.  A
+// problem may cover a range of k-steps only (k0, nk; nk = 0: to the end), so
+// that a K split is a set of problems writing separate partial products.
 struct SplitProblem {
   int M = 0, N = 0, K = 0;
   int KS = 0, mtiles = 0;  // filled by split_group_tiles
@@ -98,9 +100,26 @@ struct SplitProblem {
   cplx* C = nullptr;
   long long ldc = 0;
   long long tile_begin = 0;
+  int k0 = 0, nk = 0;  // k-steps [k0, k0 + nk) of the KS (of 16) the operands hold
 };
 long long split_group_tiles(SplitProblem* probs, int n);
 void zgemm_split_grouped(const Stream& st, const SplitProblem* d_probs, int n, long long tiles, int* err);
+// Sum of partial products: C[m + n ldc] = alpha sum_{s < nparts} part[s M N + m + n M]
+// + beta Cin[m + n ldcin] for every job, one launch (elements numbered from
+// `begin`, filled by split_reduce_jobs).
+struct SplitReduceJob {
+  int M = 0, N = 0, nparts = 0;
+  const cplx* part = nullptr;
+  cplx* C = nullptr;
+  long long ldc = 0;
+  cplx alpha = {1.0, 0.0};
+  const cplx* Cin = nullptr;
+  long long ldcin = 0;
+  cplx beta = {0.0, 0.0};
+  long long begin = 0;
+};
+long long split_reduce_jobs(SplitReduceJob* jobs, int n);
+void split_reduce_grouped(const Stream& st, const SplitReduceJob* d_jobs, int n, long long total);
 // One preparation job per operand (rows x K, entry (r, k) at X[r*rs + k*ks]).
 struct SplitPrepJob {
   int rows = 0, K = 0;
@@ -177,6 +196,14 @@ struct WContractArgs {
   const cplx* Wm = nullptr;
 };
 void wcontract(const Stream& st, const WContractArgs& a);
+// The MPO-leg contraction of n problems in one launch (grouped.cu): problem
+// q covers the pixels [pix_begin_q, pix_begin_{q+1}) of `pixels`; maxnin is
+// the largest n_i0 * n_i1 (at most 32).
+struct WGroup {
+  WContractArgs a;
+  long long pix_begin;
+};
+void wcontract_grouped(const Stream& st, const WGroup* d_wg, int n, long long pixels, int maxnin);
 
 // ---- effective-Hamiltonian contractions (heff.cu), grouped ----
 constexpr int GEMM_MAXP = 16;  // problems per launch
@@ -249,14 +276,16 @@ struct LanczosScalars {
 // entry; on exit sc->alpha[j], sc->beta[j] (and the mirror) are set and, when
 // write_next, V[:, j+1] = w / beta_j.  With nu > 0, U (n x nu, ld n) holds the
 // projector vectors (sqrt of the penalty folded in) and w += U (U^H v_j)
-// first.  Workspaces: part nrb_total x 256 complex, pn1/pn2 nrb_total, h/h2
-// ninst x 256; bar two unsigned words that are zero at rest.
+// first.  Workspaces: part and part2 nrb_total x 256 complex, pn1/pn2
+// nrb_total; bar 2 x LZ_MAXI unsigned words that are zero at rest (one pair
+// per instance).
 constexpr int LZ_THREADS = 256;
 constexpr int LZ_MAXI = 16;  // instances per launch
 constexpr int LZ_MAXU = 8;   // projector vectors per instance
 struct LzInst {
   int n = 0, j = 0, k = 0, nu = 0, write_next = 0;
-  int rb0 = 0, nrb = 0;  // row blocks, filled by lanczos_step
+  int rb0 = 0, nrb = 0;     // row blocks, filled by lanczos_step
+  int cta0 = 0, ncta = 0;   // the instance's CTAs, filled by lanczos_step
   double sigma = 0.0;
   cplx* V = nullptr;
   long long ldv = 0;
@@ -269,13 +298,11 @@ struct LzBatch {
   int ninst = 0, nrb_total = 0;
   LzInst in[LZ_MAXI];
   cplx* part = nullptr;
+  cplx* part2 = nullptr;
   double* pn1 = nullptr;
   double* pn2 = nullptr;
-  cplx* h = nullptr;
-  cplx* h2 = nullptr;
-  double* nw = nullptr;  // 2 x LZ_MAXI: summed partial norms of the two passes
   unsigned* bar = nullptr;
-  int* err = nullptr;  // set when a bounded grid barrier ran out
+  int* err = nullptr;  // set when a bounded barrier ran out
 };
 // Rows per row block (the unit of the workspaces' nrb counts).
 int lanczos_step_rows_per_block();

@@ -12,17 +12,20 @@
 //   alpha_j = sigma + Re(h_j + h2_j), beta_j = |w|, V[:, j+1] = w / beta_j.
 // Without a second pass |w''|^2 = |w'|^2 - |h|^2 (V orthonormal; the test
 // bounds the cancellation to a factor 2), so beta_j is known before the
-// update and the update writes v_{j+1} directly: two grid barriers per
-// step.  After a second pass the norm is summed explicitly.
+// update and the update writes v_{j+1} directly.
 //
-// Rows of all instances are cut into row blocks of 256 (one per thread);
-// blocks are taken in grid-stride order by a grid that is resident all at
-// once (cooperative launch).  Partial sums per row block go to global
-// memory and are reduced in a fixed order, so the results are identical
-// from run to run and do not depend on the other instances of the group.
-// Grid barriers are bounded: a CTA that waits longer than 2 s sets the
-// error word and returns (the host reports MPSGPU_TIMEOUT and resets the
-// barrier words); the kernel has no copies in flight at any barrier.
+// Work split: the rows of an instance are cut into row blocks of 256 (one
+// row per thread), and every instance owns its own set of CTAs, which take
+// its row blocks in strided order.  Partial sums per row block go to global
+// memory; after a barrier among the instance's CTAs every one of them sums
+// the partials of the instance itself, in the same fixed order, so all of
+// them hold the same coefficients and reach the same second-pass decision
+// without a second barrier.  An unflagged step therefore costs one barrier
+// among the instance's CTAs; the results are identical from run to run and do
+// not depend on the other instances of the group or on the CTA count.
+// Barriers are bounded: a CTA that waits longer than 2 s sets the error word
+// and returns (the host reports MPSGPU_TIMEOUT and resets the barrier words);
+// the kernel has no copies in flight at any barrier.
 #include <cooperative_groups.h>
 
 #include "common.cuh"
@@ -44,10 +47,10 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 
-// Bounded grid barrier over gridDim.x co-resident CTAs: bar[0] counts the
-// arrivals, bar[1] is the generation the last arrival advances.  Returns
+// Bounded barrier over the n co-resident CTAs of one instance: bar[0] counts
+// the arrivals, bar[1] is the generation the last arrival advances.  Returns
 // false (and sets *err) when the wait ran out.
-__device__ bool grid_barrier(unsigned* bar, int* err) {
+__device__ bool group_barrier(unsigned* bar, unsigned n, int* err) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -55,7 +58,7 @@ __device__ bool grid_barrier(unsigned* bar, int* err) {
     volatile unsigned* gen = bar + 1;
     const unsigned g = *gen;
     __threadfence();
-    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+    if (atomicAdd(bar, 1u) == n - 1) {
       atomicExch(bar, 0u);
       __threadfence();
       atomicAdd(bar + 1, 1u);
@@ -117,13 +120,6 @@ __device__ __forceinline__ int sum16_vector_of_lane(int lane) {
   return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
 }
 
-// instance owning global row block rb (instances hold consecutive ranges)
-__device__ __forceinline__ int inst_of(const LzBatch& b, int rb) {
-  int q = 0;
-  while (q + 1 < b.ninst && b.in[q + 1].rb0 <= rb) q++;
-  return q;
-}
-
 // Partial dots over the rows [r0, r0 + RB) of an n-row instance:
 // part[rb * KMAXS + l] = sum_rows conj(V[:, l]) x for l < k (V with leading
 // dimension ldv), and the partial |x|^2 into pn[rb] when pn is non-null.
@@ -167,12 +163,12 @@ __device__ void block_dots(const cplx* __restrict__ V, long long ldv, long long 
   __syncthreads();
 }
 
-// x -= V h over the rows of row block rb (h in shared memory, k entries);
-// partial |x|^2 into pn[rb].  Sixteen loads of V in flight per thread.
-__device__ void block_update(const LzInst& in, int rb, cplx* __restrict__ x, const cplx* hs, int k, double* pn,
+// x -= V h over row block r of the instance (h in shared memory, k entries);
+// partial |x|^2 into pn[rb0 + r].  Sixteen loads of V in flight per thread.
+__device__ void block_update(const LzInst& in, int r, cplx* __restrict__ x, const cplx* hs, int k, double* pn,
                              double* redn) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long long i = (long long)(rb - in.rb0) * RB + tid;
+  const long long i = (long long)r * RB + tid;
   double s2 = 0.0;
   if (i < in.n) {
     cplx a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
@@ -200,61 +196,17 @@ __device__ void block_update(const LzInst& in, int rb, cplx* __restrict__ x, con
   if (tid == 0) {
     double s = 0.0;
     for (int q = 0; q < NW; q++) s += redn[q];
-    pn[rb] = s;
+    pn[in.rb0 + r] = s;
   }
   __syncthreads();
 }
 
-// h[q][l] = sum over the row blocks of q of part[rb][l], one warp per (q, l),
-// for the instances selected by `sel` (bit q); further warps sum the
-// partial norms pn over the row blocks of every selected instance into
-// nw[q].  Fixed order throughout.
-__device__ void reduce_pairs(const LzBatch& b, const cplx* part, cplx* h, unsigned sel, const double* pn,
-                             double* nw) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int npairs = 0;
-  for (int q = 0; q < b.ninst; q++) npairs += b.in[q].k;
-  for (int p = blockIdx.x * NW + warp; p < npairs + b.ninst; p += gridDim.x * NW) {
-    if (p >= npairs) {
-      const int q = p - npairs;
-      if (!((sel >> q) & 1u)) continue;
-      const LzInst& in = b.in[q];
-      double s = 0.0;
-      for (int r = lane; r < in.nrb; r += 32) s += __ldcg(&pn[in.rb0 + r]);
-      s = warp_sumd(s);
-      if (lane == 0) nw[q] = s;
-      continue;
-    }
-    int q = 0, rem = p;
-    while (rem >= b.in[q].k) rem -= b.in[q].k, q++;
-    if (!((sel >> q) & 1u)) continue;
-    const LzInst& in = b.in[q];
-    cplx s = make_double2(0.0, 0.0);
-    for (int r = lane; r < in.nrb; r += 32) s = cadd(s, __ldcg(&part[(long long)(in.rb0 + r) * KMAXS + rem]));
-    s = warp_sumc(s);
-    if (lane == 0) h[q * KMAXS + rem] = s;
-  }
-}
-
-// |h[q]|^2 for every instance, one warp per instance, into hh (shared);
-// every CTA gets the same values.
-__device__ void coefficient_norms(const LzBatch& b, const cplx* h, double* hh) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int q = warp; q < b.ninst; q += NW) {
-    double s = 0.0;
-    for (int l = lane; l < b.in[q].k; l += 32) s += cabs2(__ldcg(&h[q * KMAXS + l]));
-    s = warp_sumd(s);
-    if (lane == 0) hh[q] = s;
-  }
-  __syncthreads();
-}
-
-// x -= V h over the rows of row block rb, then V[:, j+1] = x / beta (or x
-// itself stored back into w when the basis is full: the residual the
-// restart needs).  No reduction.
-__device__ void block_update_final(const LzInst& in, int rb, const cplx* hs, int k, double inv_beta) {
+// x -= V h over row block r, then V[:, j+1] = x / beta (or x itself stored
+// back into w when the basis is full: the residual the restart needs).  No
+// reduction.
+__device__ void block_update_final(const LzInst& in, int r, const cplx* hs, int k, double inv_beta) {
   const int tid = threadIdx.x;
-  const long long i = (long long)(rb - in.rb0) * RB + tid;
+  const long long i = (long long)r * RB + tid;
   if (i < in.n) {
     cplx a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
     const cplx* v = in.V + i;
@@ -277,8 +229,23 @@ __device__ void block_update_final(const LzInst& in, int rb, const cplx* hs, int
   }
 }
 
-// sum over the row blocks of instance q of pn (fixed order; every CTA gets
-// the same value)
+// out[l] = sum over the instance's nrb row blocks of part[r * KMAXS + l],
+// l < k: one warp per coefficient, lanes over the row blocks, then the warp
+// butterfly -- a fixed order, so every CTA of the instance gets the same
+// values.  Every thread of the block calls it; out is read after a barrier.
+__device__ void reduce_coeffs(const cplx* __restrict__ part, int nrb, int k, cplx* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int l = warp; l < k; l += NW) {
+    cplx s = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int r = lane; r < nrb; r += 32) s = cadd(s, __ldcg(&part[(long long)r * KMAXS + l]));
+    s = warp_sumc(s);
+    if (lane == 0) out[l] = s;
+  }
+}
+
+// sum over the row blocks of the instance of pn (fixed order; every thread
+// of every CTA gets the same value)
 __device__ double sum_norms(const LzInst& in, const double* pn, double* redn) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double s = 0.0;
@@ -293,151 +260,117 @@ __device__ double sum_norms(const LzInst& in, const double* pn, double* redn) {
   return t;
 }
 
+// sum_l |h_l|^2 over l < k in a fixed order (every thread gets the value)
+__device__ double coeff_norm(const cplx* hs, int k, double* redn) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (warp == 0) {
+    double s = 0.0;
+    for (int l = lane; l < k; l += 32) s += cabs2(hs[l]);
+    s = warp_sumd(s);
+    if (lane == 0) redn[0] = s;
+  }
+  __syncthreads();
+  const double v = redn[0];
+  __syncthreads();
+  return v;
+}
+
 __global__ void __launch_bounds__(T) lanczos_step_kernel(const __grid_constant__ LzBatch b) {
   __shared__ cplx red[NW][KMAXS];
   __shared__ double redn[NW];
   __shared__ cplx hs[KMAXS];
+  __shared__ cplx hs2[KMAXS];
   __shared__ cplx ucs[LZ_MAXU];
-  __shared__ unsigned flagged;
   const int tid = threadIdx.x;
+  // the instance this CTA serves (instances own consecutive CTA ranges)
+  int q = 0;
+  while (q + 1 < b.ninst && b.in[q + 1].cta0 <= (int)blockIdx.x) q++;
+  const LzInst& in = b.in[q];
+  const int rank = (int)blockIdx.x - in.cta0;
+  if (rank < 0 || rank >= in.ncta) return;
+  unsigned* bar = b.bar + 2 * q;
+  const unsigned nct = (unsigned)in.ncta;
 
   // ---- projector (excited states): c = U^H v_j, then w += U c ----
-  bool any_proj = false;
-  for (int q = 0; q < b.ninst; q++) any_proj |= b.in[q].nu > 0;
-  if (any_proj) {
-    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
-      const int q = inst_of(b, rb);
-      const LzInst& in = b.in[q];
-      if (in.nu == 0) continue;
-      // dots of the U columns with v_j
-      block_dots(in.U, in.n, in.n, (long long)(rb - in.rb0) * RB, rb, in.V + (long long)in.j * in.ldv, in.nu,
-                 b.part, nullptr, red, redn);
-    }
-    if (!grid_barrier(b.bar, b.err)) return;
-    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
-      const int q = inst_of(b, rb);
-      const LzInst& in = b.in[q];
-      if (in.nu == 0) continue;
-      // every CTA reduces the (few) coefficients of its instance itself
-      if (tid < 32) {
-        for (int t = 0; t < in.nu; t++) {
-          cplx s = make_double2(0.0, 0.0);
-          for (int r = tid; r < in.nrb; r += 32) s = cadd(s, __ldcg(&b.part[(long long)(in.rb0 + r) * KMAXS + t]));
-          s = warp_sumc(s);
-          if (tid == 0) ucs[t] = s;
-        }
+  if (in.nu > 0) {
+    for (int r = rank; r < in.nrb; r += in.ncta)
+      block_dots(in.U, in.n, in.n, (long long)r * RB, in.rb0 + r, in.V + (long long)in.j * in.ldv, in.nu,
+                 b.part2, nullptr, red, redn);
+    if (!group_barrier(bar, nct, b.err)) return;
+    reduce_coeffs(b.part2 + (long long)in.rb0 * KMAXS, in.nrb, in.nu, ucs);
+    __syncthreads();
+    for (int r = rank; r < in.nrb; r += in.ncta) {
+      const long long i = (long long)r * RB + tid;
+      if (i < in.n) {
+        cplx a = in.w[i];
+        for (int t = 0; t < in.nu; t++) a = cadd(a, cmul(in.U[i + (long long)t * in.n], ucs[t]));
+        in.w[i] = a;
       }
-      __syncthreads();
-      const long long r0 = (long long)(rb - in.rb0) * RB;
-      {
-        const long long i = r0 + tid;
-        if (i < in.n) {
-          cplx a = in.w[i];
-          for (int t = 0; t < in.nu; t++) a = cadd(a, cmul(in.U[i + (long long)t * in.n], ucs[t]));
-          in.w[i] = a;
-        }
-      }
-      __syncthreads();
     }
-    // the dots below read other rows only through V, never w: no barrier needed
+    // pass 1 reads w only in the rows this thread has just written
   }
 
   // ---- pass 1: w' = w - beta_{j-1} v_{j-1}; partial h = V^H w', |w'|^2 ----
-  for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
-    const int q = inst_of(b, rb);
-    const LzInst& in = b.in[q];
-    if (in.j > 0) {
-      const double bp = in.sc->beta[in.j - 1];
-      const cplx* vp = in.V + (long long)(in.j - 1) * in.ldv;
-      const long long r0 = (long long)(rb - in.rb0) * RB;
-      {
+  {
+    const double bp = in.j > 0 ? in.sc->beta[in.j - 1] : 0.0;
+    const cplx* vp = in.V + (long long)(in.j > 0 ? in.j - 1 : 0) * in.ldv;
+    for (int r = rank; r < in.nrb; r += in.ncta) {
+      const long long r0 = (long long)r * RB;
+      if (in.j > 0) {
         const long long i = r0 + tid;
         if (i < in.n) in.w[i] = csub(in.w[i], cscale(__ldcg(&vp[i]), bp));
       }
-      __syncthreads();
+      block_dots(in.V, in.ldv, in.n, r0, in.rb0 + r, in.w, in.k, b.part, b.pn1, red, redn);
     }
-    block_dots(in.V, in.ldv, in.n, (long long)(rb - in.rb0) * RB, rb, in.w, in.k, b.part, b.pn1, red, redn);
   }
-  if (!grid_barrier(b.bar, b.err)) return;
-  reduce_pairs(b, b.part, b.h, 0xffffffffu, b.pn1, b.nw);
-  if (!grid_barrier(b.bar, b.err)) return;
+  if (!group_barrier(bar, nct, b.err)) return;
 
-  // ---- DGKS test (every CTA decides the same): after the first pass
-  // |w''|^2 = |w'|^2 - |h|^2 (the basis is orthonormal); a second pass when
-  // that drops below half of |w'|^2, else beta_j = |w''| at once ----
-  __shared__ double hh[LZ_MAXI];
-  __shared__ double beta_s[LZ_MAXI];
-  coefficient_norms(b, b.h, hh);
-  if (tid == 0) {
-    unsigned f = 0u;
-    for (int q = 0; q < b.ninst; q++) {
-      const double nw = __ldcg(&b.nw[q]);
-      const double b2 = nw - hh[q];
-      if (b2 < DGKS2 * nw) f |= 1u << q;
-      beta_s[q] = sqrt(fmax(b2, 0.0));
+  // ---- every CTA of the instance: h, |w'|^2 and the DGKS test (after the
+  // first pass |w''|^2 = |w'|^2 - |h|^2, the basis being orthonormal; a second
+  // pass when that drops below half of |w'|^2, else beta_j = |w''| at once) ----
+  reduce_coeffs(b.part + (long long)in.rb0 * KMAXS, in.nrb, in.k, hs);
+  const double nw = sum_norms(in, b.pn1, redn);  // its barriers also publish hs
+  const double b2 = nw - coeff_norm(hs, in.k, redn);
+  const bool flag = b2 < DGKS2 * nw;
+  double beta = sqrt(fmax(b2, 0.0));
+  double alpha = in.sigma + hs[in.j].x;
+
+  if (!flag) {
+    // w'' / beta_j straight into the basis
+    const double inv = beta > 0.0 ? 1.0 / beta : 0.0;
+    for (int r = rank; r < in.nrb; r += in.ncta) block_update_final(in, r, hs, in.k, inv);
+  } else {
+    // keep w'' in w and take its second-pass dots
+    for (int r = rank; r < in.nrb; r += in.ncta) {
+      block_update(in, r, in.w, hs, in.k, b.pn2, redn);
+      block_dots(in.V, in.ldv, in.n, (long long)r * RB, in.rb0 + r, in.w, in.k, b.part2, nullptr, red, redn);
     }
-    flagged = f;
-  }
-  __syncthreads();
-  const unsigned fl = flagged;
-
-  // ---- update: unflagged instances finish here (w'' / beta_j into the
-  // basis); flagged ones keep w'' and take its second-pass dots ----
-  for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
-    const int q = inst_of(b, rb);
-    const LzInst& in = b.in[q];
-    for (int l = tid; l < in.k; l += T) hs[l] = __ldcg(&b.h[q * KMAXS + l]);
+    if (!group_barrier(bar, nct, b.err)) return;
+    reduce_coeffs(b.part2 + (long long)in.rb0 * KMAXS, in.nrb, in.k, hs2);
     __syncthreads();
-    if (!((fl >> q) & 1u)) {
-      block_update_final(in, rb, hs, in.k, beta_s[q] > 0.0 ? 1.0 / beta_s[q] : 0.0);
-      __syncthreads();
-    } else {
-      block_update(in, rb, in.w, hs, in.k, b.pn2, redn);
-      block_dots(in.V, in.ldv, in.n, (long long)(rb - in.rb0) * RB, rb, in.w, in.k, b.part, nullptr, red, redn);
-    }
-  }
-
-  if (fl) {
-    if (!grid_barrier(b.bar, b.err)) return;
-    reduce_pairs(b, b.part, b.h2, fl, b.pn2, b.nw + LZ_MAXI);
-    if (!grid_barrier(b.bar, b.err)) return;
-    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
-      const int q = inst_of(b, rb);
-      if (!((fl >> q) & 1u)) continue;
-      const LzInst& in = b.in[q];
-      for (int l = tid; l < in.k; l += T) hs[l] = __ldcg(&b.h2[q * KMAXS + l]);
-      __syncthreads();
-      block_update(in, rb, in.w, hs, in.k, b.pn1, redn);
-    }
+    alpha += hs2[in.j].x;
+    // pn1 is free again: every CTA of the instance read it before the barrier
+    for (int r = rank; r < in.nrb; r += in.ncta) block_update(in, r, in.w, hs2, in.k, b.pn1, redn);
     // the norm after the second pass is summed explicitly (no cancellation
     // argument holds for it)
-    if (!grid_barrier(b.bar, b.err)) return;
-    for (int q = 0; q < b.ninst; q++) {
-      if (!((fl >> q) & 1u)) continue;
-      const double b2 = sum_norms(b.in[q], b.pn1, redn);
-      if (tid == 0) beta_s[q] = sqrt(b2);
-    }
-    __syncthreads();
-    for (int rb = blockIdx.x; rb < b.nrb_total; rb += gridDim.x) {
-      const int q = inst_of(b, rb);
-      const LzInst& in = b.in[q];
-      if (!((fl >> q) & 1u) || !in.write_next) continue;
-      const double inv = beta_s[q] > 0.0 ? 1.0 / beta_s[q] : 0.0;
+    if (!group_barrier(bar, nct, b.err)) return;
+    beta = sqrt(sum_norms(in, b.pn1, redn));
+    if (in.write_next) {
+      const double inv = beta > 0.0 ? 1.0 / beta : 0.0;
       cplx* vn = in.V + (long long)(in.j + 1) * in.ldv;
-      const long long i = (long long)(rb - in.rb0) * RB + tid;
-      if (i < in.n) vn[i] = cscale(in.w[i], inv);
+      for (int r = rank; r < in.nrb; r += in.ncta) {
+        const long long i = (long long)r * RB + tid;
+        if (i < in.n) vn[i] = cscale(in.w[i], inv);
+      }
     }
   }
 
   // ---- alpha_j, beta_j ----
-  if (blockIdx.x == 0 && tid < b.ninst) {
-    const LzInst& in = b.in[tid];
-    double alpha = in.sigma + __ldcg(&b.h[tid * KMAXS + in.j].x);
-    if ((fl >> tid) & 1u) alpha += __ldcg(&b.h2[tid * KMAXS + in.j].x);
-    const double beta = beta_s[tid];
+  if (rank == 0 && tid == 0) {
     in.sc->alpha[in.j] = alpha;
     in.sc->beta[in.j] = beta;
-    in.sc->flag = (fl >> tid) & 1u;
+    in.sc->flag = flag ? 1 : 0;
     if (in.mirror) {  // mapped host memory, read by the host after the launch's event
       in.mirror->alpha[in.j] = alpha;
       in.mirror->beta[in.j] = beta;
@@ -455,6 +388,7 @@ int lanczos_step_rows_per_block() { return RB; }
 void lanczos_step(const Stream& st, LzBatch& b) {
   MPSGPU_CHECK(b.ninst >= 1 && b.ninst <= LZ_MAXI, MPSGPU_BAD_SHAPE, "lanczos step: group size");
   int rb = 0;
+  double wsum = 0.0;
   for (int q = 0; q < b.ninst; q++) {
     LzInst& in = b.in[q];
     MPSGPU_CHECK(in.k == in.j + 1 && in.k <= KMAXS && in.n > 0, MPSGPU_BAD_SHAPE, "lanczos step: basis size");
@@ -462,6 +396,7 @@ void lanczos_step(const Stream& st, LzBatch& b) {
     in.rb0 = rb;
     in.nrb = ceil_div(in.n, RB);
     rb += in.nrb;
+    wsum += (double)in.nrb * (2.0 * in.k + 6.0 + 2.0 * in.nu);
   }
   b.nrb_total = rb;
   int dev = 0;
@@ -476,7 +411,34 @@ void lanczos_step(const Stream& st, LzBatch& b) {
     g_lz_grid[dev] = nsm * std::min(per, 2);
     mark_device_done(g_lz_setup);
   }
-  const int grid = std::max(1, std::min(g_lz_grid[dev], b.nrb_total));
+  const int G = g_lz_grid[dev];
+  // CTAs per instance in proportion to its bytes, at most one per row block,
+  // then evened out so that every CTA of an instance takes the same number
+  // of row blocks; all of them co-resident (cooperative launch)
+  std::vector<int> nc(b.ninst);
+  int total = 0;
+  for (int q = 0; q < b.ninst; q++) {
+    const LzInst& in = b.in[q];
+    const double w = (double)in.nrb * (2.0 * in.k + 6.0 + 2.0 * in.nu);
+    int c = std::max(1, std::min(in.nrb, (int)(G * w / wsum)));
+    c = ceil_div(in.nrb, ceil_div(in.nrb, c));
+    nc[q] = c;
+    total += c;
+  }
+  while (total > G) {  // only when many instances took their minimum of one
+    int big = 0;
+    for (int q = 1; q < b.ninst; q++)
+      if (nc[q] > nc[big]) big = q;
+    MPSGPU_CHECK(nc[big] > 1, MPSGPU_BAD_SHAPE, "lanczos step: more instances than co-resident CTAs");
+    nc[big]--;
+    total--;
+  }
+  int c0 = 0;
+  for (int q = 0; q < b.ninst; q++) {
+    b.in[q].cta0 = c0;
+    b.in[q].ncta = nc[q];
+    c0 += nc[q];
+  }
   // algorithmic bytes: the basis read twice (projections, update), w read
   // and written three times (three-term step, update, normalisation) and
   // v_{j-1} once; the projector vectors twice
@@ -485,7 +447,7 @@ void lanczos_step(const Stream& st, LzBatch& b) {
     bytes += 16.0 * (double)b.in[q].n * (2.0 * b.in[q].k + 6.0 + 2.0 * b.in[q].nu);
   ProfScope ps(st, GemmProfiler::LZSTEP, bytes);
   void* args[] = {&b};
-  MPSGPU_CUDA(cudaLaunchCooperativeKernel((void*)lanczos_step_kernel, dim3(grid), dim3(T), args, 0, st.s));
+  MPSGPU_CUDA(cudaLaunchCooperativeKernel((void*)lanczos_step_kernel, dim3(c0), dim3(T), args, 0, st.s));
   after_launch(st);
 }
 

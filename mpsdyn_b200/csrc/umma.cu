@@ -244,8 +244,8 @@ __global__ void __launch_bounds__(SP_THREADS, 1) zgemm_split_kernel(SplitGemmPar
     mt = (int)(local % q.mtiles);
     nt = (int)(local / q.mtiles);
     sp = 0;
-    k0 = 0;
-    nk = q.KS;
+    k0 = q.k0;
+    nk = q.nk > 0 ? q.nk : q.KS - q.k0;
     p.M = q.M;
     p.N = q.N;
     p.KS = q.KS;
@@ -401,6 +401,30 @@ __global__ void split_reduce_kernel(int M, int N, int splits, const cplx* __rest
     cplx o = cmul(alpha, s);
     if (Cin) o = cadd(o, cmul(beta, Cin[m + n * ldcin]));
     C[m + n * ldc] = o;
+  }
+}
+
+// Grouped sums of partial products (split_reduce_grouped): element t of
+// job j (t in [begin_j, begin_{j+1})) is C[m + n ldc] = alpha sum_s part[s M N
+// + m + n M] + beta Cin[m + n ldcin], the partials added in order.
+__global__ void split_reduce_grouped_kernel(const SplitReduceJob* __restrict__ jobs, int n, long long total) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].begin <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const SplitReduceJob& jb = jobs[lo];
+    const long long e = t - jb.begin, mn = (long long)jb.M * jb.N;
+    const int m = (int)(e % jb.M);
+    const long long col = e / jb.M;
+    cplx s = cmake(0.0, 0.0);
+    for (int p = 0; p < jb.nparts; p++) s = cadd(s, jb.part[p * mn + e]);
+    cplx o = cmul(jb.alpha, s);
+    if (jb.Cin) o = cadd(o, cmul(jb.beta, jb.Cin[m + col * jb.ldcin]));
+    jb.C[m + col * jb.ldc] = o;
   }
 }
 
@@ -562,6 +586,22 @@ void zgemm_split_grouped(const Stream& st, const SplitProblem* d_probs, int n, l
   SplitGemmParams p{};
   const SplitGroupParams gp{d_probs, n, err};
   launch_split<SP_GROUP_BN, true>(st, p, gp, dim3((unsigned)tiles));
+}
+
+long long split_reduce_jobs(SplitReduceJob* jobs, int n) {
+  long long t = 0;
+  for (int i = 0; i < n; i++) {
+    jobs[i].begin = t;
+    t += (long long)jobs[i].M * jobs[i].N;
+  }
+  return t;
+}
+
+void split_reduce_grouped(const Stream& st, const SplitReduceJob* d_jobs, int n, long long total) {
+  if (total <= 0) return;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
+  split_reduce_grouped_kernel<<<blocks, 256, 0, st.s>>>(d_jobs, n, total);
+  after_launch(st);
 }
 
 long long split_prepare_jobs(SplitPrepJob* jobs, int n) {
