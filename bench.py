@@ -6,8 +6,11 @@ penalty (seed-11 initial MPS), convergence 1e-10, complex FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpsgpu|reference]
 
-One step is a batch of B (default 8) independent solves with different seeds,
-run concurrently, one library context (CUDA stream) and host thread each.
+One step is a batch of B (default 16) independent solves with different
+seeds, swept in lockstep as two groups of 8 (each group on its own library
+context and host thread; within a group the chains' local eigenproblems share
+the grouped launches of every Lanczos round), in the split-precision form
+(BF16-limb tcgen05 products until the energy settles, FP64 to convergence).
 One process per GPU; the path does not shard (independent solves), so N GPUs
 run N replicas of the workload ("replicas only", weak scaling) and `value`
 is the total solves of all ranks divided by the max-over-ranks device time.
@@ -41,9 +44,9 @@ MU = 2 * WORKLOAD["mg"] * np.sqrt(WORKLOAD["x"])
 PRECISION = {"schedule": 2, "mixed": 1, "fp64": 0}  # options.precision of each form
 PRECISION_TEXT = {
     "schedule": "FP64 products; eigensolver residual 1e-6 until the half-sweep energy change first falls below "
-                "1e-6, then 1e-9 for one half-sweep, then the reference's 1e-12 to convergence",
+                "1e-6, then 1e-9 to convergence (the first such half-sweep cannot end the solve)",
     "mixed": "split-precision (BF16-limb tcgen05) products and residual 1e-6 until the half-sweep energy change "
-             "first falls below 1e-6, then FP64 (1e-9 for one half-sweep, then 1e-12)",
+             "first falls below 1e-6, then FP64 products at residual 1e-9 to convergence",
     "fp64": "FP64 products, eigensolver residual 1e-12 throughout (the reference's tolerance)"}
 METRIC = "DMRG solves/s (Schwinger N=100 D=128, E0 + first gap, |dE/E|<=1e-10)"
 UNIT = "solves/s"
@@ -69,7 +72,7 @@ def parse():
     p.add_argument("--plain", type=int, default=1, help="also time one solve alone (the plain form)")
     p.add_argument("--arm-steps", type=int, default=1,
                    help="steps of each comparison arm (FP64 batch, FP64 batch with the mixed schedule)")
-    p.add_argument("--precision", default="schedule", choices=["schedule", "mixed", "fp64"],
+    p.add_argument("--precision", default="mixed", choices=["schedule", "mixed", "fp64"],
                    help="schedule: FP64 products with the mixed schedule of eigensolver tolerances; mixed: the "
                         "same schedule with split-precision (tcgen05) products until the energy settles; fp64: "
                         "FP64 with the reference's tolerance throughout")
@@ -218,8 +221,11 @@ def bf16_peak() -> tuple:
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from ncu captures of
-# the same shapes (profiles/), None until captured
-KERNEL_TRAFFIC = {"gemm_fp64_dmma": None, "gemm_split_tcgen05": None, "lanczos_step": None, "qr": None}
+# the same shapes (profiles/), None where none was taken: the Lanczos step of
+# eight D = 128 Schwinger chains (one launch of the lockstep sample),
+# profiles/lanczos_step_heff_schwinger_sample_N40_D128_batch8.md
+KERNEL_TRAFFIC = {"gemm_fp64_dmma": None, "gemm_split_tcgen05": None, "lanczos_step": 102.5e6, "qr": 0.667e6,
+                  "split_operands": None}
 
 
 def fp64_gemm_peak(torch) -> float:
@@ -494,9 +500,11 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         else:
             arms["schedule"] = batch_arm(2)
 
-    # ---- single solves alone on the GPU with the library's kernel profiler
-    # on (events around 1 in 32 launches of each kernel class): the plain
-    # FP64 form, and the mixed form of the line ----
+    # ---- with the library's kernel profiler on (events around 1 in 32
+    # launches of each kernel class): one FP64 solve alone (the plain form),
+    # and one lockstep group of the line alone (its first group's solves, the
+    # line's precision; group work on other streams runs concurrently, so the
+    # classes' shares of the group's time may add up to more than 1) ----
     def profiled_single(o):
         flush_l2()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -509,8 +517,25 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         r = results[0]
         return ev0.elapsed_time(ev1), prof, r
 
+    def profiled_group(o):
+        flush_l2()
+        lead0 = members[0][0]
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctxs[lead0].profile_begin()
+        ev0.record(exts[lead0])
+        lockstep_solves(o, False, 0)
+        ev1.record(exts[lead0])
+        ev1.synchronize()
+        prof = ctxs[lead0].profile_end()
+        return ev0.elapsed_time(ev1), prof
+
     plain_ms, prof64, r64 = profiled_single(opts64) if args.plain else (None, None, None)
-    line_ms, profln, rln = profiled_single(opts) if (args.plain and prec != 0) else (None, None, None)
+    if args.plain and lockstep:
+        line_ms, profln = profiled_group(opts)
+    elif args.plain and prec != 0:
+        line_ms, profln, _ = profiled_single(opts)
+    else:
+        line_ms, profln = None, None
 
     if rank != 0:
         for c in ctxs:
@@ -529,7 +554,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             if not k["calls"] or k["ms"] <= 0:
                 continue
             rate = k["work"] / (k["ms"] * 1e-3)
-            if name == "lanczos_step":
+            if name in ("lanczos_step", "split_operands"):
                 ach, pk, unit, bound, src = rate / 1e9, peaks["hbm_gbs"], "GB/s", "hbm", peaks["hbm_src"]
             elif name == "gemm_split_tcgen05":
                 ach, pk, unit, bound, src = rate / 1e12, peaks["bf16_sustained"], "TFLOP/s", "tensor", peaks["bf16_src"]
@@ -538,24 +563,31 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                 src = "cuBLAS complex128 GEMM 4096^3 measured in this run (FP64 tensor pipe)"
             out[name] = {"bound": bound, "achieved": ach, "peak": pk, "unit": unit, "frac": ach / pk,
                          "peak_source": src, "sampled_launches": k["calls"],
-                         "share_of_solve": 32.0 * k["ms"] / total_ms if total_ms else None}
+                         "work_per_launch": k["work"] / k["calls"],
+                         "share_of_time": 32.0 * k["ms"] / total_ms if total_ms else None}
         return out
 
     table64 = kernel_table(prof64, plain_ms)
     tableln = kernel_table(profln, line_ms)
 
     def dominant(table, note):
+        # the largest share among the kernels of the Lanczos rounds, which run
+        # one after another on the group's stream; the QRs run on the chains'
+        # own streams, up to a group's worth at once, so their summed event
+        # time overstates their share of the wall time
         if not table:
             return None
-        name = max(table, key=lambda n: table[n]["share_of_solve"] or 0.0)
+        cand = [n for n in table if n != "qr"] or list(table)
+        name = max(cand, key=lambda n: table[n]["share_of_time"] or 0.0)
         d = dict(table[name])
         d.update(kernel=name, traffic=KERNEL_TRAFFIC.get(name), traffic_unit="bytes per launch", note=note)
         return d
 
-    roofline = dominant(tableln if prec != 0 else table64,
-                        "achieved = sampled launches' algorithmic work / their summed CUDA-event time, one solve "
-                        "of the line's precision alone on the GPU; lanczos_step bytes: basis read twice + "
-                        "work vector traffic (the basis of one solve, 33 MB, is L2-resident)")
+    roofline = dominant(tableln if (prec != 0 or lockstep) else table64,
+                        "achieved = sampled launches' algorithmic work / their summed CUDA-event time, one "
+                        "lockstep group of the line's form alone on the GPU (8 solves; one Lanczos round is one "
+                        "grouped launch of each kernel for all of them); lanczos_step bytes: basis read twice + "
+                        "work vector traffic; gemm_split_tcgen05 flops: 24 BF16 MMAs per complex k-step")
 
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -590,11 +622,13 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         "plain_single_solve_ms": plain_ms,
         "plain_fp64_solves_per_s": plain_rate,
         "vs_plain_fp64": (value / plain_rate) if plain_rate else None,
-        "line_form_single_solve_ms": line_ms,
+        "line_form_profiled_ms": line_ms,
+        "line_form_profiled": ("one lockstep group of the line (solves " + str(members[0]) + ") alone"
+                               if lockstep else "one solve of the line's precision alone"),
         "arms": arms,
         "attribution": attribution(args.precision, value, arms, plain_rate),
         "roofline": roofline,
-        "kernels_line_form_single": tableln,
+        "kernels_line_form": tableln,
         "kernels_fp64_single": table64,
         "cpu_baseline": cpu,
         "clocks": clk,
@@ -766,54 +800,73 @@ def run_quench(args) -> None:
     evolution (IsingHamiltonian::getUMPO + Contractor::optimize), dt = 0.01,
     bond dimension up to `--qD`; <sigma_x> at the centre and the centre
     entropy after every step.  `--quenches` chains x `--qsteps` steps, one
-    context per chain, all chains concurrent."""
+    context per chain, all chains concurrent; run in FP64 and, unless
+    --precision fp64, again with split-precision local vectors (optimize with
+    precision 1), reporting both rates and the observables' largest deviation
+    of the split run from the FP64 one."""
     from mpsdyn_b200 import capi
     rs = np.random.default_rng(5)
     nq, ns, L, D = args.quenches, args.qsteps, 64, args.qD
     gvals = rs.uniform(0.2, 2.0, size=nq)
     sx = np.array([[0, 1], [1, 0]], dtype=complex)
-    out = [None] * nq
-    step_ms = [[] for _ in range(nq)]
-    errors = []
 
-    def chain(i):
-        try:
-            with capi.Context(0) as c:
-                U = c.mpo_ising_evolution(L, 1.0, float(gvals[i]), 0.1, 0.01, False)
-                st = c.mps_product(L, 2, 1)
-                o = c.options(convtol=1e-10)
-                obs = []
-                for _ in range(ns):
-                    t = time.perf_counter()
-                    aux = st.copy()
-                    c.optimize(U, aux, st, D, o)
-                    aux.free()
-                    m = c.expectation_local(st, sx)[L // 2]
-                    st.gauge("L")
-                    s = c.entropy(st, L // 2)
-                    step_ms[i].append((time.perf_counter() - t) * 1e3)
-                    obs.append((m, s))
-                out[i] = obs
-        except Exception as e:  # reported in the line, not swallowed
-            errors.append(f"chain {i}: {e}")
-    t0 = time.perf_counter()
-    ths = [threading.Thread(target=chain, args=(i,)) for i in range(nq)]
-    for t in ths:
-        t.start()
-    for t in ths:
-        t.join()
-    wall = time.perf_counter() - t0
-    per = np.array([x for s in step_ms for x in s]) if any(step_ms) else np.zeros(1)
-    done = sum(len(s) for s in step_ms)
-    line = {"metric": "batched quench time steps/s (L=64, D<=256, FP64)", "value": done / wall,
+    def run(precision):
+        out = [None] * nq
+        step_ms = [[] for _ in range(nq)]
+        errors = []
+
+        def chain(i):
+            try:
+                with capi.Context(0) as c:
+                    U = c.mpo_ising_evolution(L, 1.0, float(gvals[i]), 0.1, 0.01, False)
+                    st = c.mps_product(L, 2, 1)
+                    o = c.options(convtol=1e-10, precision=precision)
+                    obs = []
+                    for _ in range(ns):
+                        t = time.perf_counter()
+                        aux = st.copy()
+                        c.optimize(U, aux, st, D, o)
+                        aux.free()
+                        m = c.expectation_local(st, sx)[L // 2]
+                        st.gauge("L")
+                        s = c.entropy(st, L // 2)
+                        step_ms[i].append((time.perf_counter() - t) * 1e3)
+                        obs.append((m, s))
+                    out[i] = np.array(obs, dtype=float)
+            except Exception as e:  # reported in the line, not swallowed
+                errors.append(f"chain {i}: {e}")
+        t0 = time.perf_counter()
+        ths = [threading.Thread(target=chain, args=(i,)) for i in range(nq)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        wall = time.perf_counter() - t0
+        per = np.array([x for s in step_ms for x in s]) if any(step_ms) else np.zeros(1)
+        done = sum(len(s) for s in step_ms)
+        return {"value": done / wall, "wall_s": wall,
+                "latency_ms_per_step": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+                "errors": errors}, out
+
+    r64, o64 = run(0)
+    split = None
+    if args.precision != "fp64":
+        rsp, osp = run(1)
+        ok = [i for i in range(nq) if o64[i] is not None and osp[i] is not None]
+        dev = np.array([np.abs(osp[i] - o64[i]).max(axis=0) for i in ok]) if ok else np.zeros((1, 2))
+        split = dict(rsp, max_abs_dev_vs_fp64={"sx_center": float(dev[:, 0].max()),
+                                               "entropy_center": float(dev[:, 1].max())},
+                     speedup_vs_fp64=rsp["value"] / r64["value"] if r64["value"] else None)
+    line = {"metric": "batched quench time steps/s (L=64, D<=%d)" % D, "value": r64["value"],
             "unit": "steps/s", "n_gpus": 1, "steps": ns, "warmup": 0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (g ~ U[0.2,2], numpy seed 5)",
             "config": {"workload": "quench_ising_L64", "quenches": nq, "steps": ns, "dt": 0.01, "D_max": D},
-            "latency_ms_per_step": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
-            "errors": errors,
-            "last": {"sx_center": out[0][-1][0], "entropy_center": out[0][-1][1]} if out[0] else None}
+            "latency_ms_per_step": r64["latency_ms_per_step"], "errors": r64["errors"], "wall_s": r64["wall_s"],
+            "split": split,
+            "last": {"sx_center": float(o64[0][-1][0]), "entropy_center": float(o64[0][-1][1])}
+            if o64[0] is not None else None}
     print(json.dumps(line), flush=True)
-    if errors:
+    if r64["errors"] or (split and split["errors"]):
         sys.exit(1)
 
 

@@ -52,20 +52,26 @@ typedef struct mpsgpu_mps mpsgpu_mps;
  * Contractor's: convtol 1e-5, eigtol 0 (Contractor.cpp:39-42). */
 typedef struct {
   double convtol;      /* setConvTol (Contractor.h:213) */
-  double eigtol;       /* setEigTol; 0 = 1e-12 relative Lanczos residual */
+  double eigtol;       /* setEigTol; 0 = 1e-12 relative Lanczos residual
+                        * (1e-9 in the final half-sweeps of precision 1
+                        * and 2, see below) */
   double excorthtol;   /* setExcOrthTol (Contractor.h:229); 0 = no check */
   int max_rounds;      /* half-sweep cap; 0 = 1000 (MAX_ROUND_EXCTD, Contractor.cpp:26) */
   int max_krylov;      /* Lanczos vectors per restart; 0 = 64 */
   int precision;       /* 0 = complex FP64 throughout; 1 = mixed: the
                         * effective-Hamiltonian products of the single-site
-                        * ground-state sweep run in split precision (BF16
-                        * limbs on the tensor cores) until the half-sweep
+                        * ground- and excited-state sweeps run in split
+                        * precision (BF16 limbs on the tensor cores,
+                        * eigensolver residual 1e-6) until the half-sweep
                         * energy change falls below 1e-6 relative, then in
-                        * FP64 to convtol (at least one full FP64 round);
-                        * 2 = the schedule of 1 (its eigensolver tolerances
-                        * and phases) with FP64 products, which separates
-                        * what the schedule saves from what the tensor
-                        * cores save */
+                        * FP64 at residual 1e-9 to convtol (at least one
+                        * full FP64 round); in optimize (time evolution) 1
+                        * computes the local vector L W R x in split
+                        * precision throughout (environments stay FP64);
+                        * 2 = the schedule of 1 (its
+                        * eigensolver tolerances and phases) with FP64
+                        * products, which separates what the schedule
+                        * saves from what the tensor cores save */
   int verbose;         /* 1 = one line per half-sweep on stdout */
   /* Optional: when *cancel_flag becomes non-zero (set by another host
    * thread), the sweep stops between two site steps with MPSGPU_CANCELLED. */
@@ -124,12 +130,14 @@ mpsgpu_status mpsgpu_get_stream(mpsgpu_context* ctx, void** stream);
 mpsgpu_status mpsgpu_profile_begin(mpsgpu_context* ctx);
 mpsgpu_status mpsgpu_profile_end(mpsgpu_context* ctx, double* gemm_ms, double* gemm_flops,
                                  long long* gemm_calls);
-/* After mpsgpu_profile_end: the same per kernel class (arrays of 4, each
- * may be null): 0 complex FP64 GEMMs on the DMMA pipe, 1 split-precision
- * GEMMs on tcgen05 (work = BF16 tensor flops), 2 the fused Lanczos step
- * (work = algorithmic bytes), 3 Householder QR (flops).  Sampled launches:
- * one in 32 of each class; ms their summed device time, work their summed
- * algorithmic work. */
+/* After mpsgpu_profile_end: the same per kernel class (arrays of
+ * MPSGPU_PROFILE_CLASSES entries, each may be null): 0 complex FP64 GEMMs on
+ * the DMMA pipe, 1 split-precision GEMMs on tcgen05 (work = BF16 tensor
+ * flops), 2 the fused Lanczos step (work = algorithmic bytes), 3 Householder
+ * QR (flops), 4 the split products' operand passes (BF16 limb planes, MPO
+ * legs, sums of K chunks; work = bytes).  Sampled launches: one in 32 of each
+ * class; ms their summed device time, work their summed algorithmic work. */
+#define MPSGPU_PROFILE_CLASSES 5
 mpsgpu_status mpsgpu_profile_kernels(mpsgpu_context* ctx, double* ms, double* work, long long* calls);
 
 /* ---- MPO (replaces MPO / Operator storage, src/core/headers/MPO.h:33-176) --

@@ -40,7 +40,7 @@ EXPORTS = [
 
 # kernel classes of mpsgpu_profile_kernels (work units: flops, BF16 tensor
 # flops, bytes, flops); one launch in 32 of each class is sampled
-PROFILE_CLASSES = ("gemm_fp64_dmma", "gemm_split_tcgen05", "lanczos_step", "qr")
+PROFILE_CLASSES = ("gemm_fp64_dmma", "gemm_split_tcgen05", "lanczos_step", "qr", "split_operands")
 
 
 class Options(C.Structure):
@@ -182,7 +182,8 @@ class Context:
         ms, fl, n = C.c_double(), C.c_double(), C.c_longlong()
         self._check(self.lib.mpsgpu_profile_end(self.h, C.byref(ms), C.byref(fl), C.byref(n)))
         out = {"gemm_ms": ms.value, "gemm_flops": fl.value, "gemm_calls": n.value}
-        kms, kwork, kcalls = (C.c_double * 4)(), (C.c_double * 4)(), (C.c_longlong * 4)()
+        nc = len(PROFILE_CLASSES)
+        kms, kwork, kcalls = (C.c_double * nc)(), (C.c_double * nc)(), (C.c_longlong * nc)()
         self._check(self.lib.mpsgpu_profile_kernels(self.h, kms, kwork, kcalls))
         out["kernels"] = {name: {"ms": kms[i], "work": kwork[i], "calls": kcalls[i]}
                           for i, name in enumerate(PROFILE_CLASSES)}

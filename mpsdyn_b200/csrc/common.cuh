@@ -65,17 +65,19 @@ struct Error : public std::runtime_error {
 struct GemmProfiler {
   // 0: complex FP64 GEMMs on the DMMA pipe (zgemm, the fused contractions);
   // 1: split-precision GEMM on tcgen05 (work = BF16 tensor flops);
-  // 2: the fused Lanczos step (work = bytes); 3: Householder QR (flops)
-  enum { GEMM64 = 0, SPLIT = 1, LZSTEP = 2, QR = 3, NCLS = 4 };
+  // 2: the fused Lanczos step (work = bytes); 3: Householder QR (flops);
+  // 4: the split products' operand passes (limb planes, MPO legs, sums of
+  // K chunks; work = bytes)
+  enum { GEMM64 = 0, SPLIT = 1, LZSTEP = 2, QR = 3, SPLITOPS = 4, NCLS = 5 };
   bool on = false;
   int every = 32;
-  long long seen[NCLS] = {0, 0, 0, 0};
+  long long seen[NCLS] = {};
   std::vector<cudaEvent_t> pool;
   std::vector<int> tags;  // class of each recorded pair
   size_t used = 0;
-  double work[NCLS] = {0, 0, 0, 0};
-  long long calls[NCLS] = {0, 0, 0, 0};
-  double ms[NCLS] = {0, 0, 0, 0};  // filled by resolve()
+  double work[NCLS] = {};
+  long long calls[NCLS] = {};
+  double ms[NCLS] = {};  // filled by resolve()
   bool sample(int cls) { return on && (seen[cls]++ % every) == 0; }
   cudaEvent_t next() {
     if (used == pool.size()) {

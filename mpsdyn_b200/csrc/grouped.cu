@@ -43,47 +43,89 @@ __global__ void wperm_kernel(const WPerm* __restrict__ d, int n, long long total
   }
 }
 
-template <int NIN>
-__global__ void wcontract_grouped_kernel(const WGroup* __restrict__ g, int n, long long total) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
+// One block per chunk of PX * WC_THREADS pixels of one problem (problems start
+// on multiples of WC_CHUNK, itself a multiple of every chunk): the problem's
+// leg matrix is staged in shared memory, and every thread takes PX pixels
+// WC_THREADS apart, so that each leg entry read serves PX pixels while the
+// loads of every pixel index stay coalesced.
+template <int NIN, int PX>
+__global__ void __launch_bounds__(WC_THREADS) wcontract_grouped_kernel(const WGroup* __restrict__ g, int n,
+                                                                       long long chunks) {
+  __shared__ cplx Ws[32 * 32];
+  for (long long ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+    const long long t0 = ch * (PX * WC_THREADS);
     int lo = 0, hi = n - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (g[mid].pix_begin <= t) lo = mid;
+      if (g[mid].pix_begin <= t0) lo = mid;
       else hi = mid - 1;
     }
     const WContractArgs& a = g[lo].a;
-    const long long p = t - g[lo].pix_begin;
-    const int x = (int)(p % a.nx), y = (int)(p / a.nx);
+    const int parts = g[lo].parts;
+    const long long pstride = g[lo].part_stride;
     const int nin = a.n_i0 * a.n_i1, nout = a.n_o0 * a.n_o1;
-    cplx in[NIN];
-    const cplx* ib = a.in + x * a.ix + y * a.iy;
+    const long long npix = (long long)a.nx * a.ny;
+    __syncthreads();  // the previous chunk's reads of Ws are done
+    for (int e = threadIdx.x; e < nin * nout; e += WC_THREADS) Ws[e] = a.Wm[e];
+    __syncthreads();
+    cplx in[PX][NIN];
+    bool live[PX];
 #pragma unroll
-    for (int i = 0; i < NIN; i++) {
-      if (i < nin) in[i] = ib[(i % a.n_i0) * a.si0 + (i / a.n_i0) * a.si1];
-      else in[i] = make_double2(0.0, 0.0);
+    for (int px = 0; px < PX; px++) {
+      const long long p = t0 - g[lo].pix_begin + threadIdx.x + (long long)px * WC_THREADS;
+      live[px] = p < npix;
+      const int x = live[px] ? (int)(p % a.nx) : 0, y = live[px] ? (int)(p / a.nx) : 0;
+      const cplx* ib = a.in + x * a.ix + y * a.iy;
+#pragma unroll
+      for (int i = 0; i < NIN; i++) {
+        cplx v = make_double2(0.0, 0.0);
+        if (i < nin && live[px]) {
+          const long long off = (i % a.n_i0) * a.si0 + (i / a.n_i0) * a.si1;
+          v = ib[off];
+          for (int q = 1; q < parts; q++) v = cadd(v, ib[off + q * pstride]);
+        }
+        in[px][i] = v;
+      }
     }
-    cplx* ob = a.out + x * a.ox + y * a.oy;
     for (int o = 0; o < nout; o++) {
-      cplx s = make_double2(0.0, 0.0);
+      cplx acc[PX];
 #pragma unroll
-      for (int i = 0; i < NIN; i++)
-        if (i < nin) s = cadd(s, cmul(a.Wm[o + nout * i], in[i]));
-      ob[(o % a.n_o0) * a.so0 + (o / a.n_o0) * a.so1] = s;
+      for (int px = 0; px < PX; px++) acc[px] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int i = 0; i < NIN; i++) {
+        if (i < nin) {
+          const cplx w = Ws[o + nout * i];
+#pragma unroll
+          for (int px = 0; px < PX; px++) acc[px] = cadd(acc[px], cmul(w, in[px][i]));
+        }
+      }
+#pragma unroll
+      for (int px = 0; px < PX; px++) {
+        if (!live[px]) continue;
+        const long long p = t0 - g[lo].pix_begin + threadIdx.x + (long long)px * WC_THREADS;
+        const int x = (int)(p % a.nx), y = (int)(p / a.nx);
+        a.out[x * a.ox + y * a.oy + (o % a.n_o0) * a.so0 + (o / a.n_o0) * a.so1] = acc[px];
+      }
     }
   }
 }
 
 }  // namespace
 
-void wcontract_grouped(const Stream& st, const WGroup* d_wg, int n, long long pixels, int maxnin) {
-  MPSGPU_CHECK(maxnin >= 1 && maxnin <= 32, MPSGPU_BAD_SHAPE, "wcontract_grouped: MPO legs too wide");
+long long wcontract_chunked(long long pixels) { return (pixels + WC_CHUNK - 1) / WC_CHUNK * WC_CHUNK; }
+
+void wcontract_grouped(const Stream& st, const WGroup* d_wg, int n, long long pixels, int maxnin, int maxnout) {
+  MPSGPU_CHECK(maxnin >= 1 && maxnin <= 32 && maxnout >= 1 && maxnin * maxnout <= 32 * 32, MPSGPU_BAD_SHAPE,
+               "wcontract_grouped: MPO legs too wide");
   if (pixels <= 0) return;
-  const int g = (int)std::min<long long>((pixels + 127) / 128, 148LL * 16);
-  if (maxnin <= 8) wcontract_grouped_kernel<8><<<g, 128, 0, st.s>>>(d_wg, n, pixels);
-  else if (maxnin <= 16) wcontract_grouped_kernel<16><<<g, 128, 0, st.s>>>(d_wg, n, pixels);
-  else wcontract_grouped_kernel<32><<<g, 128, 0, st.s>>>(d_wg, n, pixels);
+  auto launch = [&](auto kernel, int px) {
+    const long long chunks = (pixels + px * WC_THREADS - 1) / (px * WC_THREADS);
+    const int g = (int)std::min<long long>(chunks, 148LL * 16);
+    kernel<<<g, WC_THREADS, 0, st.s>>>(d_wg, n, chunks);
+  };
+  if (maxnin <= 8) launch(wcontract_grouped_kernel<8, 4>, 4);
+  else if (maxnin <= 16) launch(wcontract_grouped_kernel<16, 2>, 2);
+  else launch(wcontract_grouped_kernel<32, 1>, 1);
   after_launch(st);
 }
 
@@ -125,7 +167,7 @@ void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst
     return o;
   };
   long long o1 = 0, ow = 0, pix = 0;
-  int maxnin = 1;
+  int maxnin = 1, maxnout = 1;
   for (int q = 0; q < n; q++) {
     const int i = order[q];
     const HeffInstance& h = inst[i];
@@ -154,8 +196,9 @@ void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst
     b.C = h.y; b.ldc = (long long)Dl * d;
     o1 += (long long)Dl * wl * d * Dr;
     ow += (long long)d * wl * d * wr;
-    pix += (long long)Dl * Dr;
+    pix += wcontract_chunked((long long)Dl * Dr);
     maxnin = std::max(maxnin, wl * d);
+    maxnout = std::max(maxnout, d * wr);
     if (split) {
       offL[q] = take(split_operand_bytes(Dl * wl, Dl, 128));
       offX[q] = take(split_operand_bytes(d * Dr, Dl, 128));
@@ -179,6 +222,7 @@ void grouped_matvec_plan(const Stream& st, const std::vector<HeffInstance>& inst
   plan.pixels = pix;
   plan.wel = wel_total;
   plan.maxnin = maxnin;
+  plan.maxnout = maxnout;
   // descriptor tables in device memory
   const size_t bytes = n * (2 * sizeof(GroupedGemm) + sizeof(WGroup) + sizeof(WPerm));
   MPSGPU_CUDA(cudaMallocAsync(&plan.desc, bytes, st.s));
@@ -245,7 +289,7 @@ void grouped_matvec_run(const Stream& st, GroupedMatvecPlan& plan) {
   } else {
     zgemm_grouped(st, plan.d_g1, plan.n, plan.tiles1, plan.ctas);
   }
-  wcontract_grouped(st, (const WGroup*)plan.d_wg, plan.n, plan.pixels, plan.maxnin);
+  wcontract_grouped(st, (const WGroup*)plan.d_wg, plan.n, plan.pixels, plan.maxnin, plan.maxnout);
   if (plan.split) {
     split_prepare_grouped(st, plan.d_jt, plan.n, plan.thr_t);
     zgemm_split_grouped(st, plan.d_s3, plan.n, plan.stiles3, plan.err);

@@ -161,7 +161,7 @@ struct GroupedMatvecPlan {
   void* d_wg = nullptr;
   void* d_wp = nullptr;
   long long tiles1 = 0, tiles3 = 0, pixels = 0, wel = 0;
-  int maxnin = 1, ctas = 148;
+  int maxnin = 1, maxnout = 1, ctas = 148;
   double flops = 0.0;  // algorithmic flops of one grouped product
   // split precision: BF16 limb planes of L, Rt (prepared once by
   // grouped_matvec_prepare_env), x and T2 (prepared in every product)
@@ -197,13 +197,22 @@ struct WContractArgs {
 };
 void wcontract(const Stream& st, const WContractArgs& a);
 // The MPO-leg contraction of n problems in one launch (grouped.cu): problem
-// q covers the pixels [pix_begin_q, pix_begin_{q+1}) of `pixels`; maxnin is
-// the largest n_i0 * n_i1 (at most 32).
+// q covers the pixels [pix_begin_q, pix_begin_q + nx ny), pix_begin_q a
+// multiple of WC_CHUNK (pixel ranges padded by wcontract_chunked), within
+// `pixels`; maxnin and maxnout are the largest n_i0 n_i1 and n_o0 n_o1 (at
+// most 32 inputs, 1024 leg entries).  With parts > 1 the input is the sum of
+// `parts` arrays part_stride apart (the partial products of a K split), added
+// in order.
+constexpr int WC_THREADS = 128;
+constexpr int WC_CHUNK = 512;
 struct WGroup {
   WContractArgs a;
-  long long pix_begin;
+  long long pix_begin = 0;
+  int parts = 1;
+  long long part_stride = 0;
 };
-void wcontract_grouped(const Stream& st, const WGroup* d_wg, int n, long long pixels, int maxnin);
+long long wcontract_chunked(long long pixels);
+void wcontract_grouped(const Stream& st, const WGroup* d_wg, int n, long long pixels, int maxnin, int maxnout);
 
 // ---- effective-Hamiltonian contractions (heff.cu), grouped ----
 constexpr int GEMM_MAXP = 16;  // problems per launch
