@@ -452,13 +452,15 @@ mpsgpu_status mpsgpu_heff_matvec_grouped_ex(mpsgpu_context* ctx, int n, const mp
                                             double* ms_prepare);
 
 /* Autotuner of the complex FP64 GEMM's launch configuration (tile edge
- * 32 or 64, 1 to 16 K slices).  The first GEMM of each shape (M, N, K,
- * batch, ops, epilogue) times every candidate on its own operands into a
- * scratch output and the fastest is used from then on, for all contexts of
- * the process; no tuning while a stream is captured into a graph.  On by
- * default (MPSGPU_AUTOTUNE=0 in the environment turns it off before the
- * first GEMM); results of different configurations differ only by the order
- * of the K-slice sums.  entries = shapes tuned so far. */
+ * 32 or 64, 1 to 16 K slices), and of the K chunks (1-4 and 1-8) of the two
+ * tcgen05 products of a lockstep round's split-precision products.  The
+ * first GEMM of each shape (M, N, K, batch, ops, epilogue), and the first
+ * round of each shape signature (every product's dimensions), times every
+ * candidate on its own operands and the fastest is used from then on, for
+ * all contexts of the process; no tuning while a stream is captured into a
+ * graph.  On by default (MPSGPU_AUTOTUNE=0 in the environment turns it off
+ * before the first GEMM); results of different configurations differ only
+ * by the order of the K-slice sums.  entries = shapes tuned so far. */
 void mpsgpu_set_autotune(int on);
 long long mpsgpu_autotune_entries(void);
 

@@ -838,7 +838,7 @@ mpsgpu_status mpsgpu_heff_matvec_grouped(mpsgpu_context* ctx, int n, const mpsgp
 
 void mpsgpu_set_autotune(int on) { set_gemm_autotune(on); }
 
-long long mpsgpu_autotune_entries(void) { return gemm_autotune_entries(); }
+long long mpsgpu_autotune_entries(void) { return gemm_autotune_entries() + split_autotune_entries(); }
 
 mpsgpu_status mpsgpu_zgemm_split(mpsgpu_context* ctx, int m, int n, int k, const double* A, int lda,
                                  const double* B, int ldb, double* C, int ldc, int repeats, double* ms_total,

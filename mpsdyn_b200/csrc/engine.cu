@@ -11,7 +11,9 @@
 // is one GEMM or one MPO-leg contraction; none of the explicit permutes of
 // TensorMultiplier::product (TensorMultiplier.cpp:61-93) remain.
 #include <algorithm>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -635,27 +637,11 @@ static size_t blob_put(std::vector<uint8_t>& blob, const std::vector<T>& v) {
   return off;
 }
 
-void split_round_run(Context& c, SplitRound& r) {
-  const int n = (int)r.p.size();
-  if (n == 0) return;
-  const Stream st = c.st();
-  const int nsm = device_sms(c);
-  // K of both products split into chunks of at least four k-steps, so that
-  // the round's tiles give about one CTA per SM (at most 8 chunks for the
-  // last product, 4 for the first, whose partials the MPO-leg kernel adds)
-  long long tiles1 = 0, tiles3 = 0;
-  int ks1 = 1, ks3 = 1;
-  for (const SplitProduct& q : r.p) {
-    tiles1 += (long long)q.nh * ceil_div(q.Dlb * q.wl, 128) * ceil_div(q.dd * q.Drk, 128);
-    tiles3 += (long long)q.nh * ceil_div(q.Dlb * q.du, 128) * ceil_div(q.Drb, 128);
-    ks1 = std::max(ks1, ceil_div(q.Dlk, 16));
-    ks3 = std::max(ks3, ceil_div(q.Drk * q.wr, 16));
-  }
-  auto chunks = [&](long long tiles, int ks, int cap) {
-    const int s = (int)std::min<long long>(cap, std::max<long long>(1, (nsm + tiles - 1) / std::max<long long>(1, tiles)));
-    return std::max(1, std::min(s, ks / 4));
-  };
-  const int S1 = chunks(tiles1, ks1, 4), S = chunks(tiles3, ks3, 8);
+// The launches of a split round with the K of the first product cut into S1
+// chunks and that of the last into S (each chunk at least one k-step of 16).
+static void split_round_launch(Context& c, const SplitRound& r, int S1, int S, bool profile) {
+  Stream st = c.st();
+  if (!profile) st.prof = nullptr;
   std::vector<SplitPrepJob> jx, jt;
   std::vector<SplitProblem> g1, g3;
   std::vector<WGroup> wg;
@@ -773,6 +759,99 @@ void split_round_run(Context& c, SplitRound& r) {
     ProfScope ps(st, GemmProfiler::SPLITOPS, br);
     split_reduce_grouped(st, reinterpret_cast<const SplitReduceJob*>(d + orr), (int)red.size(), rtot);
   }
+}
+
+// Autotuner of the split round's K chunks: the first round of each shape
+// signature (device; every product's dimensions and halves) times the
+// candidate chunk counts on its own operands (a round only reads its inputs
+// and overwrites its intermediates and outputs, so running it again is
+// harmless) and keeps the fastest for every later round of that signature,
+// for all contexts of the process.  Off with mpsgpu_set_autotune(0) (or
+// MPSGPU_AUTOTUNE=0), and while the stream is captured into a graph; then
+// the heuristic: about one CTA per SM over the round's tiles.
+namespace {
+std::mutex g_split_tune_mu;
+std::map<std::vector<int>, std::pair<int, int>> g_split_tune;
+}  // namespace
+
+long long split_autotune_entries() {
+  std::lock_guard<std::mutex> lk(g_split_tune_mu);
+  return (long long)g_split_tune.size();
+}
+
+void split_round_run(Context& c, SplitRound& r) {
+  const int n = (int)r.p.size();
+  if (n == 0) return;
+  const int nsm = device_sms(c);
+  long long tiles1 = 0, tiles3 = 0;
+  int ks1 = 1, ks3 = 1;
+  std::vector<int> key{c.device};
+  for (const SplitProduct& q : r.p) {
+    tiles1 += (long long)q.nh * ceil_div(q.Dlb * q.wl, 128) * ceil_div(q.dd * q.Drk, 128);
+    tiles3 += (long long)q.nh * ceil_div(q.Dlb * q.du, 128) * ceil_div(q.Drb, 128);
+    ks1 = std::max(ks1, ceil_div(q.Dlk, 16));
+    ks3 = std::max(ks3, ceil_div(q.Drk * q.wr, 16));
+    key.insert(key.end(), {q.nh, q.Dlb, q.Dlk, q.wl, q.dd, q.Drk, q.du, q.wr, q.Drb});
+  }
+  // heuristic: chunks of at least four k-steps, about one CTA per SM over the
+  // round's tiles, at most 4 for the first product (the MPO-leg kernel adds
+  // its chunks) and 8 for the last
+  auto chunks = [&](long long tiles, int ks, int cap) {
+    const int s = (int)std::min<long long>(cap, std::max<long long>(1, (nsm + tiles - 1) / std::max<long long>(1, tiles)));
+    return std::max(1, std::min(s, ks / 4));
+  };
+  int S1 = chunks(tiles1, ks1, 4), S = chunks(tiles3, ks3, 8);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool tune = gemm_autotune_on() && cudaStreamIsCapturing(c.stream, &cs) == cudaSuccess &&
+                    cs == cudaStreamCaptureStatusNone;
+  bool found = false;
+  if (tune) {
+    std::lock_guard<std::mutex> lk(g_split_tune_mu);
+    auto it = g_split_tune.find(key);
+    if (it != g_split_tune.end()) {
+      S1 = it->second.first;
+      S = it->second.second;
+      found = true;
+    }
+  }
+  if (tune && !found) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MPSGPU_CUDA(cudaEventCreate(&e0));
+    MPSGPU_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int b1 = S1, b3 = S;
+    try {
+      for (int s1 : {1, 2, 4}) {
+        if (s1 > 1 && s1 > ks1 / 2) continue;
+        for (int s3 : {1, 2, 4, 8}) {
+          if (s3 > 1 && s3 > ks3 / 2) continue;
+          split_round_launch(c, r, s1, s3, false);  // warm (buffers, descriptor slots)
+          MPSGPU_CUDA(cudaEventRecord(e0, c.stream));
+          for (int rep = 0; rep < 2; rep++) split_round_launch(c, r, s1, s3, false);
+          MPSGPU_CUDA(cudaEventRecord(e1, c.stream));
+          MPSGPU_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          MPSGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < best) {
+            best = ms;
+            b1 = s1;
+            b3 = s3;
+          }
+        }
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    S1 = b1;
+    S = b3;
+    std::lock_guard<std::mutex> lk(g_split_tune_mu);
+    g_split_tune[key] = {S1, S};
+  }
+  split_round_launch(c, r, S1, S, true);
   r.p.clear();
 }
 

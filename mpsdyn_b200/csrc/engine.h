@@ -220,8 +220,10 @@ struct SplitProduct {
 struct SplitRound {
   std::vector<SplitProduct> p;
 };
-// Enqueues the round's products on c's stream and empties the round.
+// Enqueues the round's products on c's stream and empties the round (the
+// K chunks of its two tcgen05 products autotuned per round shape).
 void split_round_run(Context& c, SplitRound& r);
+long long split_autotune_entries();
 // The grouped launches of one Lanczos round that products append to.
 struct RoundBatch {
   Gemm1wBatch g1;

@@ -49,6 +49,7 @@ void zgemm(const Stream& st, const GemmArgs& g, Scratch& scratch);
 // default (environment MPSGPU_AUTOTUNE=0 turns it off); entries = shapes tuned.
 void set_gemm_autotune(int on);
 long long gemm_autotune_entries();
+bool gemm_autotune_on();
 
 // One GEMM C = A B (op N, N) of a grouped launch; tile_begin / tiles_m are
 // filled by grouped_tiles (64 x 64 tiles).

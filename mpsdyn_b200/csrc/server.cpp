@@ -86,13 +86,15 @@ extern "C" long long mpsgpu_request_footprint(const mpsgpu_request* r) {
   // observables, w = 1 environments
   const long long states = te ? 3 * mps : 2 * mps;
   long long bytes = 16 * (states + env + lanczos + lzstep + temps + mpo) + (8 << 20);  // + scratch slack
-  if (r->precision == 1 && !te) {
-    // split-precision operands of one site solve: the limb planes of L and Rt
-    // (made once per site), of x and T2 (per product), and the K-split
-    // partial products (at most 8 splits of the larger output)
+  if (r->precision == 1) {
+    // split-precision products of one site (ground state: every Lanczos
+    // product; time evolution: the local vector): the limb planes of L and Rt
+    // (made once per site) and of x and T2 (per product), the first product
+    // in up to 4 K chunks (FP64), T2 (FP64), and the last product in up to 8
+    // K chunks (FP64)
     bytes += split_plane_bytes(D * w, D, 128) + split_plane_bytes(D, D * w, 128) +
              split_plane_bytes(d * D, D, 128) + split_plane_bytes(D * d, D * w, 128) +
-             16 * 8 * std::max(D * w * d * D, D * d * D);
+             16 * (4 * D * w * d * D + D * d * D * w + 8 * D * d * D);
   }
   return bytes;
 }

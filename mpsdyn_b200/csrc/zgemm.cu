@@ -411,6 +411,8 @@ GemmCfg choose_cfg(const Stream& st, const GemmArgs& g, Scratch& scratch) {
 
 void set_gemm_autotune(int on) { g_tune_mode.store(on ? 1 : 0); }
 
+bool gemm_autotune_on() { return autotune_enabled(); }
+
 long long gemm_autotune_entries() {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   return (long long)g_tune.size();
