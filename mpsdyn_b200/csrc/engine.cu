@@ -484,6 +484,8 @@ constexpr double kFirst64EigTol = 1e-9;
 // far inside the 1e-10 the solve converges to; measured on the headline
 // workload the energies stay within 1e-13 of the reference's.
 constexpr double kScheduleEigTol = 1e-9;
+// Products per set of split-round launches.
+constexpr int kSplitRoundMax = 16;
 // optimize with split-precision local vectors: relative distance tolerance
 // (its noise floor is the products' error)
 constexpr double kSplitOptimizeTol = 1e-6;
@@ -782,6 +784,17 @@ long long split_autotune_entries() {
 void split_round_run(Context& c, SplitRound& r) {
   const int n = (int)r.p.size();
   if (n == 0) return;
+  // at most 16 products per set of launches (the descriptor tables of one
+  // set fit one slot of the context's ring)
+  if (n > kSplitRoundMax) {
+    for (int i0 = 0; i0 < n; i0 += kSplitRoundMax) {
+      SplitRound part;
+      part.p.assign(r.p.begin() + i0, r.p.begin() + std::min(n, i0 + kSplitRoundMax));
+      split_round_run(c, part);
+    }
+    r.p.clear();
+    return;
+  }
   const int nsm = device_sms(c);
   long long tiles1 = 0, tiles3 = 0;
   int ks1 = 1, ks3 = 1;

@@ -46,8 +46,7 @@ __global__ void wperm_kernel(const WPerm* __restrict__ d, int n, long long total
 // One block per chunk of PX * WC_THREADS pixels of one problem (problems start
 // on multiples of WC_CHUNK, itself a multiple of every chunk): the problem's
 // leg matrix is staged in shared memory, and every thread takes PX pixels
-// WC_THREADS apart, so that each leg entry read serves PX pixels while the
-// loads of every pixel index stay coalesced.
+// WC_THREADS apart (coalesced loads for every pixel index).
 template <int NIN, int PX>
 __global__ void __launch_bounds__(WC_THREADS) wcontract_grouped_kernel(const WGroup* __restrict__ g, int n,
                                                                        long long chunks) {
@@ -123,8 +122,11 @@ void wcontract_grouped(const Stream& st, const WGroup* d_wg, int n, long long pi
     const int g = (int)std::min<long long>(chunks, 148LL * 16);
     kernel<<<g, WC_THREADS, 0, st.s>>>(d_wg, n, chunks);
   };
-  if (maxnin <= 8) launch(wcontract_grouped_kernel<8, 4>, 4);
-  else if (maxnin <= 16) launch(wcontract_grouped_kernel<16, 2>, 2);
+  // one pixel per thread: enough blocks to fill the SMs several times over at
+  // the sweep shapes (two or four pixels per thread halved the blocks and
+  // measured slower)
+  if (maxnin <= 8) launch(wcontract_grouped_kernel<8, 1>, 1);
+  else if (maxnin <= 16) launch(wcontract_grouped_kernel<16, 1>, 1);
   else launch(wcontract_grouped_kernel<32, 1>, 1);
   after_launch(st);
 }
