@@ -6,8 +6,8 @@ penalty (seed-11 initial MPS), convergence 1e-10, complex FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpsgpu|reference]
 
-One step is a batch of B (default 16) independent solves with different
-seeds, swept in lockstep as two groups of 8 (each group on its own library
+One step is a batch of B (default 32) independent solves with different
+seeds, swept in lockstep as four groups of 8 (each group on its own library
 context and host thread; within a group the chains' local eigenproblems share
 the grouped launches of every Lanczos round), in the split-precision form
 (BF16-limb tcgen05 products until the energy settles, FP64 to convergence).
@@ -62,11 +62,11 @@ def parse():
     p.add_argument("--ref-iter-cap", type=int, default=0,
                    help="tests only: stop the sampled eigensolves after this many products instead of the "
                         "calibrated 60 (the line is then not a measurement)")
-    p.add_argument("--batch", type=int, default=16, help="concurrent solves per step")
+    p.add_argument("--batch", type=int, default=32, help="concurrent solves per step")
     p.add_argument("--batch-form", default="lockstep", choices=["lockstep", "streams"],
                    help="lockstep: one context sweeps the batch together (grouped launches); "
                         "streams: one context, stream and host thread per solve")
-    p.add_argument("--groups", type=int, default=2,
+    p.add_argument("--groups", type=int, default=4,
                    help="lockstep: the batch as this many lockstep groups, each on its own context and host "
                         "thread, so that one group's host work and site steps overlap another's rounds")
     p.add_argument("--plain", type=int, default=1, help="also time one solve alone (the plain form)")
