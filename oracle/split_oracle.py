@@ -52,3 +52,36 @@ def split_product(A: np.ndarray, B: np.ndarray) -> np.ndarray:
             cr += ar[i] @ br[j] - ai[i] @ bi[j]
             ci += ar[i] @ bi[j] + ai[i] @ br[j]
     return cr + 1j * ci
+
+
+def split_product_fp32(A: np.ndarray, B: np.ndarray, chunk_steps: int = 0) -> np.ndarray:
+    """C = A B from the same limb products, accumulated as the tensor cores do:
+    every MMA (one limb pair of one real product over a k-step of 16) adds its
+    exact sum, rounded to FP32, into an FP32 accumulator.  With chunk_steps > 0
+    the K range is cut into chunks of that many k-steps, each accumulated from
+    zero in FP32, and the chunks' partial products are added in FP64 (the K
+    chunks of the library's grouped split products).  Emulation of the
+    rounding, not of the hardware's internal order inside one MMA."""
+    m, k = A.shape
+    n = B.shape[1]
+    ar, ai = split3(A.real), split3(A.imag)
+    br, bi = split3(B.real), split3(B.imag)
+    ksteps = (k + 15) // 16
+    per = chunk_steps if chunk_steps > 0 else ksteps
+    f32 = np.float32
+    out_r = np.zeros((m, n))
+    out_i = np.zeros((m, n))
+    for c0 in range(0, ksteps, per):
+        acc_r = np.zeros((m, n), dtype=f32)
+        acc_i = np.zeros((m, n), dtype=f32)
+        for t in range(c0, min(ksteps, c0 + per)):
+            s = slice(16 * t, min(k, 16 * t + 16))
+            for i in range(3):
+                for j in range(3 - i):
+                    acc_r = (acc_r + (ar[i][:, s] @ br[j][s, :]).astype(f32)).astype(f32)
+                    acc_r = (acc_r - (ai[i][:, s] @ bi[j][s, :]).astype(f32)).astype(f32)
+                    acc_i = (acc_i + (ar[i][:, s] @ bi[j][s, :]).astype(f32)).astype(f32)
+                    acc_i = (acc_i + (ai[i][:, s] @ br[j][s, :]).astype(f32)).astype(f32)
+        out_r += acc_r.astype(np.float64)
+        out_i += acc_i.astype(np.float64)
+    return out_r + 1j * out_i

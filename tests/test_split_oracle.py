@@ -38,3 +38,24 @@ def test_split_product_truncation_error(m, n, k):
     rel = np.abs(C - A @ B) / (np.abs(A) @ np.abs(B))
     # the scheme's own error; the GPU bound (1e-6 + 3e-9 K) is 30x or more above it
     assert rel.max() <= 3e-8, rel.max()
+
+
+def test_fp32_accumulation_error_and_k_chunks():
+    """With the tensor cores' FP32 accumulation restated, the error of a
+    product with K = 640 (the last contraction of the D = 128 Schwinger
+    matvec) stays inside the bound the GPU tests state, 1e-6 + 3e-9 K of
+    |A||B|, and cutting K into chunks of five k-steps whose partials are added
+    in FP64 (as the grouped split products do) lowers it."""
+    rng = np.random.default_rng(640)
+    m, n, k = 96, 64, 640
+    A = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
+    B = rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))
+    ref = A @ B
+    scale = np.abs(A) @ np.abs(B)
+    whole = (np.abs(so.split_product_fp32(A, B) - ref) / scale).max()
+    chunked = (np.abs(so.split_product_fp32(A, B, chunk_steps=5) - ref) / scale).max()
+    assert whole <= 1e-6 + 3e-9 * k, whole
+    assert chunked < whole, (chunked, whole)
+    # and both far above the limb truncation alone (the FP32 sums dominate)
+    exact = (np.abs(so.split_product(A, B) - ref) / scale).max()
+    assert exact < chunked
