@@ -1089,8 +1089,9 @@ cplx contract2(Context& c, const MpoDev& ops, const MpsDev& ket, const MpsDev& b
 // (TensorMultiplierProjMulti.cpp:81-90).
 //
 // One round = one iteration of every active task: FP64 products are
-// appended to grouped launches of the two contractions (heff.cu), a task in
-// its split-precision phase launches its own product chain, then one
+// appended to grouped launches of the two contractions (heff.cu), the
+// products of tasks in their split-precision phase to one split round
+// (split_round_run: six grouped launches for all of them), then one
 // cooperative launch of the Lanczos step (lzstep.cu) serves all tasks and
 // writes each task's alpha_j, beta_j into its mapped host mirror.  The host
 // enqueues round r+1 before it waits for round r, so the convergence tests
