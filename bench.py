@@ -776,11 +776,17 @@ def run_serving(args) -> None:
     fp64 = stream(0) if prec != 0 else None
     cmp = None
     if fp64:
-        common = set(main["energies"]) & set(fp64["energies"])
+        common = sorted(set(main["energies"]) & set(fp64["energies"]))
+        rel = {k: abs(main["energies"][k] - fp64["energies"][k]) / abs(fp64["energies"][k]) for k in common}
+        worst = sorted(common, key=lambda k: -rel[k])[:3]
         cmp = {"value": fp64["value"], "latency_s": fp64["latency_s"], "completed": fp64["completed"],
                "failed": fp64["failed"],
-               "max_rel_dE_vs_fp64": max((abs(main["energies"][k] - fp64["energies"][k]) /
-                                          abs(fp64["energies"][k]) for k in common), default=None),
+               "max_rel_dE_vs_fp64": max(rel.values(), default=None),
+               "median_rel_dE_vs_fp64": float(np.median(list(rel.values()))) if rel else None,
+               # the requests that differ most (request id = seed; index id - 1 of the stream)
+               "largest_dE": [{"id": k, "L": int(Ls[k - 1]), "D": int(Ds[k - 1]), "g": float(gs[k - 1]),
+                               "h": float(hs[k - 1]), "E_line": main["energies"][k], "E_fp64": fp64["energies"][k],
+                               "rel": rel[k]} for k in worst],
                "line_over_fp64": main["value"] / fp64["value"] if fp64["value"] else None}
     line = {"metric": "served DMRG solves/s (Ising mix)", "value": main["value"], "unit": "solves/s",
             "n_gpus": 1, "steps": n, "warmup": 0, "higher_is_better": True, "scaling": "weak",
